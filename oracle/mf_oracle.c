@@ -1,0 +1,671 @@
+/* Test infrastructure (the oracle). A plain-C restatement of the reference
+ * smf numeric phase, written from the reference's algorithm; it is only ever
+ * the checker of the CUDA engine (tests/, smoke(), bench.py's CPU-baseline
+ * leg), never the thing measured or shipped.
+ *
+ * Every operation on a front entry follows the reference's order and
+ * rounding: the pivot kernels multiply, then add or subtract (no FMA, as
+ * ldlt_kernel.cpp is built with -ffp-contract=off; this file too), while the
+ * GEMM steps of the deferred and Schur updates are fused multiply-adds (the
+ * reference's portable BLAS loops are contracted by GCC's C++ default). For
+ * the reference built with those loops (oracle/Makefile) the factor is then
+ * bit for bit the reference's:
+ *   process_front            solver/src/multifrontal_serial.cpp:472-1035
+ *   ldlt_factor_front        solver/src/ldlt_kernel.cpp:970-1139
+ *   select_pivot             solver/src/ldlt_kernel.cpp:127-275
+ *   two_by_two_ok            solver/src/ldlt_kernel.cpp:97-122
+ *   sym_swap                 solver/src/ldlt_kernel.cpp:333-347
+ *   eliminate_1x1 / _2x2     solver/src/ldlt_kernel.cpp:352-545
+ *   apply_pivot              solver/src/ldlt_kernel.cpp:666-698
+ *   deferred_update          solver/src/ldlt_kernel.cpp:705-761
+ *   fill_ld_column / schur   solver/src/ldlt_kernel.cpp:764-933
+ *   portable GEMM loops      solver/src/dense_kernel_lapack.cpp:182-234
+ *   add_inertia_2x2          solver/src/dense_indef.cpp:52-83
+ * Not restated: static pivoting, delay budgets, the APTP/tile kernel used by
+ * deterministic mode on indefinite fronts of >= 512 rows, and the banded SPD
+ * path (tests use configurations that do not reach them).
+ */
+#include "mf_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define WEAK_PIVOT_RATIO 1e-6 /* kWeakPivotRatio, ldlt_kernel.hpp:100 */
+
+static int is_fin(double v) { return isfinite(v); }
+static double max3(double a, double b, double c) {
+  double m = a;
+  if (m < b) m = b;
+  if (m < c) m = c;
+  return m;
+}
+static double dmax(double a, double b) { return (a < b) ? b : a; } /* std::max */
+
+typedef struct { int kind, a, b; } pchoice;
+
+static double sym_at(const double *F, int ld, int i, int j) {
+  return (i >= j) ? F[(size_t)j * ld + i] : F[(size_t)i * ld + j];
+}
+
+static int two_by_two_ok(const double *F, int ld, int f, int cand, int r, const double *col,
+                         const double *col_r, double m2, double off1, int ext0,
+                         const mfo_params *prm, double *growth) {
+  const double d00 = col[cand];
+  const double d10 = sym_at(F, ld, r, cand);
+  const double d11 = col_r[r];
+  const double s2 = max3(fabs(d00), fabs(d10), fabs(d11));
+  if (!(s2 >= prm->eff_small) || !is_fin(s2)) return 0;
+  const double a = d00 / s2, b = d10 / s2, c = d11 / s2;
+  const double det_s = a * c - b * b;
+  if (!(fabs(det_s) > prm->small_pivot)) return 0;
+  double off0 = m2;
+  for (int i = ext0; i < f; ++i) off0 = dmax(off0, fabs(col[i]));
+  double g = 0.0;
+  if (off0 > 0.0 || off1 > 0.0) {
+    const double bound0 = (fabs(c) * off0 + fabs(b) * off1) / s2;
+    const double bound1 = (fabs(b) * off0 + fabs(a) * off1) / s2;
+    if (prm->u * dmax(bound0, bound1) > fabs(det_s)) return 0;
+    g = dmax(bound0, bound1) / fabs(det_s);
+  }
+  *growth = g;
+  return 1;
+}
+
+static pchoice select_pivot(const double *F, int ld, int f, int k, int num_elig, int limit,
+                            const mfo_params *prm) {
+  pchoice none = {0, -1, -1};
+  if (prm->posdef) {
+    const double d = F[(size_t)k * ld + k];
+    if (d > 0.0 && is_fin(d)) { pchoice p1 = {1, k, -1}; return p1; }
+    return none;
+  }
+  if (k < limit) {
+    const double *col0 = F + (size_t)k * ld;
+    const double a0 = fabs(col0[k]);
+    if (a0 >= prm->eff_small) {
+      double colmax = 0.0;
+      for (int i = k + 1; i < f; ++i) {
+        const double v = fabs(col0[i]);
+        if (v > colmax) colmax = v;
+      }
+      if (!(prm->u * colmax > a0) && !(a0 < WEAK_PIVOT_RATIO * colmax)) {
+        pchoice p1 = {1, k, -1};
+        return p1;
+      }
+    }
+  }
+  for (int cand = k; cand < limit; ++cand) {
+    const double *col = F + (size_t)cand * ld;
+    const double a_cand = fabs(col[cand]);
+    double m1 = 0.0, m2 = 0.0;
+    int r_best = -1;
+    for (int i = k; i < cand; ++i) {
+      const double v = fabs(F[(size_t)i * ld + cand]);
+      if (v > m1) { m2 = m1; m1 = v; r_best = i; }
+      else if (v > m2) m2 = v;
+    }
+    for (int i = cand + 1; i < num_elig; ++i) {
+      const double v = fabs(col[i]);
+      if (v > m1) { m2 = m1; m1 = v; r_best = i; }
+      else if (v > m2) m2 = v;
+    }
+    const int ext0 = num_elig > cand + 1 ? num_elig : cand + 1;
+    int weak_1x1 = 0;
+    double weak_growth = 0.0;
+    if (a_cand >= prm->eff_small && !(prm->u * m1 > a_cand)) {
+      int ok = 1;
+      double colmax = m1;
+      for (int i = ext0; i < f; ++i) {
+        const double v = fabs(col[i]);
+        if (prm->u * v > a_cand) { ok = 0; break; }
+        colmax = dmax(colmax, v);
+      }
+      if (ok) {
+        if (!(a_cand < WEAK_PIVOT_RATIO * colmax)) { pchoice p1 = {1, cand, -1}; return p1; }
+        weak_1x1 = 1;
+        weak_growth = colmax / a_cand;
+      }
+    }
+    if (r_best < k || r_best >= limit || m1 <= 0.0) {
+      if (weak_1x1) { pchoice p1 = {1, cand, -1}; return p1; }
+      continue;
+    }
+    const double *col_r = F + (size_t)r_best * ld;
+    double om2 = 0.0, off1 = 0.0;
+    for (int i = k; i < r_best; ++i) {
+      const double v = fabs(F[(size_t)i * ld + r_best]);
+      om2 = dmax(om2, v);
+      if (i != cand) off1 = dmax(off1, v);
+    }
+    for (int i = r_best + 1; i < f; ++i) {
+      const double v = fabs(col_r[i]);
+      om2 = dmax(om2, v);
+      if (i != cand) off1 = dmax(off1, v);
+    }
+    double growth2 = 0.0;
+    if (k + 1 < limit &&
+        two_by_two_ok(F, ld, f, cand, r_best, col, col_r, m2, off1, ext0, prm, &growth2) &&
+        (!weak_1x1 || growth2 < weak_growth)) {
+      pchoice p2 = {2, cand, r_best};
+      return p2;
+    }
+    if (weak_1x1) { pchoice p1 = {1, cand, -1}; return p1; }
+    const double a_r = fabs(col_r[r_best]);
+    if (a_r >= prm->eff_small && (om2 == 0.0 || a_r >= prm->u * om2)) {
+      pchoice p1 = {1, r_best, -1};
+      return p1;
+    }
+  }
+  return none;
+}
+
+static void sym_swap(double *F, int ld, int f, int p, int q, int *rows, double *W, int w_cols) {
+  if (p == q) return;
+  if (p > q) { int t = p; p = q; q = t; }
+  const size_t sf = (size_t)ld;
+  double t;
+#define SWP(x, y) (t = (x), (x) = (y), (y) = t)
+  SWP(F[p * sf + p], F[q * sf + q]);
+  for (int m = 0; m < p; ++m) SWP(F[m * sf + p], F[m * sf + q]);
+  for (int m = p + 1; m < q; ++m) SWP(F[p * sf + m], F[m * sf + q]);
+  for (int m = q + 1; m < f; ++m) SWP(F[p * sf + m], F[q * sf + m]);
+  { int r = rows[p]; rows[p] = rows[q]; rows[q] = r; }
+  for (int c = 0; c < w_cols; ++c) SWP(W[(size_t)c * f + p], W[(size_t)c * f + q]);
+#undef SWP
+}
+
+/* eliminate_1x1: the per-entry operations of the reference (its 4-column
+ * grouping and AVX lanes change no entry's operation sequence). */
+static void eliminate_1x1(double *F, int f, int k, int ucol_end, double *W, int w_col) {
+  const size_t sf = (size_t)f;
+  double *ck = F + k * sf;
+  const double inv_d = 1.0 / ck[k];
+  if (W) {
+    double *w = W + (size_t)w_col * sf;
+    for (int i = k + 1; i < f; ++i) w[i] = ck[i];
+  }
+  for (int j = k + 1; j < ucol_end; ++j) {
+    const double lj = ck[j] * inv_d;
+    if (lj == 0.0) continue;
+    double *cj = F + (size_t)j * sf;
+    for (int i = j; i < f; ++i) cj[i] -= ck[i] * lj;
+  }
+  for (int i = k + 1; i < f; ++i) ck[i] *= inv_d;
+}
+
+static void inverse_2x2(double d00, double d10, double d11, double *i00, double *i10, double *i11) {
+  const double s = max3(fabs(d00), fabs(d10), fabs(d11));
+  const double a = d00 / s, b = d10 / s, c = d11 / s;
+  const double inv = 1.0 / ((a * c - b * b) * s);
+  *i00 = c * inv;
+  *i10 = -b * inv;
+  *i11 = a * inv;
+}
+
+static void eliminate_2x2(double *F, int f, int k, int ucol_end, double *W, int w_col) {
+  const size_t sf = (size_t)f;
+  double *c0 = F + k * sf, *c1 = F + (k + 1) * sf;
+  double i00, i10, i11;
+  inverse_2x2(c0[k], c0[k + 1], c1[k + 1], &i00, &i10, &i11);
+  if (W) {
+    double *w0 = W + (size_t)w_col * sf, *w1 = w0 + sf;
+    for (int i = k + 2; i < f; ++i) { w0[i] = c0[i]; w1[i] = c1[i]; }
+  }
+  for (int j = k + 2; j < ucol_end; ++j) {
+    const double a0 = c0[j], a1 = c1[j];
+    const double l0 = i00 * a0 + i10 * a1;
+    const double l1 = i10 * a0 + i11 * a1;
+    if (l0 == 0.0 && l1 == 0.0) continue;
+    double *d0 = F + (size_t)j * sf;
+    for (int i = j; i < f; ++i) d0[i] -= c0[i] * l0 + c1[i] * l1;
+  }
+  for (int i = k + 2; i < f; ++i) {
+    const double a0 = c0[i], a1 = c1[i];
+    c0[i] = i00 * a0 + i10 * a1;
+    c1[i] = i10 * a0 + i11 * a1;
+  }
+}
+
+static void inertia_1x1(double d, double small, mfo_factor *o) {
+  if (!is_fin(d) || fabs(d) < small) ++o->zero;
+  else if (d > 0.0) ++o->pos;
+  else ++o->neg;
+}
+
+static void inertia_2x2(double d00, double d10, double d11, double small, mfo_factor *o) {
+  if (d10 == 0.0) {
+    inertia_1x1(d00, small, o);
+    inertia_1x1(d11, small, o);
+    return;
+  }
+  const double s = max3(fabs(d00), fabs(d10), fabs(d11));
+  double det_s = 0.0;
+  if (is_fin(s) && s != 0.0) det_s = (d00 / s) * (d11 / s) - (d10 / s) * (d10 / s);
+  if (s == 0.0 || !is_fin(det_s)) { o->zero += 2; return; }
+  const double tr_s = (d00 / s) + (d11 / s);
+  if (det_s < -small) { ++o->pos; ++o->neg; }
+  else if (fabs(det_s) <= small) {
+    ++o->zero;
+    if (tr_s > small) ++o->pos;
+    else if (tr_s < -small) ++o->neg;
+    else ++o->zero;
+  } else {
+    if (tr_s > 0.0) o->pos += 2;
+    else if (tr_s < 0.0) o->neg += 2;
+    else o->zero += 2;
+  }
+}
+
+static void apply_pivot(pchoice pc, double *F, int f, int *kp, int *rows, int8_t *tags, double *W,
+                        int w_cols, int ucol_end, const mfo_params *prm, mfo_factor *o) {
+  const size_t sf = (size_t)f;
+  int k = *kp;
+  if (pc.kind == 1) {
+    sym_swap(F, f, f, k, pc.a, rows, W, w_cols);
+    inertia_1x1(F[k * sf + k], prm->eff_small, o);
+    tags[k] = 1;
+    eliminate_1x1(F, f, k, ucol_end, W, w_cols);
+    const double rem = (double)(f - (k + 1));
+    o->flops += rem + rem * (rem + 1.0);
+    *kp = k + 1;
+    return;
+  }
+  int partner = pc.b;
+  if (pc.a != k) {
+    sym_swap(F, f, f, k, pc.a, rows, W, w_cols);
+    if (partner == k) partner = pc.a;
+  }
+  if (partner != k + 1) sym_swap(F, f, f, k + 1, partner, rows, W, w_cols);
+  inertia_2x2(F[k * sf + k], F[k * sf + k + 1], F[(k + 1) * sf + k + 1], prm->small_pivot, o);
+  tags[k] = 2;
+  tags[k + 1] = -1;
+  eliminate_2x2(F, f, k, ucol_end, W, w_cols);
+  const double rem = (double)(f - (k + 2));
+  o->flops += 6.0 * rem + 2.0 * rem * (rem + 1.0);
+  *kp = k + 2;
+}
+
+/* F[c0:f, c0:e] -= L[c0:f, p0:p1] W[c0:e, :]^T: per entry, pivots in order,
+ * a zero W entry skipped (the portable dgemm / dgemmt loops,
+ * dense_kernel_lapack.cpp:182-234). Those loops are compiled with GCC's
+ * default C++ contraction, so each step is one fused multiply-add:
+ * c = fma(-a, b, c). */
+static void deferred_update(double *F, int f, int p0, int p1, int c0, int e, const double *W) {
+  const int jb = p1 - p0;
+  if (jb <= 0 || e - c0 <= 0) return;
+  const size_t sf = (size_t)f;
+  for (int j = c0; j < e; ++j) {
+    double *cj = F + (size_t)j * sf;
+    for (int p = 0; p < jb; ++p) {
+      const double b = W[(size_t)p * sf + j];
+      if (b == 0.0) continue;
+      const double *a = F + (size_t)(p0 + p) * sf;
+      for (int i = j; i < f; ++i) cj[i] = fma(-a[i], b, cj[i]);
+    }
+  }
+}
+
+static double ld_entry(const double *F, int f, const int8_t *tags, int c, int i) {
+  const size_t sf = (size_t)f;
+  const double *Lc = F + (size_t)c * sf;
+  if (tags[c] == 1) return Lc[i] * Lc[c];
+  if (tags[c] == 2) return Lc[i] * Lc[c] + Lc[sf + i] * Lc[c + 1];
+  if (tags[c] == -1) {
+    const double *L0 = Lc - sf;
+    return L0[i] * L0[c] + Lc[i] * Lc[c];
+  }
+  return 0.0;
+}
+
+/* F[e:f, e:f] -= L[e:f, p0:p] LD[e:f, p0:p]^T, LD = L D per fill_ld_column
+ * (products rounded separately: ldlt_kernel.cpp is built without
+ * contraction); the GEMM steps are fused as in deferred_update. */
+static void schur_update(double *F, int f, int p0, int p, int e, const int8_t *tags, double *buf) {
+  const int q = f - e;
+  if (p <= p0 || q <= 0) return;
+  const size_t sf = (size_t)f;
+  const int kc = p - p0;
+  for (int t = 0; t < kc; ++t)
+    for (int i = 0; i < q; ++i) buf[(size_t)t * q + i] = ld_entry(F, f, tags, p0 + t, e + i);
+  for (int j = 0; j < q; ++j) {
+    double *cj = F + (size_t)(e + j) * sf + e;
+    for (int t = 0; t < kc; ++t) {
+      const double b = buf[(size_t)t * q + j];
+      if (b == 0.0) continue;
+      const double *a = F + (size_t)(p0 + t) * sf + e;
+      for (int i = j; i < q; ++i) cj[i] = fma(-a[i], b, cj[i]);
+    }
+  }
+}
+
+/* ldlt_factor_front with first = 0, no static pivoting. Returns the number
+ * of accepted pivots. */
+static int ldlt_factor_front(double *F, int f, int num_elig, int *rows, const mfo_params *prm,
+                             int8_t *tags, double *work, mfo_factor *o) {
+  int k = 0;
+  if (f < prm->blocked_min_front || prm->nb <= 1) {
+    while (k < num_elig) {
+      pchoice pc = select_pivot(F, f, f, k, num_elig, num_elig, prm);
+      if (pc.kind == 0) break;
+      apply_pivot(pc, F, f, &k, rows, tags, NULL, 0, f, prm, o);
+    }
+    return k;
+  }
+  double *W = work; /* f x nb */
+  const size_t sf = (size_t)f;
+  if (!prm->posdef) {
+    int live = num_elig, k_paired = -1;
+    while (k < live) {
+      const int ps = k;
+      const int pl = (live < ps + prm->nb) ? live : ps + prm->nb;
+      int stalled = 0;
+      while (k < pl) {
+        pchoice pc = select_pivot(F, f, f, k, num_elig, pl, prm);
+        if (pc.kind == 0) { stalled = 1; break; }
+        apply_pivot(pc, F, f, &k, rows, tags, W, k - ps, pl, prm, o);
+      }
+      deferred_update(F, f, ps, k, pl, num_elig, W);
+      if (stalled && k != k_paired) {
+        int order[128];
+        int np = 0;
+        const int max_pairs = (prm->nb / 2 < 64) ? prm->nb / 2 : 64;
+        for (int pos = k; pos < pl && np / 2 < max_pairs; ++pos) {
+          const double *col = F + (size_t)pos * sf;
+          double in_max = 0.0;
+          for (int i = k; i < pos; ++i) in_max = dmax(in_max, fabs(F[(size_t)i * sf + pos]));
+          for (int i = pos + 1; i < pl; ++i) in_max = dmax(in_max, fabs(col[i]));
+          double out_max = 0.0;
+          int r = -1;
+          for (int i = pl; i < num_elig; ++i) {
+            const double v = fabs(col[i]);
+            if (v > out_max) { out_max = v; r = i; }
+          }
+          if (r < 0 || !(out_max > in_max)) continue;
+          int taken = 0;
+          for (int t = 1; t < np; t += 2) taken = taken || order[t] == rows[r];
+          if (taken) continue;
+          order[np++] = rows[pos];
+          order[np++] = rows[r];
+        }
+        if (np > 0) {
+          for (int t = 0; t < np; ++t) {
+            int qq = k + t;
+            while (rows[qq] != order[t]) ++qq;
+            sym_swap(F, f, f, k + t, qq, rows, NULL, 0);
+          }
+          live = (live > k + np) ? live : k + np;
+          k_paired = k;
+          continue;
+        }
+      }
+      if (stalled) {
+        const int m = pl - k;
+        const int mv = (m < live - pl) ? m : live - pl;
+        for (int t = 0; t < mv; ++t) sym_swap(F, f, f, k + t, live - mv + t, rows, NULL, 0);
+        live -= m;
+      }
+    }
+  }
+  while (k < num_elig) {
+    const int ps = k;
+    const int pl = (num_elig < ps + prm->nb) ? num_elig : ps + prm->nb;
+    int stalled = 0;
+    while (k < pl) {
+      pchoice pc = select_pivot(F, f, f, k, num_elig, pl, prm);
+      if (pc.kind == 0) { stalled = 1; break; }
+      apply_pivot(pc, F, f, &k, rows, tags, W, k - ps, pl, prm, o);
+    }
+    deferred_update(F, f, ps, k, pl, num_elig, W);
+    if (stalled && k < num_elig) {
+      const int ss = k;
+      pchoice pc = select_pivot(F, f, f, k, num_elig, num_elig, prm);
+      if (pc.kind == 0) break;
+      apply_pivot(pc, F, f, &k, rows, tags, W, 0, ss, prm, o);
+      deferred_update(F, f, ss, k, k, num_elig, W);
+    }
+  }
+  schur_update(F, f, 0, k, num_elig, tags, work);
+  return k;
+}
+
+int mfo_factorize(const mfo_analysis *a, const double *pv, const mfo_params *prm, mfo_factor *o) {
+  const int n = a->n, ns = a->nsn;
+  o->pos = o->neg = o->zero = o->delayed = o->two_by_two = o->max_front = 0;
+  o->flops = 0.0;
+  o->status = 0;
+  double **front = (double **)calloc((size_t)ns, sizeof(double *));
+  int **frows = (int **)calloc((size_t)ns, sizeof(int *));
+  int *fsz = (int *)calloc((size_t)ns, sizeof(int));
+  int *acc = (int *)calloc((size_t)ns, sizeof(int));
+  int *delayed = (int *)calloc((size_t)ns, sizeof(int));
+  int *pos = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  for (int i = 0; i < n; ++i) pos[i] = -1;
+  int64_t bo = 0, ro = 0, to = 0;
+  for (int it = 0; it < ns && o->status == 0; ++it) {
+    const int s = a->postorder[it];
+    const int c0 = a->child_ptr[s], c1 = a->child_ptr[s + 1];
+    const int fs = a->front_row_ptr[s + 1] - a->front_row_ptr[s];
+    const int psym = a->sn_end[s] - a->sn_start[s];
+    int nd = 0;
+    for (int t = c0; t < c1; ++t) nd += delayed[a->child_idx[t]];
+    const int f = nd + fs;
+    int *rows = (int *)malloc(sizeof(int) * (size_t)(f > 0 ? f : 1));
+    int ff = 0;
+    for (int t = c0; t < c1; ++t) {
+      const int c = a->child_idx[t];
+      for (int r = 0; r < delayed[c]; ++r) {
+        const int row = frows[c][acc[c] + r];
+        rows[ff] = row;
+        pos[row] = ff++;
+      }
+    }
+    for (int t = 0; t < fs; ++t) {
+      const int row = a->front_row_idx[a->front_row_ptr[s] + t];
+      rows[ff] = row;
+      pos[row] = ff++;
+    }
+    const int num_elig = nd + psym;
+    double *F = (double *)calloc((size_t)f * f + 1, sizeof(double));
+    /* original entries of the pivot columns */
+    for (int j = a->sn_start[s]; j < a->sn_end[s]; ++j) {
+      double *Fj = F + (size_t)pos[j] * f;
+      for (int k = a->pcp[j]; k < a->pcp[j + 1]; ++k) Fj[pos[a->pri[k]]] += pv[k];
+    }
+    /* extend-add, children in child_idx order */
+    for (int t = c0; t < c1; ++t) {
+      const int c = a->child_idx[t];
+      const int fc = fsz[c], pc = acc[c], q = fc - pc;
+      if (q <= 0 || a->sn_parent[c] < 0) continue;
+      const double *Fc = front[c];
+      const int *cr = frows[c] + pc;
+      for (int jj = 0; jj < q; ++jj) {
+        const int lj = pos[cr[jj]];
+        if (lj < 0) { o->status = 3; break; }
+        for (int ii = jj; ii < q; ++ii) {
+          const int li = pos[cr[ii]];
+          const double v = Fc[(size_t)(pc + jj) * fc + (pc + ii)];
+          if (li >= lj) F[(size_t)lj * f + li] += v;
+          else F[(size_t)li * f + lj] += v;
+        }
+      }
+    }
+    int8_t *tags = (int8_t *)calloc((size_t)(f > 0 ? f : 1), 1);
+    double *work = (double *)malloc(sizeof(double) * ((size_t)f * (prm->nb + 2) + (size_t)f * f + 1));
+    const int p = ldlt_factor_front(F, f, num_elig, rows, prm, tags, work, o);
+    free(work);
+    if (f > o->max_front) o->max_front = f;
+    const int is_root = a->sn_parent[s] < 0;
+    if (prm->posdef && p < num_elig) { o->status = 1; free(tags); free(F); free(rows); break; }
+    int p_store = p;
+    if (is_root && p < num_elig) {
+      for (int c = p; c < num_elig; ++c) tags[c] = 0;
+      o->zero += num_elig - p;
+      p_store = num_elig;
+    }
+    if (prm->posdef) {
+      for (int c = 0; c < p_store; ++c) {
+        double *Lc = F + (size_t)c * f;
+        const double sd = sqrt(Lc[c]);
+        for (int i = 0; i < c; ++i) Lc[i] = 0.0;
+        Lc[c] = sd;
+        for (int i = c + 1; i < f; ++i) Lc[i] *= sd;
+      }
+    } else {
+      double d10 = 0.0;
+      for (int c = 0; c < p_store; ++c) {
+        double *Lc = F + (size_t)c * f;
+        const int8_t tag = tags[c];
+        if (tag == 0) {
+          for (int i = c + 1; i < f; ++i) Lc[i] = 0.0;
+          Lc[c] = 0.0;
+        } else if (tag == 2) {
+          ++o->two_by_two;
+          if (!is_fin(Lc[c]) || !is_fin(Lc[c + 1]) || !is_fin(Lc[(size_t)f + c + 1])) o->status = 4;
+          d10 = Lc[c + 1];
+          Lc[c + 1] = 0.0;
+        } else if (tag == 1) {
+          if (!is_fin(Lc[c])) o->status = 4;
+        }
+        for (int i = 0; i < c; ++i) Lc[i] = 0.0;
+        if (tag == -1) Lc[c - 1] = d10;
+      }
+    }
+    o->f_out[s] = f;
+    o->p_out[s] = p_store;
+    o->blk_off[s] = bo;
+    o->row_off[s] = ro;
+    if (bo + (int64_t)f * p_store > o->blk_cap || ro + f > o->row_cap) { o->status = 3; }
+    else {
+      memcpy(o->blocks + bo, F, sizeof(double) * (size_t)f * p_store);
+      memcpy(o->rows + ro, rows, sizeof(int) * (size_t)f);
+      if (!prm->posdef && o->tags) memcpy(o->tags + to, tags, (size_t)p_store);
+    }
+    bo += (int64_t)f * p_store;
+    ro += f;
+    to += p_store;
+    free(tags);
+    fsz[s] = f;
+    acc[s] = p;
+    frows[s] = rows;
+    front[s] = F;
+    delayed[s] = is_root ? 0 : num_elig - p;
+    o->delayed += delayed[s];
+    for (int t = 0; t < f; ++t) pos[rows[t]] = -1;
+    /* children's fronts are consumed */
+    for (int t = c0; t < c1; ++t) {
+      const int c = a->child_idx[t];
+      free(front[c]);
+      front[c] = NULL;
+    }
+  }
+  if (o->status == 0 && o->zero > 0) o->status = 2;
+  for (int s = 0; s < ns; ++s) { free(front[s]); free(frows[s]); }
+  free(front); free(frows); free(fsz); free(acc); free(delayed); free(pos);
+  return o->status;
+}
+
+/* Forward, diagonal and backward solves on the stored blocks (in place on x,
+ * new numbering). solve_forward.cpp:116-293, solve_diag.cpp:49-123,
+ * solve_backward.cpp:135-350 compute the same quantities. */
+void mfo_solve_permuted(const mfo_analysis *a, const mfo_factor *fac, int posdef, double *x) {
+  const int ns = a->nsn;
+  for (int it = 0; it < ns; ++it) {
+    const int s = a->postorder[it];
+    const int f = fac->f_out[s], p = fac->p_out[s];
+    const double *L = fac->blocks + fac->blk_off[s];
+    const int *rows = fac->rows + fac->row_off[s];
+    for (int j = 0; j < p; ++j) {
+      const double *col = L + (size_t)j * f;
+      double xj = x[rows[j]];
+      if (posdef) xj /= col[j];
+      x[rows[j]] = xj;
+      for (int i = j + 1; i < f; ++i) x[rows[i]] -= col[i] * xj;
+    }
+  }
+  if (!posdef) {
+    for (int it = 0; it < ns; ++it) {
+      const int s = a->postorder[it];
+      const int f = fac->f_out[s], p = fac->p_out[s];
+      const double *L = fac->blocks + fac->blk_off[s];
+      const int *rows = fac->rows + fac->row_off[s];
+      for (int c = 0; c < p;) {
+        const double d00 = L[(size_t)c * f + c];
+        if (c + 1 < p) {
+          const double d10 = L[(size_t)(c + 1) * f + c];
+          if (d10 != 0.0) {
+            const double d11 = L[(size_t)(c + 1) * f + c + 1];
+            const double s2 = max3(fabs(d00), fabs(d10), fabs(d11));
+            const double aa = d00 / s2, bb = d10 / s2, cc = d11 / s2;
+            const double det = aa * cc - bb * bb;
+            const double r0 = x[rows[c]], r1 = x[rows[c + 1]];
+            double y0 = 0.0, y1 = 0.0;
+            if (s2 != 0.0 && is_fin(det) && det != 0.0) {
+              y0 = ((cc * r0 - bb * r1) / det) / s2;
+              y1 = ((-bb * r0 + aa * r1) / det) / s2;
+            }
+            x[rows[c]] = y0;
+            x[rows[c + 1]] = y1;
+            c += 2;
+            continue;
+          }
+        }
+        x[rows[c]] = (d00 == 0.0 || !is_fin(d00)) ? 0.0 : x[rows[c]] / d00;
+        ++c;
+      }
+    }
+  }
+  for (int it = ns - 1; it >= 0; --it) {
+    const int s = a->postorder[it];
+    const int f = fac->f_out[s], p = fac->p_out[s];
+    const double *L = fac->blocks + fac->blk_off[s];
+    const int *rows = fac->rows + fac->row_off[s];
+    for (int j = p - 1; j >= 0; --j) {
+      const double *col = L + (size_t)j * f;
+      double v = x[rows[j]];
+      for (int i = j + 1; i < f; ++i) v -= col[i] * x[rows[i]];
+      if (posdef) v /= col[j];
+      x[rows[j]] = v;
+    }
+  }
+}
+
+/* r = b - A x and the backward errors of refinement.cpp:39-130 (normwise
+ * eta_inf with ||A||_inf, componentwise omega), long double accumulation. */
+void mfo_residual(int n, const int *cp, const int *ri, const double *v, const double *b,
+                  const double *x, double *r, double *eta_inf, double *omega) {
+  long double *ax = (long double *)calloc((size_t)n + 1, sizeof(long double));
+  long double *aax = (long double *)calloc((size_t)n + 1, sizeof(long double));
+  long double *rowabs = (long double *)calloc((size_t)n + 1, sizeof(long double));
+  for (int j = 0; j < n; ++j)
+    for (int k = cp[j]; k < cp[j + 1]; ++k) {
+      const int i = ri[k];
+      const long double val = v[k], av = fabsl(val);
+      ax[i] += val * x[j];
+      aax[i] += av * fabsl((long double)x[j]);
+      rowabs[i] += av;
+      if (i != j) {
+        ax[j] += val * x[i];
+        aax[j] += av * fabsl((long double)x[i]);
+        rowabs[j] += av;
+      }
+    }
+  long double na = 0, nx = 0, nb = 0, rmax = 0, om = 0;
+  for (int i = 0; i < n; ++i) {
+    if (rowabs[i] > na) na = rowabs[i];
+    if (fabsl((long double)x[i]) > nx) nx = fabsl((long double)x[i]);
+    if (fabsl((long double)b[i]) > nb) nb = fabsl((long double)b[i]);
+    const long double res = (long double)b[i] - ax[i];
+    r[i] = (double)res;
+    if (fabsl(res) > rmax) rmax = fabsl(res);
+    const long double den = aax[i] + fabsl((long double)b[i]);
+    const long double oi = den > 0 ? fabsl(res) / den : (res == 0 ? 0 : 1.0L / 0.0L);
+    if (oi > om) om = oi;
+  }
+  const long double ed = na * nx + nb;
+  *eta_inf = (double)(ed > 0 ? rmax / ed : (rmax == 0 ? 0 : 1.0L / 0.0L));
+  *omega = (double)om;
+  free(ax);
+  free(aax);
+  free(rowabs);
+}

@@ -1,0 +1,62 @@
+/* Test infrastructure (the oracle): a plain-C restatement of the reference
+ * smf numeric phase, used only by tests/, smoke() and bench.py's CPU-baseline
+ * leg as the checker of the CUDA engine. Never linked into the product.
+ *
+ * Input is the reference's analysis output (AnalysisKeep arrays,
+ * solver/include/smf/analysis.hpp:25-144) and the values already placed in
+ * the permuted lower pattern (and scaled), as multifrontal_factor_serial
+ * receives them (solver/src/multifrontal_serial.cpp:1105).
+ */
+#ifndef MF_ORACLE_H
+#define MF_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  int n, nsn;
+  const int *sn_start, *sn_end, *sn_parent; /* supernodes, postorder numbering */
+  const int *child_ptr, *child_idx;         /* children, descending postorder */
+  const int *front_row_ptr, *front_row_idx; /* symbolic front rows, sorted */
+  const int *postorder;
+  const int *pcp, *pri; /* permuted lower pattern (new indices) */
+} mfo_analysis;
+
+typedef struct {
+  double u, eff_small, small_pivot;
+  int nb, blocked_min_front, posdef;
+} mfo_params;
+
+typedef struct {
+  /* outputs, sized by the caller: f_out/p_out/blk_off/row_off per supernode;
+   * blocks: capacity blk_cap doubles; rows: capacity row_cap ints;
+   * tags: per supernode p entries at tag_off = sum of earlier p (cap row_cap). */
+  int *f_out, *p_out;
+  int64_t *blk_off, *row_off;
+  double *blocks;
+  int64_t blk_cap;
+  int *rows;
+  int64_t row_cap;
+  int8_t *tags;
+  /* counts */
+  int64_t pos, neg, zero, delayed, two_by_two, max_front;
+  double flops;
+  int status; /* 0 ok, 1 not positive definite, 2 singular (zero pivots), 3 capacity, 4 non-finite D */
+} mfo_factor;
+
+int mfo_factorize(const mfo_analysis *a, const double *pvals, const mfo_params *prm, mfo_factor *out);
+
+/* In-place full solve of A x = b on the permuted, scaled system:
+ * x (n, new numbering) overwritten. */
+void mfo_solve_permuted(const mfo_analysis *a, const mfo_factor *fac, int posdef, double *x);
+
+/* r = b - A x with A given as the full lower CSC (original numbering), and
+ * the normwise / componentwise backward errors (long double accumulation). */
+void mfo_residual(int n, const int *cp, const int *ri, const double *v, const double *b,
+                  const double *x, double *r, double *eta_inf, double *omega);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
