@@ -1,0 +1,186 @@
+/*
+ * smfg.h -- C ABI of the B200 numeric phase for smf (sparse symmetric
+ * multifrontal LDL^T / Cholesky). Plain pointers and sizes only.
+ *
+ * The engine takes smf's symbolic analysis as is (the AnalysisKeep arrays,
+ * solver/include/smf/analysis.hpp:25-144) and replaces the numeric phase
+ * behind smf::Solver::factor / solve (solver/include/smf/solver.hpp:78-114),
+ * i.e. the body of multifrontal_factor_serial
+ * (solver/src/multifrontal_serial.cpp:1105) and of solve_core's forward /
+ * diagonal / backward passes (solver/src/solve.cpp:858-1075), on one GPU.
+ *
+ * All indices are 0-based int32; dense blocks are column-major.
+ */
+#ifndef SMFG_H
+#define SMFG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define SMFG_API __attribute__((visibility("default")))
+#else
+#define SMFG_API
+#endif
+
+#define SMFG_ABI_VERSION 1
+
+/* Status codes. 0..5 are smf_c.h's SMF_OK .. SMF_ERR_INEXACT_INERTIA
+ * (solver/include/smf/smf_c.h:83-88); the rest are specific to the device. */
+#define SMFG_OK 0
+#define SMFG_ERR_INVALID_ARG 1
+#define SMFG_ERR_SINGULAR 2       /* zero pivots, or not positive definite (SPD path) */
+#define SMFG_ERR_INTERNAL 3
+#define SMFG_ERR_WRONG_INERTIA 4  /* more negative pivots than max_negative_pivots */
+#define SMFG_ERR_INEXACT_INERTIA 5
+#define SMFG_ERR_CUDA 10          /* a CUDA runtime call failed */
+#define SMFG_ERR_NO_DEVICE 11
+#define SMFG_ERR_NONFINITE 12     /* non-finite input values (smf ErrorCode::IllegalValue) */
+#define SMFG_ERR_ARENA 13         /* device arena too small (delays); retried internally */
+#define SMFG_ERR_TIMEOUT 14       /* a bounded device wait gave up */
+
+/* Factor status (smf::FactorStatus, solver/include/smf/types.hpp:230-238). */
+#define SMFG_FACTOR_SUCCESS 0
+#define SMFG_FACTOR_NOT_POSDEF 1
+#define SMFG_FACTOR_SINGULAR 2
+#define SMFG_FACTOR_INERTIA_EXCEEDED 4
+
+/* Solve jobs (smf::SolveJob / SMF_SOLVE_*). */
+#define SMFG_SOLVE_FULL 0
+#define SMFG_SOLVE_FORWARD 1
+#define SMFG_SOLVE_DIAGONAL 2
+#define SMFG_SOLVE_BACKWARD 3
+
+/* Schur-update precision of large fronts. */
+#define SMFG_PREC_FP64 0          /* plain FP64, the reference's arithmetic */
+#define SMFG_PREC_MIXED 1         /* tensor-core reduced precision where the selector allows */
+
+/* The analysis the numeric phase consumes: the AnalysisKeep arrays of smf
+ * (analysis.hpp:25-144) that multifrontal_factor_serial reads. Supernodes are
+ * numbered in postorder; children are listed in descending postorder (the
+ * order the reference's LIFO contribution stack consumes them); each front's
+ * rows are sorted ascending, its first (sn_end - sn_start) rows being its
+ * pivots. The permuted lower pattern (perm_col_ptr / perm_row_idx, new
+ * numbering, rows >= column) is where the values are placed. */
+typedef struct {
+  int n;
+  int nsn;
+  const int *perm;          /* perm[new] = old, n */
+  const int *sn_start;      /* nsn */
+  const int *sn_end;        /* nsn */
+  const int *sn_parent;     /* nsn, -1 at roots */
+  const int *child_ptr;     /* nsn + 1 */
+  const int *child_idx;     /* child_ptr[nsn] */
+  const int *front_row_ptr; /* nsn + 1 */
+  const int *front_row_idx; /* front_row_ptr[nsn] */
+  const int *postorder;     /* nsn */
+  const int *perm_col_ptr;  /* n + 1 */
+  const int *perm_row_idx;  /* perm_col_ptr[n] */
+  /* Value placement: input entry k (the caller's order, nnz_in entries) goes
+   * to cleaned slot orig_to_clean[k] (-1 = dropped; duplicates summed in
+   * input order), cleaned slot c to permuted slot clean_to_perm[c]; the
+   * cleaned pattern (clean_col_ptr / clean_row_idx, original numbering)
+   * gives each slot's row and column for the scaling S A S.
+   * AnalysisKeep::orig_to_clean_idx, orig_to_perm_idx, cleaned. */
+  int64_t nnz_in;
+  const int *orig_to_clean; /* nnz_in */
+  const int *clean_to_perm; /* clean_col_ptr[n] */
+  const int *clean_col_ptr; /* n + 1 */
+  const int *clean_row_idx; /* clean_col_ptr[n] */
+} smfg_analysis_t;
+
+typedef struct {
+  int abi_version;        /* SMFG_ABI_VERSION */
+  int posdef;             /* 1: Cholesky path (smf's SPD factor_posdef) */
+  double u;               /* threshold pivoting parameter (Control::pivot_u) */
+  double small_pivot;     /* zero-pivot threshold (Control::small_pivot) */
+  int nb;                 /* panel width (Control::indef_panel_size, 16) */
+  int blocked_min_front;  /* blocked kernel from this many rows (96) */
+  int precision;          /* SMFG_PREC_* */
+  int max_negative_pivots;/* < 0: off (Control::max_negative_pivots) */
+  const double *scale;    /* optional S (length n, original numbering), NULL = none */
+  int reserved_i[8];
+  double reserved_d[8];
+} smfg_control_t;
+
+typedef struct {
+  int status;             /* SMFG_OK or an error code */
+  int factor_status;      /* SMFG_FACTOR_* */
+  int num_pos, num_neg, num_zero;
+  int delayed_pivots;
+  int two_by_two_pivots;
+  int max_front;
+  int64_t factor_entries; /* sum over fronts of f * p */
+  double flops;           /* smf's actual_flops count */
+  double max_abs;         /* max |S A S| */
+  double factor_ms;       /* device time of the last factor */
+  double solve_ms;        /* device time of the last solve */
+  int levels;
+  int kernel_launches;    /* kernels launched by the last call */
+  int mixed_fronts;       /* fronts whose Schur update ran in reduced precision */
+  int reserved_i[7];
+  double reserved_d[8];
+} smfg_info_t;
+
+typedef struct smfg_plan_s *smfg_plan_t;
+
+SMFG_API int smfg_abi_version(void);
+SMFG_API void smfg_default_control(smfg_control_t *ctrl);
+
+/* Device plan from an analysis (host arrays). Replaces the per-analysis
+ * set-up of multifrontal_factor_serial (multifrontal_serial.cpp:1105-1300):
+ * level sets of the assembly tree, child -> parent row maps, value-placement
+ * maps, arena sizes. device < 0: the current device. */
+SMFG_API int smfg_plan_create(const smfg_analysis_t *a, int device, smfg_plan_t *out);
+SMFG_API void smfg_plan_destroy(smfg_plan_t *plan);
+
+/* Numeric factorization of new values (the caller's entry order, nnz_in
+ * host doubles) -- Solver::factor(ak, values, ...) (solver.hpp:88-90). */
+SMFG_API int smfg_factor(smfg_plan_t plan, const double *values, const smfg_control_t *ctrl,
+                         smfg_info_t *info);
+/* The same with the values already in device memory. */
+SMFG_API int smfg_factor_device(smfg_plan_t plan, const double *d_values,
+                                const smfg_control_t *ctrl, smfg_info_t *info);
+
+/* Solve in place: b is n x nrhs column-major with leading dimension ldb,
+ * host memory -- Solver::solve (solver.hpp:101-114). */
+SMFG_API int smfg_solve(smfg_plan_t plan, double *b, int nrhs, int ldb, int job, smfg_info_t *info);
+/* The same with b in device memory. */
+SMFG_API int smfg_solve_device(smfg_plan_t plan, double *d_b, int nrhs, int ldb, int job,
+                               smfg_info_t *info);
+
+/* Inertia of the last factorization (smf_inertia, smf_c.h:175). */
+SMFG_API int smfg_inertia(smfg_plan_t plan, int *pos, int *neg, int *zero);
+
+/* Per-front export of the last factor, in the FactorKeep layout
+ * (factor_posdef.hpp:43-220): for supernode s, f[s] realized rows, p[s]
+ * stored pivots, its L block (f x p, leading dimension f, D inline for the
+ * indefinite path) copied to blocks + blk_off[s] (packed in supernode
+ * order), rows (pivot order) to rows + row_off[s], pivot tags (1, 2, -1, 0)
+ * to tags + tag_off (sum of earlier p). Sizes from smfg_factor_sizes. */
+SMFG_API int smfg_factor_sizes(smfg_plan_t plan, int64_t *block_entries, int64_t *row_entries);
+SMFG_API int smfg_factor_export(smfg_plan_t plan, int *f, int *p, int64_t *blk_off, double *blocks,
+                                int64_t *row_off, int *rows, int8_t *tags);
+
+/* Residual r = b - A x and backward errors against the factored values
+ * (refinement.cpp:39-130; compensated FP64 on the device). Host arrays. */
+SMFG_API int smfg_residual(smfg_plan_t plan, const double *b, const double *x, int nrhs, double *r,
+                           double *eta_inf, double *omega);
+
+/* Iterative refinement (classical, refinement.cpp:316-413) of x for b, host
+ * arrays (n x nrhs, leading dimension n): at most max_steps solves, stopping
+ * at eta_inf <= 1e-10 and omega <= omega_target. */
+SMFG_API int smfg_refine(smfg_plan_t plan, const double *b, double *x, int nrhs, int max_steps,
+                         double omega_target, double *eta_inf, double *omega, int *steps);
+
+SMFG_API const char *smfg_error_string(int code);
+/* Message of the last CUDA or internal error on the calling thread. */
+SMFG_API const char *smfg_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SMFG_H */

@@ -1,0 +1,721 @@
+// Dense partial LDL^T / Cholesky of one front by one thread block, with
+// smf's threshold 1x1 / 2x2 pivoting, stall handling and delayed columns.
+//
+// The algorithm and every per-entry operation follow the reference kernel
+// ldlt_factor_front (solver/src/ldlt_kernel.cpp:970-1139); the block of
+// threads shares each step:
+//   - pivot search (select_pivot, ldlt_kernel.cpp:127-275; two_by_two_ok
+//     :97-122) as block-wide max / top-2 reductions whose ties resolve to
+//     the lowest row, i.e. the reference's first-in-scan-order rule;
+//   - symmetric swaps (sym_swap :333-347): every swapped pair is disjoint,
+//     so one pass of the block;
+//   - eliminations (eliminate_1x1 / _2x2 :352-545): multiply, then subtract,
+//     rounded separately (__dmul_rn / __dsub_rn, never contracted), as the
+//     reference compiles ldlt_kernel.cpp with -ffp-contract=off;
+//   - deferred and Schur updates (:705-761, :764-933): one fused
+//     multiply-add per pivot and entry, pivots in order, as the reference's
+//     contracted GEMM loops (dense_kernel_lapack.cpp:182-234) compute them.
+// With the same inputs the front's L, D, pivot order, tags and Schur
+// complement are therefore the reference's, bit for bit.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace smfg {
+
+constexpr double kWeakPivotRatio = 1e-6;  // ldlt_kernel.hpp:100
+
+struct PivotParams {
+  double u, eff_small, small_pivot;
+  int nb, blocked_min_front, posdef;
+};
+
+struct FrontStats {
+  int pos, neg, zero, two_by_two;
+  double flops;
+};
+
+// Shared control block of a front kernel.
+struct FrontShared {
+  double red[32];
+  int redi[32];
+  double red2[32];
+  int kind, a, b;        // pivot choice
+  int k;                 // next pivot position
+  int order[128];        // stall partner pairs (row ids)
+  int np;
+  double vals[8];
+  int ivals[8];
+  FrontStats st;
+};
+
+__device__ __forceinline__ double dmax_ref(double a, double b) {  // std::max(a, b)
+  return (a < b) ? b : a;
+}
+
+__device__ __forceinline__ double max3_ref(double a, double b, double c) {
+  double m = a;
+  if (m < b) m = b;
+  if (m < c) m = c;
+  return m;
+}
+
+// Top-2 of a multiset of |values| with the first index of the maximum
+// (the reference's "if (v > m1) {...} else if (v > m2)" scan, NaN ignored).
+struct Top2 {
+  double m1, m2;
+  int r;
+};
+
+__device__ __forceinline__ void top2_add(Top2 &t, double v, int i) {
+  if (v > t.m1) {
+    t.m2 = t.m1;
+    t.m1 = v;
+    t.r = i;
+  } else if (v > t.m2) {
+    t.m2 = v;
+  }
+}
+
+__device__ __forceinline__ Top2 top2_merge(Top2 a, Top2 b) {
+  Top2 o;
+  if (a.m1 > b.m1) {
+    o.m1 = a.m1;
+    o.r = a.r;
+  } else if (b.m1 > a.m1) {
+    o.m1 = b.m1;
+    o.r = b.r;
+  } else {
+    o.m1 = a.m1;
+    o.r = (a.r < 0) ? b.r : ((b.r < 0) ? a.r : min(a.r, b.r));
+  }
+  o.m2 = fmax(fmin(a.m1, b.m1), fmax(a.m2, b.m2));
+  return o;
+}
+
+template <int NT>
+struct Block {
+  static_assert(NT % 32 == 0 && NT <= 1024, "block size");
+  static constexpr int NW = NT / 32;
+
+  // Max of non-negative values, NaN ignored (fmax).
+  static __device__ double max(double v, FrontShared &sh) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (NW == 1) return v;
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sh.red[w] = v;
+    __syncthreads();
+    v = (l < NW) ? sh.red[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+  }
+
+  // Two maxima at once.
+  static __device__ void max2(double &a, double &b, FrontShared &sh) {
+    for (int o = 16; o > 0; o >>= 1) {
+      a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+      b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+    }
+    if (NW == 1) return;
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) {
+      sh.red[w] = a;
+      sh.red2[w] = b;
+    }
+    __syncthreads();
+    a = (l < NW) ? sh.red[l] : 0.0;
+    b = (l < NW) ? sh.red2[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+      b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+    }
+  }
+
+  static __device__ Top2 top2(Top2 t, FrontShared &sh) {
+    for (int o = 16; o > 0; o >>= 1) {
+      Top2 u;
+      u.m1 = __shfl_xor_sync(0xffffffffu, t.m1, o);
+      u.m2 = __shfl_xor_sync(0xffffffffu, t.m2, o);
+      u.r = __shfl_xor_sync(0xffffffffu, t.r, o);
+      t = top2_merge(t, u);
+    }
+    if (NW == 1) return t;
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) {
+      sh.red[w] = t.m1;
+      sh.red2[w] = t.m2;
+      sh.redi[w] = t.r;
+    }
+    __syncthreads();
+    if (l < NW) {
+      t.m1 = sh.red[l];
+      t.m2 = sh.red2[l];
+      t.r = sh.redi[l];
+    } else {
+      t.m1 = 0.0;
+      t.m2 = 0.0;
+      t.r = -1;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      Top2 u;
+      u.m1 = __shfl_xor_sync(0xffffffffu, t.m1, o);
+      u.m2 = __shfl_xor_sync(0xffffffffu, t.m2, o);
+      u.r = __shfl_xor_sync(0xffffffffu, t.r, o);
+      t = top2_merge(t, u);
+    }
+    return t;
+  }
+
+  // First index i in [lo, hi) of the largest |col[i]| (> 0), the
+  // reference's "if (v > out_max)" scan; -1 when all are zero.
+  static __device__ void argmax(const double *col, int lo, int hi, double &m, int &r,
+                                FrontShared &sh) {
+    Top2 t{0.0, 0.0, -1};
+    for (int i = lo + (int)threadIdx.x; i < hi; i += NT) top2_add(t, fabs(col[i]), i);
+    t = top2(t, sh);
+    m = t.m1;
+    r = t.r;
+  }
+};
+
+// The front: F f x f column-major with leading dimension ld (lower triangle
+// used), its row ids, pivot tags, and W (f x nb, leading dimension f) for the
+// blocked path's unscaled pivot columns.
+struct FrontRef {
+  double *F;
+  int ld, f, ne;
+  int *rows;
+  int8_t *tags;
+  double *W;
+  int *loc;  // assembly position of the row now at each position (null: untracked)
+};
+
+__device__ __forceinline__ double fat(const FrontRef &v, int i, int j) {  // element (i, j), i >= j
+  return v.F[(size_t)j * v.ld + i];
+}
+
+template <int NT>
+__device__ void sym_swap_blk(const FrontRef &v, int p, int q, int w_cols) {
+  if (p == q) return;
+  if (p > q) {
+    const int t = p;
+    p = q;
+    q = t;
+  }
+  const size_t sf = (size_t)v.ld;
+  double *F = v.F;
+  const int f = v.f;
+  // Pairs: diagonal; m < p; p < m < q; m > q; rows; W rows. All disjoint.
+  const int n1 = p, n2 = q - p - 1, n3 = f - q - 1;
+  const int total = 1 + n1 + n2 + n3 + 1 + w_cols;
+  for (int t = threadIdx.x; t < total; t += NT) {
+    if (t == 0) {
+      const double x = F[p * sf + p];
+      F[p * sf + p] = F[q * sf + q];
+      F[q * sf + q] = x;
+    } else if (t <= n1) {
+      const int m = t - 1;
+      const double x = F[m * sf + p];
+      F[m * sf + p] = F[m * sf + q];
+      F[m * sf + q] = x;
+    } else if (t <= n1 + n2) {
+      const int m = p + 1 + (t - 1 - n1);
+      const double x = F[p * sf + m];
+      F[p * sf + m] = F[m * sf + q];
+      F[m * sf + q] = x;
+    } else if (t <= n1 + n2 + n3) {
+      const int m = q + 1 + (t - 1 - n1 - n2);
+      const double x = F[p * sf + m];
+      F[p * sf + m] = F[q * sf + m];
+      F[q * sf + m] = x;
+    } else if (t == n1 + n2 + n3 + 1) {
+      const int r = v.rows[p];
+      v.rows[p] = v.rows[q];
+      v.rows[q] = r;
+      if (v.loc) {
+        const int a = v.loc[p];
+        v.loc[p] = v.loc[q];
+        v.loc[q] = a;
+      }
+    } else {
+      const int c = t - (n1 + n2 + n3 + 2);
+      double *W = v.W + (size_t)c * f;
+      const double x = W[p];
+      W[p] = W[q];
+      W[q] = x;
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void inertia_1x1(double d, double small, FrontStats &st) {
+  if (!isfinite(d) || fabs(d) < small) ++st.zero;
+  else if (d > 0.0) ++st.pos;
+  else ++st.neg;
+}
+
+// add_inertia_2x2 (solver/src/dense_indef.cpp:52-83).
+__device__ __forceinline__ void inertia_2x2(double d00, double d10, double d11, double small,
+                                            FrontStats &st) {
+  if (d10 == 0.0) {
+    inertia_1x1(d00, small, st);
+    inertia_1x1(d11, small, st);
+    return;
+  }
+  const double s = max3_ref(fabs(d00), fabs(d10), fabs(d11));
+  double det_s = 0.0;
+  if (isfinite(s) && s != 0.0)
+    det_s = __dsub_rn(__dmul_rn(d00 / s, d11 / s), __dmul_rn(d10 / s, d10 / s));
+  if (s == 0.0 || !isfinite(det_s)) {
+    st.zero += 2;
+    return;
+  }
+  const double tr_s = __dadd_rn(d00 / s, d11 / s);
+  if (det_s < -small) {
+    ++st.pos;
+    ++st.neg;
+  } else if (fabs(det_s) <= small) {
+    ++st.zero;
+    if (tr_s > small) ++st.pos;
+    else if (tr_s < -small) ++st.neg;
+    else ++st.zero;
+  } else {
+    if (tr_s > 0.0) st.pos += 2;
+    else if (tr_s < 0.0) st.neg += 2;
+    else st.zero += 2;
+  }
+}
+
+// inverse_2x2 (ldlt_kernel.cpp:470-480).
+__device__ __forceinline__ void inverse_2x2(double d00, double d10, double d11, double &i00,
+                                            double &i10, double &i11) {
+  const double s = max3_ref(fabs(d00), fabs(d10), fabs(d11));
+  const double a = d00 / s, b = d10 / s, c = d11 / s;
+  const double inv = 1.0 / __dmul_rn(__dsub_rn(__dmul_rn(a, c), __dmul_rn(b, b)), s);
+  i00 = __dmul_rn(c, inv);
+  i10 = __dmul_rn(-b, inv);
+  i11 = __dmul_rn(a, inv);
+}
+
+template <int NT>
+__device__ void eliminate_1x1_blk(const FrontRef &v, int k, int ucol_end, bool useW, int w_col) {
+  const size_t sf = (size_t)v.ld;
+  const int f = v.f;
+  double *ck = v.F + k * sf;
+  const double inv_d = 1.0 / ck[k];
+  if (useW) {
+    double *w = v.W + (size_t)w_col * f;
+    for (int i = k + 1 + threadIdx.x; i < f; i += NT) w[i] = ck[i];
+  }
+  const int ncol = ucol_end - (k + 1);
+  if (ncol > 0) {
+    const long long tot = (long long)ncol * f;
+    for (long long t = threadIdx.x; t < tot; t += NT) {
+      const int j = k + 1 + (int)(t / f);
+      const int i = (int)(t % f);
+      if (i < j) continue;
+      const double lj = __dmul_rn(ck[j], inv_d);
+      if (lj == 0.0) continue;
+      double *cj = v.F + (size_t)j * sf;
+      cj[i] = __dsub_rn(cj[i], __dmul_rn(ck[i], lj));
+    }
+  }
+  __syncthreads();
+  for (int i = k + 1 + threadIdx.x; i < f; i += NT) ck[i] = __dmul_rn(ck[i], inv_d);
+  __syncthreads();
+}
+
+template <int NT>
+__device__ void eliminate_2x2_blk(const FrontRef &v, int k, int ucol_end, bool useW, int w_col) {
+  const size_t sf = (size_t)v.ld;
+  const int f = v.f;
+  double *c0 = v.F + k * sf;
+  double *c1 = v.F + (k + 1) * sf;
+  double i00, i10, i11;
+  inverse_2x2(c0[k], c0[k + 1], c1[k + 1], i00, i10, i11);
+  if (useW) {
+    double *w0 = v.W + (size_t)w_col * f;
+    double *w1 = w0 + f;
+    for (int i = k + 2 + threadIdx.x; i < f; i += NT) {
+      w0[i] = c0[i];
+      w1[i] = c1[i];
+    }
+  }
+  const int ncol = ucol_end - (k + 2);
+  if (ncol > 0) {
+    const long long tot = (long long)ncol * f;
+    for (long long t = threadIdx.x; t < tot; t += NT) {
+      const int j = k + 2 + (int)(t / f);
+      const int i = (int)(t % f);
+      if (i < j) continue;
+      const double a0 = c0[j], a1 = c1[j];
+      const double l0 = __dadd_rn(__dmul_rn(i00, a0), __dmul_rn(i10, a1));
+      const double l1 = __dadd_rn(__dmul_rn(i10, a0), __dmul_rn(i11, a1));
+      if (l0 == 0.0 && l1 == 0.0) continue;
+      double *d0 = v.F + (size_t)j * sf;
+      d0[i] = __dsub_rn(d0[i], __dadd_rn(__dmul_rn(c0[i], l0), __dmul_rn(c1[i], l1)));
+    }
+  }
+  __syncthreads();
+  for (int i = k + 2 + threadIdx.x; i < f; i += NT) {
+    const double a0 = c0[i], a1 = c1[i];
+    c0[i] = __dadd_rn(__dmul_rn(i00, a0), __dmul_rn(i10, a1));
+    c1[i] = __dadd_rn(__dmul_rn(i10, a0), __dmul_rn(i11, a1));
+  }
+  __syncthreads();
+}
+
+// two_by_two_ok (ldlt_kernel.cpp:97-122); off0 = max(m2, max_{i>=ext0} |col|).
+__device__ __forceinline__ bool two_by_two_ok_s(double d00, double d10, double d11, double off0,
+                                                double off1, const PivotParams &prm,
+                                                double &growth) {
+  const double s2 = max3_ref(fabs(d00), fabs(d10), fabs(d11));
+  if (!(s2 >= prm.eff_small) || !isfinite(s2)) return false;
+  const double a = d00 / s2, b = d10 / s2, c = d11 / s2;
+  const double det_s = __dsub_rn(__dmul_rn(a, c), __dmul_rn(b, b));
+  if (!(fabs(det_s) > prm.small_pivot)) return false;
+  double g = 0.0;
+  if (off0 > 0.0 || off1 > 0.0) {
+    const double bound0 = __dadd_rn(__dmul_rn(fabs(c), off0), __dmul_rn(fabs(b), off1)) / s2;
+    const double bound1 = __dadd_rn(__dmul_rn(fabs(b), off0), __dmul_rn(fabs(a), off1)) / s2;
+    if (__dmul_rn(prm.u, dmax_ref(bound0, bound1)) > fabs(det_s)) return false;
+    g = dmax_ref(bound0, bound1) / fabs(det_s);
+  }
+  growth = g;
+  return true;
+}
+
+// select_pivot (ldlt_kernel.cpp:127-275). Result in sh.kind / sh.a / sh.b.
+template <int NT>
+__device__ void select_pivot_blk(const FrontRef &v, int k, int limit, const PivotParams &prm,
+                                 FrontShared &sh) {
+  const size_t sf = (size_t)v.ld;
+  const double *F = v.F;
+  const int f = v.f, ne = v.ne;
+  int kind = 0, pa = -1, pb = -1;
+  if (prm.posdef) {
+    const double d = F[(size_t)k * sf + k];
+    if (d > 0.0 && isfinite(d)) {
+      kind = 1;
+      pa = k;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      sh.kind = kind;
+      sh.a = pa;
+      sh.b = pb;
+    }
+    __syncthreads();
+    return;
+  }
+  bool done = false;
+  if (k < limit) {
+    const double *col0 = F + (size_t)k * sf;
+    const double a0 = fabs(col0[k]);
+    if (a0 >= prm.eff_small) {
+      double cm = 0.0;
+      for (int i = k + 1 + threadIdx.x; i < f; i += NT) cm = fmax(cm, fabs(col0[i]));
+      cm = Block<NT>::max(cm, sh);
+      if (!(__dmul_rn(prm.u, cm) > a0) && !(a0 < __dmul_rn(kWeakPivotRatio, cm))) {
+        kind = 1;
+        pa = k;
+        done = true;
+      }
+    }
+  }
+  for (int cand = k; cand < limit && !done; ++cand) {
+    const double *col = F + (size_t)cand * sf;
+    const double a_cand = fabs(col[cand]);
+    Top2 t{0.0, 0.0, -1};
+    for (int i = k + threadIdx.x; i < cand; i += NT) top2_add(t, fabs(F[(size_t)i * sf + cand]), i);
+    for (int i = cand + 1 + threadIdx.x; i < ne; i += NT) top2_add(t, fabs(col[i]), i);
+    t = Block<NT>::top2(t, sh);
+    const int ext0 = ne > cand + 1 ? ne : cand + 1;
+    double ext = 0.0;
+    for (int i = ext0 + threadIdx.x; i < f; i += NT) ext = fmax(ext, fabs(col[i]));
+    ext = Block<NT>::max(ext, sh);
+    const double m1 = t.m1, m2 = t.m2;
+    const int r_best = t.r;
+    bool weak_1x1 = false;
+    double weak_growth = 0.0;
+    if (a_cand >= prm.eff_small && !(__dmul_rn(prm.u, m1) > a_cand)) {
+      if (!(__dmul_rn(prm.u, ext) > a_cand)) {
+        const double colmax = dmax_ref(m1, ext);
+        if (!(a_cand < __dmul_rn(kWeakPivotRatio, colmax))) {
+          kind = 1;
+          pa = cand;
+          done = true;
+          break;
+        }
+        weak_1x1 = true;
+        weak_growth = colmax / a_cand;
+      }
+    }
+    if (r_best < k || r_best >= limit || m1 <= 0.0) {
+      if (weak_1x1) {
+        kind = 1;
+        pa = cand;
+        done = true;
+        break;
+      }
+      continue;
+    }
+    const double *col_r = F + (size_t)r_best * sf;
+    double om2 = 0.0, off1 = 0.0;
+    for (int i = k + threadIdx.x; i < r_best; i += NT) {
+      const double x = fabs(F[(size_t)i * sf + r_best]);
+      om2 = fmax(om2, x);
+      if (i != cand) off1 = fmax(off1, x);
+    }
+    for (int i = r_best + 1 + threadIdx.x; i < f; i += NT) {
+      const double x = fabs(col_r[i]);
+      om2 = fmax(om2, x);
+      if (i != cand) off1 = fmax(off1, x);
+    }
+    Block<NT>::max2(om2, off1, sh);
+    double growth2 = 0.0;
+    const double d00 = col[cand];
+    const double d10 = (r_best >= cand) ? F[(size_t)cand * sf + r_best] : F[(size_t)r_best * sf + cand];
+    const double d11 = col_r[r_best];
+    if (k + 1 < limit && two_by_two_ok_s(d00, d10, d11, dmax_ref(m2, ext), off1, prm, growth2) &&
+        (!weak_1x1 || growth2 < weak_growth)) {
+      kind = 2;
+      pa = cand;
+      pb = r_best;
+      done = true;
+      break;
+    }
+    if (weak_1x1) {
+      kind = 1;
+      pa = cand;
+      done = true;
+      break;
+    }
+    const double a_r = fabs(d11);
+    if (a_r >= prm.eff_small && (om2 == 0.0 || a_r >= __dmul_rn(prm.u, om2))) {
+      kind = 1;
+      pa = r_best;
+      done = true;
+      break;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    sh.kind = kind;
+    sh.a = pa;
+    sh.b = pb;
+  }
+  __syncthreads();
+}
+
+// apply_pivot (ldlt_kernel.cpp:666-698). The pivot choice is in sh.
+template <int NT>
+__device__ void apply_pivot_blk(const FrontRef &v, int &k, bool useW, int w_cols, int ucol_end,
+                                const PivotParams &prm, FrontShared &sh) {
+  const size_t sf = (size_t)v.ld;
+  const int f = v.f;
+  const int kind = sh.kind, pa = sh.a, pb = sh.b;
+  if (kind == 1) {
+    sym_swap_blk<NT>(v, k, pa, useW ? w_cols : 0);
+    if (threadIdx.x == 0) {
+      inertia_1x1(v.F[k * sf + k], prm.eff_small, sh.st);
+      v.tags[k] = 1;
+      const double rem = (double)(f - (k + 1));
+      sh.st.flops += rem + rem * (rem + 1.0);
+    }
+    eliminate_1x1_blk<NT>(v, k, ucol_end, useW, w_cols);
+    k += 1;
+    return;
+  }
+  int partner = pb;
+  if (pa != k) {
+    sym_swap_blk<NT>(v, k, pa, useW ? w_cols : 0);
+    if (partner == k) partner = pa;
+  }
+  if (partner != k + 1) sym_swap_blk<NT>(v, k + 1, partner, useW ? w_cols : 0);
+  if (threadIdx.x == 0) {
+    inertia_2x2(v.F[k * sf + k], v.F[k * sf + k + 1], v.F[(k + 1) * sf + k + 1], prm.small_pivot,
+                sh.st);
+    v.tags[k] = 2;
+    v.tags[k + 1] = -1;
+    const double rem = (double)(f - (k + 2));
+    sh.st.flops += 6.0 * rem + 2.0 * rem * (rem + 1.0);
+    ++sh.st.two_by_two;
+  }
+  eliminate_2x2_blk<NT>(v, k, ucol_end, useW, w_cols);
+  k += 2;
+}
+
+// deferred_update (ldlt_kernel.cpp:705-761): F[c0:f, c0:e] -= L[c0:f, p0:p1]
+// W[c0:e, :]^T, one fused multiply-add per pivot in order, zero W skipped.
+template <int NT>
+__device__ void deferred_update_blk(const FrontRef &v, int p0, int p1, int c0, int e) {
+  const int jb = p1 - p0, m = e - c0;
+  if (jb <= 0 || m <= 0) return;
+  const size_t sf = (size_t)v.ld;
+  const int f = v.f;
+  const int h = f - c0;
+  const long long tot = (long long)m * h;
+  for (long long t = threadIdx.x; t < tot; t += NT) {
+    const int j = c0 + (int)(t / h);
+    const int i = c0 + (int)(t % h);
+    if (i < j) continue;
+    double c = v.F[(size_t)j * sf + i];
+    for (int p = 0; p < jb; ++p) {
+      const double b = v.W[(size_t)p * f + j];
+      if (b == 0.0) continue;
+      c = fma(-v.F[(size_t)(p0 + p) * sf + i], b, c);
+    }
+    v.F[(size_t)j * sf + i] = c;
+  }
+  __syncthreads();
+}
+
+// (L D)(j, c) as fill_ld_column computes it (ldlt_kernel.cpp:764-818).
+__device__ __forceinline__ double ld_entry(const FrontRef &v, int c, int j) {
+  const size_t sf = (size_t)v.ld;
+  const double *Lc = v.F + (size_t)c * sf;
+  const int8_t tag = v.tags[c];
+  if (tag == 1) return __dmul_rn(Lc[j], Lc[c]);
+  if (tag == 2) return __dadd_rn(__dmul_rn(Lc[j], Lc[c]), __dmul_rn(Lc[sf + j], Lc[c + 1]));
+  if (tag == -1) {
+    const double *L0 = Lc - sf;
+    return __dadd_rn(__dmul_rn(L0[j], L0[c]), __dmul_rn(Lc[j], Lc[c]));
+  }
+  return 0.0;
+}
+
+// schur_update (ldlt_kernel.cpp:820-933): F[e:f, e:f] -= L LD^T over the
+// pivots [p0, p) in order.
+template <int NT>
+__device__ void schur_update_blk(const FrontRef &v, int p0, int p, int e) {
+  const int q = v.f - e;
+  if (p <= p0 || q <= 0) return;
+  const size_t sf = (size_t)v.ld;
+  const long long tot = (long long)q * q;
+  for (long long t = threadIdx.x; t < tot; t += NT) {
+    const int j = e + (int)(t / q);
+    const int i = e + (int)(t % q);
+    if (i < j) continue;
+    double c = v.F[(size_t)j * sf + i];
+    for (int cc = p0; cc < p; ++cc) {
+      const double b = ld_entry(v, cc, j);
+      if (b == 0.0) continue;
+      c = fma(-v.F[(size_t)cc * sf + i], b, c);
+    }
+    v.F[(size_t)j * sf + i] = c;
+  }
+  __syncthreads();
+}
+
+// ldlt_factor_front (first = 0, no static pivoting). Returns the accepted
+// pivot count (uniform across the block); statistics in sh.st.
+template <int NT>
+__device__ int ldlt_factor_front_blk(const FrontRef &v, const PivotParams &prm, FrontShared &sh,
+                                     bool do_schur = true) {
+  const int f = v.f, ne = v.ne;
+  const size_t sf = (size_t)v.ld;
+  int k = 0;
+  if (f < prm.blocked_min_front || prm.nb <= 1) {
+    while (k < ne) {
+      select_pivot_blk<NT>(v, k, ne, prm, sh);
+      if (sh.kind == 0) break;
+      apply_pivot_blk<NT>(v, k, false, 0, f, prm, sh);
+    }
+    return k;
+  }
+  if (!prm.posdef) {
+    int live = ne, k_paired = -1;
+    while (k < live) {
+      const int ps = k;
+      const int pl = min(live, ps + prm.nb);
+      bool stalled = false;
+      while (k < pl) {
+        select_pivot_blk<NT>(v, k, pl, prm, sh);
+        if (sh.kind == 0) {
+          stalled = true;
+          break;
+        }
+        apply_pivot_blk<NT>(v, k, true, k - ps, pl, prm, sh);
+      }
+      deferred_update_blk<NT>(v, ps, k, pl, ne);
+      if (stalled && k != k_paired) {
+        if (threadIdx.x == 0) sh.np = 0;
+        __syncthreads();
+        const int max_pairs = min(prm.nb / 2, 64);
+        for (int pos = k; pos < pl; ++pos) {
+          if (sh.np / 2 >= max_pairs) break;
+          const double *col = v.F + (size_t)pos * sf;
+          double in_max = 0.0;
+          for (int i = k + threadIdx.x; i < pos; i += NT) in_max = fmax(in_max, fabs(v.F[(size_t)i * sf + pos]));
+          for (int i = pos + 1 + threadIdx.x; i < pl; i += NT) in_max = fmax(in_max, fabs(col[i]));
+          in_max = Block<NT>::max(in_max, sh);
+          double out_max;
+          int r;
+          Block<NT>::argmax(col, pl, ne, out_max, r, sh);
+          __syncthreads();
+          if (threadIdx.x == 0 && r >= 0 && out_max > in_max) {
+            bool taken = false;
+            for (int t = 1; t < sh.np; t += 2) taken = taken || sh.order[t] == v.rows[r];
+            if (!taken) {
+              sh.order[sh.np++] = v.rows[pos];
+              sh.order[sh.np++] = v.rows[r];
+            }
+          }
+          __syncthreads();
+        }
+        const int np = sh.np;
+        if (np > 0) {
+          for (int t = 0; t < np; ++t) {
+            if (threadIdx.x == 0) {
+              int qq = k + t;
+              while (qq < f - 1 && v.rows[qq] != sh.order[t]) ++qq;
+              sh.ivals[0] = qq;
+            }
+            __syncthreads();
+            const int qq = sh.ivals[0];
+            __syncthreads();
+            sym_swap_blk<NT>(v, k + t, qq, 0);
+          }
+          live = max(live, k + np);
+          k_paired = k;
+          continue;
+        }
+      }
+      if (stalled) {
+        const int m = pl - k;
+        const int mv = min(m, live - pl);
+        for (int t = 0; t < mv; ++t) sym_swap_blk<NT>(v, k + t, live - mv + t, 0);
+        live -= m;
+      }
+    }
+  }
+  while (k < ne) {
+    const int ps = k;
+    const int pl = min(ne, ps + prm.nb);
+    bool stalled = false;
+    while (k < pl) {
+      select_pivot_blk<NT>(v, k, pl, prm, sh);
+      if (sh.kind == 0) {
+        stalled = true;
+        break;
+      }
+      apply_pivot_blk<NT>(v, k, true, k - ps, pl, prm, sh);
+    }
+    deferred_update_blk<NT>(v, ps, k, pl, ne);
+    if (stalled && k < ne) {
+      const int ss = k;
+      select_pivot_blk<NT>(v, k, ne, prm, sh);
+      if (sh.kind == 0) break;
+      apply_pivot_blk<NT>(v, k, true, 0, ss, prm, sh);
+      deferred_update_blk<NT>(v, ss, k, k, ne);
+    }
+  }
+  if (do_schur) schur_update_blk<NT>(v, 0, k, ne);
+  return k;
+}
+
+}  // namespace smfg

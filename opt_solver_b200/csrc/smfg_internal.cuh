@@ -1,0 +1,88 @@
+// Internal types of the B200 numeric phase: the device plan built once per
+// analysis and the per-factorization device state.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/smfg.h"
+#include "smfg_front.cuh"
+
+namespace smfg {
+
+// Size classes of the front kernels (rows f after delays).
+constexpr int kSmallMax = 32;    // one warp, front in shared memory
+constexpr int kMediumMax = 128;  // one block, front in shared memory
+constexpr int kAsmCols = 32;     // columns per assembly work item
+
+// Device copies of the analysis-derived arrays (one per plan).
+struct DevPlan {
+  int n = 0, nsn = 0, nlevels = 0;
+  int64_t nnz = 0;      // permuted pattern entries
+  int64_t nnz_in = 0;   // caller's entries
+  int *sn_start = nullptr, *sn_width = nullptr, *sn_fsym = nullptr, *sn_parent = nullptr;
+  int *child_ptr = nullptr, *child_idx = nullptr;
+  int *frow_ptr = nullptr, *frow_idx = nullptr;
+  int *cpr_off = nullptr, *cpr_idx = nullptr;  // per child slot: parent symbolic positions
+  int *lvl_sn = nullptr;                       // supernodes by level
+  int *pcp = nullptr, *pri = nullptr;          // permuted lower pattern
+  int *pcol = nullptr;                         // column of each permuted slot
+  int *amap = nullptr;                         // entry -> symbolic row position in its front
+  int *vptr = nullptr, *vsrc = nullptr;        // permuted slot -> caller entries (input order)
+  int *perm = nullptr;                         // perm[new] = old
+  int *srow = nullptr, *sptr = nullptr;        // full symmetric CSR (residual), new numbering
+  int64_t *sidx = nullptr;                     // its entry -> permuted slot
+  int *sn_level = nullptr;
+};
+
+// Device state of one factorization (sized per plan, grown on demand).
+struct DevFactor {
+  double *pv = nullptr;      // permuted (scaled) values
+  double *pv_raw = nullptr;  // permuted unscaled values (residual)
+  double *scale = nullptr;   // S (original numbering) or null
+  int *sn_nd = nullptr, *sn_f = nullptr, *sn_ne = nullptr, *sn_p = nullptr, *sn_pstore = nullptr,
+      *sn_dout = nullptr;
+  int64_t *sn_off = nullptr, *sn_roff = nullptr;
+  int *child_doff = nullptr;  // per child slot: first delayed row's position in the parent
+  int *sn_stat = nullptr;     // 4 ints per supernode: pos, neg, zero, 2x2
+  double *sn_flops = nullptr;
+  int *lvl_blk = nullptr;     // per level entry: prefix of assembly work items (size nsn + nlevels)
+  double *arena = nullptr;    // fronts (f x f) + W (f x nb)
+  int64_t arena_cap = 0;
+  int *rows = nullptr;        // realized row ids, per front at sn_roff
+  int8_t *tags = nullptr;     // pivot tags, per front at sn_roff
+  int *cbmap = nullptr;       // CB row -> parent position, at the child's sn_roff + p
+  int *ploc = nullptr;        // 2 x rows_cap: pivot-order tracking of global-memory fronts
+  int64_t rows_cap = 0;
+  unsigned long long *counters = nullptr;  // [0] arena base, [1] rows base, [2] error flags, [3] max|A| bits, [4] blocks
+  double *work = nullptr;     // solve / refinement scratch
+  int64_t work_cap = 0;
+};
+
+struct Plan {
+  int device = 0;
+  int n = 0, nsn = 0, nlevels = 0;
+  int64_t nnz = 0, nnz_in = 0;
+  std::vector<int> lvl_ptr;      // host copy: level l = lvl_sn[lvl_ptr[l] .. lvl_ptr[l+1])
+  std::vector<int> lvl_maxf;     // symbolic max front per level
+  std::vector<int> lvl_maxkids;
+  int64_t sum_f2 = 0, sum_f = 0; // symbolic
+  int max_fsym = 0;
+  int64_t max_factor = 0;
+  DevPlan d;
+  DevFactor x;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // last factorization
+  bool factored = false;
+  int posdef = 0;
+  int nb = 16;
+  int factor_status = -1;
+  smfg_info_t info{};
+  std::vector<int> h_child_ptr, h_child_idx, h_sn_parent, h_postorder;
+  std::vector<void *> allocs;
+};
+
+}  // namespace smfg

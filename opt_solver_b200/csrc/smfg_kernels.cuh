@@ -1,0 +1,677 @@
+// Device kernels of the numeric phase: value placement, per-level front
+// set-up, assembly / extend-add, front factorization by size class, the
+// supernodal solves and the residual.
+#pragma once
+#include "smfg_internal.cuh"
+
+namespace smfg {
+
+// counters[] slots
+enum : int { kCArena = 0, kCRows = 1, kCFlags = 2, kCMaxAbs = 3, kCAux = 4, kCEffSmall = 5, kCCount = 8 };
+// error flag bits (counters[kCFlags])
+enum : unsigned { kFArena = 1u, kFRows = 2u, kFNonfinite = 4u, kFNotPosdef = 8u, kFNonfiniteD = 16u,
+                  kFMap = 32u, kFInternal = 64u };
+
+__device__ __forceinline__ void set_flag(unsigned long long *cnt, unsigned bit) {
+  atomicOr(cnt + kCFlags, (unsigned long long)bit);
+}
+
+// ---------------------------------------------------------------------------
+// Value placement: map_values_to_permuted + S A S (workspace.cpp:129-281,
+// factor_indef.cpp:513-559). Each permuted slot sums its caller entries in
+// input order, then takes v * (s_row * s_col). max |S A S| and the
+// finiteness of every input value are reduced on the way.
+__global__ void k_values(const double *__restrict__ vin, int64_t nnz_in, const int *__restrict__ vptr,
+                         const int *__restrict__ vsrc, const int *__restrict__ pcp_col,
+                         const int *__restrict__ pri, const int *__restrict__ perm,
+                         const double *__restrict__ scale, int64_t nnz, double *__restrict__ pv,
+                         double *__restrict__ pv_raw, unsigned long long *cnt) {
+  __shared__ double red[32];
+  double m = 0.0;
+  bool bad = false;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz_in; k += stride)
+    bad = bad || !isfinite(vin[k]);
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nnz; s += stride) {
+    double v = 0.0;
+    for (int k = vptr[s]; k < vptr[s + 1]; ++k) v = __dadd_rn(v, vin[vsrc[k]]);
+    pv_raw[s] = v;
+    if (scale) v = __dmul_rn(v, __dmul_rn(scale[perm[pri[s]]], scale[perm[pcp_col[s]]]));
+    pv[s] = v;
+    m = fmax(m, fabs(v));
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) set_flag(cnt, kFNonfinite);
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) atomicMax(cnt + kCMaxAbs, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+// eff_small of factor_indef.cpp:631-636 from max |S A S|.
+__global__ void k_eff_small(unsigned long long *cnt, double small_pivot) {
+  const double m = __longlong_as_double((long long)cnt[kCMaxAbs]);
+  const double e = (m > 0.0 && m < small_pivot) ? small_pivot * m : small_pivot;
+  cnt[kCEffSmall] = (unsigned long long)__double_as_longlong(e);
+}
+
+// ---------------------------------------------------------------------------
+// Per-level set-up (one block): realized front sizes (delays in), storage
+// offsets by exclusive scan, delay offsets of the children in the parent's
+// row list (multifrontal_serial.cpp:510-545), assembly work items.
+template <int NT>
+__global__ void k_level_setup(DevPlan P, DevFactor X, int lo, int hi, int lvl, int nb) {
+  __shared__ long long sa[NT], sr[NT], sb[NT];
+  __shared__ long long base_a, base_r, run_a, run_r, run_b;
+  unsigned long long *cnt = X.counters;
+  if (threadIdx.x == 0) {
+    base_a = (long long)cnt[kCArena];
+    base_r = (long long)cnt[kCRows];
+    run_a = run_r = run_b = 0;
+  }
+  __syncthreads();
+  for (int c0 = lo; c0 < hi; c0 += NT) {
+    const int i = c0 + threadIdx.x;
+    long long fa = 0, fr = 0, fb = 0;
+    int s = -1, f = 0;
+    if (i < hi) {
+      s = P.lvl_sn[i];
+      int nd = 0;
+      for (int t = P.child_ptr[s]; t < P.child_ptr[s + 1]; ++t) {
+        X.child_doff[t] = nd;
+        nd += X.sn_dout[P.child_idx[t]];
+      }
+      f = nd + P.sn_fsym[s];
+      X.sn_nd[s] = nd;
+      X.sn_f[s] = f;
+      X.sn_ne[s] = nd + P.sn_width[s];
+      fa = (long long)f * f + (long long)f * nb;
+      fr = f;
+      fb = (f + kAsmCols - 1) / kAsmCols;
+    }
+    sa[threadIdx.x] = fa;
+    sr[threadIdx.x] = fr;
+    sb[threadIdx.x] = fb;
+    __syncthreads();
+    for (int o = 1; o < NT; o <<= 1) {  // inclusive scan (Hillis-Steele)
+      long long xa = 0, xr = 0, xb = 0;
+      if (threadIdx.x >= (unsigned)o) {
+        xa = sa[threadIdx.x - o];
+        xr = sr[threadIdx.x - o];
+        xb = sb[threadIdx.x - o];
+      }
+      __syncthreads();
+      sa[threadIdx.x] += xa;
+      sr[threadIdx.x] += xr;
+      sb[threadIdx.x] += xb;
+      __syncthreads();
+    }
+    if (i < hi) {
+      X.sn_off[s] = base_a + run_a + sa[threadIdx.x] - fa;
+      X.sn_roff[s] = base_r + run_r + sr[threadIdx.x] - fr;
+      X.lvl_blk[i + lvl] = (int)(run_b + sb[threadIdx.x] - fb);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      run_a += sa[NT - 1];
+      run_r += sr[NT - 1];
+      run_b += sb[NT - 1];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    X.lvl_blk[hi + lvl] = (int)run_b;
+    cnt[kCArena] = (unsigned long long)(base_a + run_a);
+    cnt[kCRows] = (unsigned long long)(base_r + run_r);
+    cnt[kCAux] = (unsigned long long)run_b;
+    if (base_a + run_a > X.arena_cap) set_flag(cnt, kFArena);
+    if (base_r + run_r > X.rows_cap) set_flag(cnt, kFRows);
+  }
+}
+
+// Rows of each front (children's delayed rows in child order, then its
+// symbolic rows) and each child's contribution-block row map into it.
+__global__ void k_level_rows(DevPlan P, DevFactor X, int lo, int hi) {
+  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  const int s = P.lvl_sn[lo + blockIdx.x];
+  const int64_t roff = X.sn_roff[s];
+  const int nd = X.sn_nd[s], f = X.sn_f[s], fsym = P.sn_fsym[s];
+  int *rows = X.rows + roff;
+  for (int t = P.child_ptr[s]; t < P.child_ptr[s + 1]; ++t) {
+    const int c = P.child_idx[t];
+    const int dc = X.sn_dout[c];
+    const int pc = X.sn_p[c];
+    const int fc = X.sn_f[c];
+    const int q = fc - pc;
+    const int doff = X.child_doff[t];
+    const int *crow = X.rows + X.sn_roff[c] + pc;
+    int *cmap = X.cbmap + X.sn_roff[c] + pc;
+    const int *cpr = P.cpr_idx + P.cpr_off[t];
+    for (int u = threadIdx.x; u < q; u += blockDim.x) {
+      if (u < dc) {
+        rows[doff + u] = crow[u];
+        cmap[u] = doff + u;
+      } else {
+        cmap[u] = nd + cpr[u - dc];
+      }
+    }
+  }
+  const int *fr = P.frow_idx + P.frow_ptr[s];
+  for (int u = threadIdx.x; u < fsym; u += blockDim.x) rows[nd + u] = fr[u];
+  for (int u = threadIdx.x; u < f; u += blockDim.x) X.tags[roff + u] = 0;
+}
+
+// Assembly of one level (process_front, multifrontal_serial.cpp:720-789):
+// each work item is a block of kAsmCols columns of one front. It zeroes the
+// lower part of its columns, adds the original entries of the pivot columns,
+// then extend-adds the children's Schur blocks in child order (the
+// reference's order of additions, so every entry is the reference's sum).
+// A child's block is read in place from its own front.
+__global__ void k_level_assemble(DevPlan P, DevFactor X, int lo, int hi, int lvl) {
+  unsigned long long *cnt = X.counters;
+  if (cnt[kCFlags] & (kFArena | kFRows)) return;
+  const int *pref = X.lvl_blk + lo + lvl;  // m + 1 prefix entries
+  const int m = hi - lo;
+  const int total = pref[m];
+  __shared__ int rng[2];
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    int a = 0, b = m;  // largest i with pref[i] <= w
+    while (b - a > 1) {
+      const int mid = (a + b) >> 1;
+      if (pref[mid] <= w) a = mid;
+      else b = mid;
+    }
+    const int s = P.lvl_sn[lo + a];
+    const int f = X.sn_f[s], nd = X.sn_nd[s];
+    const int j0 = (w - pref[a]) * kAsmCols;
+    const int j1 = min(j0 + kAsmCols, f);
+    double *F = X.arena + X.sn_off[s];
+    const size_t sf = (size_t)f;
+    // 1. zero the lower part of columns [j0, j1)
+    for (int jj = j0; jj < j1; ++jj)
+      for (int i = jj + threadIdx.x; i < f; i += blockDim.x) F[jj * sf + i] = 0.0;
+    __syncthreads();
+    // 2. original entries of the pivot columns in [j0, j1)
+    const int cs = P.sn_start[s], wdt = P.sn_width[s];
+    const int ca = max(j0 - nd, 0), cb = min(j1 - nd, wdt);
+    for (int c = ca; c < cb; ++c) {
+      const int jcol = cs + c;
+      const int colpos = nd + c;
+      for (int k = P.pcp[jcol] + threadIdx.x; k < P.pcp[jcol + 1]; k += blockDim.x)
+        F[colpos * sf + nd + P.amap[k]] += X.pv[k];
+    }
+    __syncthreads();
+    // 3. children in order
+    for (int t = P.child_ptr[s]; t < P.child_ptr[s + 1]; ++t) {
+      const int c = P.child_idx[t];
+      const int pc = X.sn_p[c], fc = X.sn_f[c];
+      const int q = fc - pc;
+      if (q <= 0) continue;
+      const int *cmap = X.cbmap + X.sn_roff[c] + pc;
+      if (threadIdx.x == 0) {
+        int lo2 = 0, hi2 = q;  // first jj with cmap[jj] >= j0
+        while (lo2 < hi2) {
+          const int mid = (lo2 + hi2) >> 1;
+          if (cmap[mid] < j0) lo2 = mid + 1;
+          else hi2 = mid;
+        }
+        int lo3 = lo2, hi3 = q;  // first jj with cmap[jj] >= j1
+        while (lo3 < hi3) {
+          const int mid = (lo3 + hi3) >> 1;
+          if (cmap[mid] < j1) lo3 = mid + 1;
+          else hi3 = mid;
+        }
+        rng[0] = lo2;
+        rng[1] = lo3;
+      }
+      __syncthreads();
+      const int ja = rng[0], jb = rng[1];
+      const double *Fc = X.arena + X.sn_off[c];
+      const size_t sfc = (size_t)fc;
+      for (int jj = ja; jj < jb; ++jj) {
+        const int lj = cmap[jj];
+        const double *src = Fc + (size_t)(pc + jj) * sfc + pc;
+        double *dst = F + (size_t)lj * sf;
+        for (int ii = jj + threadIdx.x; ii < q; ii += blockDim.x) {
+          const int li = cmap[ii];
+          if (li < lj) {
+            set_flag(cnt, kFMap);
+            continue;
+          }
+          dst[li] += src[ii];
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Front factorization + store (process_front's kernel call and D handling,
+// multifrontal_serial.cpp:790-945): one block per front of the size class
+// [FMIN, FMAX]; SMEM: the front is copied into shared memory.
+template <int NT, bool SMEM>
+__device__ void factor_one_front(DevPlan &P, DevFactor &X, int s, const PivotParams &prm0,
+                                 double *smem) {
+  __shared__ FrontShared sh;
+  const int f = X.sn_f[s], ne = X.sn_ne[s], nb = prm0.nb;
+  const size_t sf = (size_t)f;
+  double *Fg = X.arena + X.sn_off[s];
+  int *rows_g = X.rows + X.sn_roff[s];
+  int8_t *tags_g = X.tags + X.sn_roff[s];
+  PivotParams prm = prm0;
+  prm.eff_small = __longlong_as_double((long long)X.counters[kCEffSmall]);
+  FrontRef v;
+  v.ld = f;
+  v.f = f;
+  v.ne = ne;
+  int *inv;
+  if (SMEM) {
+    double *F = smem;
+    double *W = F + sf * sf;
+    int *rows = (int *)(W + sf * nb);
+    int *loc = rows + f;
+    inv = loc + f;
+    int8_t *tags = (int8_t *)(inv + f);
+    for (size_t t = threadIdx.x; t < sf * sf; t += NT) F[t] = Fg[t];
+    for (int t = threadIdx.x; t < f; t += NT) {
+      rows[t] = rows_g[t];
+      loc[t] = t;
+      tags[t] = 0;
+    }
+    v.F = F;
+    v.W = W;
+    v.rows = rows;
+    v.tags = tags;
+    v.loc = loc;
+  } else {
+    v.F = Fg;
+    v.W = Fg + sf * sf;
+    v.rows = rows_g;
+    v.tags = tags_g;
+    v.loc = X.ploc + X.sn_roff[s];
+    inv = X.ploc + X.rows_cap + X.sn_roff[s];
+    for (int t = threadIdx.x; t < f; t += NT) v.loc[t] = t;
+  }
+  if (threadIdx.x == 0) sh.st = FrontStats{0, 0, 0, 0, 0.0};
+  __syncthreads();
+  const int p = ldlt_factor_front_blk<NT>(v, prm, sh);
+  // D and the stored L (multifrontal_serial.cpp:884-945)
+  const bool is_root = P.sn_parent[s] < 0;
+  int pstore = p;
+  if (is_root && p < ne) {
+    for (int c = p + threadIdx.x; c < ne; c += NT) v.tags[c] = 0;
+    if (threadIdx.x == 0) sh.st.zero += ne - p;
+    pstore = ne;
+  }
+  __syncthreads();
+  if (prm.posdef) {
+    if (p < ne && threadIdx.x == 0) set_flag(X.counters, kFNotPosdef);
+    // L = L_unit sqrt(D), upper part zero
+    for (long long t = threadIdx.x; t < (long long)pstore * f; t += NT) {
+      const int c = (int)(t / f), i = (int)(t % f);
+      double *Lc = v.F + (size_t)c * sf;
+      if (i < c) Lc[i] = 0.0;
+      else if (i > c) Lc[i] = __dmul_rn(Lc[i], sqrt(Lc[c]));
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < pstore; c += NT) {
+      double *Lc = v.F + (size_t)c * sf;
+      Lc[c] = sqrt(Lc[c]);
+    }
+  } else {
+    // D inline: d on the diagonal, a 2x2 block's off-diagonal in the upper
+    // slot (c, c + 1); zero pivots' columns zero.
+    bool bad = false;
+    for (int c = threadIdx.x; c < pstore; c += NT) {
+      const double *Lc = v.F + (size_t)c * sf;
+      const int8_t tag = v.tags[c];
+      if (tag == 1) bad = bad || !isfinite(Lc[c]);
+      else if (tag == 2) bad = bad || !isfinite(Lc[c]) || !isfinite(Lc[c + 1]) || !isfinite(Lc[sf + c + 1]);
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) set_flag(X.counters, kFNonfiniteD);
+    for (int c = threadIdx.x; c < pstore; c += NT) {
+      if (v.tags[c] == -1) {  // move d10 from (c, c-1) to the upper slot (c-1, c)
+        double *Lc = v.F + (size_t)c * sf;
+        Lc[c - 1] = v.F[(size_t)(c - 1) * sf + c];
+      }
+    }
+    __syncthreads();
+    for (long long t = threadIdx.x; t < (long long)pstore * f; t += NT) {
+      const int c = (int)(t / f), i = (int)(t % f);
+      double *Lc = v.F + (size_t)c * sf;
+      const int8_t tag = v.tags[c];
+      if (tag == 0) {
+        if (i >= c) Lc[i] = 0.0;
+        else Lc[i] = 0.0;
+      } else if (i < c) {
+        if (!(tag == -1 && i == c - 1)) Lc[i] = 0.0;
+      } else if (tag == 2 && i == c + 1) {
+        Lc[i] = 0.0;
+      }
+    }
+  }
+  __syncthreads();
+  if (SMEM) {
+    for (size_t t = threadIdx.x; t < sf * sf; t += NT) Fg[t] = v.F[t];
+    for (int t = threadIdx.x; t < f; t += NT) {
+      rows_g[t] = v.rows[t];
+      tags_g[t] = v.tags[t];
+    }
+  }
+  // The children's row maps, built in assembly order, now point at the
+  // rows' final (pivot-order) positions: the solves read them that way.
+  for (int t = threadIdx.x; t < f; t += NT) inv[v.loc[t]] = t;
+  __syncthreads();
+  for (int t = P.child_ptr[s]; t < P.child_ptr[s + 1]; ++t) {
+    const int c = P.child_idx[t];
+    const int pc = X.sn_p[c];
+    int *cmap = X.cbmap + X.sn_roff[c] + pc;
+    for (int u = threadIdx.x; u < X.sn_f[c] - pc; u += NT) cmap[u] = inv[cmap[u]];
+  }
+  if (threadIdx.x == 0) {
+    X.sn_p[s] = p;
+    X.sn_pstore[s] = pstore;
+    X.sn_dout[s] = is_root ? 0 : ne - p;
+    int *st = X.sn_stat + 4 * s;
+    st[0] = sh.st.pos;
+    st[1] = sh.st.neg;
+    st[2] = sh.st.zero;
+    st[3] = sh.st.two_by_two;
+    X.sn_flops[s] = sh.st.flops;
+  }
+}
+
+template <int NT, int FMIN, int FMAX, bool SMEM>
+__global__ void __launch_bounds__(NT) k_factor(DevPlan P, DevFactor X, int lo, int hi, PivotParams prm) {
+  extern __shared__ __align__(16) double smem[];
+  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  const int s = P.lvl_sn[lo + blockIdx.x];
+  const int f = X.sn_f[s];
+  if (f < FMIN || f > FMAX) return;
+  factor_one_front<NT, SMEM>(P, X, s, prm, smem);
+}
+
+// Totals over all fronts, in supernode order (deterministic).
+struct FactorTotals {
+  long long pos, neg, zero, two_by_two, delayed, entries;
+  int max_front, pad;
+  double flops;
+};
+
+__global__ void k_finish(DevPlan P, DevFactor X, FactorTotals *out) {
+  __shared__ long long acc[6][32];
+  __shared__ int mf[32];
+  __shared__ double fl[32];
+  long long a[6] = {0, 0, 0, 0, 0, 0};
+  int mx = 0;
+  double fsum = 0.0;
+  for (int s = threadIdx.x; s < P.nsn; s += blockDim.x) {
+    const int *st = X.sn_stat + 4 * s;
+    a[0] += st[0];
+    a[1] += st[1];
+    a[2] += st[2];
+    a[3] += st[3];
+    a[4] += X.sn_dout[s];
+    a[5] += (long long)X.sn_f[s] * X.sn_pstore[s];
+    mx = max(mx, X.sn_f[s]);
+    fsum += X.sn_flops[s];  // integer-valued: exact in any order
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    for (int q = 0; q < 6; ++q) a[q] += __shfl_xor_sync(0xffffffffu, a[q], o);
+    mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    fsum += __shfl_xor_sync(0xffffffffu, fsum, o);
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    for (int q = 0; q < 6; ++q) acc[q][w] = a[q];
+    mf[w] = mx;
+    fl[w] = fsum;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    FactorTotals t{};
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+      t.pos += acc[0][i];
+      t.neg += acc[1][i];
+      t.zero += acc[2][i];
+      t.two_by_two += acc[3][i];
+      t.delayed += acc[4][i];
+      t.entries += acc[5][i];
+      t.max_front = max(t.max_front, mf[i]);
+      t.flops += fl[i];
+    }
+    *out = t;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Solves. x (new numbering, n x nrhs) and per-front work vectors w at the
+// fronts' row offsets (rows_total x nrhs).
+__global__ void k_solve_gather(const double *__restrict__ b, int ldb, int nrhs, int n,
+                               const int *__restrict__ perm, const double *__restrict__ scale,
+                               double *__restrict__ x) {
+  const int64_t tot = (int64_t)n * nrhs;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(t / n), i = (int)(t % n);
+    const int o = perm[i];
+    double v = b[(int64_t)r * ldb + o];
+    if (scale) v = __dmul_rn(v, scale[o]);
+    x[t] = v;
+  }
+}
+
+__global__ void k_solve_scatter(double *__restrict__ b, int ldb, int nrhs, int n,
+                                const int *__restrict__ perm, const double *__restrict__ scale,
+                                const double *__restrict__ x) {
+  const int64_t tot = (int64_t)n * nrhs;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(t / n), i = (int)(t % n);
+    const int o = perm[i];
+    double v = x[t];
+    if (scale) v = __dmul_rn(v, scale[o]);
+    b[(int64_t)r * ldb + o] = v;
+  }
+}
+
+// Forward solve of one level (solve_forward.cpp:116-293 computes the same
+// L^-1 b): each front gathers its pivot rows, adds its children's update
+// vectors in child order, eliminates its pivots and leaves its update
+// vector (rows p..f) for its parent; the pivot results go to x.
+__global__ void k_forward(DevPlan P, DevFactor X, int lo, int hi, int posdef, double *x, double *wk,
+                          int64_t rows_total, int nrhs) {
+  const int s = P.lvl_sn[lo + blockIdx.x];
+  const int f = X.sn_f[s], p = X.sn_pstore[s];
+  const int64_t roff = X.sn_roff[s];
+  const int *rows = X.rows + roff;
+  const double *L = X.arena + X.sn_off[s];
+  const size_t sf = (size_t)f;
+  for (int r = 0; r < nrhs; ++r) {
+    double *w = wk + (int64_t)r * rows_total + roff;
+    const double *xr = x + (int64_t)r * P.n;
+    for (int i = threadIdx.x; i < f; i += blockDim.x) w[i] = (i < p) ? xr[rows[i]] : 0.0;
+    __syncthreads();
+    for (int t = P.child_ptr[s]; t < P.child_ptr[s + 1]; ++t) {
+      const int c = P.child_idx[t];
+      const int pc = X.sn_pstore[c], q = X.sn_f[c] - pc;
+      const int *cmap = X.cbmap + X.sn_roff[c] + pc;
+      const double *u = wk + (int64_t)r * rows_total + X.sn_roff[c] + pc;
+      for (int i = threadIdx.x; i < q; i += blockDim.x) w[cmap[i]] += u[i];
+      __syncthreads();
+    }
+    for (int j = 0; j < p; ++j) {
+      const double *Lj = L + (size_t)j * sf;
+      double wj = w[j];
+      if (posdef) wj = wj / Lj[j];
+      __syncthreads();
+      if (threadIdx.x == 0) w[j] = wj;
+      for (int i = j + 1 + threadIdx.x; i < f; i += blockDim.x) w[i] = fma(-Lj[i], wj, w[i]);
+      __syncthreads();
+    }
+    double *xw = x + (int64_t)r * P.n;
+    for (int i = threadIdx.x; i < p; i += blockDim.x) xw[rows[i]] = w[i];
+    __syncthreads();
+  }
+}
+
+// Backward solve of one level, D^-1 applied first for the indefinite factor
+// (apply_inline_d, solve_backward.cpp:135-171; scaled Cramer rule of
+// solve_2x2_scaled, pivoting.cpp:30-62), then x_piv -= L21^T x_ext and
+// L11^-T (solve_backward.cpp:186-350).
+__global__ void k_backward(DevPlan P, DevFactor X, int lo, int hi, int posdef, double *x,
+                           double *wk, int64_t rows_total, int nrhs, int apply_d, int apply_lt) {
+  const int s = P.lvl_sn[lo + blockIdx.x];
+  const int f = X.sn_f[s], p = X.sn_pstore[s];
+  const int64_t roff = X.sn_roff[s];
+  const int *rows = X.rows + roff;
+  const double *L = X.arena + X.sn_off[s];
+  const size_t sf = (size_t)f;
+  for (int r = 0; r < nrhs; ++r) {
+    double *v = wk + (int64_t)r * rows_total + roff;
+    double *xr = x + (int64_t)r * P.n;
+    for (int i = threadIdx.x; i < f; i += blockDim.x) v[i] = xr[rows[i]];
+    __syncthreads();
+    if (!posdef && apply_d && threadIdx.x == 0) {
+      for (int c = 0; c < p;) {
+        const double d00 = L[(size_t)c * sf + c];
+        if (c + 1 < p) {
+          const double d10 = L[(size_t)(c + 1) * sf + c];
+          if (d10 != 0.0) {
+            const double d11 = L[(size_t)(c + 1) * sf + c + 1];
+            const double s2 = max3_ref(fabs(d00), fabs(d10), fabs(d11));
+            double y0 = 0.0, y1 = 0.0;
+            const double r0 = v[c], r1 = v[c + 1];
+            if (isfinite(s2) && s2 != 0.0) {
+              const double a = d00 / s2, bb = d10 / s2, cc = d11 / s2;
+              const double det = __dsub_rn(__dmul_rn(a, cc), __dmul_rn(bb, bb));
+              if (isfinite(det) && det != 0.0) {
+                if (!isfinite(r0) || !isfinite(r1)) {
+                  y0 = r0;
+                  y1 = r1;
+                } else {
+                  const double rs = fmax(fabs(r0), fabs(r1));
+                  if (rs != 0.0) {
+                    const double q0 = r0 / rs, q1 = r1 / rs;
+                    const double u0 = __dsub_rn(__dmul_rn(cc, q0), __dmul_rn(bb, q1)) / det;
+                    const double u1 = __dadd_rn(__dmul_rn(-bb, q0), __dmul_rn(a, q1)) / det;
+                    const double ratio = rs / s2;
+                    y0 = __dmul_rn(u0, ratio);
+                    y1 = __dmul_rn(u1, ratio);
+                  }
+                }
+              }
+            }
+            v[c] = y0;
+            v[c + 1] = y1;
+            c += 2;
+            continue;
+          }
+        }
+        v[c] = (d00 == 0.0 || !isfinite(d00)) ? 0.0 : v[c] / d00;
+        ++c;
+      }
+    }
+    __syncthreads();
+    if (!apply_lt) {
+      for (int i = threadIdx.x; i < p; i += blockDim.x) xr[rows[i]] = v[i];
+      __syncthreads();
+      continue;
+    }
+    // x_piv -= L21^T x_ext (each pivot's dot product in row order)
+    for (int j = threadIdx.x; j < p; j += blockDim.x) {
+      const double *Lj = L + (size_t)j * sf;
+      double acc = v[j];
+      for (int i = p; i < f; ++i) acc = fma(-Lj[i], v[i], acc);
+      v[j] = acc;
+    }
+    __syncthreads();
+    for (int j = p - 1; j >= 0; --j) {
+      double vj = v[j];
+      if (posdef) vj = vj / L[(size_t)j * sf + j];
+      __syncthreads();
+      if (threadIdx.x == 0) v[j] = vj;
+      for (int i = threadIdx.x; i < j; i += blockDim.x) v[i] = fma(-L[(size_t)i * sf + j], vj, v[i]);
+      __syncthreads();
+    }
+    for (int i = threadIdx.x; i < p; i += blockDim.x) xr[rows[i]] = v[i];
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Residual r = b - A x and backward errors (refinement.cpp:39-130), on the
+// full symmetric pattern, one warp per row, compensated dot products
+// (Ogita, Rump & Oishi, "Accurate sum and dot product", SIAM J. Sci.
+// Comput. 26(6), 2005: TwoProduct via fma, TwoSum) in the new numbering.
+__device__ __forceinline__ void two_sum(double a, double b, double &s, double &e) {
+  s = a + b;
+  const double bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+
+__global__ void k_residual(DevPlan P, const double *__restrict__ vals, const double *__restrict__ x,
+                           const double *__restrict__ b, double *__restrict__ r, int n,
+                           unsigned long long *mx /* [0] |r|max [1] row |A| sum max [2] |x| max [3] |b| max [4] omega */) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  double m_r = 0.0, m_a = 0.0, m_x = 0.0, m_b = 0.0, m_o = 0.0;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+    double s = 0.0, c = 0.0, as = 0.0, ra = 0.0;
+    for (int k = P.sptr[i] + lane; k < P.sptr[i + 1]; k += 32) {
+      const double a = vals[P.sidx[k]];
+      const double xj = x[P.srow[k]];
+      const double pr = a * xj;
+      const double pe = fma(a, xj, -pr);
+      double t, e;
+      two_sum(s, pr, t, e);
+      s = t;
+      c += e + pe;
+      as = fma(fabs(a), fabs(xj), as);
+      ra += fabs(a);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double s2 = __shfl_xor_sync(0xffffffffu, s, o);
+      const double c2 = __shfl_xor_sync(0xffffffffu, c, o);
+      double t, e;
+      two_sum(s, s2, t, e);
+      s = t;
+      c += c2 + e;
+      as += __shfl_xor_sync(0xffffffffu, as, o);
+      ra += __shfl_xor_sync(0xffffffffu, ra, o);
+    }
+    if (lane == 0) {
+      const double bi = b[i];
+      double t, e;
+      two_sum(bi, -s, t, e);
+      const double res = t + (e - c);
+      r[i] = res;
+      m_r = fmax(m_r, fabs(res));
+      m_a = fmax(m_a, ra);
+      m_x = fmax(m_x, fabs(x[i]));
+      m_b = fmax(m_b, fabs(bi));
+      const double den = as + fabs(bi);
+      const double om = den > 0.0 ? fabs(res) / den : (res == 0.0 ? 0.0 : INFINITY);
+      m_o = fmax(m_o, om);
+    }
+  }
+  if (lane == 0) {
+    atomicMax(mx + 0, (unsigned long long)__double_as_longlong(m_r));
+    atomicMax(mx + 1, (unsigned long long)__double_as_longlong(m_a));
+    atomicMax(mx + 2, (unsigned long long)__double_as_longlong(m_x));
+    atomicMax(mx + 3, (unsigned long long)__double_as_longlong(m_b));
+    atomicMax(mx + 4, (unsigned long long)__double_as_longlong(m_o));
+  }
+}
+
+__global__ void k_axpy(double *__restrict__ x, const double *__restrict__ dx, int64_t len) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < len;
+       t += (int64_t)gridDim.x * blockDim.x)
+    x[t] += dx[t];
+}
+
+}  // namespace smfg

@@ -1,0 +1,306 @@
+"""Python host of the B200 numeric phase, over the C ABI of libsmfg.so
+(include/smfg.h).
+
+It mirrors smf's numeric API (solver/include/smf/solver.hpp:33-140): a
+``Solver`` is created from an analysis (the AnalysisKeep arrays of
+solver/include/smf/analysis.hpp:25-144), then ``factor`` / ``solve`` /
+``inertia`` / ``refine`` follow ``Solver::factor``, ``Solver::solve``,
+``smf_inertia`` and ``refine``. There is no CPU fallback: without the
+CUDA library or a GPU every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import build as _build
+
+SMFG_OK = 0
+SMFG_ERR_SINGULAR = 2
+SOLVE_FULL, SOLVE_FORWARD, SOLVE_DIAGONAL, SOLVE_BACKWARD = 0, 1, 2, 3
+PREC_FP64, PREC_MIXED = 0, 1
+
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_i8p = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
+
+
+class SmfgError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        self.code = code
+        detail = ""
+        try:
+            detail = lib().smfg_last_error().decode()
+        except Exception:  # noqa: BLE001
+            pass
+        super().__init__(f"{where}: {error_string(code)} ({code}){': ' + detail if detail else ''}")
+
+
+class _Analysis(C.Structure):
+    _fields_ = [("n", C.c_int), ("nsn", C.c_int)] + [
+        (nm, C.c_void_p) for nm in ("perm", "sn_start", "sn_end", "sn_parent", "child_ptr",
+                                    "child_idx", "front_row_ptr", "front_row_idx", "postorder",
+                                    "perm_col_ptr", "perm_row_idx")] + [
+        ("nnz_in", C.c_int64)] + [
+        (nm, C.c_void_p) for nm in ("orig_to_clean", "clean_to_perm", "clean_col_ptr",
+                                    "clean_row_idx")]
+
+
+class Control(C.Structure):
+    """smfg_control_t (include/smfg.h)."""
+    _fields_ = [("abi_version", C.c_int), ("posdef", C.c_int), ("u", C.c_double),
+                ("small_pivot", C.c_double), ("nb", C.c_int), ("blocked_min_front", C.c_int),
+                ("precision", C.c_int), ("max_negative_pivots", C.c_int),
+                ("scale", C.c_void_p), ("reserved_i", C.c_int * 8),
+                ("reserved_d", C.c_double * 8)]
+
+
+class Info(C.Structure):
+    """smfg_info_t (include/smfg.h)."""
+    _fields_ = [("status", C.c_int), ("factor_status", C.c_int), ("num_pos", C.c_int),
+                ("num_neg", C.c_int), ("num_zero", C.c_int), ("delayed_pivots", C.c_int),
+                ("two_by_two_pivots", C.c_int), ("max_front", C.c_int),
+                ("factor_entries", C.c_int64), ("flops", C.c_double), ("max_abs", C.c_double),
+                ("factor_ms", C.c_double), ("solve_ms", C.c_double), ("levels", C.c_int),
+                ("kernel_launches", C.c_int), ("mixed_fronts", C.c_int),
+                ("reserved_i", C.c_int * 7), ("reserved_d", C.c_double * 8)]
+
+    @property
+    def inertia(self):
+        return (self.num_pos, self.num_neg, self.num_zero)
+
+
+_lib = None
+
+
+def library_path() -> str:
+    return _build.LIB
+
+
+def lib():
+    """Load libsmfg.so (building it first when the sources are newer)."""
+    global _lib
+    if _lib is None:
+        path = _build.LIB
+        if not os.path.exists(path) or _build.needs_build():
+            _build.build()
+        L = C.CDLL(path)
+        L.smfg_abi_version.restype = C.c_int
+        L.smfg_default_control.argtypes = [C.POINTER(Control)]
+        L.smfg_plan_create.argtypes = [C.POINTER(_Analysis), C.c_int, C.POINTER(C.c_void_p)]
+        L.smfg_plan_create.restype = C.c_int
+        L.smfg_plan_destroy.argtypes = [C.POINTER(C.c_void_p)]
+        L.smfg_factor.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Control), C.POINTER(Info)]
+        L.smfg_factor.restype = C.c_int
+        L.smfg_factor_device.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Control), C.POINTER(Info)]
+        L.smfg_factor_device.restype = C.c_int
+        L.smfg_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(Info)]
+        L.smfg_solve.restype = C.c_int
+        L.smfg_solve_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                        C.POINTER(Info)]
+        L.smfg_solve_device.restype = C.c_int
+        L.smfg_inertia.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                   C.POINTER(C.c_int)]
+        L.smfg_inertia.restype = C.c_int
+        L.smfg_factor_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.smfg_factor_sizes.restype = C.c_int
+        L.smfg_factor_export.argtypes = [C.c_void_p, _i32p, _i32p, _i64p, _f64p, _i64p, _i32p,
+                                         C.c_void_p]
+        L.smfg_factor_export.restype = C.c_int
+        L.smfg_residual.argtypes = [C.c_void_p, _f64p, _f64p, C.c_int, C.c_void_p,
+                                    C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.smfg_residual.restype = C.c_int
+        L.smfg_refine.argtypes = [C.c_void_p, _f64p, _f64p, C.c_int, C.c_int, C.c_double,
+                                  C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        L.smfg_refine.restype = C.c_int
+        L.smfg_error_string.argtypes = [C.c_int]
+        L.smfg_error_string.restype = C.c_char_p
+        L.smfg_last_error.argtypes = []
+        L.smfg_last_error.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def error_string(code: int) -> str:
+    try:
+        return lib().smfg_error_string(code).decode()
+    except Exception:  # noqa: BLE001
+        return "error"
+
+
+def default_control(posdef: bool = False, u: float = 0.01, small: float = 1e-20,
+                    precision: int = PREC_FP64, max_negative_pivots: int = -1) -> Control:
+    c = Control()
+    lib().smfg_default_control(C.byref(c))
+    c.posdef = int(posdef)
+    c.u = u
+    c.small_pivot = small
+    c.precision = precision
+    c.max_negative_pivots = max_negative_pivots
+    return c
+
+
+@dataclass
+class FrontFactor:
+    """Per-front export of a factor (the FactorKeep layout)."""
+    f: np.ndarray
+    p: np.ndarray
+    blk_off: np.ndarray
+    blocks: np.ndarray
+    row_off: np.ndarray
+    rows: np.ndarray
+    tags: np.ndarray | None
+
+    def block(self, s: int) -> np.ndarray:
+        f, p = int(self.f[s]), int(self.p[s])
+        o = int(self.blk_off[s])
+        return self.blocks[o:o + f * p].reshape(p, f).T
+
+    def front_rows(self, s: int) -> np.ndarray:
+        o = int(self.row_off[s])
+        return self.rows[o:o + int(self.f[s])]
+
+
+_ANALYSIS_FIELDS = ("perm", "sn_start", "sn_end", "sn_parent", "child_ptr", "child_idx",
+                    "front_row_ptr", "front_row_idx", "postorder", "perm_col_ptr",
+                    "perm_row_idx", "orig_to_clean", "clean_to_perm", "clean_col_ptr",
+                    "clean_row_idx")
+
+
+class Solver:
+    """The numeric phase on one GPU for one analysis (smf::Solver's factor /
+    solve / inertia / refine; AnalysisKeep arrays from any object with the
+    attributes n, perm, sn_start, sn_end, sn_parent, child_ptr, child_idx,
+    front_row_ptr, front_row_idx, postorder, perm_col_ptr, perm_row_idx,
+    orig_to_clean, clean_to_perm, clean_col_ptr, clean_row_idx)."""
+
+    def __init__(self, analysis, device: int = -1):
+        L = lib()
+        self._arrays = {k: np.ascontiguousarray(getattr(analysis, k), dtype=np.int32)
+                        for k in _ANALYSIS_FIELDS}
+        self.n = int(analysis.n)
+        self.nsn = int(self._arrays["sn_start"].size)
+        self.nnz_in = int(self._arrays["orig_to_clean"].size)
+        a = self._arrays
+        ca = _Analysis(self.n, self.nsn, *[a[k].ctypes.data for k in _ANALYSIS_FIELDS[:11]],
+                       self.nnz_in, *[a[k].ctypes.data for k in _ANALYSIS_FIELDS[11:]])
+        h = C.c_void_p()
+        rc = L.smfg_plan_create(C.byref(ca), device, C.byref(h))
+        if rc != SMFG_OK:
+            raise SmfgError(rc, "smfg_plan_create")
+        self._h = h
+        self.posdef = False
+        self.info = Info()
+        self._scale = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().smfg_plan_destroy(C.byref(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+    # -- factor ------------------------------------------------------------
+    def factor(self, values, posdef: bool = False, u: float = 0.01, small: float = 1e-20,
+               scale=None, precision: int = PREC_FP64, max_negative_pivots: int = -1,
+               raise_on_singular: bool = False) -> Info:
+        """Factor new values (the caller's entry order). ``values`` is a
+        numpy array, or any object with ``data_ptr()`` (a CUDA tensor) for
+        values already in device memory."""
+        c = default_control(posdef, u, small, precision, max_negative_pivots)
+        if scale is not None and len(scale):
+            self._scale = np.ascontiguousarray(scale, dtype=np.float64)
+            c.scale = self._scale.ctypes.data
+        else:
+            self._scale = None
+        info = Info()
+        if hasattr(values, "data_ptr"):
+            rc = lib().smfg_factor_device(self._h, C.c_void_p(values.data_ptr()), C.byref(c),
+                                          C.byref(info))
+        else:
+            v = np.ascontiguousarray(values, dtype=np.float64)
+            if v.size != self.nnz_in:
+                raise ValueError(f"expected {self.nnz_in} values, got {v.size}")
+            rc = lib().smfg_factor(self._h, v.ctypes.data, C.byref(c), C.byref(info))
+        self.posdef = posdef
+        self.info = info
+        if rc not in (SMFG_OK, SMFG_ERR_SINGULAR) or (rc == SMFG_ERR_SINGULAR and raise_on_singular):
+            raise SmfgError(rc, "smfg_factor")
+        return info
+
+    # -- solve -------------------------------------------------------------
+    def solve(self, b, job: int = SOLVE_FULL):
+        """x = A^-1 b. b: (n,) or (nrhs, n) numpy array (returned as a new
+        array), or a CUDA tensor solved in place (returned)."""
+        info = Info()
+        if hasattr(b, "data_ptr"):
+            nrhs = 1 if b.dim() == 1 else int(b.shape[0])
+            rc = lib().smfg_solve_device(self._h, C.c_void_p(b.data_ptr()), nrhs, self.n, job,
+                                         C.byref(info))
+            if rc != SMFG_OK:
+                raise SmfgError(rc, "smfg_solve_device")
+            self.info.solve_ms = info.solve_ms
+            return b
+        x = np.array(b, dtype=np.float64, copy=True, order="C")
+        nrhs = 1 if x.ndim == 1 else x.shape[0]
+        rc = lib().smfg_solve(self._h, x.ctypes.data, nrhs, self.n, job, C.byref(info))
+        if rc != SMFG_OK:
+            raise SmfgError(rc, "smfg_solve")
+        self.info.solve_ms = info.solve_ms
+        self.last_solve_launches = info.kernel_launches
+        return x
+
+    def inertia(self):
+        p, n, z = C.c_int(), C.c_int(), C.c_int()
+        rc = lib().smfg_inertia(self._h, C.byref(p), C.byref(n), C.byref(z))
+        if rc != SMFG_OK:
+            raise SmfgError(rc, "smfg_inertia")
+        return (p.value, n.value, z.value)
+
+    def export(self) -> FrontFactor:
+        be, re_ = C.c_int64(), C.c_int64()
+        lib().smfg_factor_sizes(self._h, C.byref(be), C.byref(re_))
+        ns = self.nsn
+        f = np.zeros(ns, dtype=np.int32)
+        p = np.zeros(ns, dtype=np.int32)
+        bo = np.zeros(ns, dtype=np.int64)
+        ro = np.zeros(ns, dtype=np.int64)
+        blocks = np.zeros(max(1, be.value), dtype=np.float64)
+        rows = np.zeros(max(1, re_.value), dtype=np.int32)
+        tags = None if self.posdef else np.zeros(max(1, self.n), dtype=np.int8)
+        rc = lib().smfg_factor_export(self._h, f, p, bo, blocks, ro, rows,
+                                      None if tags is None else tags.ctypes.data)
+        if rc != SMFG_OK:
+            raise SmfgError(rc, "smfg_factor_export")
+        return FrontFactor(f, p, bo, blocks, ro, rows, tags)
+
+    def residual(self, b, x):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        nrhs = 1 if b.ndim == 1 else b.shape[0]
+        r = np.zeros_like(b)
+        eta, om = C.c_double(), C.c_double()
+        rc = lib().smfg_residual(self._h, b.reshape(-1), x.reshape(-1), nrhs, r.ctypes.data,
+                                 C.byref(eta), C.byref(om))
+        if rc != SMFG_OK:
+            raise SmfgError(rc, "smfg_residual")
+        return r, eta.value, om.value
+
+    def refine(self, b, x, max_steps: int = 10, omega_target: float = 1e-8):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.array(x, dtype=np.float64, copy=True, order="C")
+        nrhs = 1 if b.ndim == 1 else b.shape[0]
+        eta, om, st = C.c_double(), C.c_double(), C.c_int()
+        rc = lib().smfg_refine(self._h, b.reshape(-1), x.reshape(-1), nrhs, max_steps,
+                               omega_target, C.byref(eta), C.byref(om), C.byref(st))
+        if rc != SMFG_OK:
+            raise SmfgError(rc, "smfg_refine")
+        return x, eta.value, om.value, st.value

