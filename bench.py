@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 numeric phase of smf: factor + solve ms.
+
+Default workload (the headline metric's configuration): the SPD
+variable-coefficient 7-point operator on a 64^3 grid (n = 262,144; edge
+conductivities log-uniform in [1e-3, 1e3], seed 0), nested-dissection
+analysis, one right-hand side uniform in [-1, 1]. One step = numeric
+factorization of the values + one solve.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--config spd3d|lap2d|traj|kkt] [--precision fp64|mixed]
+
+`value` is device time (CUDA events on the engine's stream) with the
+inputs already in HBM; `e2e` is the same step through the C ABI with host
+buffers (values and right-hand side copied in, solution copied out).
+Multi-GPU: one process per GPU; the 64^3 factorization does not shard, so
+N ranks run N replicas ("replicas only") and the max over ranks is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    # name: (description, builder, posdef, nrhs)
+    "spd3d": ("SPD variable-coefficient 7-point 64^3 (n=262,144), 1 RHS", "varcoef_3d(64)", True, 1),
+    "lap2d": ("2D 5-point Laplacian 150x150 (n=22,500), 1 RHS", "laplacian_2d(150)", True, 1),
+    "traj": ("trajectory KKT T=200 (n=5,612), 8 RHS", "traj200", False, 8),
+    "kkt": ("IPM KKT 20^3 + 4,000 constraints (n=12,000), 1 RHS", "kkt_ipm(20, 4000)", False, 1),
+}
+
+
+def build_matrix(cfg: str):
+    from opt_solver_b200 import workloads as W
+    if cfg == "spd3d":
+        return W.varcoef_3d(64, seed=0)
+    if cfg == "lap2d":
+        return W.laplacian_2d(150)
+    if cfg == "traj":
+        return W.trajectory_kkt(200, np.random.default_rng(0))
+    if cfg == "kkt":
+        return W.kkt_ipm(20, 4000, seed=0)
+    raise ValueError(cfg)
+
+
+def sample_matrix(cfg: str):
+    """The bounded CPU sample of each workload (reference on the host cores)."""
+    from opt_solver_b200 import workloads as W
+    if cfg == "spd3d":
+        return W.varcoef_3d(32, seed=0), "varcoef_3d(32) (n=32,768), same generator"
+    return build_matrix(cfg), "the full workload"
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl" if _cuda_ok() else "gloo", timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def _cuda_ok():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:  # noqa: BLE001
+        return False
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda" if _cuda_ok() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:  # noqa: BLE001
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:  # noqa: BLE001
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh)
+    except Exception:  # noqa: BLE001
+        return {}
+
+
+def dgemm_peak_tflops():
+    """cuBLAS FP64 GEMM throughput on this GPU (the FP64 roofline's
+    denominator: the driver's peak file measures bf16 and copy bandwidth)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    from opt_solver_b200 import smfg
+    from opt_solver_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    desc, _, posdef, nrhs = CONFIGS[args.config]
+    n, cp, ri, v = build_matrix(args.config)
+    t0 = time.time()
+    a = smfg.analyse(n, cp, ri)
+    analyse_s = time.time() - t0
+    sv = smfg.Solver(a, device=local)
+    prec = smfg.PREC_MIXED if args.precision == "mixed" else smfg.PREC_FP64
+    b = W.rhs(n, nrhs, seed=1)
+    d_vals = torch.from_numpy(np.ascontiguousarray(v)).cuda()
+    d_b0 = torch.from_numpy(np.ascontiguousarray(b)).cuda()
+    d_b = d_b0.clone()
+
+    def step():
+        info = sv.factor(d_vals, posdef=posdef, precision=prec)
+        d_b.copy_(d_b0)
+        sv.solve(d_b)
+        return info.factor_ms + sv.info.solve_ms, info
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    dev_ms = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            ms, info = step()
+            dev_ms.append(ms)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms_step = allmax(sum(dev_ms) / len(dev_ms), world)
+    # e2e: host buffers through the C ABI (copies inside the timed region)
+    e2e = []
+    for _ in range(max(2, min(args.steps, 5))):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        sv.factor(v, posdef=posdef, precision=prec)
+        x = sv.solve(b)
+        e2e.append((time.perf_counter() - t) * 1e3)
+    e2e_ms = allmax(sum(e2e) / len(e2e), world)
+    # accuracy of the last solve
+    _, eta, om = sv.residual(b, x)
+    info = sv.info
+    out = {
+        "ms_per_step": ms_step, "info": info, "eta": eta, "omega": om, "analyse_s": analyse_s,
+        "e2e_ms": e2e_ms, "n": n, "nnz": int(cp[-1]), "nrhs": nrhs, "desc": desc,
+        "clocks": clk.summary(), "nsn": a.nsn,
+        "h2d": int(cp[-1]) * 8 + n * nrhs * 8, "d2h": n * nrhs * 8,
+    }
+    # roofline pass (untimed): per-kernel device time of the large-front
+    # GEMMs with their algorithmic flops
+    prof = sv.profile_factor(d_vals, posdef=posdef, precision=prec)
+    out["profile"] = prof
+    return out
+
+
+def cpu_reference_sample(cfg, threads):
+    """The reference smf solver (oracle/_ref, compiled from its sources) on
+    the host cores: its own analysis, fastest host mode, one bounded sample."""
+    from oracle import oracle as O
+    from opt_solver_b200 import workloads as W
+    (n, cp, ri, v), sample = sample_matrix(cfg)
+    posdef = CONFIGS[cfg][2]
+    ordering = O.ORDER_METIS if cfg == "spd3d" else O.ORDER_AUTO_PARALLEL
+    ref = O.Reference(posdef=posdef, ordering=ordering, deterministic=False, num_threads=threads,
+                      scaling=O.SCALE_AUTO, posdef_kernel=O.POSDEF_KERNEL_LAPACK)
+    a = ref.analyse(n, cp, ri, v)
+    nrhs = CONFIGS[cfg][3]
+    b = W.rhs(n, nrhs, seed=1)
+    t = time.perf_counter()
+    fx = ref.factor(v)
+    _x, _ = ref.solve(b)
+    ms = (time.perf_counter() - t) * 1e3
+    return ms, fx.flops, sample, a
+
+
+def delay_free_flops(a):
+    f = np.diff(a.front_row_ptr).astype(np.float64)
+    p = (np.asarray(a.sn_end) - np.asarray(a.sn_start)).astype(np.float64)
+    # sum over k < p of r + r (r + 1), r = f - k - 1
+    tot = 0.0
+    for fi, pi in zip(f, p):
+        r = fi - 1 - np.arange(pi)
+        tot += float(np.sum(r + r * (r + 1.0)))
+    return tot
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return None
+    from oracle import oracle as O
+    if not O.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref not built (no /root/reference at build time)"}
+    threads = os.cpu_count() or 1
+    cfg = args.config
+    times = []
+    flops_s = None
+    for i in range(args.warmup + args.steps):
+        ms, flops_s, sample, a_s = cpu_reference_sample(cfg, threads)
+        if i >= args.warmup:
+            times.append(ms)
+    scale = 1.0
+    if cfg == "spd3d":
+        # extrapolate the sample to the full workload by the reference's own
+        # delay-free flop counts of both analyses
+        n, cp, ri, v = build_matrix(cfg)
+        ref = O.Reference(posdef=True, ordering=O.ORDER_METIS, deterministic=False, num_threads=threads)
+        a_full = ref.analyse(n, cp, ri, v)
+        scale = delay_free_flops(a_full) / max(delay_free_flops(a_s), 1.0)
+    ms_step = statistics.median(times) * scale
+    desc = CONFIGS[cfg][0]
+    line = {
+        "impl": "reference", "metric": "factor+solve ms", "value": ms_step, "unit": "ms",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generators of the configuration)",
+        "config": {"workload": desc, "precision": "fp64"},
+        "cpu_baseline": {"value": ms_step, "unit": "ms", "cores": threads, "kind": "reference",
+                         "sample": f"{sample}; reference smf (oracle/_ref) non-deterministic, "
+                                   f"{threads} threads, METIS, LAPACK-style SPD fronts; "
+                                   f"time x{scale:.2f} (delay-free flops full / sample)"},
+        "e2e": {"value": ms_step, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="spd3d", choices=sorted(CONFIGS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    rank, world, local = dist_init()
+    if args.impl == "reference":
+        line = run_reference_arm(args, rank, world)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    r = run_ours(args, rank, world, local)
+    if rank != 0:
+        return
+    info = r["info"]
+    peaks = measured_peaks()
+    prof = r["profile"]
+    dpeak = dgemm_peak_tflops()
+    achieved = prof["gemm_flops"] / (prof["gemm_ms"] * 1e-3) / 1e12 if prof["gemm_ms"] > 0 else 0.0
+    roof = {
+        "kernel": "k_large_gemm + k_large_schur (FP64 FMA tile GEMMs of the large fronts)",
+        "bound": "tensor", "achieved": achieved, "peak": dpeak, "unit": "TFLOP/s",
+        "frac": achieved / dpeak if dpeak else None, "traffic": None,
+        "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (FP64 is not in MEASURED_PEAKS.json)",
+        "launches": prof["gemm_launches"], "avg_launch_ms": prof["gemm_ms"] / max(prof["gemm_launches"], 1),
+        "algorithmic_flops_per_launch": prof["gemm_flops"] / max(prof["gemm_launches"], 1),
+    }
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            from oracle import oracle as O
+            if O.ref_available():
+                threads = os.cpu_count() or 1
+                ms, _fl, sample, a_s = cpu_reference_sample(args.config, threads)
+                scale = 1.0
+                if args.config == "spd3d":
+                    n, cp, ri, v = build_matrix(args.config)
+                    ref = O.Reference(posdef=True, ordering=O.ORDER_METIS, deterministic=False,
+                                      num_threads=threads)
+                    a_full = ref.analyse(n, cp, ri, v)
+                    scale = delay_free_flops(a_full) / max(delay_free_flops(a_s), 1.0)
+                cpu = {"value": ms * scale, "unit": "ms", "cores": threads, "kind": "reference",
+                       "sample": f"{sample}; reference smf (oracle/_ref), non-deterministic, "
+                                 f"{threads} threads, METIS; x{scale:.2f} by delay-free flops"}
+        except Exception as exc:  # noqa: BLE001
+            cpu = {"value": None, "unit": "ms", "cores": 0, "kind": "reference", "sample": f"failed: {exc}"}
+    line = {
+        "metric": "factor+solve ms", "value": r["ms_per_step"], "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator of the configuration)",
+        "config": {"workload": r["desc"], "n": r["n"], "nnz_lower": r["nnz"], "nrhs": r["nrhs"],
+                   "supernodes": r["nsn"], "analysis": "engine nested dissection (smfg_analyse)",
+                   "precision": args.precision, "parallelism": "replicas" if world > 1 else "1 GPU",
+                   "l2": "inputs larger than L2 (front arena %.1f GB)" % (prof.get("arena_bytes", 0) / 1e9)},
+        "e2e": {"value": r["e2e_ms"], "unit": "ms", "h2d_bytes_per_step": r["h2d"],
+                "d2h_bytes_per_step": r["d2h"]},
+        "gpu_launches": int(info.kernel_launches),
+        "factor_ms": info.factor_ms, "solve_ms": info.solve_ms, "flops": info.flops,
+        "gflops": info.flops / (info.factor_ms * 1e-3) / 1e9 if info.factor_ms else None,
+        "inertia": list(info.inertia), "eta_inf": r["eta"], "omega": r["omega"],
+        "roofline": roof, "cpu_baseline": cpu, "clocks": r["clocks"],
+        "measured_peaks": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops")},
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

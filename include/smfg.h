@@ -176,6 +176,24 @@ SMFG_API int smfg_residual(smfg_plan_t plan, const double *b, const double *x, i
 SMFG_API int smfg_refine(smfg_plan_t plan, const double *b, double *x, int nrhs, int max_steps,
                          double omega_target, double *eta_inf, double *omega, int *steps);
 
+/* A symbolic analysis of the engine's own (host code, no GPU needed),
+ * producing the smfg_analysis_t contract above when smf's analyse
+ * (solver/src/symbolic_analysis.cpp:434, out of this library's scope) is not
+ * at hand: nested-dissection ordering, elimination tree, supernodes and
+ * relaxed amalgamation. Input: lower CSC (0-based; entries above the
+ * diagonal are mirrored, duplicates allowed). ordering: SMFG_ORDER_*. */
+#define SMFG_ORDER_ND 0
+#define SMFG_ORDER_NATURAL 1
+#define SMFG_ORDER_ND_FINE 2
+typedef struct smfg_symbolic_s *smfg_symbolic_t;
+SMFG_API int smfg_analyse(int n, const int *col_ptr, const int *row_idx, int ordering, int nemin,
+                          smfg_symbolic_t *out);
+/* Pointers into the analysis (valid until smfg_symbolic_free); flops: the
+ * delay-free factorization flops in smf's count; factor_entries: |L|. */
+SMFG_API int smfg_symbolic_view(smfg_symbolic_t s, smfg_analysis_t *a, double *flops,
+                                int64_t *factor_entries);
+SMFG_API void smfg_symbolic_free(smfg_symbolic_t *s);
+
 SMFG_API const char *smfg_error_string(int code);
 /* Message of the last CUDA or internal error on the calling thread. */
 SMFG_API const char *smfg_last_error(void);

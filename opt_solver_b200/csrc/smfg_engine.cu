@@ -103,6 +103,21 @@ static void build_plan(Plan &pl, const smfg_analysis_t &a) {
     const int s = a.postorder[i];
     lvl_sn[fill[level[s]]++] = s;
   }
+  // large fronts (multi-block path), by level, in the level's order
+  pl.lvl_large_ptr.assign(nl + 1, 0);
+  pl.lvl_large_maxw.assign(nl, 0);
+  std::vector<int> lvl_large;
+  for (int l = 0; l < nl; ++l) {
+    for (int i = pl.lvl_ptr[l]; i < pl.lvl_ptr[l + 1]; ++i) {
+      const int s = lvl_sn[i];
+      if (fsym[s] >= kLargeMin) {
+        lvl_large.push_back(s);
+        pl.lvl_large_maxw[l] = std::max(pl.lvl_large_maxw[l], width[s]);
+      }
+    }
+    pl.lvl_large_ptr[l + 1] = (int)lvl_large.size();
+    pl.max_large = std::max(pl.max_large, pl.lvl_large_ptr[l + 1] - pl.lvl_large_ptr[l]);
+  }
   pl.lvl_maxf.assign(nl, 0);
   pl.lvl_maxkids.assign(nl, 0);
   for (int s = 0; s < ns; ++s) {
@@ -219,6 +234,7 @@ static void build_plan(Plan &pl, const smfg_analysis_t &a) {
   d.cpr_off = dupload(pl, cpr_off);
   d.cpr_idx = dupload(pl, cpr_idx);
   d.lvl_sn = dupload(pl, lvl_sn);
+  d.lvl_large = dupload(pl, lvl_large);
   d.sn_level = dupload(pl, level);
   d.pcp = dupload(pl, std::vector<int>(a.perm_col_ptr, a.perm_col_ptr + n + 1));
   d.pri = dupload(pl, std::vector<int>(a.perm_row_idx, a.perm_row_idx + pl.nnz));
@@ -249,6 +265,7 @@ static void build_plan(Plan &pl, const smfg_analysis_t &a) {
   x.sn_flops = dalloc<double>(pl, ns);
   x.lvl_blk = dalloc<int>(pl, (size_t)ns + nl + 1);
   x.counters = dalloc<unsigned long long>(pl, kCCount + 8);
+  x.tpp = dalloc<TppState>(pl, std::max(1, pl.max_large));
   x.arena = nullptr;
   x.arena_cap = 0;
   x.rows = nullptr;
@@ -282,7 +299,37 @@ struct LaunchCount {
   int n = 0;
 };
 
-static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_t &c, LaunchCount &lc) {
+// Optional per-launch timing of the large-front GEMM kernels (events on the
+// engine's stream around each launch).
+struct GemmProfile {
+  bool on = false;
+  std::vector<cudaEvent_t> ev;
+  size_t used = 0;
+  void mark(cudaStream_t st) {
+    if (!on) return;
+    if (used == ev.size()) {
+      cudaEvent_t e;
+      SMFG_CUDA(cudaEventCreate(&e));
+      ev.push_back(e);
+    }
+    SMFG_CUDA(cudaEventRecord(ev[used++], st));
+  }
+  double total_ms() {
+    double t = 0.0;
+    for (size_t i = 0; i + 1 < used; i += 2) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+      t += ms;
+    }
+    return t;
+  }
+  ~GemmProfile() {
+    for (auto e : ev) cudaEventDestroy(e);
+  }
+};
+
+static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_t &c, LaunchCount &lc,
+                           GemmProfile &gp) {
   DevPlan &d = pl.d;
   DevFactor &x = pl.x;
   cudaStream_t st = pl.stream;
@@ -314,6 +361,47 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
     k_factor<256, kSmallMax + 1, kMediumMax, true><<<m, 256, smem_m, st>>>(d, x, lo, hi, prm);
     k_factor<512, kMediumMax + 1, 1 << 30, false><<<m, 512, 0, st>>>(d, x, lo, hi, prm);
     lc.n += 6;
+    const int nL = pl.lvl_large_ptr[l + 1] - pl.lvl_large_ptr[l];
+    if (nL > 0) {
+      const int *lg = d.lvl_large + pl.lvl_large_ptr[l];
+      k_large_init<<<nL, 256, 0, st>>>(d, x, lg, nL, c.posdef);
+      SMFG_CUDA(cudaMemsetAsync(x.counters + kCActive, 0, sizeof(unsigned long long), st));
+      const int ggrid = 2 * sms;
+      int it = 0;
+      if (c.posdef) {
+        // no delays, no search: one step per panel, then the closing step
+        const int steps = (pl.lvl_large_maxw[l] + c.nb - 1) / c.nb + 1;
+        for (; it < steps; ++it) {
+          k_large_panel<512><<<nL, 512, 0, st>>>(d, x, lg, prm, it);
+          gp.mark(st);
+          k_large_gemm<<<ggrid, 256, 0, st>>>(d, x, lg, nL);
+          gp.mark(st);
+        }
+        lc.n += 2 * steps;
+      } else {
+        // data-dependent: batches, then a look at the last step that
+        // still asked for an update
+        const int batch = 32;
+        for (int guard = 0; guard < 1 << 20; guard += batch) {
+          for (int b = 0; b < batch; ++b, ++it) {
+            k_large_panel<512><<<nL, 512, 0, st>>>(d, x, lg, prm, it);
+            gp.mark(st);
+            k_large_gemm<<<ggrid, 256, 0, st>>>(d, x, lg, nL);
+            gp.mark(st);
+          }
+          lc.n += 2 * batch;
+          unsigned long long act = 0;
+          SMFG_CUDA(cudaMemcpyAsync(&act, x.counters + kCActive, sizeof(act), cudaMemcpyDeviceToHost, st));
+          SMFG_CUDA(cudaStreamSynchronize(st));
+          if (act < (unsigned long long)it) break;
+        }
+      }
+      gp.mark(st);
+      k_large_schur<<<ggrid, 256, 0, st>>>(d, x, lg, nL);
+      gp.mark(st);
+      k_large_finish<512><<<nL, 512, 0, st>>>(d, x, lg, prm);
+      lc.n += 3;
+    }
   }
   SMFG_CUDA(cudaGetLastError());
 }
@@ -342,12 +430,15 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
   unsigned long long h_cnt[kCCount];
   FactorTotals tot{};
   LaunchCount lc;
+  GemmProfile gp;
+  gp.on = c.reserved_i[0] != 0;
   float ms = 0.0f;
   for (int attempt = 0; attempt < 4; ++attempt) {
     ensure_arena(pl, std::max(need_a, pl.x.arena_cap), std::max(need_r, pl.x.rows_cap));
     lc = LaunchCount{};
+    gp.used = 0;
     SMFG_CUDA(cudaEventRecord(pl.ev0, pl.stream));
-    enqueue_factor(pl, d_values, c, lc);
+    enqueue_factor(pl, d_values, c, lc, gp);
     if (!d_tot) d_tot = reinterpret_cast<FactorTotals *>(pl.x.counters + kCCount);
     static_assert(sizeof(FactorTotals) <= 8 * sizeof(unsigned long long), "totals slot");
     k_finish<<<1, 1024, 0, pl.stream>>>(pl.d, pl.x, d_tot);
@@ -380,6 +471,12 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
   inf.factor_ms = ms;
   inf.levels = pl.nlevels;
   inf.kernel_launches = lc.n;
+  // profile (ctrl.reserved_i[0]): large-front GEMM device time, launches,
+  // algorithmic flops; arena bytes in use
+  inf.reserved_d[0] = gp.on ? gp.total_ms() : 0.0;
+  std::memcpy(&inf.reserved_d[1], &h_cnt[kCGemmFlops], sizeof(double));
+  inf.reserved_d[2] = (double)h_cnt[kCArena] * 8.0;
+  inf.reserved_i[0] = (int)(gp.used / 2);
   int rc = SMFG_OK;
   pl.factor_status = SMFG_FACTOR_SUCCESS;
   if (flags & (kFArena | kFRows)) rc = SMFG_ERR_ARENA;

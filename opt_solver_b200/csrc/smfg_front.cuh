@@ -611,38 +611,43 @@ __device__ void schur_update_blk(const FrontRef &v, int p0, int p, int e) {
   __syncthreads();
 }
 
-// ldlt_factor_front (first = 0, no static pivoting). Returns the accepted
-// pivot count (uniform across the block); statistics in sh.st.
+// State of the blocked path of ldlt_factor_front between its panel steps
+// (ldlt_kernel.cpp:1010-1131): the first pass over the columns (phase 0,
+// indefinite only), the main panel loop (phase 1), done (phase 2); `post`
+// says what follows the deferred update the last step asked for. Every
+// thread of the block holds the same copy (all decisions are uniform).
+struct TppState {
+  int phase, k, live, k_paired;
+  int post, ps, pl, stalled;
+  int g_p0, g_p1, g_c0, g_e;  // the deferred update asked for
+  int pad[4];
+  FrontStats st;
+};
+
+__device__ __forceinline__ void tpp_init(TppState &S, int ne, bool posdef) {
+  S.phase = posdef ? 1 : 0;
+  S.k = 0;
+  S.live = ne;
+  S.k_paired = -1;
+  S.post = 0;
+  S.ps = S.pl = S.stalled = 0;
+  S.g_p0 = S.g_p1 = S.g_c0 = S.g_e = 0;
+  S.st = FrontStats{0, 0, 0, 0, 0.0};
+}
+
+// Runs the blocked algorithm up to its next deferred update, which it leaves
+// in S.g_* (returns true), or to its end (returns false: the Schur update of
+// the pivots [0, S.k) remains). The caller applies F[c0:f, c0:e] -=
+// L[c0:f, p0:p1] W[c0:e, :]^T between two calls.
 template <int NT>
-__device__ int ldlt_factor_front_blk(const FrontRef &v, const PivotParams &prm, FrontShared &sh,
-                                     bool do_schur = true) {
+__device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontShared &sh, TppState &S) {
   const int f = v.f, ne = v.ne;
   const size_t sf = (size_t)v.ld;
-  int k = 0;
-  if (f < prm.blocked_min_front || prm.nb <= 1) {
-    while (k < ne) {
-      select_pivot_blk<NT>(v, k, ne, prm, sh);
-      if (sh.kind == 0) break;
-      apply_pivot_blk<NT>(v, k, false, 0, f, prm, sh);
-    }
-    return k;
-  }
-  if (!prm.posdef) {
-    int live = ne, k_paired = -1;
-    while (k < live) {
-      const int ps = k;
-      const int pl = min(live, ps + prm.nb);
-      bool stalled = false;
-      while (k < pl) {
-        select_pivot_blk<NT>(v, k, pl, prm, sh);
-        if (sh.kind == 0) {
-          stalled = true;
-          break;
-        }
-        apply_pivot_blk<NT>(v, k, true, k - ps, pl, prm, sh);
-      }
-      deferred_update_blk<NT>(v, ps, k, pl, ne);
-      if (stalled && k != k_paired) {
+  for (int guard = 0; guard < 4 * (ne + 8); ++guard) {
+    if (S.post == 1) {  // after a first-pass panel (ldlt_kernel.cpp:1047-1095)
+      S.post = 0;
+      const int k = S.k, pl = S.pl;
+      if (S.stalled && k != S.k_paired) {
         if (threadIdx.x == 0) sh.np = 0;
         __syncthreads();
         const int max_pairs = min(prm.nb / 2, 64);
@@ -680,42 +685,112 @@ __device__ int ldlt_factor_front_blk(const FrontRef &v, const PivotParams &prm, 
             __syncthreads();
             sym_swap_blk<NT>(v, k + t, qq, 0);
           }
-          live = max(live, k + np);
-          k_paired = k;
+          S.live = max(S.live, k + np);
+          S.k_paired = k;
           continue;
         }
       }
-      if (stalled) {
+      if (S.stalled) {
         const int m = pl - k;
-        const int mv = min(m, live - pl);
-        for (int t = 0; t < mv; ++t) sym_swap_blk<NT>(v, k + t, live - mv + t, 0);
-        live -= m;
+        const int mv = min(m, S.live - pl);
+        for (int t = 0; t < mv; ++t) sym_swap_blk<NT>(v, k + t, S.live - mv + t, 0);
+        S.live -= m;
       }
+      continue;
     }
+    if (S.post == 2) {  // after a main-loop panel (ldlt_kernel.cpp:1113-1127)
+      S.post = 0;
+      if (S.stalled && S.k < ne) {
+        const int ss = S.k;
+        select_pivot_blk<NT>(v, S.k, ne, prm, sh);
+        if (sh.kind == 0) {
+          S.phase = 2;
+          return false;
+        }
+        apply_pivot_blk<NT>(v, S.k, true, 0, ss, prm, sh);
+        S.g_p0 = ss;
+        S.g_p1 = S.k;
+        S.g_c0 = S.k;
+        S.g_e = ne;
+        S.post = 3;
+        return true;
+      }
+      continue;
+    }
+    if (S.post == 3) {
+      S.post = 0;
+      continue;
+    }
+    if (S.phase == 0) {
+      if (S.k < S.live) {
+        S.ps = S.k;
+        S.pl = min(S.live, S.ps + prm.nb);
+        S.stalled = 0;
+        while (S.k < S.pl) {
+          select_pivot_blk<NT>(v, S.k, S.pl, prm, sh);
+          if (sh.kind == 0) {
+            S.stalled = 1;
+            break;
+          }
+          apply_pivot_blk<NT>(v, S.k, true, S.k - S.ps, S.pl, prm, sh);
+        }
+        S.g_p0 = S.ps;
+        S.g_p1 = S.k;
+        S.g_c0 = S.pl;
+        S.g_e = ne;
+        S.post = 1;
+        return true;
+      }
+      S.phase = 1;
+    }
+    if (S.phase == 1) {
+      if (S.k < ne) {
+        S.ps = S.k;
+        S.pl = min(ne, S.ps + prm.nb);
+        S.stalled = 0;
+        while (S.k < S.pl) {
+          select_pivot_blk<NT>(v, S.k, S.pl, prm, sh);
+          if (sh.kind == 0) {
+            S.stalled = 1;
+            break;
+          }
+          apply_pivot_blk<NT>(v, S.k, true, S.k - S.ps, S.pl, prm, sh);
+        }
+        S.g_p0 = S.ps;
+        S.g_p1 = S.k;
+        S.g_c0 = S.pl;
+        S.g_e = ne;
+        S.post = 2;
+        return true;
+      }
+      S.phase = 2;
+    }
+    return false;
   }
-  while (k < ne) {
-    const int ps = k;
-    const int pl = min(ne, ps + prm.nb);
-    bool stalled = false;
-    while (k < pl) {
-      select_pivot_blk<NT>(v, k, pl, prm, sh);
-      if (sh.kind == 0) {
-        stalled = true;
-        break;
-      }
-      apply_pivot_blk<NT>(v, k, true, k - ps, pl, prm, sh);
-    }
-    deferred_update_blk<NT>(v, ps, k, pl, ne);
-    if (stalled && k < ne) {
-      const int ss = k;
+  S.phase = 2;
+  return false;
+}
+
+// ldlt_factor_front (first = 0, no static pivoting). Returns the accepted
+// pivot count (uniform across the block); statistics in sh.st.
+template <int NT>
+__device__ int ldlt_factor_front_blk(const FrontRef &v, const PivotParams &prm, FrontShared &sh,
+                                     bool do_schur = true) {
+  const int f = v.f, ne = v.ne;
+  int k = 0;
+  if (f < prm.blocked_min_front || prm.nb <= 1) {
+    while (k < ne) {
       select_pivot_blk<NT>(v, k, ne, prm, sh);
       if (sh.kind == 0) break;
-      apply_pivot_blk<NT>(v, k, true, 0, ss, prm, sh);
-      deferred_update_blk<NT>(v, ss, k, k, ne);
+      apply_pivot_blk<NT>(v, k, false, 0, f, prm, sh);
     }
+    return k;
   }
-  if (do_schur) schur_update_blk<NT>(v, 0, k, ne);
-  return k;
+  TppState S;
+  tpp_init(S, ne, prm.posdef != 0);
+  while (tpp_step_blk<NT>(v, prm, sh, S)) deferred_update_blk<NT>(v, S.g_p0, S.g_p1, S.g_c0, S.g_e);
+  if (do_schur) schur_update_blk<NT>(v, 0, S.k, ne);
+  return S.k;
 }
 
 }  // namespace smfg

@@ -35,6 +35,7 @@ struct DevPlan {
   int *srow = nullptr, *sptr = nullptr;        // full symmetric CSR (residual), new numbering
   int64_t *sidx = nullptr;                     // its entry -> permuted slot
   int *sn_level = nullptr;
+  int *lvl_large = nullptr;                    // large fronts by level
 };
 
 // Device state of one factorization (sized per plan, grown on demand).
@@ -57,6 +58,7 @@ struct DevFactor {
   int *ploc = nullptr;        // 2 x rows_cap: pivot-order tracking of global-memory fronts
   int64_t rows_cap = 0;
   unsigned long long *counters = nullptr;  // [0] arena base, [1] rows base, [2] error flags, [3] max|A| bits, [4] blocks
+  TppState *tpp = nullptr;    // per large front of a level: blocked-pivoting state
   double *work = nullptr;     // solve / refinement scratch
   int64_t work_cap = 0;
 };
@@ -68,6 +70,9 @@ struct Plan {
   std::vector<int> lvl_ptr;      // host copy: level l = lvl_sn[lvl_ptr[l] .. lvl_ptr[l+1])
   std::vector<int> lvl_maxf;     // symbolic max front per level
   std::vector<int> lvl_maxkids;
+  std::vector<int> lvl_large_ptr;  // level l's large fronts: d.lvl_large[lvl_large_ptr[l] ..]
+  std::vector<int> lvl_large_maxw; // widest large front per level
+  int max_large = 0;
   int64_t sum_f2 = 0, sum_f = 0; // symbolic
   int max_fsym = 0;
   int64_t max_factor = 0;

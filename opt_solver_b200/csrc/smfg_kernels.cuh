@@ -7,7 +7,8 @@
 namespace smfg {
 
 // counters[] slots
-enum : int { kCArena = 0, kCRows = 1, kCFlags = 2, kCMaxAbs = 3, kCAux = 4, kCEffSmall = 5, kCCount = 8 };
+enum : int { kCArena = 0, kCRows = 1, kCFlags = 2, kCMaxAbs = 3, kCAux = 4, kCEffSmall = 5,
+             kCActive = 6, kCGemmFlops = 7, kCCount = 8 };
 // error flag bits (counters[kCFlags])
 enum : unsigned { kFArena = 1u, kFRows = 2u, kFNonfinite = 4u, kFNotPosdef = 8u, kFNonfiniteD = 16u,
                   kFMap = 32u, kFInternal = 64u };
@@ -250,6 +251,14 @@ __global__ void k_level_assemble(DevPlan P, DevFactor X, int lo, int hi, int lvl
 }
 
 // ---------------------------------------------------------------------------
+template <int NT, bool SMEM>
+__device__ void store_front(DevPlan &P, DevFactor &X, int s, const FrontRef &v, int p,
+                            const PivotParams &prm, FrontShared &sh, int *inv, double *Fg,
+                            int *rows_g, int8_t *tags_g);
+
+// Fronts of at least this many symbolic rows take the multi-block path.
+constexpr int kLargeMin = 384;
+
 // Front factorization + store (process_front's kernel call and D handling,
 // multifrontal_serial.cpp:790-945): one block per front of the size class
 // [FMIN, FMAX]; SMEM: the front is copied into shared memory.
@@ -299,7 +308,17 @@ __device__ void factor_one_front(DevPlan &P, DevFactor &X, int s, const PivotPar
   if (threadIdx.x == 0) sh.st = FrontStats{0, 0, 0, 0, 0.0};
   __syncthreads();
   const int p = ldlt_factor_front_blk<NT>(v, prm, sh);
-  // D and the stored L (multifrontal_serial.cpp:884-945)
+  store_front<NT, SMEM>(P, X, s, v, p, prm, sh, inv, Fg, rows_g, tags_g);
+}
+
+// D and the stored L of a factored front, its counts, and its children's
+// row maps in pivot order (multifrontal_serial.cpp:884-945).
+template <int NT, bool SMEM>
+__device__ void store_front(DevPlan &P, DevFactor &X, int s, const FrontRef &v, int p,
+                            const PivotParams &prm, FrontShared &sh, int *inv, double *Fg,
+                            int *rows_g, int8_t *tags_g) {
+  const int f = v.f, ne = v.ne;
+  const size_t sf = (size_t)f;
   const bool is_root = P.sn_parent[s] < 0;
   int pstore = p;
   if (is_root && p < ne) {
@@ -391,8 +410,298 @@ __global__ void __launch_bounds__(NT) k_factor(DevPlan P, DevFactor X, int lo, i
   if (X.counters[kCFlags] & (kFArena | kFRows)) return;
   const int s = P.lvl_sn[lo + blockIdx.x];
   const int f = X.sn_f[s];
-  if (f < FMIN || f > FMAX) return;
+  if (f < FMIN || f > FMAX || P.sn_fsym[s] >= kLargeMin) return;
   factor_one_front<NT, SMEM>(P, X, s, prm, smem);
+}
+
+// ---------------------------------------------------------------------------
+// Large fronts: one block per front steps the blocked pivoting (tpp_step_blk)
+// while all blocks of the GPU run its deferred updates and, at the end, its
+// Schur update, as tiled GEMMs whose every entry takes the same fused
+// multiply-adds in the same pivot order as the block kernel.
+
+__device__ __forceinline__ FrontRef large_view(DevPlan &P, DevFactor &X, int s) {
+  FrontRef v;
+  const int f = X.sn_f[s];
+  v.F = X.arena + X.sn_off[s];
+  v.ld = f;
+  v.f = f;
+  v.ne = X.sn_ne[s];
+  v.rows = X.rows + X.sn_roff[s];
+  v.tags = X.tags + X.sn_roff[s];
+  v.W = v.F + (size_t)f * f;
+  v.loc = X.ploc + X.sn_roff[s];
+  return v;
+}
+
+__global__ void k_large_init(DevPlan P, DevFactor X, const int *__restrict__ large, int nlarge,
+                             int posdef) {
+  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  const int s = large[blockIdx.x];
+  const int f = X.sn_f[s];
+  int *loc = X.ploc + X.sn_roff[s];
+  for (int t = threadIdx.x; t < f; t += blockDim.x) loc[t] = t;
+  if (threadIdx.x == 0) {
+    TppState S;
+    tpp_init(S, X.sn_ne[s], posdef != 0);
+    S.pad[0] = 0;  // deferred update pending
+    X.tpp[blockIdx.x] = S;
+  }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_large_panel(DevPlan P, DevFactor X, const int *__restrict__ large,
+                                                    PivotParams prm, int iter) {
+  __shared__ FrontShared sh;
+  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  const int s = large[blockIdx.x];
+  TppState S = X.tpp[blockIdx.x];
+  if (S.phase == 2) {
+    if (threadIdx.x == 0) X.tpp[blockIdx.x].pad[0] = 0;
+    return;
+  }
+  prm.eff_small = __longlong_as_double((long long)X.counters[kCEffSmall]);
+  const FrontRef v = large_view(P, X, s);
+  if (threadIdx.x == 0) sh.st = S.st;
+  __syncthreads();
+  const bool more = tpp_step_blk<NT>(v, prm, sh, S);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    S.st = sh.st;
+    S.pad[0] = more ? 1 : 0;
+    X.tpp[blockIdx.x] = S;
+    if (more) {
+      atomicMax(X.counters + kCActive, (unsigned long long)(iter + 1));
+      // algorithmic flops of the deferred update asked for (2 per FMA)
+      const long long m = S.g_e - S.g_c0, h = v.f - S.g_c0;
+      if (m > 0 && S.g_p1 > S.g_p0)
+        atomicAdd(reinterpret_cast<double *>(X.counters + kCGemmFlops),
+                  2.0 * (double)(S.g_p1 - S.g_p0) * (double)(m * h - m * (m - 1) / 2));
+    }
+  }
+}
+
+// Work items of a level's tiled GEMMs: each large front contributes tiles of
+// kGT x kGT over a lower-trapezoidal region [r0, f) x [r0, c1) with tile
+// (ti, tj) needed when ti >= tj.
+constexpr int kGT = 64;
+
+__device__ __forceinline__ int trap_tiles(int rows, int cols) {  // rows >= cols
+  const int rt = (rows + kGT - 1) / kGT, ct = (cols + kGT - 1) / kGT;
+  return ct * rt - ct * (ct - 1) / 2;
+}
+
+__device__ __forceinline__ void trap_tile(int w, int rows, int cols, int &ti, int &tj) {
+  const int rt = (rows + kGT - 1) / kGT;
+  tj = 0;
+  while (w >= rt - tj) {
+    w -= rt - tj;
+    ++tj;
+  }
+  ti = tj + w;
+}
+
+// Deferred updates of all large fronts with one pending (ldlt_kernel.cpp:705-761).
+__global__ void __launch_bounds__(256) k_large_gemm(DevPlan P, DevFactor X, const int *__restrict__ large,
+                                                    int nlarge) {
+  __shared__ double As[16][kGT], Bs[16][kGT];
+  __shared__ int pref[257];
+  __shared__ int base_front;
+  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  for (int chunk = 0; chunk < nlarge; chunk += 256) {
+    const int cnt = min(256, nlarge - chunk);
+    if (threadIdx.x == 0) {
+      pref[0] = 0;
+      for (int q = 0; q < cnt; ++q) {
+        const TppState &S = X.tpp[chunk + q];
+        int nt = 0;
+        if (S.pad[0] && S.g_p1 > S.g_p0 && S.g_e > S.g_c0) {
+          const int s = large[chunk + q];
+          nt = trap_tiles(X.sn_f[s] - S.g_c0, S.g_e - S.g_c0);
+        }
+        pref[q + 1] = pref[q] + nt;
+      }
+      base_front = chunk;
+    }
+    __syncthreads();
+    const int total = pref[cnt];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    for (int w = blockIdx.x; w < total; w += gridDim.x) {
+      int a = 0, b = cnt;
+      while (b - a > 1) {
+        const int mid = (a + b) >> 1;
+        if (pref[mid] <= w) a = mid;
+        else b = mid;
+      }
+      const int q = base_front + a;
+      const int s = large[q];
+      const TppState S = X.tpp[q];
+      const int f = X.sn_f[s];
+      const size_t sf = (size_t)f;
+      double *F = X.arena + X.sn_off[s];
+      const double *W = F + sf * sf;
+      const int c0 = S.g_c0, e = S.g_e, p0 = S.g_p0, jb = S.g_p1 - S.g_p0;
+      int ti, tj;
+      trap_tile(w - pref[a], f - c0, e - c0, ti, tj);
+      const int i0 = c0 + ti * kGT, j0 = c0 + tj * kGT;
+      for (int t = threadIdx.x; t < 16 * kGT; t += 256) {
+        const int p = t / kGT, r = t % kGT;
+        double av = 0.0, bv = 0.0;
+        if (p < jb) {
+          if (i0 + r < f) av = F[(size_t)(p0 + p) * sf + i0 + r];
+          if (j0 + r < e) bv = W[(size_t)p * f + j0 + r];
+        }
+        As[p][r] = av;
+        Bs[p][r] = bv;
+      }
+      __syncthreads();
+      double c[4][4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int q2 = 0; q2 < 4; ++q2) {
+          const int i = i0 + tx + 16 * r, j = j0 + ty + 16 * q2;
+          c[r][q2] = (i < f && j < e && i >= j) ? F[(size_t)j * sf + i] : 0.0;
+        }
+      for (int p = 0; p < jb; ++p) {
+        double av[4], bv[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) av[r] = As[p][tx + 16 * r];
+#pragma unroll
+        for (int q2 = 0; q2 < 4; ++q2) bv[q2] = Bs[p][ty + 16 * q2];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int q2 = 0; q2 < 4; ++q2)
+            if (bv[q2] != 0.0) c[r][q2] = fma(-av[r], bv[q2], c[r][q2]);
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int q2 = 0; q2 < 4; ++q2) {
+          const int i = i0 + tx + 16 * r, j = j0 + ty + 16 * q2;
+          if (i < f && j < e && i >= j) F[(size_t)j * sf + i] = c[r][q2];
+        }
+      __syncthreads();
+    }
+    __syncthreads();
+  }
+}
+
+// (L D)(j, c) of a front in global memory (fill_ld_column).
+__device__ __forceinline__ double ld_entry_g(const double *F, size_t sf, const int8_t *tags, int c, int j) {
+  const double *Lc = F + (size_t)c * sf;
+  const int8_t tag = tags[c];
+  if (tag == 1) return __dmul_rn(Lc[j], Lc[c]);
+  if (tag == 2) return __dadd_rn(__dmul_rn(Lc[j], Lc[c]), __dmul_rn(Lc[sf + j], Lc[c + 1]));
+  if (tag == -1) {
+    const double *L0 = Lc - sf;
+    return __dadd_rn(__dmul_rn(L0[j], L0[c]), __dmul_rn(Lc[j], Lc[c]));
+  }
+  return 0.0;
+}
+
+// Schur updates of all large fronts of a level (schur_update,
+// ldlt_kernel.cpp:820-933): F[e:f, e:f] -= L LD^T over pivots [0, k).
+__global__ void __launch_bounds__(256) k_large_schur(DevPlan P, DevFactor X, const int *__restrict__ large,
+                                                     int nlarge) {
+  __shared__ double As[16][kGT], Bs[16][kGT];
+  __shared__ int pref[257];
+  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  for (int chunk = 0; chunk < nlarge; chunk += 256) {
+    const int cnt = min(256, nlarge - chunk);
+    if (threadIdx.x == 0) {
+      pref[0] = 0;
+      for (int q = 0; q < cnt; ++q) {
+        const int s = large[chunk + q];
+        const int e = X.sn_ne[s], f = X.sn_f[s], k = X.tpp[chunk + q].k;
+        pref[q + 1] = pref[q] + ((f > e && k > 0) ? trap_tiles(f - e, f - e) : 0);
+      }
+    }
+    __syncthreads();
+    const int total = pref[cnt];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    for (int w = blockIdx.x; w < total; w += gridDim.x) {
+      int a = 0, b = cnt;
+      while (b - a > 1) {
+        const int mid = (a + b) >> 1;
+        if (pref[mid] <= w) a = mid;
+        else b = mid;
+      }
+      const int q = chunk + a;
+      const int s = large[q];
+      const int f = X.sn_f[s], e = X.sn_ne[s], kk = X.tpp[q].k;
+      const size_t sf = (size_t)f;
+      double *F = X.arena + X.sn_off[s];
+      const int8_t *tags = X.tags + X.sn_roff[s];
+      int ti, tj;
+      trap_tile(w - pref[a], f - e, f - e, ti, tj);
+      const int i0 = e + ti * kGT, j0 = e + tj * kGT;
+      double c[4][4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int q2 = 0; q2 < 4; ++q2) {
+          const int i = i0 + tx + 16 * r, j = j0 + ty + 16 * q2;
+          c[r][q2] = (i < f && j < f && i >= j) ? F[(size_t)j * sf + i] : 0.0;
+        }
+      for (int k0 = 0; k0 < kk; k0 += 16) {
+        const int kc = min(16, kk - k0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < 16 * kGT; t += 256) {
+          const int p = t / kGT, r = t % kGT;
+          double av = 0.0, bv = 0.0;
+          if (p < kc) {
+            if (i0 + r < f) av = F[(size_t)(k0 + p) * sf + i0 + r];
+            if (j0 + r < f) bv = ld_entry_g(F, sf, tags, k0 + p, j0 + r);
+          }
+          As[p][r] = av;
+          Bs[p][r] = bv;
+        }
+        __syncthreads();
+        for (int p = 0; p < kc; ++p) {
+          double av[4], bv[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) av[r] = As[p][tx + 16 * r];
+#pragma unroll
+          for (int q2 = 0; q2 < 4; ++q2) bv[q2] = Bs[p][ty + 16 * q2];
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int q2 = 0; q2 < 4; ++q2)
+              if (bv[q2] != 0.0) c[r][q2] = fma(-av[r], bv[q2], c[r][q2]);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int q2 = 0; q2 < 4; ++q2) {
+          const int i = i0 + tx + 16 * r, j = j0 + ty + 16 * q2;
+          if (i < f && j < f && i >= j) F[(size_t)j * sf + i] = c[r][q2];
+        }
+      __syncthreads();
+    }
+    __syncthreads();
+  }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_large_finish(DevPlan P, DevFactor X, const int *__restrict__ large,
+                                                     PivotParams prm) {
+  __shared__ FrontShared sh;
+  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  const int s = large[blockIdx.x];
+  const TppState S = X.tpp[blockIdx.x];
+  const FrontRef v = large_view(P, X, s);
+  if (threadIdx.x == 0) {
+    sh.st = S.st;
+    const double q = (double)(v.f - v.ne);
+    if (q > 0 && S.k > 0)
+      atomicAdd(reinterpret_cast<double *>(X.counters + kCGemmFlops), 2.0 * S.k * (q * (q + 1) / 2));
+  }
+  __syncthreads();
+  int *inv = X.ploc + X.rows_cap + X.sn_roff[s];
+  store_front<NT, false>(P, X, s, v, S.k, prm, sh, inv, v.F, v.rows, v.tags);
 }
 
 // Totals over all fronts, in supernode order (deterministic).

@@ -121,6 +121,12 @@ def lib():
         L.smfg_error_string.restype = C.c_char_p
         L.smfg_last_error.argtypes = []
         L.smfg_last_error.restype = C.c_char_p
+        L.smfg_analyse.argtypes = [C.c_int, _i32p, _i32p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+        L.smfg_analyse.restype = C.c_int
+        L.smfg_symbolic_view.argtypes = [C.c_void_p, C.POINTER(_Analysis), C.POINTER(C.c_double),
+                                         C.POINTER(C.c_int64)]
+        L.smfg_symbolic_view.restype = C.c_int
+        L.smfg_symbolic_free.argtypes = [C.POINTER(C.c_void_p)]
         _lib = L
     return _lib
 
@@ -169,6 +175,66 @@ _ANALYSIS_FIELDS = ("perm", "sn_start", "sn_end", "sn_parent", "child_ptr", "chi
                     "front_row_ptr", "front_row_idx", "postorder", "perm_col_ptr",
                     "perm_row_idx", "orig_to_clean", "clean_to_perm", "clean_col_ptr",
                     "clean_row_idx")
+
+ORDER_ND, ORDER_NATURAL, ORDER_ND_FINE = 0, 1, 2
+
+
+class Analysis:
+    """AnalysisKeep arrays (numpy int32) with smf's conventions; from
+    ``analyse`` below or from smf's own analyse."""
+
+    def __init__(self, n, arrays, flops=0.0, factor_entries=0):
+        self.n = int(n)
+        for k, v in arrays.items():
+            setattr(self, k, v)
+        self.flops = flops
+        self.factor_entries = factor_entries
+
+    @property
+    def nsn(self) -> int:
+        return int(self.sn_start.size)
+
+
+def analyse(n, col_ptr, row_idx, ordering: int = ORDER_ND, nemin: int = 8) -> Analysis:
+    """Symbolic analysis of a lower CSC pattern (smfg_analyse: the engine's
+    own nested-dissection analysis, host code)."""
+    L = lib()
+    cp = np.ascontiguousarray(col_ptr, dtype=np.int32)
+    ri = np.ascontiguousarray(row_idx, dtype=np.int32)
+    h = C.c_void_p()
+    rc = L.smfg_analyse(int(n), cp, ri, ordering, nemin, C.byref(h))
+    if rc != SMFG_OK:
+        raise SmfgError(rc, "smfg_analyse")
+    try:
+        ca = _Analysis()
+        fl = C.c_double()
+        fe = C.c_int64()
+        L.smfg_symbolic_view(h, C.byref(ca), C.byref(fl), C.byref(fe))
+        nsn = ca.nsn
+        nslots = None
+        sizes = {
+            "perm": n, "sn_start": nsn, "sn_end": nsn, "sn_parent": nsn, "child_ptr": nsn + 1,
+            "front_row_ptr": nsn + 1, "postorder": nsn, "perm_col_ptr": n + 1,
+            "clean_col_ptr": n + 1, "orig_to_clean": ca.nnz_in,
+        }
+        arrays = {}
+
+        def grab(name, count):
+            ptr = getattr(ca, name)
+            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_int32)), shape=(count,)).copy()
+
+        for k, cnt in sizes.items():
+            arrays[k] = grab(k, cnt)
+        nslots = int(arrays["child_ptr"][-1])
+        arrays["child_idx"] = grab("child_idx", max(nslots, 0)) if nslots else np.zeros(0, np.int32)
+        arrays["front_row_idx"] = grab("front_row_idx", int(arrays["front_row_ptr"][-1]))
+        cnnz = int(arrays["clean_col_ptr"][-1])
+        arrays["perm_row_idx"] = grab("perm_row_idx", int(arrays["perm_col_ptr"][-1]))
+        arrays["clean_row_idx"] = grab("clean_row_idx", cnnz)
+        arrays["clean_to_perm"] = grab("clean_to_perm", cnnz)
+        return Analysis(n, arrays, fl.value, fe.value)
+    finally:
+        L.smfg_symbolic_free(C.byref(h))
 
 
 class Solver:
@@ -235,6 +301,30 @@ class Solver:
         if rc not in (SMFG_OK, SMFG_ERR_SINGULAR) or (rc == SMFG_ERR_SINGULAR and raise_on_singular):
             raise SmfgError(rc, "smfg_factor")
         return info
+
+    def profile_factor(self, values, posdef: bool = False, precision: int = PREC_FP64,
+                       scale=None) -> dict:
+        """One factorization with CUDA events around every launch of the
+        large-front GEMM kernels: their total device time, launch count and
+        algorithmic flops (2 per fused multiply-add of the updates)."""
+        c = default_control(posdef, 0.01, 1e-20, precision)
+        c.reserved_i[0] = 1
+        if scale is not None and len(scale):
+            self._scale = np.ascontiguousarray(scale, dtype=np.float64)
+            c.scale = self._scale.ctypes.data
+        info = Info()
+        if hasattr(values, "data_ptr"):
+            rc = lib().smfg_factor_device(self._h, C.c_void_p(values.data_ptr()), C.byref(c),
+                                          C.byref(info))
+        else:
+            v = np.ascontiguousarray(values, dtype=np.float64)
+            rc = lib().smfg_factor(self._h, v.ctypes.data, C.byref(c), C.byref(info))
+        if rc not in (SMFG_OK, SMFG_ERR_SINGULAR):
+            raise SmfgError(rc, "smfg_factor")
+        self.info = info
+        return {"gemm_ms": info.reserved_d[0], "gemm_flops": info.reserved_d[1],
+                "gemm_launches": info.reserved_i[0], "arena_bytes": info.reserved_d[2],
+                "factor_ms": info.factor_ms}
 
     # -- solve -------------------------------------------------------------
     def solve(self, b, job: int = SOLVE_FULL):

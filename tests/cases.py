@@ -35,6 +35,14 @@ def cases(size: str = "small"):
          (16 * 40 + 12, 12 * 40, 0)),
         ("kkt_6_100", lambda: W.kkt_ipm(6, 100, seed=3), False, "auto", "auto", (216, 100, 0)),
     ]
+    if size in ("full", "large"):
+        out += [
+            # fronts above 384 rows: the multi-block large-front path
+            ("var3d_24", lambda: W.varcoef_3d(24, seed=4), True, "metis", "none", (24 ** 3, 0, 0)),
+            # large indefinite fronts with delays (reference in its one-thread
+            # threshold mode: no APTP tiles, see reference_for)
+            ("kkt_10_700", lambda: W.kkt_ipm(10, 700, seed=6), False, "auto1t", "auto", (1000, 700, 0)),
+        ]
     if size == "full":
         out += [
             ("lap2d_150", lambda: W.laplacian_2d(150), True, "amd", "none", (22500, 0, 0)),
@@ -47,6 +55,14 @@ def cases(size: str = "small"):
 
 
 def reference_for(O, posdef, ordering, scaling, deterministic=True):
+    """The reference configured as the parity oracle: deterministic mode, one
+    thread. Ordering "auto1t": AutoParallel in the one-thread default mode
+    instead, whose indefinite fronts of >= 512 rows keep the threshold
+    pivoting kernel (deterministic mode tiles them with its APTP kernel,
+    which this engine does not restate)."""
+    if ordering == "auto1t":
+        ordering, deterministic = "auto", False
     order = {"amd": O.ORDER_AMD, "metis": O.ORDER_METIS, "auto": O.ORDER_AUTO_PARALLEL}[ordering]
     scal = {"none": O.SCALE_NONE, "auto": O.SCALE_AUTO}[scaling]
-    return O.Reference(posdef=posdef, ordering=order, scaling=scal, deterministic=deterministic)
+    return O.Reference(posdef=posdef, ordering=order, scaling=scal, deterministic=deterministic,
+                       num_threads=1, top_tiles=deterministic)
