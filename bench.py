@@ -311,6 +311,27 @@ def run_reference_arm(args, rank, world):
     return line
 
 
+def ncu_step(args):
+    """One factorization and one solve of the workload, nothing else: the
+    command the committed ncu launch lists are taken from."""
+    import torch
+    from opt_solver_b200 import smfg
+    from opt_solver_b200 import workloads as W
+    _desc, _, posdef, nrhs = CONFIGS[args.config]
+    n, cp, ri, v = build_matrix(args.config)
+    a = smfg.analyse(n, cp, ri)
+    sv = smfg.Solver(a, device=0)
+    prec = smfg.PREC_MIXED if args.precision == "mixed" else smfg.PREC_FP64
+    d_vals = torch.from_numpy(np.ascontiguousarray(v)).cuda()
+    d_b = torch.from_numpy(np.ascontiguousarray(W.rhs(n, nrhs, seed=1))).cuda()
+    info = sv.factor(d_vals, posdef=posdef, precision=prec)
+    fl = info.kernel_launches
+    sv.solve(d_b)
+    torch.cuda.synchronize()
+    print(json.dumps({"factor_launches": fl, "solve_launches": sv.info.kernel_launches,
+                      "factor_ms": info.factor_ms, "solve_ms": sv.info.solve_ms}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -320,7 +341,12 @@ def main():
     ap.add_argument("--config", default="spd3d", choices=sorted(CONFIGS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ncu-step", action="store_true",
+                    help="one factorization + solve and exit (for an ncu launch list)")
     args = ap.parse_args()
+    if args.ncu_step:
+        ncu_step(args)
+        return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank, world, local = dist_init()
     if args.impl == "reference":

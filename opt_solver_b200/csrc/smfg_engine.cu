@@ -106,6 +106,7 @@ static void build_plan(Plan &pl, const smfg_analysis_t &a) {
   // large fronts (multi-block path), by level, in the level's order
   pl.lvl_large_ptr.assign(nl + 1, 0);
   pl.lvl_large_maxw.assign(nl, 0);
+  pl.lvl_large_maxf.assign(nl, 0);
   std::vector<int> lvl_large;
   for (int l = 0; l < nl; ++l) {
     for (int i = pl.lvl_ptr[l]; i < pl.lvl_ptr[l + 1]; ++i) {
@@ -113,6 +114,7 @@ static void build_plan(Plan &pl, const smfg_analysis_t &a) {
       if (fsym[s] >= kLargeMin) {
         lvl_large.push_back(s);
         pl.lvl_large_maxw[l] = std::max(pl.lvl_large_maxw[l], width[s]);
+        pl.lvl_large_maxf[l] = std::max(pl.lvl_large_maxf[l], fsym[s]);
       }
     }
     pl.lvl_large_ptr[l + 1] = (int)lvl_large.size();
@@ -265,7 +267,7 @@ static void build_plan(Plan &pl, const smfg_analysis_t &a) {
   x.sn_flops = dalloc<double>(pl, ns);
   x.lvl_blk = dalloc<int>(pl, (size_t)ns + nl + 1);
   x.counters = dalloc<unsigned long long>(pl, kCCount + 8);
-  x.tpp = dalloc<TppState>(pl, std::max(1, pl.max_large));
+  x.tpp = dalloc<TppState>(pl, 2 * (size_t)std::max(1, pl.max_large));  // two buffers (SPD panels)
   x.arena = nullptr;
   x.arena_cap = 0;
   x.rows = nullptr;
@@ -368,13 +370,28 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
       SMFG_CUDA(cudaMemsetAsync(x.counters + kCActive, 0, sizeof(unsigned long long), st));
       const int ggrid = 2 * sms;
       int it = 0;
-      if (c.posdef) {
-        // no delays, no search: one step per panel, then the closing step
+      TppState *fin = x.tpp;  // where the final state of the level's fronts ends up
+      if (c.posdef && c.nb == 16) {
+        // no delays, no search: one multi-block step per panel, states
+        // double-buffered; the closing step leaves phase 2
+        const int steps = (pl.lvl_large_maxw[l] + c.nb - 1) / c.nb + 1;
+        const dim3 pgrid((pl.lvl_large_maxf[l] + 255) / 256, nL);
+        for (; it < steps; ++it) {
+          TppState *cur = x.tpp + (size_t)(it & 1) * pl.max_large;
+          TppState *nxt = x.tpp + (size_t)((it + 1) & 1) * pl.max_large;
+          k_large_panel_spd<16><<<pgrid, 256, 0, st>>>(d, x, lg, cur, nxt, it);
+          gp.mark(st);
+          k_large_gemm<<<ggrid, 256, 0, st>>>(d, x, lg, nL, nxt);
+          gp.mark(st);
+        }
+        fin = x.tpp + (size_t)(steps & 1) * pl.max_large;
+        lc.n += 2 * steps;
+      } else if (c.posdef) {
         const int steps = (pl.lvl_large_maxw[l] + c.nb - 1) / c.nb + 1;
         for (; it < steps; ++it) {
           k_large_panel<512><<<nL, 512, 0, st>>>(d, x, lg, prm, it);
           gp.mark(st);
-          k_large_gemm<<<ggrid, 256, 0, st>>>(d, x, lg, nL);
+          k_large_gemm<<<ggrid, 256, 0, st>>>(d, x, lg, nL, x.tpp);
           gp.mark(st);
         }
         lc.n += 2 * steps;
@@ -386,7 +403,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
           for (int b = 0; b < batch; ++b, ++it) {
             k_large_panel<512><<<nL, 512, 0, st>>>(d, x, lg, prm, it);
             gp.mark(st);
-            k_large_gemm<<<ggrid, 256, 0, st>>>(d, x, lg, nL);
+            k_large_gemm<<<ggrid, 256, 0, st>>>(d, x, lg, nL, x.tpp);
             gp.mark(st);
           }
           lc.n += 2 * batch;
@@ -397,10 +414,11 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
         }
       }
       gp.mark(st);
-      k_large_schur<<<ggrid, 256, 0, st>>>(d, x, lg, nL);
+      k_large_schur<<<ggrid, 256, 0, st>>>(d, x, lg, nL, fin);
       gp.mark(st);
-      k_large_finish<512><<<nL, 512, 0, st>>>(d, x, lg, prm);
-      lc.n += 3;
+      k_large_finish<512><<<nL, 512, 0, st>>>(d, x, lg, fin, prm);
+      k_large_store<<<ggrid, 256, 0, st>>>(d, x, lg, nL, c.posdef);
+      lc.n += 4;
     }
   }
   SMFG_CUDA(cudaGetLastError());
@@ -540,18 +558,29 @@ static void enqueue_solve(Plan &pl, double *d_b, int nrhs, int ldb, int job, boo
   const double *sc_out = (scaled && (job == SMFG_SOLVE_FULL || job == SMFG_SOLVE_BACKWARD)) ? x.scale : nullptr;
   k_solve_gather<<<g, 256, 0, st>>>(d_b, ldb, nrhs, pl.n, d.perm, sc_in, xv);
   lc.n++;
+  const int lgrid = 2 * sms;
   if (fwd) {
     for (int l = 0; l < pl.nlevels; ++l) {
       const int lo = pl.lvl_ptr[l], m = pl.lvl_ptr[l + 1] - lo;
-      k_forward<<<m, 128, 0, st>>>(d, x, lo, lo + m, pl.posdef, xv, wk, rows_total, nrhs);
+      k_fwd_front<<<m, kSolveNT, 0, st>>>(d, x, lo, pl.posdef, xv, wk, rows_total, nrhs);
       lc.n++;
+      const int nL = pl.lvl_large_ptr[l + 1] - pl.lvl_large_ptr[l];
+      if (nL > 0) {
+        k_fwd_l21<<<lgrid, 256, 0, st>>>(d, x, d.lvl_large + pl.lvl_large_ptr[l], nL, wk, rows_total, nrhs);
+        lc.n++;
+      }
     }
   }
   if (use_lt || (use_d && !pl.posdef)) {
     for (int l = pl.nlevels - 1; l >= 0; --l) {
       const int lo = pl.lvl_ptr[l], m = pl.lvl_ptr[l + 1] - lo;
-      k_backward<<<m, 128, 0, st>>>(d, x, lo, lo + m, pl.posdef, xv, wk, rows_total, nrhs,
-                                     use_d ? 1 : 0, use_lt ? 1 : 0);
+      const int nL = pl.lvl_large_ptr[l + 1] - pl.lvl_large_ptr[l];
+      if (nL > 0 && use_lt) {
+        k_bwd_l21<<<lgrid, 256, 0, st>>>(d, x, d.lvl_large + pl.lvl_large_ptr[l], nL, xv, wk, rows_total, nrhs);
+        lc.n++;
+      }
+      k_bwd_front<<<m, kSolveNT, 0, st>>>(d, x, lo, pl.posdef, xv, wk, rows_total, nrhs,
+                                          use_d ? 1 : 0, use_lt ? 1 : 0);
       lc.n++;
     }
   }

@@ -300,8 +300,19 @@ __device__ __forceinline__ void inverse_2x2(double d00, double d10, double d11, 
   i11 = __dmul_rn(a, inv);
 }
 
+// Thread layout of the block's update loops: kRB consecutive rows per pass
+// (coalesced column-major accesses), NT / kRB column groups.
+template <int NT>
+struct Lay {
+  static constexpr int RB = NT < 128 ? NT : 128;
+  static constexpr int G = NT / RB;
+  static __device__ __forceinline__ int r() { return threadIdx.x % RB; }
+  static __device__ __forceinline__ int g() { return threadIdx.x / RB; }
+};
+
 template <int NT>
 __device__ void eliminate_1x1_blk(const FrontRef &v, int k, int ucol_end, bool useW, int w_col) {
+  using LY = Lay<NT>;
   const size_t sf = (size_t)v.ld;
   const int f = v.f;
   double *ck = v.F + k * sf;
@@ -310,17 +321,15 @@ __device__ void eliminate_1x1_blk(const FrontRef &v, int k, int ucol_end, bool u
     double *w = v.W + (size_t)w_col * f;
     for (int i = k + 1 + threadIdx.x; i < f; i += NT) w[i] = ck[i];
   }
-  const int ncol = ucol_end - (k + 1);
-  if (ncol > 0) {
-    const long long tot = (long long)ncol * f;
-    for (long long t = threadIdx.x; t < tot; t += NT) {
-      const int j = k + 1 + (int)(t / f);
-      const int i = (int)(t % f);
-      if (i < j) continue;
+  // column j of (k, ucol_end), row i >= j: F(i, j) -= F(i, k) * l_j
+  for (int i = k + 1 + LY::r(); i < f; i += LY::RB) {
+    const double cki = ck[i];
+    const int jend = min(ucol_end, i + 1);
+    for (int j = k + 1 + LY::g(); j < jend; j += LY::G) {
       const double lj = __dmul_rn(ck[j], inv_d);
       if (lj == 0.0) continue;
       double *cj = v.F + (size_t)j * sf;
-      cj[i] = __dsub_rn(cj[i], __dmul_rn(ck[i], lj));
+      cj[i] = __dsub_rn(cj[i], __dmul_rn(cki, lj));
     }
   }
   __syncthreads();
@@ -330,6 +339,7 @@ __device__ void eliminate_1x1_blk(const FrontRef &v, int k, int ucol_end, bool u
 
 template <int NT>
 __device__ void eliminate_2x2_blk(const FrontRef &v, int k, int ucol_end, bool useW, int w_col) {
+  using LY = Lay<NT>;
   const size_t sf = (size_t)v.ld;
   const int f = v.f;
   double *c0 = v.F + k * sf;
@@ -344,19 +354,16 @@ __device__ void eliminate_2x2_blk(const FrontRef &v, int k, int ucol_end, bool u
       w1[i] = c1[i];
     }
   }
-  const int ncol = ucol_end - (k + 2);
-  if (ncol > 0) {
-    const long long tot = (long long)ncol * f;
-    for (long long t = threadIdx.x; t < tot; t += NT) {
-      const int j = k + 2 + (int)(t / f);
-      const int i = (int)(t % f);
-      if (i < j) continue;
+  for (int i = k + 2 + LY::r(); i < f; i += LY::RB) {
+    const double c0i = c0[i], c1i = c1[i];
+    const int jend = min(ucol_end, i + 1);
+    for (int j = k + 2 + LY::g(); j < jend; j += LY::G) {
       const double a0 = c0[j], a1 = c1[j];
       const double l0 = __dadd_rn(__dmul_rn(i00, a0), __dmul_rn(i10, a1));
       const double l1 = __dadd_rn(__dmul_rn(i10, a0), __dmul_rn(i11, a1));
       if (l0 == 0.0 && l1 == 0.0) continue;
       double *d0 = v.F + (size_t)j * sf;
-      d0[i] = __dsub_rn(d0[i], __dadd_rn(__dmul_rn(c0[i], l0), __dmul_rn(c1[i], l1)));
+      d0[i] = __dsub_rn(d0[i], __dadd_rn(__dmul_rn(c0i, l0), __dmul_rn(c1i, l1)));
     }
   }
   __syncthreads();
@@ -553,23 +560,22 @@ __device__ void apply_pivot_blk(const FrontRef &v, int &k, bool useW, int w_cols
 // W[c0:e, :]^T, one fused multiply-add per pivot in order, zero W skipped.
 template <int NT>
 __device__ void deferred_update_blk(const FrontRef &v, int p0, int p1, int c0, int e) {
-  const int jb = p1 - p0, m = e - c0;
-  if (jb <= 0 || m <= 0) return;
+  using LY = Lay<NT>;
+  const int jb = p1 - p0;
+  if (jb <= 0 || e - c0 <= 0) return;
   const size_t sf = (size_t)v.ld;
   const int f = v.f;
-  const int h = f - c0;
-  const long long tot = (long long)m * h;
-  for (long long t = threadIdx.x; t < tot; t += NT) {
-    const int j = c0 + (int)(t / h);
-    const int i = c0 + (int)(t % h);
-    if (i < j) continue;
-    double c = v.F[(size_t)j * sf + i];
-    for (int p = 0; p < jb; ++p) {
-      const double b = v.W[(size_t)p * f + j];
-      if (b == 0.0) continue;
-      c = fma(-v.F[(size_t)(p0 + p) * sf + i], b, c);
+  for (int i = c0 + LY::r(); i < f; i += LY::RB) {
+    const int jend = min(e, i + 1);
+    for (int j = c0 + LY::g(); j < jend; j += LY::G) {
+      double c = v.F[(size_t)j * sf + i];
+      for (int p = 0; p < jb; ++p) {
+        const double b = v.W[(size_t)p * f + j];
+        if (b == 0.0) continue;
+        c = fma(-v.F[(size_t)(p0 + p) * sf + i], b, c);
+      }
+      v.F[(size_t)j * sf + i] = c;
     }
-    v.F[(size_t)j * sf + i] = c;
   }
   __syncthreads();
 }
@@ -592,21 +598,20 @@ __device__ __forceinline__ double ld_entry(const FrontRef &v, int c, int j) {
 // pivots [p0, p) in order.
 template <int NT>
 __device__ void schur_update_blk(const FrontRef &v, int p0, int p, int e) {
-  const int q = v.f - e;
-  if (p <= p0 || q <= 0) return;
+  using LY = Lay<NT>;
+  const int f = v.f;
+  if (p <= p0 || f - e <= 0) return;
   const size_t sf = (size_t)v.ld;
-  const long long tot = (long long)q * q;
-  for (long long t = threadIdx.x; t < tot; t += NT) {
-    const int j = e + (int)(t / q);
-    const int i = e + (int)(t % q);
-    if (i < j) continue;
-    double c = v.F[(size_t)j * sf + i];
-    for (int cc = p0; cc < p; ++cc) {
-      const double b = ld_entry(v, cc, j);
-      if (b == 0.0) continue;
-      c = fma(-v.F[(size_t)cc * sf + i], b, c);
+  for (int i = e + LY::r(); i < f; i += LY::RB) {
+    for (int j = e + LY::g(); j <= i; j += LY::G) {
+      double c = v.F[(size_t)j * sf + i];
+      for (int cc = p0; cc < p; ++cc) {
+        const double b = ld_entry(v, cc, j);
+        if (b == 0.0) continue;
+        c = fma(-v.F[(size_t)cc * sf + i], b, c);
+      }
+      v.F[(size_t)j * sf + i] = c;
     }
-    v.F[(size_t)j * sf + i] = c;
   }
   __syncthreads();
 }

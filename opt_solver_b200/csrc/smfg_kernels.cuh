@@ -503,7 +503,7 @@ __device__ __forceinline__ void trap_tile(int w, int rows, int cols, int &ti, in
 
 // Deferred updates of all large fronts with one pending (ldlt_kernel.cpp:705-761).
 __global__ void __launch_bounds__(256) k_large_gemm(DevPlan P, DevFactor X, const int *__restrict__ large,
-                                                    int nlarge) {
+                                                    int nlarge, const TppState *__restrict__ tpp) {
   __shared__ double As[16][kGT], Bs[16][kGT];
   __shared__ int pref[257];
   __shared__ int base_front;
@@ -513,7 +513,7 @@ __global__ void __launch_bounds__(256) k_large_gemm(DevPlan P, DevFactor X, cons
     if (threadIdx.x == 0) {
       pref[0] = 0;
       for (int q = 0; q < cnt; ++q) {
-        const TppState &S = X.tpp[chunk + q];
+        const TppState &S = tpp[chunk + q];
         int nt = 0;
         if (S.pad[0] && S.g_p1 > S.g_p0 && S.g_e > S.g_c0) {
           const int s = large[chunk + q];
@@ -535,7 +535,7 @@ __global__ void __launch_bounds__(256) k_large_gemm(DevPlan P, DevFactor X, cons
       }
       const int q = base_front + a;
       const int s = large[q];
-      const TppState S = X.tpp[q];
+      const TppState S = tpp[q];
       const int f = X.sn_f[s];
       const size_t sf = (size_t)f;
       double *F = X.arena + X.sn_off[s];
@@ -604,7 +604,7 @@ __device__ __forceinline__ double ld_entry_g(const double *F, size_t sf, const i
 // Schur updates of all large fronts of a level (schur_update,
 // ldlt_kernel.cpp:820-933): F[e:f, e:f] -= L LD^T over pivots [0, k).
 __global__ void __launch_bounds__(256) k_large_schur(DevPlan P, DevFactor X, const int *__restrict__ large,
-                                                     int nlarge) {
+                                                     int nlarge, const TppState *__restrict__ tpp) {
   __shared__ double As[16][kGT], Bs[16][kGT];
   __shared__ int pref[257];
   if (X.counters[kCFlags] & (kFArena | kFRows)) return;
@@ -614,7 +614,7 @@ __global__ void __launch_bounds__(256) k_large_schur(DevPlan P, DevFactor X, con
       pref[0] = 0;
       for (int q = 0; q < cnt; ++q) {
         const int s = large[chunk + q];
-        const int e = X.sn_ne[s], f = X.sn_f[s], k = X.tpp[chunk + q].k;
+        const int e = X.sn_ne[s], f = X.sn_f[s], k = tpp[chunk + q].k;
         pref[q + 1] = pref[q] + ((f > e && k > 0) ? trap_tiles(f - e, f - e) : 0);
       }
     }
@@ -630,7 +630,7 @@ __global__ void __launch_bounds__(256) k_large_schur(DevPlan P, DevFactor X, con
       }
       const int q = chunk + a;
       const int s = large[q];
-      const int f = X.sn_f[s], e = X.sn_ne[s], kk = X.tpp[q].k;
+      const int f = X.sn_f[s], e = X.sn_ne[s], kk = tpp[q].k;
       const size_t sf = (size_t)f;
       double *F = X.arena + X.sn_off[s];
       const int8_t *tags = X.tags + X.sn_roff[s];
@@ -685,23 +685,247 @@ __global__ void __launch_bounds__(256) k_large_schur(DevPlan P, DevFactor X, con
   }
 }
 
+// Bookkeeping of a factored large front (one block): zero pivots at a root,
+// status flags, 2x2 off-diagonals moved to their upper slots, counts, and
+// the children's row maps in pivot order. The column-parallel part of the
+// store (the SPD sqrt(D) fold, zeroing) is k_large_store.
 template <int NT>
 __global__ void __launch_bounds__(NT) k_large_finish(DevPlan P, DevFactor X, const int *__restrict__ large,
-                                                     PivotParams prm) {
-  __shared__ FrontShared sh;
+                                                     const TppState *__restrict__ tpp, PivotParams prm) {
   if (X.counters[kCFlags] & (kFArena | kFRows)) return;
   const int s = large[blockIdx.x];
-  const TppState S = X.tpp[blockIdx.x];
+  const TppState S = tpp[blockIdx.x];
   const FrontRef v = large_view(P, X, s);
+  const int f = v.f, ne = v.ne, p = S.k;
+  const size_t sf = (size_t)f;
   if (threadIdx.x == 0) {
-    sh.st = S.st;
-    const double q = (double)(v.f - v.ne);
-    if (q > 0 && S.k > 0)
-      atomicAdd(reinterpret_cast<double *>(X.counters + kCGemmFlops), 2.0 * S.k * (q * (q + 1) / 2));
+    const double q = (double)(f - ne);
+    if (q > 0 && p > 0)
+      atomicAdd(reinterpret_cast<double *>(X.counters + kCGemmFlops), 2.0 * p * (q * (q + 1) / 2));
+  }
+  const bool is_root = P.sn_parent[s] < 0;
+  int pstore = p;
+  if (is_root && p < ne) {
+    for (int c = p + threadIdx.x; c < ne; c += NT) v.tags[c] = 0;
+    pstore = ne;
   }
   __syncthreads();
+  if (prm.posdef) {
+    if (p < ne && threadIdx.x == 0) set_flag(X.counters, kFNotPosdef);
+  } else {
+    bool bad = false;
+    for (int c = threadIdx.x; c < pstore; c += NT) {
+      double *Lc = v.F + (size_t)c * sf;
+      const int8_t tag = v.tags[c];
+      if (tag == 1) bad = bad || !isfinite(Lc[c]);
+      else if (tag == 2) bad = bad || !isfinite(Lc[c]) || !isfinite(Lc[c + 1]) || !isfinite(Lc[sf + c + 1]);
+      else if (tag == -1) Lc[c - 1] = v.F[(size_t)(c - 1) * sf + c];
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) set_flag(X.counters, kFNonfiniteD);
+  }
   int *inv = X.ploc + X.rows_cap + X.sn_roff[s];
-  store_front<NT, false>(P, X, s, v, S.k, prm, sh, inv, v.F, v.rows, v.tags);
+  for (int t = threadIdx.x; t < f; t += NT) inv[v.loc[t]] = t;
+  __syncthreads();
+  for (int t = P.child_ptr[s]; t < P.child_ptr[s + 1]; ++t) {
+    const int c = P.child_idx[t];
+    const int pc = X.sn_p[c];
+    int *cmap = X.cbmap + X.sn_roff[c] + pc;
+    for (int u = threadIdx.x; u < X.sn_f[c] - pc; u += NT) cmap[u] = inv[cmap[u]];
+  }
+  if (threadIdx.x == 0) {
+    X.sn_p[s] = p;
+    X.sn_pstore[s] = pstore;
+    X.sn_dout[s] = is_root ? 0 : ne - p;
+    int *st = X.sn_stat + 4 * s;
+    st[0] = S.st.pos;
+    st[1] = S.st.neg;
+    st[2] = S.st.zero + (is_root ? ne - p : 0);
+    st[3] = S.st.two_by_two;
+    X.sn_flops[s] = S.st.flops;
+  }
+}
+
+// Column-parallel store of the large fronts' pivot columns
+// (multifrontal_serial.cpp:903-945): SPD L = L_unit sqrt(D) with the upper
+// part zero; indefinite D inline (zero pivots' columns zero, the 2x2
+// blocks' lower off-diagonal slot zero, the upper part zero but for the
+// slot k_large_finish filled). Work items: 32 columns of one front.
+__global__ void __launch_bounds__(256) k_large_store(DevPlan P, DevFactor X, const int *__restrict__ large,
+                                                     int nlarge, int posdef) {
+  __shared__ int pref[65];
+  __shared__ double sdv[32];
+  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  for (int chunk = 0; chunk < nlarge; chunk += 64) {
+    const int cnt = min(64, nlarge - chunk);
+    if (threadIdx.x == 0) {
+      pref[0] = 0;
+      for (int q = 0; q < cnt; ++q) pref[q + 1] = pref[q] + (X.sn_pstore[large[chunk + q]] + 31) / 32;
+    }
+    __syncthreads();
+    const int total = pref[cnt];
+    for (int w = blockIdx.x; w < total; w += gridDim.x) {
+      int a = 0, b = cnt;
+      while (b - a > 1) {
+        const int mid = (a + b) >> 1;
+        if (pref[mid] <= w) a = mid;
+        else b = mid;
+      }
+      const int s = large[chunk + a];
+      const int f = X.sn_f[s], pstore = X.sn_pstore[s];
+      const size_t sf = (size_t)f;
+      double *F = X.arena + X.sn_off[s];
+      const int8_t *tags = X.tags + X.sn_roff[s];
+      const int c0 = (w - pref[a]) * 32, c1 = min(c0 + 32, pstore);
+      if (posdef) {
+        if (threadIdx.x < c1 - c0) sdv[threadIdx.x] = sqrt(F[(size_t)(c0 + threadIdx.x) * sf + c0 + threadIdx.x]);
+        __syncthreads();
+        for (int c = c0; c < c1; ++c) {
+          double *Lc = F + (size_t)c * sf;
+          const double sd = sdv[c - c0];
+          for (int i = threadIdx.x; i < f; i += 256) {
+            if (i < c) Lc[i] = 0.0;
+            else if (i > c) Lc[i] = __dmul_rn(Lc[i], sd);
+          }
+        }
+        __syncthreads();
+        if (threadIdx.x < c1 - c0) F[(size_t)(c0 + threadIdx.x) * sf + c0 + threadIdx.x] = sdv[threadIdx.x];
+      } else {
+        for (int c = c0; c < c1; ++c) {
+          double *Lc = F + (size_t)c * sf;
+          const int8_t tag = tags[c];
+          for (int i = threadIdx.x; i < f; i += 256) {
+            if (tag == 0) Lc[i] = 0.0;
+            else if (i < c) {
+              if (!(tag == -1 && i == c - 1)) Lc[i] = 0.0;
+            } else if (tag == 2 && i == c + 1) {
+              Lc[i] = 0.0;
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+    __syncthreads();
+  }
+}
+
+// The SPD panel of the large fronts on many blocks (the posdef case of
+// ldlt_factor_front's panel loop, ldlt_kernel.cpp:1100-1112 with
+// select_pivot's in-order test :130-134 and eliminate_1x1 :352-458). Every
+// block factors the panel's diagonal block in shared memory (the pivots'
+// multipliers l_j = F(j, k) / d... as ck[j] * inv_d), then takes its own
+// rows through the same pivots in registers: per entry the reference's
+// operations in the reference's order, with no synchronization between
+// blocks. Grid: (row blocks of 256 rows, large fronts). The state is read
+// from `cur` and the next one written to `nxt` (one block per front).
+template <int NB>
+__global__ void __launch_bounds__(256) k_large_panel_spd(DevPlan P, DevFactor X, const int *__restrict__ large,
+                                                         const TppState *__restrict__ cur,
+                                                         TppState *__restrict__ nxt, int iter) {
+  __shared__ double T[NB][NB + 1];
+  __shared__ double lm[NB][NB];
+  __shared__ double linv[NB];
+  __shared__ int np_sh;
+  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  const int q = blockIdx.y;
+  const int s = large[q];
+  const TppState S = cur[q];
+  const bool lead = blockIdx.x == 0;
+  if (S.phase == 2) {
+    if (lead && threadIdx.x == 0) {
+      TppState o = S;
+      o.pad[0] = 0;
+      nxt[q] = o;
+    }
+    return;
+  }
+  const int f = X.sn_f[s], ne = X.sn_ne[s];
+  const int ps = S.k, pl = min(ne, ps + NB), nbp = pl - ps;
+  const int r0 = ps + blockIdx.x * 256;
+  if (r0 >= f) return;
+  const size_t sf = (size_t)f;
+  double *F = X.arena + X.sn_off[s];
+  double *W = F + sf * sf;
+  const double eff_small = __longlong_as_double((long long)X.counters[kCEffSmall]);
+  for (int t = threadIdx.x; t < NB * NB; t += 256) {
+    const int r = t / NB, c = t % NB;
+    T[r][c] = (r < nbp && c <= r) ? F[(size_t)(ps + c) * sf + ps + r] : 0.0;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    int np = 0;
+    for (int k = 0; k < nbp; ++k) {
+      const double d = T[k][k];
+      if (!(d > 0.0 && isfinite(d))) break;
+      const double inv = 1.0 / d;
+      if (lane == 0) linv[k] = inv;
+      if (lane > k && lane < nbp) lm[k][lane] = __dmul_rn(T[lane][k], inv);
+      __syncwarp();
+      if (lane > k && lane < nbp) {
+        const double tik = T[lane][k];
+        for (int j = k + 1; j <= lane; ++j) {
+          const double l = lm[k][j];
+          if (l != 0.0) T[lane][j] = __dsub_rn(T[lane][j], __dmul_rn(tik, l));
+        }
+        T[lane][k] = __dmul_rn(tik, inv);
+      }
+      __syncwarp();
+      ++np;
+    }
+    if (lane == 0) np_sh = np;
+  }
+  __syncthreads();
+  const int np = np_sh;
+  const int i = r0 + threadIdx.x;
+  if (i < f) {
+    double a[NB];
+#pragma unroll
+    for (int c = 0; c < NB; ++c) a[c] = (c < nbp && ps + c <= i) ? F[(size_t)(ps + c) * sf + i] : 0.0;
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+      if (k < np && i > ps + k) {
+        const double w = a[k];
+        W[(size_t)k * f + i] = w;
+#pragma unroll
+        for (int j = k + 1; j < NB; ++j) {
+          if (j < nbp && ps + j <= i) {
+            const double l = lm[k][j];
+            if (l != 0.0) a[j] = __dsub_rn(a[j], __dmul_rn(w, l));
+          }
+        }
+        a[k] = __dmul_rn(w, linv[k]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < NB; ++c)
+      if (c < nbp && ps + c <= i) F[(size_t)(ps + c) * sf + i] = a[c];
+  }
+  if (lead && threadIdx.x == 0) {
+    TppState o = S;
+    int8_t *tags = X.tags + X.sn_roff[s];
+    for (int k = 0; k < np; ++k) {
+      tags[ps + k] = 1;
+      inertia_1x1(T[k][k], eff_small, o.st);
+      const double rem = (double)(f - (ps + k + 1));
+      o.st.flops += rem + rem * (rem + 1.0);
+    }
+    o.k = ps + np;
+    o.g_p0 = ps;
+    o.g_p1 = ps + np;
+    o.g_c0 = pl;
+    o.g_e = ne;
+    o.pad[0] = np > 0 ? 1 : 0;
+    if (np < nbp || o.k >= ne) o.phase = 2;
+    nxt[q] = o;
+    if (np > 0) {
+      atomicMax(X.counters + kCActive, (unsigned long long)(iter + 1));
+      const long long m = ne - pl, h = f - pl;
+      if (m > 0)
+        atomicAdd(reinterpret_cast<double *>(X.counters + kCGemmFlops),
+                  2.0 * (double)np * (double)(m * h - m * (m - 1) / 2));
+    }
+  }
 }
 
 // Totals over all fronts, in supernode order (deterministic).
@@ -788,126 +1012,270 @@ __global__ void k_solve_scatter(double *__restrict__ b, int ldb, int nrhs, int n
   }
 }
 
-// Forward solve of one level (solve_forward.cpp:116-293 computes the same
-// L^-1 b): each front gathers its pivot rows, adds its children's update
-// vectors in child order, eliminates its pivots and leaves its update
-// vector (rows p..f) for its parent; the pivot results go to x.
-__global__ void k_forward(DevPlan P, DevFactor X, int lo, int hi, int posdef, double *x, double *wk,
-                          int64_t rows_total, int nrhs) {
+// Solves by level. Each front's work vector w (length f, at the front's row
+// offset) holds its pivot rows' values and, in the forward sweep, its update
+// vector for the parent (rows p..f); x (new numbering) holds the pivot
+// results. Large fronts (symbolic rows >= kLargeMin) leave their L21 part
+// to the multi-block kernels k_fwd_l21 / k_bwd_l21. Sums run in a fixed
+// order (deterministic); solve_forward.cpp:116-293 and
+// solve_backward.cpp:135-350 compute the same quantities.
+constexpr int kSolveNT = 128;
+
+// Forward sweep of one level: gather, children's update vectors in child
+// order, blocked unit (indefinite) or non-unit (SPD) L11 solve, then
+// w[p:f) -= L21 w[0:p) unless the front is large.
+__global__ void __launch_bounds__(kSolveNT) k_fwd_front(DevPlan P, DevFactor X, int lo, int posdef,
+                                                        double *x, double *wk, int64_t rows_total,
+                                                        int nrhs) {
   const int s = P.lvl_sn[lo + blockIdx.x];
   const int f = X.sn_f[s], p = X.sn_pstore[s];
   const int64_t roff = X.sn_roff[s];
   const int *rows = X.rows + roff;
   const double *L = X.arena + X.sn_off[s];
   const size_t sf = (size_t)f;
+  const bool large = P.sn_fsym[s] >= kLargeMin;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int r = 0; r < nrhs; ++r) {
     double *w = wk + (int64_t)r * rows_total + roff;
-    const double *xr = x + (int64_t)r * P.n;
-    for (int i = threadIdx.x; i < f; i += blockDim.x) w[i] = (i < p) ? xr[rows[i]] : 0.0;
+    double *xr = x + (int64_t)r * P.n;
+    for (int i = threadIdx.x; i < f; i += kSolveNT) w[i] = (i < p) ? xr[rows[i]] : 0.0;
     __syncthreads();
     for (int t = P.child_ptr[s]; t < P.child_ptr[s + 1]; ++t) {
       const int c = P.child_idx[t];
       const int pc = X.sn_pstore[c], q = X.sn_f[c] - pc;
       const int *cmap = X.cbmap + X.sn_roff[c] + pc;
       const double *u = wk + (int64_t)r * rows_total + X.sn_roff[c] + pc;
-      for (int i = threadIdx.x; i < q; i += blockDim.x) w[cmap[i]] += u[i];
+      for (int i = threadIdx.x; i < q; i += kSolveNT) w[cmap[i]] += u[i];
       __syncthreads();
     }
-    for (int j = 0; j < p; ++j) {
-      const double *Lj = L + (size_t)j * sf;
-      double wj = w[j];
-      if (posdef) wj = wj / Lj[j];
+    const int rend = large ? p : f;
+    for (int jb = 0; jb < p; jb += 32) {
+      const int nb = min(32, p - jb);
+      if (warp == 0) {
+        double wi = (lane < nb) ? w[jb + lane] : 0.0;
+        for (int j = 0; j < nb; ++j) {
+          const double *Lj = L + (size_t)(jb + j) * sf;
+          double wj = __shfl_sync(0xffffffffu, wi, j);
+          if (posdef) wj = wj / Lj[jb + j];
+          if (lane == j) wi = wj;
+          if (lane > j && lane < nb) wi = fma(-Lj[jb + lane], wj, wi);
+        }
+        if (lane < nb) w[jb + lane] = wi;
+      }
       __syncthreads();
-      if (threadIdx.x == 0) w[j] = wj;
-      for (int i = j + 1 + threadIdx.x; i < f; i += blockDim.x) w[i] = fma(-Lj[i], wj, w[i]);
+      for (int i = jb + nb + threadIdx.x; i < rend; i += kSolveNT) {
+        double acc = w[i];
+        for (int j = jb; j < jb + nb; ++j) acc = fma(-L[(size_t)j * sf + i], w[j], acc);
+        w[i] = acc;
+      }
       __syncthreads();
     }
-    double *xw = x + (int64_t)r * P.n;
-    for (int i = threadIdx.x; i < p; i += blockDim.x) xw[rows[i]] = w[i];
+    for (int i = threadIdx.x; i < p; i += kSolveNT) xr[rows[i]] = w[i];
     __syncthreads();
   }
 }
 
-// Backward solve of one level, D^-1 applied first for the indefinite factor
-// (apply_inline_d, solve_backward.cpp:135-171; scaled Cramer rule of
-// solve_2x2_scaled, pivoting.cpp:30-62), then x_piv -= L21^T x_ext and
-// L11^-T (solve_backward.cpp:186-350).
-__global__ void k_backward(DevPlan P, DevFactor X, int lo, int hi, int posdef, double *x,
-                           double *wk, int64_t rows_total, int nrhs, int apply_d, int apply_lt) {
+// w[p:f) -= L21 w[0:p) of the level's large fronts, rows split over blocks.
+__global__ void __launch_bounds__(256) k_fwd_l21(DevPlan P, DevFactor X, const int *__restrict__ large,
+                                                 int nlarge, double *wk, int64_t rows_total, int nrhs) {
+  __shared__ double ws[256];
+  __shared__ int pref[65];
+  for (int chunk = 0; chunk < nlarge; chunk += 64) {
+    const int cnt = min(64, nlarge - chunk);
+    if (threadIdx.x == 0) {
+      pref[0] = 0;
+      for (int q = 0; q < cnt; ++q) {
+        const int s = large[chunk + q];
+        pref[q + 1] = pref[q] + (X.sn_f[s] - X.sn_pstore[s] + 255) / 256 * nrhs;
+      }
+    }
+    __syncthreads();
+    const int total = pref[cnt];
+    for (int wi = blockIdx.x; wi < total; wi += gridDim.x) {
+      int a = 0, b = cnt;
+      while (b - a > 1) {
+        const int mid = (a + b) >> 1;
+        if (pref[mid] <= wi) a = mid;
+        else b = mid;
+      }
+      const int s = large[chunk + a];
+      const int f = X.sn_f[s], p = X.sn_pstore[s];
+      const int nchunks = (f - p + 255) / 256;
+      const int item = wi - pref[a];
+      const int r = item / nchunks, rc = item % nchunks;
+      double *w = wk + (int64_t)r * rows_total + X.sn_roff[s];
+      const double *L = X.arena + X.sn_off[s];
+      const size_t sf = (size_t)f;
+      const int i = p + rc * 256 + threadIdx.x;
+      double acc = (i < f) ? w[i] : 0.0;
+      for (int j0 = 0; j0 < p; j0 += 256) {
+        const int nj = min(256, p - j0);
+        __syncthreads();
+        if (threadIdx.x < nj) ws[threadIdx.x] = w[j0 + threadIdx.x];
+        __syncthreads();
+        if (i < f)
+          for (int j = 0; j < nj; ++j) acc = fma(-L[(size_t)(j0 + j) * sf + i], ws[j], acc);
+      }
+      if (i < f) w[i] = acc;
+      __syncthreads();
+    }
+    __syncthreads();
+  }
+}
+
+// t[0:p) = L21^T x_ext of the level's large fronts (warp per column),
+// stored at the front's work vector positions [0, p).
+__global__ void __launch_bounds__(256) k_bwd_l21(DevPlan P, DevFactor X, const int *__restrict__ large,
+                                                 int nlarge, const double *x, double *wk,
+                                                 int64_t rows_total, int nrhs) {
+  __shared__ int pref[65];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int chunk = 0; chunk < nlarge; chunk += 64) {
+    const int cnt = min(64, nlarge - chunk);
+    if (threadIdx.x == 0) {
+      pref[0] = 0;
+      for (int q = 0; q < cnt; ++q) {
+        const int s = large[chunk + q];
+        pref[q + 1] = pref[q] + (X.sn_pstore[s] + 7) / 8 * nrhs;
+      }
+    }
+    __syncthreads();
+    const int total = pref[cnt];
+    for (int wi = blockIdx.x; wi < total; wi += gridDim.x) {
+      int a = 0, b = cnt;
+      while (b - a > 1) {
+        const int mid = (a + b) >> 1;
+        if (pref[mid] <= wi) a = mid;
+        else b = mid;
+      }
+      const int s = large[chunk + a];
+      const int f = X.sn_f[s], p = X.sn_pstore[s];
+      const int ncc = (p + 7) / 8;
+      const int item = wi - pref[a];
+      const int r = item / ncc, cc = item % ncc;
+      const int j = cc * 8 + warp;
+      if (j < p) {
+        const int *rows = X.rows + X.sn_roff[s];
+        const double *Lj = X.arena + X.sn_off[s] + (size_t)j * f;
+        const double *xr = x + (int64_t)r * P.n;
+        double acc = 0.0;
+        for (int i = p + lane; i < f; i += 32) acc = fma(Lj[i], xr[rows[i]], acc);
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) wk[(int64_t)r * rows_total + X.sn_roff[s] + j] = acc;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Backward sweep of one level: v = D^-1 w_piv (indefinite, apply_inline_d
+// with solve_2x2_scaled's scaled Cramer rule, solve_backward.cpp:135-171,
+// pivoting.cpp:30-62), v -= L21^T x_ext (here for small fronts, from
+// k_bwd_l21 for large ones), then the blocked L11^-T solve.
+__global__ void __launch_bounds__(kSolveNT) k_bwd_front(DevPlan P, DevFactor X, int lo, int posdef,
+                                                        double *x, double *wk, int64_t rows_total,
+                                                        int nrhs, int apply_d, int apply_lt) {
+  __shared__ double vs_small[1];
+  (void)vs_small;
   const int s = P.lvl_sn[lo + blockIdx.x];
   const int f = X.sn_f[s], p = X.sn_pstore[s];
   const int64_t roff = X.sn_roff[s];
   const int *rows = X.rows + roff;
   const double *L = X.arena + X.sn_off[s];
   const size_t sf = (size_t)f;
+  const bool large = P.sn_fsym[s] >= kLargeMin;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int r = 0; r < nrhs; ++r) {
-    double *v = wk + (int64_t)r * rows_total + roff;
+    double *v = wk + (int64_t)r * rows_total + roff;  // large: v[0:p) holds L21^T x_ext
     double *xr = x + (int64_t)r * P.n;
-    for (int i = threadIdx.x; i < f; i += blockDim.x) v[i] = xr[rows[i]];
-    __syncthreads();
-    if (!posdef && apply_d && threadIdx.x == 0) {
-      for (int c = 0; c < p;) {
+    // D^-1 of each pivot block; 2x2 blocks start where the upper slot
+    // (c, c+1) is nonzero
+    for (int c = threadIdx.x; c < p; c += kSolveNT) {
+      const bool second = apply_d && !posdef && (c > 0) && L[(size_t)c * sf + c - 1] != 0.0;
+      if (second) continue;
+      double y0 = xr[rows[c]];
+      if (!posdef && apply_d) {
         const double d00 = L[(size_t)c * sf + c];
-        if (c + 1 < p) {
-          const double d10 = L[(size_t)(c + 1) * sf + c];
-          if (d10 != 0.0) {
-            const double d11 = L[(size_t)(c + 1) * sf + c + 1];
-            const double s2 = max3_ref(fabs(d00), fabs(d10), fabs(d11));
-            double y0 = 0.0, y1 = 0.0;
-            const double r0 = v[c], r1 = v[c + 1];
-            if (isfinite(s2) && s2 != 0.0) {
-              const double a = d00 / s2, bb = d10 / s2, cc = d11 / s2;
-              const double det = __dsub_rn(__dmul_rn(a, cc), __dmul_rn(bb, bb));
-              if (isfinite(det) && det != 0.0) {
-                if (!isfinite(r0) || !isfinite(r1)) {
-                  y0 = r0;
-                  y1 = r1;
-                } else {
-                  const double rs = fmax(fabs(r0), fabs(r1));
-                  if (rs != 0.0) {
-                    const double q0 = r0 / rs, q1 = r1 / rs;
-                    const double u0 = __dsub_rn(__dmul_rn(cc, q0), __dmul_rn(bb, q1)) / det;
-                    const double u1 = __dadd_rn(__dmul_rn(-bb, q0), __dmul_rn(a, q1)) / det;
-                    const double ratio = rs / s2;
-                    y0 = __dmul_rn(u0, ratio);
-                    y1 = __dmul_rn(u1, ratio);
-                  }
+        const double d10 = (c + 1 < p) ? L[(size_t)(c + 1) * sf + c] : 0.0;
+        if (d10 != 0.0) {
+          const double d11 = L[(size_t)(c + 1) * sf + c + 1];
+          const double r0 = y0, r1 = xr[rows[c + 1]];
+          const double s2 = max3_ref(fabs(d00), fabs(d10), fabs(d11));
+          double z0 = 0.0, z1 = 0.0;
+          if (isfinite(s2) && s2 != 0.0) {
+            const double a = d00 / s2, bb = d10 / s2, cc = d11 / s2;
+            const double det = __dsub_rn(__dmul_rn(a, cc), __dmul_rn(bb, bb));
+            if (isfinite(det) && det != 0.0) {
+              if (!isfinite(r0) || !isfinite(r1)) {
+                z0 = r0;
+                z1 = r1;
+              } else {
+                const double rs = fmax(fabs(r0), fabs(r1));
+                if (rs != 0.0) {
+                  const double q0 = r0 / rs, q1 = r1 / rs;
+                  const double u0 = __dsub_rn(__dmul_rn(cc, q0), __dmul_rn(bb, q1)) / det;
+                  const double u1 = __dadd_rn(__dmul_rn(-bb, q0), __dmul_rn(a, q1)) / det;
+                  const double ratio = rs / s2;
+                  z0 = __dmul_rn(u0, ratio);
+                  z1 = __dmul_rn(u1, ratio);
                 }
               }
             }
-            v[c] = y0;
-            v[c + 1] = y1;
-            c += 2;
-            continue;
           }
+          if (apply_lt && large) {
+            z0 -= v[c];
+            z1 -= v[c + 1];
+          }
+          v[c] = z0;
+          v[c + 1] = z1;
+          continue;
         }
-        v[c] = (d00 == 0.0 || !isfinite(d00)) ? 0.0 : v[c] / d00;
-        ++c;
+        y0 = (d00 == 0.0 || !isfinite(d00)) ? 0.0 : y0 / d00;
       }
+      if (apply_lt && large) y0 -= v[c];
+      v[c] = y0;
     }
     __syncthreads();
     if (!apply_lt) {
-      for (int i = threadIdx.x; i < p; i += blockDim.x) xr[rows[i]] = v[i];
+      for (int i = threadIdx.x; i < p; i += kSolveNT) xr[rows[i]] = v[i];
       __syncthreads();
       continue;
     }
-    // x_piv -= L21^T x_ext (each pivot's dot product in row order)
-    for (int j = threadIdx.x; j < p; j += blockDim.x) {
-      const double *Lj = L + (size_t)j * sf;
-      double acc = v[j];
-      for (int i = p; i < f; ++i) acc = fma(-Lj[i], v[i], acc);
-      v[j] = acc;
-    }
-    __syncthreads();
-    for (int j = p - 1; j >= 0; --j) {
-      double vj = v[j];
-      if (posdef) vj = vj / L[(size_t)j * sf + j];
-      __syncthreads();
-      if (threadIdx.x == 0) v[j] = vj;
-      for (int i = threadIdx.x; i < j; i += blockDim.x) v[i] = fma(-L[(size_t)i * sf + j], vj, v[i]);
+    if (!large) {  // v -= L21^T x_ext, warp per column
+      for (int j = warp; j < p; j += kSolveNT / 32) {
+        const double *Lj = L + (size_t)j * sf;
+        double acc = 0.0;
+        for (int i = p + lane; i < f; i += 32) acc = fma(Lj[i], xr[rows[i]], acc);
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) v[j] -= acc;
+      }
       __syncthreads();
     }
-    for (int i = threadIdx.x; i < p; i += blockDim.x) xr[rows[i]] = v[i];
+    // blocked L11^-T: blocks from the end; dots with the solved part, then
+    // the 32 x 32 triangle by one warp
+    for (int je = p; je > 0; je -= 32) {
+      const int jb = max(0, je - 32), nb = je - jb;
+      for (int j = jb + warp; j < je; j += kSolveNT / 32) {
+        const double *Lj = L + (size_t)j * sf;
+        double acc = 0.0;
+        for (int i = je + lane; i < p; i += 32) acc = fma(Lj[i], v[i], acc);
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) v[j] -= acc;
+      }
+      __syncthreads();
+      if (warp == 0) {
+        double vi = (lane < nb) ? v[jb + lane] : 0.0;
+        for (int j = nb - 1; j >= 0; --j) {
+          double xj = __shfl_sync(0xffffffffu, vi, j);
+          if (posdef) xj = xj / L[(size_t)(jb + j) * sf + jb + j];
+          if (lane == j) vi = xj;
+          if (lane < j) vi = fma(-L[(size_t)(jb + lane) * sf + jb + j], xj, vi);
+        }
+        if (lane < nb) v[jb + lane] = vi;
+      }
+      __syncthreads();
+    }
+    for (int i = threadIdx.x; i < p; i += kSolveNT) xr[rows[i]] = v[i];
     __syncthreads();
   }
 }
