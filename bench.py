@@ -37,6 +37,8 @@ CONFIGS = {
     "lap2d": ("2D 5-point Laplacian 150x150 (n=22,500), 1 RHS", "laplacian_2d(150)", True, 1),
     "traj": ("trajectory KKT T=200 (n=5,612), 8 RHS", "traj200", False, 8),
     "kkt": ("IPM KKT 20^3 + 4,000 constraints (n=12,000), 1 RHS", "kkt_ipm(20, 4000)", False, 1),
+    # the same generator as spd3d at 40^3: the small case of the ncu captures
+    "spd3d40": ("SPD variable-coefficient 7-point 40^3 (n=64,000), 1 RHS", "varcoef_3d(40)", True, 1),
 }
 
 
@@ -50,6 +52,8 @@ def build_matrix(cfg: str):
         return W.trajectory_kkt(200, np.random.default_rng(0))
     if cfg == "kkt":
         return W.kkt_ipm(20, 4000, seed=0)
+    if cfg == "spd3d40":
+        return W.varcoef_3d(40, seed=0)
     raise ValueError(cfg)
 
 

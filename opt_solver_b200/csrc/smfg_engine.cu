@@ -237,6 +237,7 @@ static void build_plan(Plan &pl, const smfg_analysis_t &a) {
   d.cpr_idx = dupload(pl, cpr_idx);
   d.lvl_sn = dupload(pl, lvl_sn);
   d.lvl_large = dupload(pl, lvl_large);
+  pl.h_lvl_large = lvl_large;
   d.sn_level = dupload(pl, level);
   d.pcp = dupload(pl, std::vector<int>(a.perm_col_ptr, a.perm_col_ptr + n + 1));
   d.pri = dupload(pl, std::vector<int>(a.perm_row_idx, a.perm_row_idx + pl.nnz));
@@ -381,7 +382,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
           TppState *nxt = x.tpp + (size_t)((it + 1) & 1) * pl.max_large;
           k_large_panel_spd<16><<<pgrid, 256, 0, st>>>(d, x, lg, cur, nxt, it);
           gp.mark(st);
-          k_large_gemm<<<ggrid, 256, 0, st>>>(d, x, lg, nL, nxt);
+          k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, nxt);
           gp.mark(st);
         }
         fin = x.tpp + (size_t)(steps & 1) * pl.max_large;
@@ -391,7 +392,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
         for (; it < steps; ++it) {
           k_large_panel<512><<<nL, 512, 0, st>>>(d, x, lg, prm, it);
           gp.mark(st);
-          k_large_gemm<<<ggrid, 256, 0, st>>>(d, x, lg, nL, x.tpp);
+          k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, x.tpp);
           gp.mark(st);
         }
         lc.n += 2 * steps;
@@ -403,7 +404,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
           for (int b = 0; b < batch; ++b, ++it) {
             k_large_panel<512><<<nL, 512, 0, st>>>(d, x, lg, prm, it);
             gp.mark(st);
-            k_large_gemm<<<ggrid, 256, 0, st>>>(d, x, lg, nL, x.tpp);
+            k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, x.tpp);
             gp.mark(st);
           }
           lc.n += 2 * batch;
@@ -414,7 +415,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
         }
       }
       gp.mark(st);
-      k_large_schur<<<ggrid, 256, 0, st>>>(d, x, lg, nL, fin);
+      k_large_schur<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, fin);
       gp.mark(st);
       k_large_finish<512><<<nL, 512, 0, st>>>(d, x, lg, fin, prm);
       k_large_store<<<ggrid, 256, 0, st>>>(d, x, lg, nL, c.posdef);
@@ -433,6 +434,8 @@ static void set_kernel_attrs(int nb) {
   SMFG_CUDA(cudaFuncSetAttribute(k_factor<256, kSmallMax + 1, kMediumMax, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)front_smem_bytes(kMediumMax, nb)));
+  SMFG_CUDA(cudaFuncSetAttribute(k_large_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem)));
+  SMFG_CUDA(cudaFuncSetAttribute(k_large_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem)));
   done_nb = nb;
 }
 
@@ -475,6 +478,15 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
     break;
   }
   const unsigned flags = (unsigned)h_cnt[kCFlags];
+  // stored pivots of the large fronts by level (the solves' block counts)
+  pl.lvl_large_pmax.assign(pl.nlevels, 0);
+  if (!pl.h_lvl_large.empty()) {
+    std::vector<int> pst(pl.nsn);
+    SMFG_CUDA(cudaMemcpy(pst.data(), pl.x.sn_pstore, sizeof(int) * pl.nsn, cudaMemcpyDeviceToHost));
+    for (int l = 0; l < pl.nlevels; ++l)
+      for (int i = pl.lvl_large_ptr[l]; i < pl.lvl_large_ptr[l + 1]; ++i)
+        pl.lvl_large_pmax[l] = std::max(pl.lvl_large_pmax[l], pst[pl.h_lvl_large[i]]);
+  }
   smfg_info_t inf{};
   inf.status = SMFG_OK;
   inf.num_pos = (int)tot.pos;
@@ -537,6 +549,12 @@ static void ensure_work(Plan &pl, int64_t need) {
   }
 }
 
+// Upper bound of the stored pivots of level l's large fronts: their width
+// (SPD: no delays), else their symbolic rows (delays may add pivots).
+static int large_pmax(const Plan &pl, int l) {
+  return l < (int)pl.lvl_large_pmax.size() ? pl.lvl_large_pmax[l] : pl.lvl_large_maxf[l];
+}
+
 static void enqueue_solve(Plan &pl, double *d_b, int nrhs, int ldb, int job, bool scaled, LaunchCount &lc) {
   DevPlan &d = pl.d;
   DevFactor &x = pl.x;
@@ -566,8 +584,13 @@ static void enqueue_solve(Plan &pl, double *d_b, int nrhs, int ldb, int job, boo
       lc.n++;
       const int nL = pl.lvl_large_ptr[l + 1] - pl.lvl_large_ptr[l];
       if (nL > 0) {
-        k_fwd_l21<<<lgrid, 256, 0, st>>>(d, x, d.lvl_large + pl.lvl_large_ptr[l], nL, wk, rows_total, nrhs);
-        lc.n++;
+        const int *lg = d.lvl_large + pl.lvl_large_ptr[l];
+        const int nb = (large_pmax(pl, l) + kSB - 1) / kSB;
+        for (int b = 0; b < nb; ++b) {
+          k_fwd_tri<<<nL, kSolveNT, 0, st>>>(d, x, lg, b, pl.posdef, xv, wk, rows_total, nrhs);
+          k_fwd_gemv<<<lgrid, 256, 0, st>>>(d, x, lg, nL, b, wk, rows_total, nrhs);
+        }
+        lc.n += 2 * nb;
       }
     }
   }
@@ -582,6 +605,15 @@ static void enqueue_solve(Plan &pl, double *d_b, int nrhs, int ldb, int job, boo
       k_bwd_front<<<m, kSolveNT, 0, st>>>(d, x, lo, pl.posdef, xv, wk, rows_total, nrhs,
                                           use_d ? 1 : 0, use_lt ? 1 : 0);
       lc.n++;
+      if (nL > 0 && use_lt) {
+        const int *lg = d.lvl_large + pl.lvl_large_ptr[l];
+        const int nb = (large_pmax(pl, l) + kSB - 1) / kSB;
+        for (int b = nb - 1; b >= 0; --b) {
+          k_bwd_dots<<<lgrid, 256, 0, st>>>(d, x, lg, nL, b, wk, rows_total, nrhs);
+          k_bwd_tri<<<nL, kSolveNT, 0, st>>>(d, x, lg, b, pl.posdef, xv, wk, rows_total, nrhs);
+        }
+        lc.n += 2 * nb;
+      }
     }
   }
   k_solve_scatter<<<g, 256, 0, st>>>(d_b, ldb, nrhs, pl.n, d.perm, sc_out, xv);

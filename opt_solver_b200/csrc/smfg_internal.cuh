@@ -73,6 +73,8 @@ struct Plan {
   std::vector<int> lvl_large_ptr;  // level l's large fronts: d.lvl_large[lvl_large_ptr[l] ..]
   std::vector<int> lvl_large_maxw; // widest large front per level
   std::vector<int> lvl_large_maxf; // largest symbolic front among them
+  std::vector<int> lvl_large_pmax; // most stored pivots among them (last factorization)
+  std::vector<int> h_lvl_large;    // host copy of the large-front lists
   int max_large = 0;
   int64_t sum_f2 = 0, sum_f = 0; // symbolic
   int max_fsym = 0;

@@ -501,93 +501,6 @@ __device__ __forceinline__ void trap_tile(int w, int rows, int cols, int &ti, in
   ti = tj + w;
 }
 
-// Deferred updates of all large fronts with one pending (ldlt_kernel.cpp:705-761).
-__global__ void __launch_bounds__(256) k_large_gemm(DevPlan P, DevFactor X, const int *__restrict__ large,
-                                                    int nlarge, const TppState *__restrict__ tpp) {
-  __shared__ double As[16][kGT], Bs[16][kGT];
-  __shared__ int pref[257];
-  __shared__ int base_front;
-  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
-  for (int chunk = 0; chunk < nlarge; chunk += 256) {
-    const int cnt = min(256, nlarge - chunk);
-    if (threadIdx.x == 0) {
-      pref[0] = 0;
-      for (int q = 0; q < cnt; ++q) {
-        const TppState &S = tpp[chunk + q];
-        int nt = 0;
-        if (S.pad[0] && S.g_p1 > S.g_p0 && S.g_e > S.g_c0) {
-          const int s = large[chunk + q];
-          nt = trap_tiles(X.sn_f[s] - S.g_c0, S.g_e - S.g_c0);
-        }
-        pref[q + 1] = pref[q] + nt;
-      }
-      base_front = chunk;
-    }
-    __syncthreads();
-    const int total = pref[cnt];
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    for (int w = blockIdx.x; w < total; w += gridDim.x) {
-      int a = 0, b = cnt;
-      while (b - a > 1) {
-        const int mid = (a + b) >> 1;
-        if (pref[mid] <= w) a = mid;
-        else b = mid;
-      }
-      const int q = base_front + a;
-      const int s = large[q];
-      const TppState S = tpp[q];
-      const int f = X.sn_f[s];
-      const size_t sf = (size_t)f;
-      double *F = X.arena + X.sn_off[s];
-      const double *W = F + sf * sf;
-      const int c0 = S.g_c0, e = S.g_e, p0 = S.g_p0, jb = S.g_p1 - S.g_p0;
-      int ti, tj;
-      trap_tile(w - pref[a], f - c0, e - c0, ti, tj);
-      const int i0 = c0 + ti * kGT, j0 = c0 + tj * kGT;
-      for (int t = threadIdx.x; t < 16 * kGT; t += 256) {
-        const int p = t / kGT, r = t % kGT;
-        double av = 0.0, bv = 0.0;
-        if (p < jb) {
-          if (i0 + r < f) av = F[(size_t)(p0 + p) * sf + i0 + r];
-          if (j0 + r < e) bv = W[(size_t)p * f + j0 + r];
-        }
-        As[p][r] = av;
-        Bs[p][r] = bv;
-      }
-      __syncthreads();
-      double c[4][4];
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int q2 = 0; q2 < 4; ++q2) {
-          const int i = i0 + tx + 16 * r, j = j0 + ty + 16 * q2;
-          c[r][q2] = (i < f && j < e && i >= j) ? F[(size_t)j * sf + i] : 0.0;
-        }
-      for (int p = 0; p < jb; ++p) {
-        double av[4], bv[4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) av[r] = As[p][tx + 16 * r];
-#pragma unroll
-        for (int q2 = 0; q2 < 4; ++q2) bv[q2] = Bs[p][ty + 16 * q2];
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-#pragma unroll
-          for (int q2 = 0; q2 < 4; ++q2)
-            if (bv[q2] != 0.0) c[r][q2] = fma(-av[r], bv[q2], c[r][q2]);
-      }
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int q2 = 0; q2 < 4; ++q2) {
-          const int i = i0 + tx + 16 * r, j = j0 + ty + 16 * q2;
-          if (i < f && j < e && i >= j) F[(size_t)j * sf + i] = c[r][q2];
-        }
-      __syncthreads();
-    }
-    __syncthreads();
-  }
-}
-
 // (L D)(j, c) of a front in global memory (fill_ld_column).
 __device__ __forceinline__ double ld_entry_g(const double *F, size_t sf, const int8_t *tags, int c, int j) {
   const double *Lc = F + (size_t)c * sf;
@@ -601,26 +514,194 @@ __device__ __forceinline__ double ld_entry_g(const double *F, size_t sf, const i
   return 0.0;
 }
 
+// One 128 x 64 tile of C -= A B^T (lower part: i >= j, i < rmax, j < cmax)
+// over K = kk pivots in order: A(i, p) = F(i, a0 + p); B(j, p) = W(j, p)
+// (deferred update) or (L D)(j, a0 + p) (Schur update). 256 threads, 8 x 4
+// entries each, K in chunks of 16 staged in shared memory with the next
+// chunk prefetched in registers. Every entry takes one fused multiply-add
+// per pivot in pivot order, a zero B(j, p) skipped, as the reference's
+// GEMM loops do.
+constexpr int kTM = 128, kTN = 64, kTK = 16;
+
+struct TileSmem {
+  double A[2][kTK][kTM];
+  double B[2][kTK][kTN];
+};
+
+template <bool SCHUR>
+__device__ __forceinline__ void tile_update(double *F, size_t sf, const double *W, int wld, const int8_t *tags,
+                                            int i0, int j0, int rmax, int cmax, int a0, int kk, TileSmem &sm) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double c[8][4];
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = i0 + tx + 16 * r, j = j0 + ty + 16 * q;
+      c[r][q] = (i < rmax && j < cmax && i >= j) ? F[(size_t)j * sf + i] : 0.0;
+    }
+  double pa[8], pb[4];
+  auto fetch = [&](int k0) {
+    const int kc = min(kTK, kk - k0);
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int t = threadIdx.x + 256 * u;
+      const int p = t / kTM, r = t % kTM;
+      pa[u] = (p < kc && i0 + r < rmax) ? F[(size_t)(a0 + k0 + p) * sf + i0 + r] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int t = threadIdx.x + 256 * u;
+      const int p = t / kTN, r = t % kTN;
+      double bv = 0.0;
+      if (p < kc && j0 + r < cmax) {
+        if (SCHUR) bv = ld_entry_g(F, sf, tags, a0 + k0 + p, j0 + r);
+        else bv = W[(size_t)(k0 + p) * wld + j0 + r];
+      }
+      pb[u] = bv;
+    }
+  };
+  auto stash = [&](int buf) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int t = threadIdx.x + 256 * u;
+      sm.A[buf][t / kTM][t % kTM] = pa[u];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int t = threadIdx.x + 256 * u;
+      sm.B[buf][t / kTN][t % kTN] = pb[u];
+    }
+  };
+  int buf = 0;
+  fetch(0);
+  __syncthreads();
+  stash(0);
+  __syncthreads();
+  for (int k0 = 0; k0 < kk; k0 += kTK) {
+    const int kc = min(kTK, kk - k0);
+    if (k0 + kTK < kk) fetch(k0 + kTK);
+    for (int p = 0; p < kc; ++p) {
+      double av[8], bv[4];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) av[r] = sm.A[buf][p][tx + 16 * r];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) bv[q] = sm.B[buf][p][ty + 16 * q];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (bv[q] != 0.0) {
+#pragma unroll
+          for (int r = 0; r < 8; ++r) c[r][q] = fma(-av[r], bv[q], c[r][q]);
+        }
+      }
+    }
+    if (k0 + kTK < kk) {
+      stash(buf ^ 1);
+      __syncthreads();
+      buf ^= 1;
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = i0 + tx + 16 * r, j = j0 + ty + 16 * q;
+      if (i < rmax && j < cmax && i >= j) F[(size_t)j * sf + i] = c[r][q];
+    }
+  __syncthreads();
+}
+
+// Tiles of a lower-trapezoidal region rows [r0, f) x cols [r0, c1): tile
+// (ti, tj) of kTM x kTN is needed when its last row reaches its first column.
+__device__ __forceinline__ int trap_tiles2(int rows, int cols) {
+  const int ct = (cols + kTN - 1) / kTN;
+  int n = 0;
+  for (int tj = 0; tj < ct; ++tj) {
+    const int first_ti = (tj * kTN) / kTM;  // tile rows from where column tile tj starts
+    n += (rows + kTM - 1) / kTM - first_ti;
+  }
+  return n;
+}
+
+__device__ __forceinline__ void trap_tile2(int w, int rows, int cols, int &ti, int &tj) {
+  const int rt = (rows + kTM - 1) / kTM;
+  tj = 0;
+  while (true) {
+    const int first = (tj * kTN) / kTM;
+    const int cnt = rt - first;
+    if (w < cnt) {
+      ti = first + w;
+      return;
+    }
+    w -= cnt;
+    ++tj;
+  }
+}
+
+// Deferred updates of all large fronts with one pending (ldlt_kernel.cpp:705-761).
+__global__ void __launch_bounds__(256) k_large_gemm(DevPlan P, DevFactor X, const int *__restrict__ large,
+                                                    int nlarge, const TppState *__restrict__ tpp) {
+  extern __shared__ __align__(16) double dsm_g[];
+  TileSmem &sm = *reinterpret_cast<TileSmem *>(dsm_g);
+  __shared__ int pref[129];
+  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  for (int chunk = 0; chunk < nlarge; chunk += 128) {
+    const int cnt = min(128, nlarge - chunk);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      pref[0] = 0;
+      for (int q = 0; q < cnt; ++q) {
+        const TppState &S = tpp[chunk + q];
+        int nt = 0;
+        if (S.pad[0] && S.g_p1 > S.g_p0 && S.g_e > S.g_c0)
+          nt = trap_tiles2(X.sn_f[large[chunk + q]] - S.g_c0, S.g_e - S.g_c0);
+        pref[q + 1] = pref[q] + nt;
+      }
+    }
+    __syncthreads();
+    const int total = pref[cnt];
+    for (int w = blockIdx.x; w < total; w += gridDim.x) {
+      int a = 0, b = cnt;
+      while (b - a > 1) {
+        const int mid = (a + b) >> 1;
+        if (pref[mid] <= w) a = mid;
+        else b = mid;
+      }
+      const int q = chunk + a;
+      const int s = large[q];
+      const TppState S = tpp[q];
+      const int f = X.sn_f[s];
+      const size_t sf = (size_t)f;
+      double *F = X.arena + X.sn_off[s];
+      int ti, tj;
+      trap_tile2(w - pref[a], f - S.g_c0, S.g_e - S.g_c0, ti, tj);
+      tile_update<false>(F, sf, F + sf * sf, f, nullptr, S.g_c0 + ti * kTM, S.g_c0 + tj * kTN, f, S.g_e,
+                         S.g_p0, S.g_p1 - S.g_p0, sm);
+    }
+  }
+}
+
 // Schur updates of all large fronts of a level (schur_update,
 // ldlt_kernel.cpp:820-933): F[e:f, e:f] -= L LD^T over pivots [0, k).
 __global__ void __launch_bounds__(256) k_large_schur(DevPlan P, DevFactor X, const int *__restrict__ large,
                                                      int nlarge, const TppState *__restrict__ tpp) {
-  __shared__ double As[16][kGT], Bs[16][kGT];
-  __shared__ int pref[257];
+  extern __shared__ __align__(16) double dsm_g[];
+  TileSmem &sm = *reinterpret_cast<TileSmem *>(dsm_g);
+  __shared__ int pref[129];
   if (X.counters[kCFlags] & (kFArena | kFRows)) return;
-  for (int chunk = 0; chunk < nlarge; chunk += 256) {
-    const int cnt = min(256, nlarge - chunk);
+  for (int chunk = 0; chunk < nlarge; chunk += 128) {
+    const int cnt = min(128, nlarge - chunk);
+    __syncthreads();
     if (threadIdx.x == 0) {
       pref[0] = 0;
       for (int q = 0; q < cnt; ++q) {
         const int s = large[chunk + q];
         const int e = X.sn_ne[s], f = X.sn_f[s], k = tpp[chunk + q].k;
-        pref[q + 1] = pref[q] + ((f > e && k > 0) ? trap_tiles(f - e, f - e) : 0);
+        pref[q + 1] = pref[q] + ((f > e && k > 0) ? trap_tiles2(f - e, f - e) : 0);
       }
     }
     __syncthreads();
     const int total = pref[cnt];
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     for (int w = blockIdx.x; w < total; w += gridDim.x) {
       int a = 0, b = cnt;
       while (b - a > 1) {
@@ -633,55 +714,10 @@ __global__ void __launch_bounds__(256) k_large_schur(DevPlan P, DevFactor X, con
       const int f = X.sn_f[s], e = X.sn_ne[s], kk = tpp[q].k;
       const size_t sf = (size_t)f;
       double *F = X.arena + X.sn_off[s];
-      const int8_t *tags = X.tags + X.sn_roff[s];
       int ti, tj;
-      trap_tile(w - pref[a], f - e, f - e, ti, tj);
-      const int i0 = e + ti * kGT, j0 = e + tj * kGT;
-      double c[4][4];
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int q2 = 0; q2 < 4; ++q2) {
-          const int i = i0 + tx + 16 * r, j = j0 + ty + 16 * q2;
-          c[r][q2] = (i < f && j < f && i >= j) ? F[(size_t)j * sf + i] : 0.0;
-        }
-      for (int k0 = 0; k0 < kk; k0 += 16) {
-        const int kc = min(16, kk - k0);
-        __syncthreads();
-        for (int t = threadIdx.x; t < 16 * kGT; t += 256) {
-          const int p = t / kGT, r = t % kGT;
-          double av = 0.0, bv = 0.0;
-          if (p < kc) {
-            if (i0 + r < f) av = F[(size_t)(k0 + p) * sf + i0 + r];
-            if (j0 + r < f) bv = ld_entry_g(F, sf, tags, k0 + p, j0 + r);
-          }
-          As[p][r] = av;
-          Bs[p][r] = bv;
-        }
-        __syncthreads();
-        for (int p = 0; p < kc; ++p) {
-          double av[4], bv[4];
-#pragma unroll
-          for (int r = 0; r < 4; ++r) av[r] = As[p][tx + 16 * r];
-#pragma unroll
-          for (int q2 = 0; q2 < 4; ++q2) bv[q2] = Bs[p][ty + 16 * q2];
-#pragma unroll
-          for (int r = 0; r < 4; ++r)
-#pragma unroll
-            for (int q2 = 0; q2 < 4; ++q2)
-              if (bv[q2] != 0.0) c[r][q2] = fma(-av[r], bv[q2], c[r][q2]);
-        }
-      }
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int q2 = 0; q2 < 4; ++q2) {
-          const int i = i0 + tx + 16 * r, j = j0 + ty + 16 * q2;
-          if (i < f && j < f && i >= j) F[(size_t)j * sf + i] = c[r][q2];
-        }
-      __syncthreads();
+      trap_tile2(w - pref[a], f - e, f - e, ti, tj);
+      tile_update<true>(F, sf, nullptr, 0, X.tags + X.sn_roff[s], e + ti * kTM, e + tj * kTN, f, f, 0, kk, sm);
     }
-    __syncthreads();
   }
 }
 
@@ -1021,6 +1057,44 @@ __global__ void k_solve_scatter(double *__restrict__ b, int ldb, int nrhs, int n
 // solve_backward.cpp:135-350 compute the same quantities.
 constexpr int kSolveNT = 128;
 
+// The 32 x 32 lower block L[jb:jb+nb, jb:jb+nb) staged in shared memory
+// (coalesced column reads) for the warp triangle solves below.
+template <int NT>
+__device__ __forceinline__ void load_tri32(const double *L, size_t sf, int jb, int nb, double (*Ls)[33]) {
+  __syncthreads();
+  for (int t = threadIdx.x; t < 1024; t += NT) {
+    const int r = t & 31, c = t >> 5;
+    Ls[r][c] = (r < nb && c < nb && c <= r) ? L[(size_t)(jb + c) * sf + jb + r] : 0.0;
+  }
+  __syncthreads();
+}
+
+// w[jb:jb+nb) <- L11^-1 w (unit, or non-unit for SPD): lane = row.
+__device__ __forceinline__ void tri_fwd_warp(double *w, int jb, int nb, int posdef, const double (*Ls)[33]) {
+  const int lane = threadIdx.x & 31;
+  double wi = (lane < nb) ? w[jb + lane] : 0.0;
+  for (int j = 0; j < nb; ++j) {
+    double wj = __shfl_sync(0xffffffffu, wi, j);
+    if (posdef) wj = wj / Ls[j][j];
+    if (lane == j) wi = wj;
+    if (lane > j && lane < nb) wi = fma(-Ls[lane][j], wj, wi);
+  }
+  if (lane < nb) w[jb + lane] = wi;
+}
+
+// v[jb:jb+nb) <- L11^-T v: lane = row.
+__device__ __forceinline__ void tri_bwd_warp(double *v, int jb, int nb, int posdef, const double (*Ls)[33]) {
+  const int lane = threadIdx.x & 31;
+  double vi = (lane < nb) ? v[jb + lane] : 0.0;
+  for (int j = nb - 1; j >= 0; --j) {
+    double xj = __shfl_sync(0xffffffffu, vi, j);
+    if (posdef) xj = xj / Ls[j][j];
+    if (lane == j) vi = xj;
+    if (lane < j) vi = fma(-Ls[j][lane], xj, vi);
+  }
+  if (lane < nb) v[jb + lane] = vi;
+}
+
 // Forward sweep of one level: gather, children's update vectors in child
 // order, blocked unit (indefinite) or non-unit (SPD) L11 solve, then
 // w[p:f) -= L21 w[0:p) unless the front is large.
@@ -1034,6 +1108,7 @@ __global__ void __launch_bounds__(kSolveNT) k_fwd_front(DevPlan P, DevFactor X, 
   const double *L = X.arena + X.sn_off[s];
   const size_t sf = (size_t)f;
   const bool large = P.sn_fsym[s] >= kLargeMin;
+  __shared__ double Ls[32][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int r = 0; r < nrhs; ++r) {
     double *w = wk + (int64_t)r * rows_total + roff;
@@ -1048,20 +1123,12 @@ __global__ void __launch_bounds__(kSolveNT) k_fwd_front(DevPlan P, DevFactor X, 
       for (int i = threadIdx.x; i < q; i += kSolveNT) w[cmap[i]] += u[i];
       __syncthreads();
     }
-    const int rend = large ? p : f;
+    if (large) continue;  // the block kernels (k_fwd_tri / k_fwd_gemv) go on
+    const int rend = f;
     for (int jb = 0; jb < p; jb += 32) {
       const int nb = min(32, p - jb);
-      if (warp == 0) {
-        double wi = (lane < nb) ? w[jb + lane] : 0.0;
-        for (int j = 0; j < nb; ++j) {
-          const double *Lj = L + (size_t)(jb + j) * sf;
-          double wj = __shfl_sync(0xffffffffu, wi, j);
-          if (posdef) wj = wj / Lj[jb + j];
-          if (lane == j) wi = wj;
-          if (lane > j && lane < nb) wi = fma(-Lj[jb + lane], wj, wi);
-        }
-        if (lane < nb) w[jb + lane] = wi;
-      }
+      load_tri32<kSolveNT>(L, sf, jb, nb, Ls);
+      if (warp == 0) tri_fwd_warp(w, jb, nb, posdef, Ls);
       __syncthreads();
       for (int i = jb + nb + threadIdx.x; i < rend; i += kSolveNT) {
         double acc = w[i];
@@ -1184,6 +1251,7 @@ __global__ void __launch_bounds__(kSolveNT) k_bwd_front(DevPlan P, DevFactor X, 
   const double *L = X.arena + X.sn_off[s];
   const size_t sf = (size_t)f;
   const bool large = P.sn_fsym[s] >= kLargeMin;
+  __shared__ double Ls[32][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int r = 0; r < nrhs; ++r) {
     double *v = wk + (int64_t)r * rows_total + roff;  // large: v[0:p) holds L21^T x_ext
@@ -1241,7 +1309,8 @@ __global__ void __launch_bounds__(kSolveNT) k_bwd_front(DevPlan P, DevFactor X, 
       __syncthreads();
       continue;
     }
-    if (!large) {  // v -= L21^T x_ext, warp per column
+    if (large) continue;  // the block kernels (k_bwd_dots / k_bwd_tri) go on
+    {  // v -= L21^T x_ext, warp per column
       for (int j = warp; j < p; j += kSolveNT / 32) {
         const double *Lj = L + (size_t)j * sf;
         double acc = 0.0;
@@ -1262,20 +1331,180 @@ __global__ void __launch_bounds__(kSolveNT) k_bwd_front(DevPlan P, DevFactor X, 
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (lane == 0) v[j] -= acc;
       }
-      __syncthreads();
-      if (warp == 0) {
-        double vi = (lane < nb) ? v[jb + lane] : 0.0;
-        for (int j = nb - 1; j >= 0; --j) {
-          double xj = __shfl_sync(0xffffffffu, vi, j);
-          if (posdef) xj = xj / L[(size_t)(jb + j) * sf + jb + j];
-          if (lane == j) vi = xj;
-          if (lane < j) vi = fma(-L[(size_t)(jb + lane) * sf + jb + j], xj, vi);
-        }
-        if (lane < nb) v[jb + lane] = vi;
-      }
+      load_tri32<kSolveNT>(L, sf, jb, nb, Ls);
+      if (warp == 0) tri_bwd_warp(v, jb, nb, posdef, Ls);
       __syncthreads();
     }
     for (int i = threadIdx.x; i < p; i += kSolveNT) xr[rows[i]] = v[i];
+    __syncthreads();
+  }
+}
+
+// Large fronts' L11 solves in blocks of kSB columns: one block of threads
+// per front solves the block's triangle (32-column steps), then all blocks
+// of the GPU update the rows below it (forward) or the dot products of the
+// next block's columns with the solved rows (backward).
+constexpr int kSB = 256;
+
+__global__ void __launch_bounds__(kSolveNT) k_fwd_tri(DevPlan P, DevFactor X, const int *__restrict__ large,
+                                                      int b, int posdef, double *x, double *wk,
+                                                      int64_t rows_total, int nrhs) {
+  const int s = large[blockIdx.x];
+  const int f = X.sn_f[s], p = X.sn_pstore[s];
+  const int j0 = b * kSB;
+  if (j0 >= p) return;
+  const int j1 = min(p, j0 + kSB);
+  const int64_t roff = X.sn_roff[s];
+  const int *rows = X.rows + roff;
+  const double *L = X.arena + X.sn_off[s];
+  const size_t sf = (size_t)f;
+  const int warp = threadIdx.x >> 5;
+  __shared__ double Ls[32][33];
+  for (int r = 0; r < nrhs; ++r) {
+    double *w = wk + (int64_t)r * rows_total + roff;
+    for (int jb = j0; jb < j1; jb += 32) {
+      const int nb = min(32, j1 - jb);
+      load_tri32<kSolveNT>(L, sf, jb, nb, Ls);
+      if (warp == 0) tri_fwd_warp(w, jb, nb, posdef, Ls);
+      __syncthreads();
+      for (int i = jb + nb + threadIdx.x; i < j1; i += kSolveNT) {
+        double acc = w[i];
+        for (int j = jb; j < jb + nb; ++j) acc = fma(-L[(size_t)j * sf + i], w[j], acc);
+        w[i] = acc;
+      }
+      __syncthreads();
+    }
+    double *xr = x + (int64_t)r * P.n;
+    for (int j = j0 + threadIdx.x; j < j1; j += kSolveNT) xr[rows[j]] = w[j];
+    __syncthreads();
+  }
+}
+
+// w[j1:f) -= L[j1:f, j0:j1) w[j0:j1) of each large front, rows over blocks.
+__global__ void __launch_bounds__(256) k_fwd_gemv(DevPlan P, DevFactor X, const int *__restrict__ large,
+                                                  int nlarge, int b, double *wk, int64_t rows_total,
+                                                  int nrhs) {
+  __shared__ double ws[kSB];
+  __shared__ int pref[65];
+  for (int chunk = 0; chunk < nlarge; chunk += 64) {
+    const int cnt = min(64, nlarge - chunk);
+    if (threadIdx.x == 0) {
+      pref[0] = 0;
+      for (int q = 0; q < cnt; ++q) {
+        const int s = large[chunk + q];
+        const int f = X.sn_f[s], p = X.sn_pstore[s], j1 = min(p, (b + 1) * kSB);
+        pref[q + 1] = pref[q] + ((b * kSB < p && f > j1) ? (f - j1 + 255) / 256 * nrhs : 0);
+      }
+    }
+    __syncthreads();
+    const int total = pref[cnt];
+    for (int wi = blockIdx.x; wi < total; wi += gridDim.x) {
+      int a = 0, bb = cnt;
+      while (bb - a > 1) {
+        const int mid = (a + bb) >> 1;
+        if (pref[mid] <= wi) a = mid;
+        else bb = mid;
+      }
+      const int s = large[chunk + a];
+      const int f = X.sn_f[s], p = X.sn_pstore[s];
+      const int j0 = b * kSB, j1 = min(p, j0 + kSB);
+      const int nchunks = (f - j1 + 255) / 256;
+      const int item = wi - pref[a];
+      const int r = item / nchunks, rc = item % nchunks;
+      double *w = wk + (int64_t)r * rows_total + X.sn_roff[s];
+      const double *L = X.arena + X.sn_off[s];
+      const size_t sf = (size_t)f;
+      __syncthreads();
+      for (int t = threadIdx.x; t < j1 - j0; t += 256) ws[t] = w[j0 + t];
+      __syncthreads();
+      const int i = j1 + rc * 256 + threadIdx.x;
+      if (i < f) {
+        double acc = w[i];
+        for (int j = j0; j < j1; ++j) acc = fma(-L[(size_t)j * sf + i], ws[j - j0], acc);
+        w[i] = acc;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// v[j] -= sum_{i in [j1, p)} L(i, j) v[i] for the columns j of block b of
+// each large front (warp per column; the rows below are solved).
+__global__ void __launch_bounds__(256) k_bwd_dots(DevPlan P, DevFactor X, const int *__restrict__ large,
+                                                  int nlarge, int b, double *wk, int64_t rows_total,
+                                                  int nrhs) {
+  __shared__ int pref[65];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int chunk = 0; chunk < nlarge; chunk += 64) {
+    const int cnt = min(64, nlarge - chunk);
+    if (threadIdx.x == 0) {
+      pref[0] = 0;
+      for (int q = 0; q < cnt; ++q) {
+        const int s = large[chunk + q];
+        const int p = X.sn_pstore[s], j0 = b * kSB, j1 = min(p, j0 + kSB);
+        pref[q + 1] = pref[q] + ((j0 < p && j1 < p) ? (j1 - j0 + 7) / 8 * nrhs : 0);
+      }
+    }
+    __syncthreads();
+    const int total = pref[cnt];
+    for (int wi = blockIdx.x; wi < total; wi += gridDim.x) {
+      int a = 0, bb = cnt;
+      while (bb - a > 1) {
+        const int mid = (a + bb) >> 1;
+        if (pref[mid] <= wi) a = mid;
+        else bb = mid;
+      }
+      const int s = large[chunk + a];
+      const int f = X.sn_f[s], p = X.sn_pstore[s];
+      const int j0 = b * kSB, j1 = min(p, j0 + kSB);
+      const int ncc = (j1 - j0 + 7) / 8;
+      const int item = wi - pref[a];
+      const int r = item / ncc, cc = item % ncc;
+      const int j = j0 + cc * 8 + warp;
+      if (j < j1) {
+        double *v = wk + (int64_t)r * rows_total + X.sn_roff[s];
+        const double *Lj = X.arena + X.sn_off[s] + (size_t)j * f;
+        double acc = 0.0;
+        for (int i = j1 + lane; i < p; i += 32) acc = fma(Lj[i], v[i], acc);
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) v[j] -= acc;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kSolveNT) k_bwd_tri(DevPlan P, DevFactor X, const int *__restrict__ large,
+                                                      int b, int posdef, double *x, double *wk,
+                                                      int64_t rows_total, int nrhs) {
+  const int s = large[blockIdx.x];
+  const int f = X.sn_f[s], p = X.sn_pstore[s];
+  const int j0 = b * kSB;
+  if (j0 >= p) return;
+  const int j1 = min(p, j0 + kSB);
+  const int64_t roff = X.sn_roff[s];
+  const int *rows = X.rows + roff;
+  const double *L = X.arena + X.sn_off[s];
+  const size_t sf = (size_t)f;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ double Ls[32][33];
+  for (int r = 0; r < nrhs; ++r) {
+    double *v = wk + (int64_t)r * rows_total + roff;
+    for (int je = j1; je > j0; je -= 32) {
+      const int jb = max(j0, je - 32), nb = je - jb;
+      for (int j = jb + warp; j < je; j += kSolveNT / 32) {
+        const double *Lj = L + (size_t)j * sf;
+        double acc = 0.0;
+        for (int i = je + lane; i < j1; i += 32) acc = fma(Lj[i], v[i], acc);
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) v[j] -= acc;
+      }
+      load_tri32<kSolveNT>(L, sf, jb, nb, Ls);
+      if (warp == 0) tri_bwd_warp(v, jb, nb, posdef, Ls);
+      __syncthreads();
+    }
+    double *xr = x + (int64_t)r * P.n;
+    for (int j = j0 + threadIdx.x; j < j1; j += kSolveNT) xr[rows[j]] = v[j];
     __syncthreads();
   }
 }
