@@ -170,6 +170,24 @@ SMFG_API int smfg_factor_export(smfg_plan_t plan, int *f, int *p, int64_t *blk_o
 SMFG_API int smfg_residual(smfg_plan_t plan, const double *b, const double *x, int nrhs, double *r,
                            double *eta_inf, double *omega);
 
+/* smfg_residual for callers that cannot allocate memory. Not a counterpart
+ * of any reference interface: smf has no such entry point. Some callers may
+ * not allocate device memory while they run, such as an interior-point
+ * iteration captured into a CUDA graph (an allocation there breaks the
+ * capture) or a real-time controller that does all its allocation up front.
+ * smfg_residual allocates its scratch per call; this variant takes device
+ * buffers (b, x and r: n x nrhs, leading dimension n; r may be NULL) and
+ * works in a fixed scratch array compiled into the library, sized for
+ * n <= SMFG_NOALLOC_MAX_N (262,144: 6 MB that every GPU loading the library
+ * keeps until the process exits). A larger plan is rejected with
+ * SMFG_ERR_INVALID_ARG. The first call on a device looks up the array's
+ * device address, so make it before any stream capture. All calls share the
+ * one array: calls that overlap on the GPU (other threads or streams) race,
+ * so serialize them. Synchronizes the plan's stream. */
+#define SMFG_NOALLOC_MAX_N 262144
+SMFG_API int smfg_residual_noalloc(smfg_plan_t plan, const double *d_b, const double *d_x, double *d_r,
+                                   int nrhs, double *eta_inf, double *omega);
+
 /* Iterative refinement (classical, refinement.cpp:316-413) of x for b, host
  * arrays (n x nrhs, leading dimension n): at most max_steps solves, stopping
  * at eta_inf <= 1e-10 and omega <= omega_target. */

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <stdexcept>
 #include <vector>
@@ -900,6 +901,87 @@ static void device_residual(Plan &pl, const double *db, const double *dx, double
   SMFG_CUDA(cudaFreeAsync(mx, pl.stream));
   *eta = e_max;
   *omega = o_max;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Residual without allocation. Its scratch (the permuted copies of x, b and
+// r for one right-hand side, and the five maxima) lives in this file-scope
+// device array, which every GPU that loads the library holds until the
+// process exits. Host code cannot use the array's name as a device address,
+// so each device's address is looked up once with cudaGetSymbolAddress and
+// passed to the kernels.
+namespace {
+
+constexpr int kNoAllocMaxN = SMFG_NOALLOC_MAX_N;
+constexpr size_t kNoAllocDoubles = 3 * (size_t)kNoAllocMaxN + 8;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[kMaxDevices] = {};
+
+// The calling thread's current device must be `dev`.
+double *noalloc_scratch(int dev) {
+  if (dev < 0 || dev >= kMaxDevices) throw std::invalid_argument("device index");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    SMFG_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_ptr[dev] = static_cast<double *>(p);
+  }
+  return g_noalloc_ptr[dev];
+}
+
+}  // namespace
+
+extern "C" {
+
+SMFG_API int smfg_residual_noalloc(smfg_plan_t plan, const double *d_b, const double *d_x, double *d_r,
+                                   int nrhs, double *eta_inf, double *omega) {
+  if (!plan || !d_b || !d_x || nrhs < 1) return SMFG_ERR_INVALID_ARG;
+  Plan &pl = plan->pl;
+  if (pl.n > kNoAllocMaxN) {
+    set_last_error("smfg_residual_noalloc: matrix order exceeds SMFG_NOALLOC_MAX_N");
+    return SMFG_ERR_INVALID_ARG;
+  }
+  try {
+    SMFG_CUDA(cudaSetDevice(pl.device));
+    clear_stale_error();
+    double *sc = noalloc_scratch(pl.device);
+    const size_t n = (size_t)pl.n;
+    double *xp = sc, *bp = sc + n, *rp = sc + 2 * n;
+    unsigned long long *mx = reinterpret_cast<unsigned long long *>(sc + 3 * (size_t)kNoAllocMaxN);
+    const int sms = sm_count(pl.device);
+    const int g = (int)std::max<int64_t>(1, std::min<int64_t>(4 * sms, ((int64_t)n + 255) / 256));
+    const int rg = (int)std::max<int64_t>(1, std::min<int64_t>(8 * sms, ((int64_t)n + 7) / 8));
+    double e_max = 0.0, o_max = 0.0;
+    for (int r = 0; r < nrhs; ++r) {
+      // the maxima start from zero on every call (the array keeps the last
+      // call's contents)
+      SMFG_CUDA(cudaMemsetAsync(mx, 0, sizeof(unsigned long long) * 8, pl.stream));
+      k_solve_gather<<<g, 256, 0, pl.stream>>>(d_x + r * n, (int)n, 1, (int)n, pl.d.perm, nullptr, xp);
+      k_solve_gather<<<g, 256, 0, pl.stream>>>(d_b + r * n, (int)n, 1, (int)n, pl.d.perm, nullptr, bp);
+      k_residual<<<rg, 256, 0, pl.stream>>>(pl.d, pl.x.pv_raw, xp, bp, rp, (int)n, mx);
+      if (d_r) k_solve_scatter<<<g, 256, 0, pl.stream>>>(d_r + r * n, (int)n, 1, (int)n, pl.d.perm, nullptr, rp);
+      SMFG_CUDA(cudaGetLastError());
+      unsigned long long h[5];
+      SMFG_CUDA(cudaMemcpyAsync(h, mx, sizeof(h), cudaMemcpyDeviceToHost, pl.stream));
+      SMFG_CUDA(cudaStreamSynchronize(pl.stream));
+      double v[5];
+      for (int i = 0; i < 5; ++i) std::memcpy(&v[i], &h[i], 8);
+      const double den = v[1] * v[2] + v[3];
+      e_max = std::max(e_max, den > 0 ? v[0] / den : (v[0] == 0 ? 0.0 : INFINITY));
+      o_max = std::max(o_max, v[4]);
+    }
+    if (eta_inf) *eta_inf = e_max;
+    if (omega) *omega = o_max;
+    return SMFG_OK;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return SMFG_ERR_CUDA;
+  }
 }
 
 SMFG_API int smfg_residual(smfg_plan_t plan, const double *b, const double *x, int nrhs, double *r,

@@ -22,6 +22,7 @@ SMFG_OK = 0
 SMFG_ERR_SINGULAR = 2
 SOLVE_FULL, SOLVE_FORWARD, SOLVE_DIAGONAL, SOLVE_BACKWARD = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
+NOALLOC_MAX_N = 262144  # SMFG_NOALLOC_MAX_N
 
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
@@ -117,6 +118,9 @@ def lib():
         L.smfg_refine.argtypes = [C.c_void_p, _f64p, _f64p, C.c_int, C.c_int, C.c_double,
                                   C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int)]
         L.smfg_refine.restype = C.c_int
+        L.smfg_residual_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                            C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.smfg_residual_noalloc.restype = C.c_int
         L.smfg_error_string.argtypes = [C.c_int]
         L.smfg_error_string.restype = C.c_char_p
         L.smfg_last_error.argtypes = []
@@ -383,6 +387,22 @@ class Solver:
         if rc != SMFG_OK:
             raise SmfgError(rc, "smfg_residual")
         return r, eta.value, om.value
+
+    def residual_noalloc(self, d_b, d_x, d_r=None):
+        """smfg_residual_noalloc: the residual of device buffers (CUDA
+        tensors, shape (n,) or (nrhs, n)) computed without allocating
+        anything, for callers that may not allocate (a loop captured into a
+        CUDA graph, a real-time controller). Returns (eta_inf, omega); r is
+        written to d_r when given. The plan's order must not exceed
+        NOALLOC_MAX_N."""
+        nrhs = 1 if d_b.dim() == 1 else int(d_b.shape[0])
+        eta, om = C.c_double(), C.c_double()
+        rc = lib().smfg_residual_noalloc(self._h, C.c_void_p(d_b.data_ptr()), C.c_void_p(d_x.data_ptr()),
+                                         None if d_r is None else C.c_void_p(d_r.data_ptr()), nrhs,
+                                         C.byref(eta), C.byref(om))
+        if rc != SMFG_OK:
+            raise SmfgError(rc, "smfg_residual_noalloc")
+        return eta.value, om.value
 
     def refine(self, b, x, max_steps: int = 10, omega_target: float = 1e-8):
         b = np.ascontiguousarray(b, dtype=np.float64)
