@@ -8,7 +8,7 @@ analysis, one right-hand side uniform in [-1, 1]. One step = numeric
 factorization of the values + one solve.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--config spd3d|lap2d|traj|kkt] [--precision fp64|mixed]
+                  [--config spd3d|spd3d40|lap2d|traj|kkt|batch] [--precision fp64|mixed]
 
 `value` is device time (CUDA events on the engine's stream) with the
 inputs already in HBM; `e2e` is the same step through the C ABI with host
@@ -39,7 +39,64 @@ CONFIGS = {
     "kkt": ("IPM KKT 20^3 + 4,000 constraints (n=12,000), 1 RHS", "kkt_ipm(20, 4000)", False, 1),
     # the same generator as spd3d at 40^3: the small case of the ncu captures
     "spd3d40": ("SPD variable-coefficient 7-point 40^3 (n=64,000), 1 RHS", "varcoef_3d(40)", True, 1),
+    # configuration 4: 1,024 trajectory KKTs (T uniform in 10..200) in one batch
+    "batch": ("1,024 trajectory KKT systems, T in {10..200} (n = 28T + 12 each), 8 RHS each",
+              "trajectory_batch(1024)", False, 8),
 }
+BATCH_COUNT = 1024
+
+
+def batch_systems(rank: int = 0, world: int = 1):
+    """This rank's contiguous share of configuration 4's systems."""
+    from opt_solver_b200 import workloads as W
+    mats = W.trajectory_batch(BATCH_COUNT, seed=0)
+    lo = rank * BATCH_COUNT // world
+    hi = (rank + 1) * BATCH_COUNT // world
+    return mats[lo:hi]
+
+
+class _Workload:
+    """One system (Solver) or a batch of systems merged into one forest
+    (BatchSolver), with its values and right-hand sides."""
+
+    def __init__(self, cfg, device, rank=0, world=1):
+        from opt_solver_b200 import smfg
+        from opt_solver_b200 import workloads as W
+        from opt_solver_b200.batch import BatchSolver
+        self.desc, _, self.posdef, self.nrhs = CONFIGS[cfg]
+        t0 = time.time()
+        if cfg == "batch":
+            mats = batch_systems(rank, world)
+            ans = [smfg.analyse(n, cp, ri) for n, cp, ri, v in mats]
+            self.analyse_s = time.time() - t0
+            self.solver = BatchSolver(ans, device=device)
+            self.values = np.concatenate([m[3] for m in mats])
+            self.b = self.solver.stack_rhs([W.rhs(m[0], self.nrhs, seed=i, kind="normal")
+                                            for i, m in enumerate(mats)])
+            self.n = self.solver.n
+            self.nnz = int(sum(int(m[1][-1]) for m in mats))
+            self.nsn = self.solver.merged.nsn
+            self.systems = len(mats)
+            self.sv = self.solver.solver
+            self.expected = [(16 * ((m[0] - 12) // 28) + 12, 12 * ((m[0] - 12) // 28), 0) for m in mats]
+        else:
+            n, cp, ri, v = build_matrix(cfg)
+            a = smfg.analyse(n, cp, ri)
+            self.analyse_s = time.time() - t0
+            self.sv = smfg.Solver(a, device=device)
+            self.solver = self.sv
+            self.values = v
+            self.b = W.rhs(n, self.nrhs, seed=1)
+            self.n = n
+            self.nnz = int(cp[-1])
+            self.nsn = a.nsn
+            self.systems = 1
+            self.expected = None
+
+    def inertia_ok(self):
+        if self.expected is None:
+            return True
+        return [s[:3] for s in self.solver.system_stats()] == self.expected
 
 
 def build_matrix(cfg: str):
@@ -58,11 +115,16 @@ def build_matrix(cfg: str):
 
 
 def sample_matrix(cfg: str):
-    """The bounded CPU sample of each workload (reference on the host cores)."""
+    """The bounded CPU sample of each workload (reference on the host cores):
+    (list of matrices, description, factor to scale the time to the full
+    workload or None to scale by the reference's delay-free flop counts)."""
     from opt_solver_b200 import workloads as W
     if cfg == "spd3d":
-        return W.varcoef_3d(32, seed=0), "varcoef_3d(32) (n=32,768), same generator"
-    return build_matrix(cfg), "the full workload"
+        return [W.varcoef_3d(32, seed=0)], "varcoef_3d(32) (n=32,768), same generator", None
+    if cfg == "batch":
+        mats = batch_systems()[:64]
+        return mats, "the first 64 of the 1,024 systems, one smf analyse/factor/solve each", BATCH_COUNT / 64
+    return [build_matrix(cfg)], "the full workload", 1.0
 
 
 def dist_init():
@@ -187,19 +249,13 @@ def dgemm_peak_tflops():
 def run_ours(args, rank, world, local):
     import torch
     from opt_solver_b200 import smfg
-    from opt_solver_b200 import workloads as W
 
     torch.cuda.set_device(local)
-    desc, _, posdef, nrhs = CONFIGS[args.config]
-    n, cp, ri, v = build_matrix(args.config)
-    t0 = time.time()
-    a = smfg.analyse(n, cp, ri)
-    analyse_s = time.time() - t0
-    sv = smfg.Solver(a, device=local)
+    wl = _Workload(args.config, local, rank, world)
+    sv, posdef = wl.sv, wl.posdef
     prec = smfg.PREC_MIXED if args.precision == "mixed" else smfg.PREC_FP64
-    b = W.rhs(n, nrhs, seed=1)
-    d_vals = torch.from_numpy(np.ascontiguousarray(v)).cuda()
-    d_b0 = torch.from_numpy(np.ascontiguousarray(b)).cuda()
+    d_vals = torch.from_numpy(np.ascontiguousarray(wl.values)).cuda()
+    d_b0 = torch.from_numpy(np.ascontiguousarray(wl.b)).cuda()
     d_b = d_b0.clone()
 
     def step():
@@ -220,49 +276,63 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize()
     barrier(world)
     ms_step = allmax(sum(dev_ms) / len(dev_ms), world)
+    inertia_ok = wl.inertia_ok()
     # e2e: host buffers through the C ABI (copies inside the timed region)
     e2e = []
     for _ in range(max(2, min(args.steps, 5))):
         torch.cuda.synchronize()
         t = time.perf_counter()
-        sv.factor(v, posdef=posdef, precision=prec)
-        x = sv.solve(b)
+        sv.factor(wl.values, posdef=posdef, precision=prec)
+        x = sv.solve(wl.b)
         e2e.append((time.perf_counter() - t) * 1e3)
     e2e_ms = allmax(sum(e2e) / len(e2e), world)
-    # accuracy of the last solve
-    _, eta, om = sv.residual(b, x)
-    info = sv.info
+    _, eta, om = sv.residual(wl.b, x)
     out = {
-        "ms_per_step": ms_step, "info": info, "eta": eta, "omega": om, "analyse_s": analyse_s,
-        "e2e_ms": e2e_ms, "n": n, "nnz": int(cp[-1]), "nrhs": nrhs, "desc": desc,
-        "clocks": clk.summary(), "nsn": a.nsn,
-        "h2d": int(cp[-1]) * 8 + n * nrhs * 8, "d2h": n * nrhs * 8,
+        "ms_per_step": ms_step, "info": sv.info, "eta": eta, "omega": om,
+        "analyse_s": wl.analyse_s, "e2e_ms": e2e_ms, "n": wl.n, "nnz": wl.nnz, "nrhs": wl.nrhs,
+        "desc": wl.desc, "clocks": clk.summary(), "nsn": wl.nsn, "systems": wl.systems,
+        "inertia_ok": inertia_ok,
+        "h2d": wl.nnz * 8 + wl.n * wl.nrhs * 8, "d2h": wl.n * wl.nrhs * 8,
     }
-    # roofline pass (untimed): per-kernel device time of the large-front
-    # GEMMs with their algorithmic flops
     prof = sv.profile_factor(d_vals, posdef=posdef, precision=prec)
     out["profile"] = prof
+    out["info"] = info
     return out
 
 
-def cpu_reference_sample(cfg, threads):
+def cpu_reference_ms(cfg, threads):
     """The reference smf solver (oracle/_ref, compiled from its sources) on
-    the host cores: its own analysis, fastest host mode, one bounded sample."""
+    the host cores, fastest host mode (non-deterministic, `threads` threads,
+    its own analysis: METIS on the 3D grid, its automatic choice otherwise;
+    LAPACK-style SPD fronts): factor + solve ms of a bounded sample, scaled to
+    the full workload. Returns (ms, sample description)."""
     from oracle import oracle as O
     from opt_solver_b200 import workloads as W
-    (n, cp, ri, v), sample = sample_matrix(cfg)
+    mats, sample, scale = sample_matrix(cfg)
     posdef = CONFIGS[cfg][2]
-    ordering = O.ORDER_METIS if cfg == "spd3d" else O.ORDER_AUTO_PARALLEL
-    ref = O.Reference(posdef=posdef, ordering=ordering, deterministic=False, num_threads=threads,
-                      scaling=O.SCALE_AUTO, posdef_kernel=O.POSDEF_KERNEL_LAPACK)
-    a = ref.analyse(n, cp, ri, v)
     nrhs = CONFIGS[cfg][3]
-    b = W.rhs(n, nrhs, seed=1)
-    t = time.perf_counter()
-    fx = ref.factor(v)
-    _x, _ = ref.solve(b)
-    ms = (time.perf_counter() - t) * 1e3
-    return ms, fx.flops, sample, a
+    ordering = O.ORDER_METIS if cfg.startswith("spd3d") else O.ORDER_AUTO_PARALLEL
+    total = 0.0
+    analyses = []
+    for i, (n, cp, ri, v) in enumerate(mats):
+        ref = O.Reference(posdef=posdef, ordering=ordering, deterministic=False, num_threads=threads,
+                          scaling=O.SCALE_AUTO, posdef_kernel=O.POSDEF_KERNEL_LAPACK)
+        a = ref.analyse(n, cp, ri, v)
+        analyses.append(a)
+        b = W.rhs(n, nrhs, seed=i, kind="normal")
+        t = time.perf_counter()
+        ref.factor(v, export=False)
+        ref.solve(b)
+        total += (time.perf_counter() - t) * 1e3
+    if scale is None:
+        n, cp, ri, v = build_matrix(cfg)
+        ref = O.Reference(posdef=posdef, ordering=ordering, deterministic=False, num_threads=threads)
+        a_full = ref.analyse(n, cp, ri, v)
+        scale = delay_free_flops(a_full) / max(delay_free_flops(analyses[0]), 1.0)
+        sample += f"; time x{scale:.2f} (the reference's delay-free flops, full / sample)"
+    elif scale != 1.0:
+        sample += f"; time x{scale:.0f}"
+    return total * scale, sample
 
 
 def delay_free_flops(a):
@@ -283,36 +353,24 @@ def run_reference_arm(args, rank, world):
     if not O.ref_available():
         return {"impl": "reference", "unavailable": "oracle/_ref not built (no /root/reference at build time)"}
     threads = os.cpu_count() or 1
-    cfg = args.config
     times = []
-    flops_s = None
+    sample = ""
     for i in range(args.warmup + args.steps):
-        ms, flops_s, sample, a_s = cpu_reference_sample(cfg, threads)
+        ms, sample = cpu_reference_ms(args.config, threads)
         if i >= args.warmup:
             times.append(ms)
-    scale = 1.0
-    if cfg == "spd3d":
-        # extrapolate the sample to the full workload by the reference's own
-        # delay-free flop counts of both analyses
-        n, cp, ri, v = build_matrix(cfg)
-        ref = O.Reference(posdef=True, ordering=O.ORDER_METIS, deterministic=False, num_threads=threads)
-        a_full = ref.analyse(n, cp, ri, v)
-        scale = delay_free_flops(a_full) / max(delay_free_flops(a_s), 1.0)
-    ms_step = statistics.median(times) * scale
-    desc = CONFIGS[cfg][0]
-    line = {
+    ms_step = statistics.median(times)
+    desc = CONFIGS[args.config][0]
+    return {
         "impl": "reference", "metric": "factor+solve ms", "value": ms_step, "unit": "ms",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generators of the configuration)",
         "config": {"workload": desc, "precision": "fp64"},
         "cpu_baseline": {"value": ms_step, "unit": "ms", "cores": threads, "kind": "reference",
-                         "sample": f"{sample}; reference smf (oracle/_ref) non-deterministic, "
-                                   f"{threads} threads, METIS, LAPACK-style SPD fronts; "
-                                   f"time x{scale:.2f} (delay-free flops full / sample)"},
+                         "sample": sample},
         "e2e": {"value": ms_step, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    return line
 
 
 def ncu_step(args):
@@ -320,20 +378,16 @@ def ncu_step(args):
     command the committed ncu launch lists are taken from."""
     import torch
     from opt_solver_b200 import smfg
-    from opt_solver_b200 import workloads as W
-    _desc, _, posdef, nrhs = CONFIGS[args.config]
-    n, cp, ri, v = build_matrix(args.config)
-    a = smfg.analyse(n, cp, ri)
-    sv = smfg.Solver(a, device=0)
+    wl = _Workload(args.config, 0)
     prec = smfg.PREC_MIXED if args.precision == "mixed" else smfg.PREC_FP64
-    d_vals = torch.from_numpy(np.ascontiguousarray(v)).cuda()
-    d_b = torch.from_numpy(np.ascontiguousarray(W.rhs(n, nrhs, seed=1))).cuda()
-    info = sv.factor(d_vals, posdef=posdef, precision=prec)
+    d_vals = torch.from_numpy(np.ascontiguousarray(wl.values)).cuda()
+    d_b = torch.from_numpy(np.ascontiguousarray(wl.b)).cuda()
+    info = wl.sv.factor(d_vals, posdef=wl.posdef, precision=prec)
     fl = info.kernel_launches
-    sv.solve(d_b)
+    wl.sv.solve(d_b)
     torch.cuda.synchronize()
-    print(json.dumps({"factor_launches": fl, "solve_launches": sv.info.kernel_launches,
-                      "factor_ms": info.factor_ms, "solve_ms": sv.info.solve_ms}), flush=True)
+    print(json.dumps({"factor_launches": fl, "factor_ms": info.factor_ms,
+                      "solve_ms": wl.sv.info.solve_ms}), flush=True)
 
 
 def main():
@@ -364,50 +418,60 @@ def main():
     info = r["info"]
     peaks = measured_peaks()
     prof = r["profile"]
-    dpeak = dgemm_peak_tflops()
-    achieved = prof["gemm_flops"] / (prof["gemm_ms"] * 1e-3) / 1e12 if prof["gemm_ms"] > 0 else 0.0
-    roof = {
-        "kernel": "k_large_gemm + k_large_schur (FP64 FMA tile GEMMs of the large fronts)",
-        "bound": "tensor", "achieved": achieved, "peak": dpeak, "unit": "TFLOP/s",
-        "frac": achieved / dpeak if dpeak else None, "traffic": None,
-        "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (FP64 is not in MEASURED_PEAKS.json)",
-        "launches": prof["gemm_launches"], "avg_launch_ms": prof["gemm_ms"] / max(prof["gemm_launches"], 1),
-        "algorithmic_flops_per_launch": prof["gemm_flops"] / max(prof["gemm_launches"], 1),
-    }
+    if prof["gemm_ms"] > 0:
+        dpeak = dgemm_peak_tflops()
+        achieved = prof["gemm_flops"] / (prof["gemm_ms"] * 1e-3) / 1e12
+        roof = {
+            "kernel": "k_large_gemm + k_large_schur (FP64 FMA tile GEMMs of the large fronts)",
+            "bound": "tensor", "achieved": achieved, "peak": dpeak, "unit": "TFLOP/s",
+            "frac": achieved / dpeak if dpeak else None, "traffic": None,
+            "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (FP64 is not in MEASURED_PEAKS.json)",
+            "launches": prof["gemm_launches"], "avg_launch_ms": prof["gemm_ms"] / max(prof["gemm_launches"], 1),
+            "algorithmic_flops_per_launch": prof["gemm_flops"] / max(prof["gemm_launches"], 1),
+        }
+    else:
+        # no large fronts (the batch of small systems): the factor as a
+        # whole against HBM, its algorithmic bytes the front arena written by
+        # assembly and read + written by the front kernels (3 passes)
+        hbm = peaks.get("hbm_gbs") or 6650.0
+        achieved = 3.0 * prof.get("arena_bytes", 0.0) / (info.factor_ms * 1e-3) / 1e9 if info.factor_ms else 0.0
+        roof = {
+            "kernel": "whole factorization (level kernels of small fronts)", "bound": "hbm",
+            "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks.get("hbm_gbs") else "fallback 6650 GB/s",
+            "algorithmic_bytes_per_factor": 3.0 * prof.get("arena_bytes", 0.0),
+        }
     cpu = None
     if not args.no_cpu_baseline:
         try:
             from oracle import oracle as O
             if O.ref_available():
                 threads = os.cpu_count() or 1
-                ms, _fl, sample, a_s = cpu_reference_sample(args.config, threads)
-                scale = 1.0
-                if args.config == "spd3d":
-                    n, cp, ri, v = build_matrix(args.config)
-                    ref = O.Reference(posdef=True, ordering=O.ORDER_METIS, deterministic=False,
-                                      num_threads=threads)
-                    a_full = ref.analyse(n, cp, ri, v)
-                    scale = delay_free_flops(a_full) / max(delay_free_flops(a_s), 1.0)
-                cpu = {"value": ms * scale, "unit": "ms", "cores": threads, "kind": "reference",
-                       "sample": f"{sample}; reference smf (oracle/_ref), non-deterministic, "
-                                 f"{threads} threads, METIS; x{scale:.2f} by delay-free flops"}
+                ms, sample = cpu_reference_ms(args.config, threads)
+                cpu = {"value": ms, "unit": "ms", "cores": threads, "kind": "reference",
+                       "sample": sample}
         except Exception as exc:  # noqa: BLE001
             cpu = {"value": None, "unit": "ms", "cores": 0, "kind": "reference", "sample": f"failed: {exc}"}
+    batch = args.config == "batch"
     line = {
         "metric": "factor+solve ms", "value": r["ms_per_step"], "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
-        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": False, "scaling": "strong" if batch else "weak", "vs_baseline": None,
+        "dtype": "f64",
         "data": "synthetic (seeded generator of the configuration)",
         "config": {"workload": r["desc"], "n": r["n"], "nnz_lower": r["nnz"], "nrhs": r["nrhs"],
-                   "supernodes": r["nsn"], "analysis": "engine nested dissection (smfg_analyse)",
-                   "precision": args.precision, "parallelism": "replicas" if world > 1 else "1 GPU",
+                   "supernodes": r["nsn"], "systems_this_rank": r["systems"],
+                   "analysis": "engine nested dissection (smfg_analyse)",
+                   "precision": args.precision,
+                   "parallelism": ("systems sharded over ranks" if batch else "replicas") if world > 1 else "1 GPU",
                    "l2": "inputs larger than L2 (front arena %.1f GB)" % (prof.get("arena_bytes", 0) / 1e9)},
         "e2e": {"value": r["e2e_ms"], "unit": "ms", "h2d_bytes_per_step": r["h2d"],
                 "d2h_bytes_per_step": r["d2h"]},
         "gpu_launches": int(info.kernel_launches),
         "factor_ms": info.factor_ms, "solve_ms": info.solve_ms, "flops": info.flops,
         "gflops": info.flops / (info.factor_ms * 1e-3) / 1e9 if info.factor_ms else None,
-        "inertia": list(info.inertia), "eta_inf": r["eta"], "omega": r["omega"],
+        "inertia": list(info.inertia), "inertia_exact_per_system": r["inertia_ok"],
+        "eta_inf": r["eta"], "omega": r["omega"],
         "roofline": roof, "cpu_baseline": cpu, "clocks": r["clocks"],
         "measured_peaks": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops")},
     }

@@ -165,6 +165,13 @@ SMFG_API int smfg_factor_sizes(smfg_plan_t plan, int64_t *block_entries, int64_t
 SMFG_API int smfg_factor_export(smfg_plan_t plan, int *f, int *p, int64_t *blk_off, double *blocks,
                                 int64_t *row_off, int *rows, int8_t *tags);
 
+/* Per-front counts of the last factorization: stats[5 s .. 5 s + 4] =
+ * positive, negative and zero pivots, 2x2 pivots, delayed columns passed to
+ * the parent (the per-front parts of Info's counts). Lets a caller that
+ * factors many independent systems as one forest read each system's
+ * inertia. */
+SMFG_API int smfg_front_stats(smfg_plan_t plan, int *stats);
+
 /* Residual r = b - A x and backward errors against the factored values
  * (refinement.cpp:39-130; compensated FP64 on the device). Host arrays. */
 SMFG_API int smfg_residual(smfg_plan_t plan, const double *b, const double *x, int nrhs, double *r,

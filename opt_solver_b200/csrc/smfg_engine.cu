@@ -362,7 +362,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
     const int asm_grid = std::max(1, std::min(4 * sms, m * 64));
     k_level_assemble<<<asm_grid, 256, 0, st>>>(d, x, lo, hi, l);
     k_factor<32, 1, kSmallMax, true><<<m, 32, smem_s, st>>>(d, x, lo, hi, prm);
-    k_factor<256, kSmallMax + 1, kMediumMax, true><<<m, 256, smem_m, st>>>(d, x, lo, hi, prm);
+    k_factor<128, kSmallMax + 1, kMediumMax, true><<<m, 128, smem_m, st>>>(d, x, lo, hi, prm);
     k_factor<512, kMediumMax + 1, 1 << 30, false><<<m, 512, 0, st>>>(d, x, lo, hi, prm);
     lc.n += 6;
     const int nL = pl.lvl_large_ptr[l + 1] - pl.lvl_large_ptr[l];
@@ -432,7 +432,7 @@ static void set_kernel_attrs(int nb) {
   SMFG_CUDA(cudaFuncSetAttribute(k_factor<32, 1, kSmallMax, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)front_smem_bytes(kSmallMax, nb)));
-  SMFG_CUDA(cudaFuncSetAttribute(k_factor<256, kSmallMax + 1, kMediumMax, true>,
+  SMFG_CUDA(cudaFuncSetAttribute(k_factor<128, kSmallMax + 1, kMediumMax, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)front_smem_bytes(kMediumMax, nb)));
   SMFG_CUDA(cudaFuncSetAttribute(k_large_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem)));
@@ -815,6 +815,25 @@ SMFG_API int smfg_inertia(smfg_plan_t plan, int *pos, int *neg, int *zero) {
   *pos = plan->pl.info.num_pos;
   *neg = plan->pl.info.num_neg;
   *zero = plan->pl.info.num_zero;
+  return SMFG_OK;
+}
+
+SMFG_API int smfg_front_stats(smfg_plan_t plan, int *stats) {
+  if (!plan || !stats) return SMFG_ERR_INVALID_ARG;
+  Plan &pl = plan->pl;
+  try {
+    SMFG_CUDA(cudaSetDevice(pl.device));
+    std::vector<int> st(4 * (size_t)pl.nsn), dout(pl.nsn);
+    SMFG_CUDA(cudaMemcpy(st.data(), pl.x.sn_stat, sizeof(int) * st.size(), cudaMemcpyDeviceToHost));
+    SMFG_CUDA(cudaMemcpy(dout.data(), pl.x.sn_dout, sizeof(int) * dout.size(), cudaMemcpyDeviceToHost));
+    for (int s = 0; s < pl.nsn; ++s) {
+      for (int k = 0; k < 4; ++k) stats[5 * (size_t)s + k] = st[4 * (size_t)s + k];
+      stats[5 * (size_t)s + 4] = dout[s];
+    }
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return SMFG_ERR_CUDA;
+  }
   return SMFG_OK;
 }
 

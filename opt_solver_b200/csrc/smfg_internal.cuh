@@ -13,7 +13,7 @@
 namespace smfg {
 
 // Size classes of the front kernels (rows f after delays).
-constexpr int kSmallMax = 32;    // one warp, front in shared memory
+constexpr int kSmallMax = 64;    // one warp, front in shared memory
 constexpr int kMediumMax = 128;  // one block, front in shared memory
 constexpr int kAsmCols = 32;     // columns per assembly work item
 

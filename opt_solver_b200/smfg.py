@@ -121,6 +121,8 @@ def lib():
         L.smfg_residual_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                             C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.smfg_residual_noalloc.restype = C.c_int
+        L.smfg_front_stats.argtypes = [C.c_void_p, _i32p]
+        L.smfg_front_stats.restype = C.c_int
         L.smfg_error_string.argtypes = [C.c_int]
         L.smfg_error_string.restype = C.c_char_p
         L.smfg_last_error.argtypes = []
@@ -358,6 +360,14 @@ class Solver:
         if rc != SMFG_OK:
             raise SmfgError(rc, "smfg_inertia")
         return (p.value, n.value, z.value)
+
+    def front_stats(self) -> np.ndarray:
+        """(nsn, 5): positive, negative, zero, 2x2 pivots, delayed columns."""
+        st = np.zeros(5 * self.nsn, dtype=np.int32)
+        rc = lib().smfg_front_stats(self._h, st)
+        if rc != SMFG_OK:
+            raise SmfgError(rc, "smfg_front_stats")
+        return st.reshape(self.nsn, 5)
 
     def export(self) -> FrontFactor:
         be, re_ = C.c_int64(), C.c_int64()

@@ -180,11 +180,19 @@ class Reference:
         self.analyse_ms = self.L.refshim_analyse_ms(self.h)
         return a
 
-    def factor(self, values) -> FactorExport:
+    def factor(self, values, export: bool = True) -> FactorExport:
+        """Factor; with export, copy the FactorKeep out per front (needs the
+        serial engine's step layout: deterministic mode or one thread)."""
         vals = np.ascontiguousarray(values, dtype=np.float64)
         st = np.zeros(10, dtype=np.int64)
         fm = np.zeros(2, dtype=np.float64)
         self.L.refshim_factor(self.h, vals, st, fm)
+        if not export:
+            z = np.zeros(0, dtype=np.int32)
+            return FactorExport(status=int(st[0]), inertia=(int(st[1]), int(st[2]), int(st[3])),
+                                delayed=int(st[4]), two_by_two=int(st[5]), max_front=int(st[6]),
+                                flops=float(fm[0]), factor_ms=float(fm[1]), f=z, p=z, blk_off=z,
+                                blocks=np.zeros(0), row_off=z, rows=z, tags=None, scale=np.zeros(0))
         fs = np.zeros(6, dtype=np.int64)
         self.L.refshim_factor_sizes(self.h, fs)
         nsteps, fext, rows_total, _nd, _pd, nscale = (int(x) for x in fs)
