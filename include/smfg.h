@@ -213,12 +213,31 @@ SMFG_API int smfg_refine(smfg_plan_t plan, const double *b, double *x, int nrhs,
 typedef struct smfg_symbolic_s *smfg_symbolic_t;
 SMFG_API int smfg_analyse(int n, const int *col_ptr, const int *row_idx, int ordering, int nemin,
                           smfg_symbolic_t *out);
+/* The same analysis on a caller-given fill-reducing ordering (perm[new] =
+ * old, e.g. the permutation of smf's METIS analysis, AnalysisKeep::perm):
+ * elimination tree, supernodes, amalgamation and front rows are built on it.
+ * SMFG_ERR_INVALID_ARG when perm is not a permutation of 0..n-1. */
+SMFG_API int smfg_analyse_ordered(int n, const int *col_ptr, const int *row_idx, const int *perm,
+                                  int nemin, smfg_symbolic_t *out);
 /* Pointers into the analysis (valid until smfg_symbolic_free); flops: the
  * delay-free factorization flops in smf's count; factor_entries: |L|. */
 SMFG_API int smfg_symbolic_view(smfg_symbolic_t s, smfg_analysis_t *a, double *flops,
                                 int64_t *factor_entries);
 SMFG_API void smfg_symbolic_free(smfg_symbolic_t *s);
 
+/* Tensor-core symmetric rank-k update with split products: the lower
+ * triangle of the n x n matrix C minus L W^T (C, L, W in device memory,
+ * column-major; L and W n x k). Each FP64 operand is split as hi + lo in
+ * TF32 (SMFG_TC_TF32X3) or BF16 (SMFG_TC_BF16X3) and hi*hi + hi*lo + lo*hi
+ * accumulate in FP32 on the tensor cores; the sum is subtracted from C in
+ * FP64. The kernel of the mixed-precision path's trailing updates, exposed
+ * for callers and tests. No reference counterpart: smf computes this
+ * product in FP64 (schur_update, solver/src/ldlt_kernel.cpp:764-933).
+ * Synchronous on the legacy default stream of the current device. */
+#define SMFG_TC_TF32X3 0
+#define SMFG_TC_BF16X3 1
+SMFG_API int smfg_tc_update(double *d_C, int ldc, int n, const double *d_L, int ldl, const double *d_W,
+                            int ldw, int k, int kind);
 SMFG_API const char *smfg_error_string(int code);
 /* Message of the last CUDA or internal error on the calling thread. */
 SMFG_API const char *smfg_last_error(void);

@@ -19,7 +19,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsmfg.so")
 SOURCES = ["smfg_engine.cu", "smfg_analyse.cpp"]
-DEPS = ["smfg_front.cuh", "smfg_kernels.cuh", "smfg_internal.cuh"]
+DEPS = ["smfg_front.cuh", "smfg_kernels.cuh", "smfg_internal.cuh", "smfg_tc.cuh"]
 
 
 def nvcc() -> str:

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "smfg_kernels.cuh"
+#include "smfg_tc.cuh"
 
 namespace smfg {
 
@@ -1073,6 +1074,80 @@ SMFG_API int smfg_refine(smfg_plan_t plan, const double *b, double *x, int nrhs,
     if (eta_inf) *eta_inf = be;
     if (omega) *omega = bo;
     if (steps) *steps = it;
+    return SMFG_OK;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return SMFG_ERR_CUDA;
+  }
+}
+
+SMFG_API int smfg_tc_update(double *d_C, int ldc, int n, const double *d_L, int ldl, const double *d_W,
+                           int ldw, int k, int kind) {
+  if (!d_C || !d_L || !d_W || n < 0 || k < 0 || ldc < std::max(1, n) || ldl < std::max(1, n) ||
+      ldw < std::max(1, n) || (kind != SMFG_TC_TF32X3 && kind != SMFG_TC_BF16X3))
+    return SMFG_ERR_INVALID_ARG;
+  if (n == 0 || k == 0) return SMFG_OK;
+  try {
+    clear_stale_error();
+    int dev = 0;
+    SMFG_CUDA(cudaGetDevice(&dev));
+    const int sms = sm_count(dev);
+    tc::Job J{};
+    J.C = d_C;
+    J.Ls = d_L;
+    J.Ws = d_W;
+    J.tags = nullptr;
+    J.ld = ldc;
+    J.ldl = ldl;
+    J.ldw = ldw;
+    J.r0 = J.lr0 = J.wr0 = 0;
+    J.n = n;
+    J.k0 = 0;
+    J.kc = k;
+    const int ke = kind == SMFG_TC_TF32X3 ? 32 : 64;  // elements per k-block row
+    J.ntr = (n + tc::kBM - 1) / tc::kBM;
+    J.nkb = (k + ke - 1) / ke;
+    J.tiles = J.ntr * (J.ntr + 1) / 2;
+    J.img = 0;
+    const int64_t items = (int64_t)J.ntr * tc::kBM * 8 * J.nkb;
+    const int64_t ipref[2] = {0, items};
+    const int tpref[2] = {0, J.tiles};
+    const int64_t img_bytes = tc::image_bytes(J.ntr, J.nkb);
+    const size_t meta = 256 + 2 * sizeof(int64_t) + 2 * sizeof(int) + 8;
+    uint8_t *buf = nullptr;
+    cudaStream_t st = nullptr;
+    SMFG_CUDA(cudaMalloc((void **)&buf, meta + img_bytes + 256));
+    uint8_t *img = buf + ((meta + 255) / 256) * 256;
+    tc::Job *dj = reinterpret_cast<tc::Job *>(buf);
+    int64_t *dip = reinterpret_cast<int64_t *>(buf + sizeof(tc::Job) + 8);
+    int *dtp = reinterpret_cast<int *>(dip + 2);
+    unsigned long long *derr = reinterpret_cast<unsigned long long *>(dtp + 2);
+    static_assert(sizeof(tc::Job) + 8 + 2 * sizeof(int64_t) + 2 * sizeof(int) + 8 <= 256 + 2 * sizeof(int64_t) + 2 * sizeof(int) + 8, "meta");
+    SMFG_CUDA(cudaMemcpyAsync(dj, &J, sizeof(J), cudaMemcpyHostToDevice, st));
+    SMFG_CUDA(cudaMemcpyAsync(dip, ipref, sizeof(ipref), cudaMemcpyHostToDevice, st));
+    SMFG_CUDA(cudaMemcpyAsync(dtp, tpref, sizeof(tpref), cudaMemcpyHostToDevice, st));
+    SMFG_CUDA(cudaMemsetAsync(derr, 0, sizeof(unsigned long long), st));
+    const int sg = (int)std::max<int64_t>(1, std::min<int64_t>(8 * sms, (items + 255) / 256));
+    const int gg = std::max(1, std::min(J.tiles, sms));
+    const int smem = (int)sizeof(tc::Smem);
+    if (kind == SMFG_TC_TF32X3) {
+      SMFG_CUDA(cudaFuncSetAttribute(tc::k_tc_syrk<tc::kTF32x3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      tc::k_tc_split<tc::kTF32x3><<<sg, 256, 0, st>>>(dj, 1, dip, img);
+      tc::k_tc_syrk<tc::kTF32x3><<<gg, tc::kThreads, smem, st>>>(dj, 1, dtp, img, derr);
+    } else {
+      SMFG_CUDA(cudaFuncSetAttribute(tc::k_tc_syrk<tc::kBF16x3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      tc::k_tc_split<tc::kBF16x3><<<sg, 256, 0, st>>>(dj, 1, dip, img);
+      tc::k_tc_syrk<tc::kBF16x3><<<gg, tc::kThreads, smem, st>>>(dj, 1, dtp, img, derr);
+    }
+    SMFG_CUDA(cudaGetLastError());
+    unsigned long long herr = 0;
+    SMFG_CUDA(cudaMemcpyAsync(&herr, derr, sizeof(herr), cudaMemcpyDeviceToHost, st));
+    SMFG_CUDA(cudaStreamSynchronize(st));
+    SMFG_CUDA(cudaFree(buf));
+    if (herr) {
+      set_last_error("tensor-core update: a bounded wait gave up");
+      return SMFG_ERR_TIMEOUT;
+    }
     return SMFG_OK;
   } catch (const std::exception &e) {
     set_last_error(e.what());

@@ -129,10 +129,16 @@ def lib():
         L.smfg_last_error.restype = C.c_char_p
         L.smfg_analyse.argtypes = [C.c_int, _i32p, _i32p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
         L.smfg_analyse.restype = C.c_int
+        L.smfg_analyse_ordered.argtypes = [C.c_int, _i32p, _i32p, _i32p, C.c_int,
+                                           C.POINTER(C.c_void_p)]
+        L.smfg_analyse_ordered.restype = C.c_int
         L.smfg_symbolic_view.argtypes = [C.c_void_p, C.POINTER(_Analysis), C.POINTER(C.c_double),
                                          C.POINTER(C.c_int64)]
         L.smfg_symbolic_view.restype = C.c_int
         L.smfg_symbolic_free.argtypes = [C.POINTER(C.c_void_p)]
+        L.smfg_tc_update.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                     C.c_int, C.c_int, C.c_int]
+        L.smfg_tc_update.restype = C.c_int
         _lib = L
     return _lib
 
@@ -201,14 +207,20 @@ class Analysis:
         return int(self.sn_start.size)
 
 
-def analyse(n, col_ptr, row_idx, ordering: int = ORDER_ND, nemin: int = 8) -> Analysis:
+def analyse(n, col_ptr, row_idx, ordering: int = ORDER_ND, nemin: int = 8,
+            perm=None) -> Analysis:
     """Symbolic analysis of a lower CSC pattern (smfg_analyse: the engine's
-    own nested-dissection analysis, host code)."""
+    own nested-dissection analysis, host code). perm (perm[new] = old): a
+    caller-given fill-reducing ordering instead (smfg_analyse_ordered)."""
     L = lib()
     cp = np.ascontiguousarray(col_ptr, dtype=np.int32)
     ri = np.ascontiguousarray(row_idx, dtype=np.int32)
     h = C.c_void_p()
-    rc = L.smfg_analyse(int(n), cp, ri, ordering, nemin, C.byref(h))
+    if perm is not None:
+        pm = np.ascontiguousarray(perm, dtype=np.int32)
+        rc = L.smfg_analyse_ordered(int(n), cp, ri, pm, nemin, C.byref(h))
+    else:
+        rc = L.smfg_analyse(int(n), cp, ri, ordering, nemin, C.byref(h))
     if rc != SMFG_OK:
         raise SmfgError(rc, "smfg_analyse")
     try:
@@ -241,6 +253,25 @@ def analyse(n, col_ptr, row_idx, ordering: int = ORDER_ND, nemin: int = 8) -> An
         return Analysis(n, arrays, fl.value, fe.value)
     finally:
         L.smfg_symbolic_free(C.byref(h))
+
+
+TC_TF32X3, TC_BF16X3 = 0, 1
+
+
+def tc_update(C_t, L_t, W_t, kind: int = TC_TF32X3):
+    """smfg_tc_update on CUDA float64 tensors given TRANSPOSED (row-major
+    (k, n) / (n, n) tensors are the column-major n x k / n x n matrices):
+    lower(C) -= L W^T with tensor-core split products, in place."""
+    n = C_t.shape[0]
+    k = L_t.shape[0]
+    for t in (C_t, L_t, W_t):
+        if not (t.is_cuda and t.dtype.is_floating_point and t.element_size() == 8 and t.is_contiguous()):
+            raise ValueError("CUDA float64 contiguous tensors expected")
+    if C_t.shape != (n, n) or L_t.shape != (k, n) or W_t.shape != (k, n):
+        raise ValueError("shapes: C (n, n), L and W (k, n)")
+    rc = lib().smfg_tc_update(C_t.data_ptr(), n, n, L_t.data_ptr(), n, W_t.data_ptr(), n, k, kind)
+    if rc != SMFG_OK:
+        raise SmfgError(rc, "smfg_tc_update")
 
 
 class Solver:

@@ -291,10 +291,42 @@ static void apply_pivot(pchoice pc, double *F, int f, int *kp, int *rows, int8_t
  * dense_kernel_lapack.cpp:182-234). Those loops are compiled with GCC's
  * default C++ contraction, so each step is one fused multiply-add:
  * c = fma(-a, b, c). */
+/* x rounded to `bits` significant bits, to nearest (ties to even). */
+static double round_bits(double x, int bits) {
+  if (x == 0.0 || !is_fin(x)) return x;
+  int e;
+  const double m = frexp(x, &e);
+  return ldexp(nearbyint(ldexp(m, bits)), e - bits);
+}
+
+/* One entry of a split-product contraction: sum over t of a[t] b[t], each
+ * operand split as hi + lo at `bits` bits, hi*hi + hi*lo + lo*hi summed in
+ * FP32 in t order (the tensor-core accumulator). */
+static double split_dot(const double *a, size_t as, const double *b, size_t bs, int n, int bits) {
+  float acc = 0.0f;
+  for (int t = 0; t < n; ++t) {
+    const double x = a[(size_t)t * as], y = b[(size_t)t * bs];
+    const double xh = round_bits(x, bits), xl = round_bits(x - xh, bits);
+    const double yh = round_bits(y, bits), yl = round_bits(y - yh, bits);
+    acc = acc + (float)(xh * yh);
+    acc = acc + (float)(xh * yl);
+    acc = acc + (float)(xl * yh);
+  }
+  return (double)acc;
+}
+
+static int g_mixed_bits = 0; /* set per front by ldlt_factor_front */
+
 static void deferred_update(double *F, int f, int p0, int p1, int c0, int e, const double *W) {
   const int jb = p1 - p0;
   if (jb <= 0 || e - c0 <= 0) return;
   const size_t sf = (size_t)f;
+  if (g_mixed_bits) {
+    for (int j = c0; j < e; ++j)
+      for (int i = j; i < f; ++i)
+        F[(size_t)j * sf + i] -= split_dot(F + (size_t)p0 * sf + i, sf, W + j, sf, jb, g_mixed_bits);
+    return;
+  }
   for (int j = c0; j < e; ++j) {
     double *cj = F + (size_t)j * sf;
     for (int p = 0; p < jb; ++p) {
@@ -328,6 +360,13 @@ static void schur_update(double *F, int f, int p0, int p, int e, const int8_t *t
   const int kc = p - p0;
   for (int t = 0; t < kc; ++t)
     for (int i = 0; i < q; ++i) buf[(size_t)t * q + i] = ld_entry(F, f, tags, p0 + t, e + i);
+  if (g_mixed_bits) {
+    for (int j = 0; j < q; ++j)
+      for (int i = j; i < q; ++i)
+        F[(size_t)(e + j) * sf + e + i] -=
+            split_dot(F + (size_t)p0 * sf + e + i, sf, buf + j, (size_t)q, kc, g_mixed_bits);
+    return;
+  }
   for (int j = 0; j < q; ++j) {
     double *cj = F + (size_t)(e + j) * sf + e;
     for (int t = 0; t < kc; ++t) {
@@ -344,6 +383,8 @@ static void schur_update(double *F, int f, int p0, int p, int e, const int8_t *t
 static int ldlt_factor_front(double *F, int f, int num_elig, int *rows, const mfo_params *prm,
                              int8_t *tags, double *work, mfo_factor *o) {
   int k = 0;
+  g_mixed_bits = (prm->mixed_bits > 0 && prm->mixed_min_front > 0 && f >= prm->mixed_min_front)
+                     ? prm->mixed_bits : 0;
   if (f < prm->blocked_min_front || prm->nb <= 1) {
     while (k < num_elig) {
       pchoice pc = select_pivot(F, f, f, k, num_elig, num_elig, prm);

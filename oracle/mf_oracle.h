@@ -26,6 +26,12 @@ typedef struct {
 typedef struct {
   double u, eff_small, small_pivot;
   int nb, blocked_min_front, posdef;
+  /* Emulation of the engine's mixed-precision updates (0 = plain FP64):
+   * fronts of at least mixed_min_front rows take their deferred and Schur
+   * updates as split products (each operand x = hi + lo, both rounded to
+   * mixed_bits significant bits: 8 for BF16x3, 11 for TF32x3; the three
+   * products hi*hi, hi*lo, lo*hi summed in FP32) subtracted from FP64. */
+  int mixed_min_front, mixed_bits;
 } mfo_params;
 
 typedef struct {

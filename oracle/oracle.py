@@ -247,7 +247,8 @@ class _MfoAnalysis(C.Structure):
 
 class _MfoParams(C.Structure):
     _fields_ = [("u", C.c_double), ("eff_small", C.c_double), ("small_pivot", C.c_double),
-                ("nb", C.c_int), ("blocked_min_front", C.c_int), ("posdef", C.c_int)]
+                ("nb", C.c_int), ("blocked_min_front", C.c_int), ("posdef", C.c_int),
+                ("mixed_min_front", C.c_int), ("mixed_bits", C.c_int)]
 
 
 class _MfoFactor(C.Structure):
@@ -302,14 +303,18 @@ def eff_small_of(pv, small=1e-20):
 
 
 def restated_factorize(a: Analysis, pv, posdef: bool, u: float = 0.01, small: float = 1e-20,
-                       nb: int = 16, blocked_min_front: int = 96):
-    """Run mf_oracle.c on analysis `a` and permuted values `pv`."""
+                       nb: int = 16, blocked_min_front: int = 96, mixed_min_front: int = 0,
+                       mixed_bits: int = 0):
+    """Run mf_oracle.c on analysis `a` and permuted values `pv`. mixed_*:
+    emulate the engine's split-product updates on fronts of at least
+    mixed_min_front rows (mixed_bits 8: BF16x3, 11: TF32x3)."""
     lib = _oracle_lib()
     keep = [np.ascontiguousarray(x, dtype=np.int32) for x in (
         a.sn_start, a.sn_end, a.sn_parent, a.child_ptr, a.child_idx, a.front_row_ptr,
         a.front_row_idx, a.postorder, a.perm_col_ptr, a.perm_row_idx)]
     ca = _MfoAnalysis(a.n, a.nsn, *[x.ctypes.data for x in keep])
-    prm = _MfoParams(u, eff_small_of(pv, small), small, nb, blocked_min_front, int(posdef))
+    prm = _MfoParams(u, eff_small_of(pv, small), small, nb, blocked_min_front, int(posdef),
+                     int(mixed_min_front), int(mixed_bits))
     ns = a.nsn
     fsz = np.diff(a.front_row_ptr).astype(np.int64)
     # capacity: front rows grow with delays; allow generous room
