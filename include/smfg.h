@@ -102,7 +102,16 @@ typedef struct {
   int precision;          /* SMFG_PREC_* */
   int max_negative_pivots;/* < 0: off (Control::max_negative_pivots) */
   const double *scale;    /* optional S (length n, original numbering), NULL = none */
-  int reserved_i[8];
+  int profile;            /* 1: time the large-front update kernels (info.reserved_d[0..1]) */
+  /* SMFG_PREC_MIXED: large fronts of at least mixed_min_front rows (0: 384)
+   * that smfg_set_front_precision allows are factored in outer blocks of
+   * mixed_block pivots (0: 256; a multiple of 64): the threshold-pivoting
+   * panels stay FP64 and the columns past each block get one tensor-core
+   * update of kind mixed_kind (SMFG_TC_TF32X3 or SMFG_TC_BF16X3). */
+  int mixed_block;
+  int mixed_kind;
+  int mixed_min_front;
+  int reserved_i[4];
   double reserved_d[8];
 } smfg_control_t;
 
@@ -120,9 +129,10 @@ typedef struct {
   double solve_ms;        /* device time of the last solve */
   int levels;
   int kernel_launches;    /* kernels launched by the last call */
-  int mixed_fronts;       /* fronts whose Schur update ran in reduced precision */
-  int reserved_i[7];
-  double reserved_d[8];
+  int mixed_fronts;       /* fronts whose trailing updates ran on the tensor cores */
+  int reserved_i[7];      /* [0]: profiled launches */
+  double reserved_d[8];   /* [0] profiled ms, [1] FP64 update flops, [2] arena bytes,
+                             [3] tensor-core update flops (2 per multiply-add) */
 } smfg_info_t;
 
 typedef struct smfg_plan_s *smfg_plan_t;
@@ -154,6 +164,13 @@ SMFG_API int smfg_solve_device(smfg_plan_t plan, double *d_b, int nrhs, int ldb,
 
 /* Inertia of the last factorization (smf_inertia, smf_c.h:175). */
 SMFG_API int smfg_inertia(smfg_plan_t plan, int *pos, int *neg, int *zero);
+
+/* Per-front precision choice for SMFG_PREC_MIXED factorizations (a
+ * learned selector's output, or the FP64 fallback after a misjudged
+ * front): mask[s] = 1 lets supernode s take tensor-core trailing updates
+ * (large fronts only), 0 keeps it in FP64. NULL: every large front may.
+ * Kept for later factorizations until changed. */
+SMFG_API int smfg_set_front_precision(smfg_plan_t plan, const int8_t *mask);
 
 /* Per-front export of the last factor, in the FactorKeep layout
  * (factor_posdef.hpp:43-220): for supernode s, f[s] realized rows, p[s]
@@ -200,6 +217,23 @@ SMFG_API int smfg_residual_noalloc(smfg_plan_t plan, const double *d_b, const do
  * at eta_inf <= 1e-10 and omega <= omega_target. */
 SMFG_API int smfg_refine(smfg_plan_t plan, const double *b, double *x, int nrhs, int max_steps,
                          double omega_target, double *eta_inf, double *omega, int *steps);
+
+/* Refinement methods (smf::RefineMethod, solver/include/smf/types.hpp:160-170):
+ * classical x += M^-1 r; right-preconditioned FGMRES(restart) with the
+ * factor as preconditioner (refinement.cpp:451-643); auto = classical,
+ * escalating to FGMRES when a step contracts the gate measure by less than
+ * 0.5. Gate: eta_inf <= 1e-10 and omega <= omega_target; at most max_iters
+ * solves in all; x is left at the best iterate. restart <= 0: 20. */
+#define SMFG_REFINE_CLASSICAL 0
+#define SMFG_REFINE_FGMRES 1
+#define SMFG_REFINE_AUTO 2
+SMFG_API int smfg_refine_method(smfg_plan_t plan, const double *b, double *x, int nrhs, int method,
+                                int max_iters, int restart, double omega_target, double *eta_inf,
+                                double *omega, int *iters);
+/* The same with b and x in device memory (n x nrhs, leading dimension n). */
+SMFG_API int smfg_refine_device(smfg_plan_t plan, const double *d_b, double *d_x, int nrhs, int method,
+                                int max_iters, int restart, double omega_target, double *eta_inf,
+                                double *omega, int *iters);
 
 /* A symbolic analysis of the engine's own (host code, no GPU needed),
  * producing the smfg_analysis_t contract above when smf's analyse

@@ -271,6 +271,13 @@ static void build_plan(Plan &pl, const smfg_analysis_t &a) {
   x.lvl_blk = dalloc<int>(pl, (size_t)ns + nl + 1);
   x.counters = dalloc<unsigned long long>(pl, kCCount + 8);
   x.tpp = dalloc<TppState>(pl, 2 * (size_t)std::max(1, pl.max_large));  // two buffers (SPD panels)
+  x.sn_mixed = dalloc<int8_t>(pl, ns);
+  SMFG_CUDA(cudaMemsetAsync(x.sn_mixed, 0, ns, pl.stream));
+  x.tc_jobs = dalloc<tc::Job>(pl, std::max(1, pl.max_large));
+  x.tc_ipref = dalloc<int64_t>(pl, (size_t)std::max(1, pl.max_large) + 1);
+  x.tc_tpref = dalloc<int>(pl, (size_t)std::max(1, pl.max_large) + 1);
+  x.tc_njobs = dalloc<int>(pl, 1);
+  pl.h_fsym = fsym;
   x.arena = nullptr;
   x.arena_cap = 0;
   x.rows = nullptr;
@@ -333,6 +340,46 @@ struct GemmProfile {
   }
 };
 
+// Mixed-precision settings of one factorization (smfg_control_t.mixed_*).
+struct MixedCfg {
+  bool on = false;
+  int nbo = 256;   // outer block (pivots per tensor-core update), multiple of 64
+  int kind = tc::kTF32x3;
+  int min_front = kLargeMin;
+};
+
+static MixedCfg mixed_cfg(const smfg_control_t &c) {
+  MixedCfg m;
+  m.on = c.precision == SMFG_PREC_MIXED;
+  if (c.mixed_block > 0) m.nbo = std::max(64, (c.mixed_block + 63) / 64 * 64);
+  if (c.mixed_kind == SMFG_TC_BF16X3) m.kind = tc::kBF16x3;
+  if (c.mixed_min_front > 0) m.min_front = std::max(kLargeMin, c.mixed_min_front);
+  return m;
+}
+
+// The tensor-core updates due on a level's large fronts (states `states`).
+static void enqueue_tc(Plan &pl, const MixedCfg &mc, const int *lg, int nL, TppState *states, int posdef,
+                       LaunchCount &lc, GemmProfile &gp) {
+  DevFactor &x = pl.x;
+  cudaStream_t st = pl.stream;
+  const int sms = sm_count(pl.device);
+  const int smem = (int)sizeof(tc::Smem);
+  k_tc_jobs<<<1, 32, 0, st>>>(pl.d, x, lg, nL, states, mc.nbo, posdef, tc::kblock_elems(mc.kind));
+  const tc::Job *jobs = static_cast<const tc::Job *>(x.tc_jobs);
+  gp.mark(st);
+  if (mc.kind == tc::kTF32x3) {
+    tc::k_tc_split<tc::kTF32x3><<<4 * sms, 256, 0, st>>>(jobs, x.tc_njobs, x.tc_ipref, x.tc_img);
+    tc::k_tc_syrk<tc::kTF32x3><<<sms, tc::kThreads, smem, st>>>(jobs, x.tc_njobs, x.tc_tpref, x.tc_img,
+                                                                 x.counters + kCFlags, kFTcWait);
+  } else {
+    tc::k_tc_split<tc::kBF16x3><<<4 * sms, 256, 0, st>>>(jobs, x.tc_njobs, x.tc_ipref, x.tc_img);
+    tc::k_tc_syrk<tc::kBF16x3><<<sms, tc::kThreads, smem, st>>>(jobs, x.tc_njobs, x.tc_tpref, x.tc_img,
+                                                                 x.counters + kCFlags, kFTcWait);
+  }
+  gp.mark(st);
+  lc.n += 3;
+}
+
 static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_t &c, LaunchCount &lc,
                            GemmProfile &gp) {
   DevPlan &d = pl.d;
@@ -354,6 +401,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
   k_eff_small<<<1, 1, 0, st>>>(x.counters, c.small_pivot);
   lc.n += 2;
   PivotParams prm{c.u, c.small_pivot, c.small_pivot, c.nb, c.blocked_min_front, c.posdef};
+  const MixedCfg mc = mixed_cfg(c);
   const size_t smem_s = front_smem_bytes(kSmallMax, c.nb);
   const size_t smem_m = front_smem_bytes(kMediumMax, c.nb);
   for (int l = 0; l < pl.nlevels; ++l) {
@@ -369,7 +417,11 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
     const int nL = pl.lvl_large_ptr[l + 1] - pl.lvl_large_ptr[l];
     if (nL > 0) {
       const int *lg = d.lvl_large + pl.lvl_large_ptr[l];
-      k_large_init<<<nL, 256, 0, st>>>(d, x, lg, nL, c.posdef);
+      bool lvl_mixed = false;
+      if (mc.on)
+        for (int i = pl.lvl_large_ptr[l]; i < pl.lvl_large_ptr[l + 1] && !lvl_mixed; ++i)
+          lvl_mixed = pl.h_mixed[pl.h_lvl_large[i]] != 0;
+      k_large_init<<<nL, 256, 0, st>>>(d, x, lg, nL, c.posdef, lvl_mixed ? mc.nbo : 0);
       SMFG_CUDA(cudaMemsetAsync(x.counters + kCActive, 0, sizeof(unsigned long long), st));
       const int ggrid = 2 * sms;
       int it = 0;
@@ -386,6 +438,8 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
           gp.mark(st);
           k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, nxt);
           gp.mark(st);
+          if (lvl_mixed && ((it + 1) * c.nb % mc.nbo == 0 || it == steps - 1))
+            enqueue_tc(pl, mc, lg, nL, nxt, c.posdef, lc, gp);
         }
         fin = x.tpp + (size_t)(steps & 1) * pl.max_large;
         lc.n += 2 * steps;
@@ -396,6 +450,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
           gp.mark(st);
           k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, x.tpp);
           gp.mark(st);
+          if (lvl_mixed) enqueue_tc(pl, mc, lg, nL, x.tpp, c.posdef, lc, gp);
         }
         lc.n += 2 * steps;
       } else {
@@ -408,6 +463,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
             gp.mark(st);
             k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, x.tpp);
             gp.mark(st);
+            if (lvl_mixed) enqueue_tc(pl, mc, lg, nL, x.tpp, c.posdef, lc, gp);
           }
           lc.n += 2 * batch;
           unsigned long long act = 0;
@@ -437,6 +493,10 @@ static void set_kernel_attrs(int nb) {
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)front_smem_bytes(kMediumMax, nb)));
   SMFG_CUDA(cudaFuncSetAttribute(k_large_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem)));
+  SMFG_CUDA(cudaFuncSetAttribute(tc::k_tc_syrk<tc::kTF32x3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(tc::Smem)));
+  SMFG_CUDA(cudaFuncSetAttribute(tc::k_tc_syrk<tc::kBF16x3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(tc::Smem)));
   SMFG_CUDA(cudaFuncSetAttribute(k_large_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem)));
   done_nb = nb;
 }
@@ -449,15 +509,44 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
   const int64_t base_a = pl.sum_f2, base_r = pl.sum_f;
   int64_t need_a = c.posdef ? base_a : base_a + base_a / 4 + (int64_t)pl.max_fsym * pl.max_fsym * 2 + 4096;
   int64_t need_r = c.posdef ? base_r : base_r + base_r / 2 + 4096;
+  // mixed fronts: large, at least min_front rows, allowed by the caller's mask
+  const MixedCfg mc = mixed_cfg(c);
+  pl.h_mixed.assign(pl.nsn, 0);
+  pl.mixed_count = 0;
+  int64_t tc_need = 0;
+  if (mc.on) {
+    for (int l = 0; l < pl.nlevels; ++l) {
+      int64_t lvl_bytes = 0;
+      for (int i = pl.lvl_large_ptr[l]; i < pl.lvl_large_ptr[l + 1]; ++i) {
+        const int s = pl.h_lvl_large[i];
+        if (pl.h_fsym[s] < mc.min_front) continue;
+        if (!pl.front_mask.empty() && !pl.front_mask[s]) continue;
+        pl.h_mixed[s] = 1;
+        ++pl.mixed_count;
+        // rows grow with delays: room for a quarter more, regrown on overflow
+        const int f = pl.h_fsym[s] + pl.h_fsym[s] / 4 + 64;
+        const int ntr = (f + tc::kBM - 1) / tc::kBM;
+        const int nkb = (mc.nbo + c.nb + tc::kblock_elems(mc.kind) - 1) / tc::kblock_elems(mc.kind);
+        lvl_bytes += tc::image_bytes(ntr, nkb);
+      }
+      tc_need = std::max(tc_need, lvl_bytes);
+    }
+  }
+  SMFG_CUDA(cudaMemcpyAsync(pl.x.sn_mixed, pl.h_mixed.data(), pl.nsn, cudaMemcpyHostToDevice, pl.stream));
   FactorTotals *d_tot = nullptr;
   unsigned long long h_cnt[kCCount];
   FactorTotals tot{};
   LaunchCount lc;
   GemmProfile gp;
-  gp.on = c.reserved_i[0] != 0;
+  gp.on = c.profile != 0;
   float ms = 0.0f;
   for (int attempt = 0; attempt < 4; ++attempt) {
     ensure_arena(pl, std::max(need_a, pl.x.arena_cap), std::max(need_r, pl.x.rows_cap));
+    if (pl.x.tc_img_cap < tc_need) {
+      dfree(pl, pl.x.tc_img);
+      pl.x.tc_img = dalloc<uint8_t>(pl, tc_need);
+      pl.x.tc_img_cap = tc_need;
+    }
     lc = LaunchCount{};
     gp.used = 0;
     SMFG_CUDA(cudaEventRecord(pl.ev0, pl.stream));
@@ -475,6 +564,10 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
     if (flags & (kFArena | kFRows)) {
       need_a = std::max<int64_t>(need_a * 2, (int64_t)h_cnt[kCArena] * 2);
       need_r = std::max<int64_t>(need_r * 2, (int64_t)h_cnt[kCRows] * 2);
+      continue;
+    }
+    if (flags & kFTcCap) {
+      tc_need = std::max<int64_t>(tc_need * 2, 1 << 24);
       continue;
     }
     break;
@@ -503,15 +596,18 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
   inf.factor_ms = ms;
   inf.levels = pl.nlevels;
   inf.kernel_launches = lc.n;
-  // profile (ctrl.reserved_i[0]): large-front GEMM device time, launches,
+  // profile (ctrl.profile): large-front GEMM device time, launches,
   // algorithmic flops; arena bytes in use
   inf.reserved_d[0] = gp.on ? gp.total_ms() : 0.0;
   std::memcpy(&inf.reserved_d[1], &h_cnt[kCGemmFlops], sizeof(double));
   inf.reserved_d[2] = (double)h_cnt[kCArena] * 8.0;
   inf.reserved_i[0] = (int)(gp.used / 2);
+  std::memcpy(&inf.reserved_d[3], &h_cnt[kCTcFlops], sizeof(double));
+  inf.mixed_fronts = pl.mixed_count;
   int rc = SMFG_OK;
   pl.factor_status = SMFG_FACTOR_SUCCESS;
-  if (flags & (kFArena | kFRows)) rc = SMFG_ERR_ARENA;
+  if (flags & (kFArena | kFRows | kFTcCap)) rc = SMFG_ERR_ARENA;
+  else if (flags & kFTcWait) rc = SMFG_ERR_TIMEOUT;
   else if (flags & kFNonfinite) rc = SMFG_ERR_NONFINITE;
   else if (flags & (kFMap | kFInternal)) rc = SMFG_ERR_INTERNAL;
   else if (flags & kFNotPosdef) {
@@ -810,6 +906,14 @@ SMFG_API int smfg_solve_device(smfg_plan_t plan, double *d_b, int nrhs, int ldb,
   return solve_common(plan, d_b, true, nrhs, ldb, job, info);
 }
 
+SMFG_API int smfg_set_front_precision(smfg_plan_t plan, const int8_t *mask) {
+  if (!plan) return SMFG_ERR_INVALID_ARG;
+  Plan &pl = plan->pl;
+  if (mask) pl.front_mask.assign(mask, mask + pl.nsn);
+  else pl.front_mask.clear();
+  return SMFG_OK;
+}
+
 SMFG_API int smfg_inertia(smfg_plan_t plan, int *pos, int *neg, int *zero) {
   if (!plan || !pos || !neg || !zero) return SMFG_ERR_INVALID_ARG;
   if (!plan->pl.factored) return SMFG_ERR_SINGULAR;
@@ -888,7 +992,7 @@ SMFG_API int smfg_factor_export(smfg_plan_t plan, int *f, int *p, int64_t *blk_o
 
 // Device residual of x for b (both n x nrhs, leading dimension n, device).
 static void device_residual(Plan &pl, const double *db, const double *dx, double *dr, int nrhs,
-                            double *eta, double *omega) {
+                            double *eta, double *omega, double *norms = nullptr) {
   unsigned long long *mx = nullptr;
   SMFG_CUDA(cudaMallocAsync((void **)&mx, sizeof(unsigned long long) * 8, pl.stream));
   // permuted copies: the residual works in the new numbering
@@ -916,6 +1020,11 @@ static void device_residual(Plan &pl, const double *db, const double *dx, double
     const double e = den > 0 ? v[0] / den : (v[0] == 0 ? 0.0 : INFINITY);
     e_max = std::max(e_max, e);
     o_max = std::max(o_max, v[4]);
+    if (norms) {  // ||A||inf, ||x||inf, ||b||inf of the last column
+      norms[0] = v[1];
+      norms[1] = v[2];
+      norms[2] = v[3];
+    }
   }
   SMFG_CUDA(cudaFreeAsync(xp, pl.stream));
   SMFG_CUDA(cudaFreeAsync(mx, pl.stream));
@@ -1030,51 +1139,283 @@ SMFG_API int smfg_residual(smfg_plan_t plan, const double *b, const double *x, i
   }
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Iterative refinement on the device (refinement.cpp:316-643). The gate of
+// every column: eta_inf <= 1e-10 and omega <= omega_target (residuals with
+// compensated sums). Classical: x += M^-1 r, stopping after two steps that
+// contract max(eta / 1e-10, omega / target) by less than 0.85 or one that
+// does not reduce it. FGMRES: right-preconditioned FGMRES(restart) in FP64,
+// modified Gram-Schmidt, every iteration forms its iterate and checks the
+// true residual, restarts from the best iterate, rejects iterates 1e8 times
+// larger than max(||x||, ||b|| / ||A||) at the start. Auto: classical while
+// each step contracts by at least 0.5, then FGMRES on the remaining budget.
+// The factor's solves are the preconditioner. x is left at the best iterate.
+
+namespace {
+
+double gate_score(double e, double o, double tgt) { return std::max(e / 1e-10, o / tgt); }
+
+struct DevVec {
+  Plan &pl;
+  double *p = nullptr;
+  DevVec(Plan &pl_, size_t n) : pl(pl_) {
+    SMFG_CUDA(cudaMallocAsync((void **)&p, sizeof(double) * std::max<size_t>(1, n), pl.stream));
+  }
+  ~DevVec() { cudaFreeAsync(p, pl.stream); }
+};
+
+// Device dot product into out (device), a fixed summation order.
+void dev_dot(Plan &pl, const double *a, const double *b, int64_t n, double *part, double *out) {
+  k_dot_part<<<kDotBlocks, 256, 0, pl.stream>>>(a, b, n, part);
+  k_dot_fin<<<1, 1024, 0, pl.stream>>>(part, kDotBlocks, out);
+}
+
+// y = A x, original numbering (gather, product, scatter).
+void dev_spmv(Plan &pl, const double *x, double *y, double *tmp2n) {
+  const int sms = sm_count(pl.device);
+  const int g = (int)std::max<int64_t>(1, std::min<int64_t>(4 * sms, (pl.n + 255) / 256));
+  double *xp = tmp2n, *yp = tmp2n + pl.n;
+  k_solve_gather<<<g, 256, 0, pl.stream>>>(x, pl.n, 1, pl.n, pl.d.perm, nullptr, xp);
+  const int rg = (int)std::max<int64_t>(1, std::min<int64_t>(8 * sms, (pl.n + 7) / 8));
+  k_spmv<<<rg, 256, 0, pl.stream>>>(pl.d, pl.x.pv_raw, xp, yp, pl.n);
+  k_solve_scatter<<<g, 256, 0, pl.stream>>>(y, pl.n, 1, pl.n, pl.d.perm, nullptr, yp);
+}
+
+// Classical steps on all columns together; returns the steps taken. With
+// escalate (Auto), stops at the first step contracting by less than 0.5.
+int classical_refine(smfg_plan_s *plan, double *db, double *dx, double *dr, double *dbest, int nrhs,
+                     int budget, double tgt, bool escalate, double &be, double &bo, bool &stalled) {
+  Plan &pl = plan->pl;
+  const size_t len = (size_t)pl.n * nrhs;
+  const int sms = sm_count(pl.device);
+  double e = 0, o = 0;
+  device_residual(pl, db, dx, dr, nrhs, &e, &o);
+  SMFG_CUDA(cudaMemcpyAsync(dbest, dx, sizeof(double) * len, cudaMemcpyDeviceToDevice, pl.stream));
+  be = e;
+  bo = o;
+  stalled = false;
+  int it = 0;
+  while (it < budget && !(be <= 1e-10 && bo <= tgt)) {
+    LaunchCount lc;
+    enqueue_solve(pl, dr, nrhs, pl.n, SMFG_SOLVE_FULL, plan->has_scale, lc);
+    const int g = (int)std::max<int64_t>(1, std::min<int64_t>(4 * sms, ((int64_t)len + 255) / 256));
+    k_axpy<<<g, 256, 0, pl.stream>>>(dx, dr, (int64_t)len);
+    ++it;
+    device_residual(pl, db, dx, dr, nrhs, &e, &o);
+    const double sc = gate_score(e, o, tgt), bsc = gate_score(be, bo, tgt);
+    if (sc < bsc) {
+      be = e;
+      bo = o;
+      SMFG_CUDA(cudaMemcpyAsync(dbest, dx, sizeof(double) * len, cudaMemcpyDeviceToDevice, pl.stream));
+      if (escalate && sc / bsc > 0.5) {
+        stalled = true;
+        break;
+      }
+      if (sc / bsc > 0.85 && it >= 2) break;
+    } else {
+      stalled = true;
+      break;
+    }
+  }
+  // continue from the best iterate
+  SMFG_CUDA(cudaMemcpyAsync(dx, dbest, sizeof(double) * len, cudaMemcpyDeviceToDevice, pl.stream));
+  return it;
+}
+
+// FGMRES on one column (b, x device vectors of length n); x left at the
+// best iterate. Returns the iterations used.
+int fgmres_column(smfg_plan_s *plan, const double *b, double *x, int budget, int restart, double tgt,
+                  double &eta_out, double &omega_out) {
+  Plan &pl = plan->pl;
+  const int64_t n = pl.n;
+  const int sms = sm_count(pl.device);
+  const int g = (int)std::max<int64_t>(1, std::min<int64_t>(4 * sms, (n + 255) / 256));
+  double norms[3] = {0, 0, 0};
+  DevVec r_best(pl, n), r_cand(pl, n);
+  double e = 0, o = 0;
+  device_residual(pl, b, x, r_best.p, 1, &e, &o, norms);
+  eta_out = e;
+  omega_out = o;
+  if (budget <= 0 || !std::isfinite(e) || !std::isfinite(o)) return 0;
+  if (e <= 1e-10 && o <= tgt) return 0;
+  const double x_limit = 1e8 * std::max(norms[1], norms[0] > 0 ? norms[2] / norms[0] : 0.0);
+  const int m_max = std::max(1, std::min(restart, budget));
+  DevVec V(pl, (size_t)(m_max + 1) * n), Z(pl, (size_t)m_max * n), x0(pl, n), xc(pl, n), tmp(pl, 2 * n);
+  DevVec part(pl, kDotBlocks), hdev(pl, m_max + 2), ydev(pl, m_max);
+  std::vector<double> H((size_t)(m_max + 1) * m_max, 0.0), cs(m_max), sn(m_max), gv(m_max + 1), y(m_max);
+  auto h = [&](int i, int j) -> double & { return H[(size_t)j * (m_max + 1) + i]; };
+  SMFG_CUDA(cudaMemcpyAsync(x0.p, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, pl.stream));
+  double best = gate_score(e, o, tgt);
+  int used = 0;
+  bool done = false;
+  while (used < budget && !done) {
+    double bb = 0.0;
+    dev_dot(pl, r_best.p, r_best.p, n, part.p, hdev.p);
+    SMFG_CUDA(cudaMemcpyAsync(&bb, hdev.p, sizeof(double), cudaMemcpyDeviceToHost, pl.stream));
+    SMFG_CUDA(cudaStreamSynchronize(pl.stream));
+    const double beta = std::sqrt(bb);
+    if (!(beta > 0.0) || !std::isfinite(beta)) break;
+    k_scale<<<g, 256, 0, pl.stream>>>(V.p, r_best.p, 1.0 / beta, n);
+    std::fill(gv.begin(), gv.end(), 0.0);
+    gv[0] = beta;
+    const int m = std::min(m_max, budget - used);
+    bool improved = false, stop = false;
+    for (int j = 0; j < m; ++j) {
+      double *vj = V.p + (size_t)j * n, *zj = Z.p + (size_t)j * n, *w = V.p + (size_t)(j + 1) * n;
+      SMFG_CUDA(cudaMemcpyAsync(zj, vj, sizeof(double) * n, cudaMemcpyDeviceToDevice, pl.stream));
+      LaunchCount lc;
+      enqueue_solve(pl, zj, 1, pl.n, SMFG_SOLVE_FULL, plan->has_scale, lc);
+      ++used;
+      dev_spmv(pl, zj, w, tmp.p);
+      for (int i = 0; i <= j; ++i) {  // modified Gram-Schmidt, coefficients on the device
+        dev_dot(pl, w, V.p + (size_t)i * n, n, part.p, hdev.p + i);
+        k_axpy_coef<<<g, 256, 0, pl.stream>>>(w, V.p + (size_t)i * n, hdev.p + i, n);
+      }
+      dev_dot(pl, w, w, n, part.p, hdev.p + j + 1);
+      std::vector<double> hc(j + 2);
+      SMFG_CUDA(cudaMemcpyAsync(hc.data(), hdev.p, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, pl.stream));
+      SMFG_CUDA(cudaStreamSynchronize(pl.stream));
+      for (int i = 0; i <= j; ++i) h(i, j) = hc[i];
+      const double hnext = std::sqrt(std::max(0.0, hc[j + 1]));
+      if (!std::isfinite(hnext)) {
+        stop = true;
+        break;
+      }
+      for (int i = 0; i < j; ++i) {
+        const double a = h(i, j), c = h(i + 1, j);
+        h(i, j) = cs[i] * a + sn[i] * c;
+        h(i + 1, j) = -sn[i] * a + cs[i] * c;
+      }
+      const double diag = h(j, j);
+      const double rho = std::hypot(diag, hnext);
+      if (rho == 0.0) {
+        stop = true;
+        break;
+      }
+      cs[j] = diag / rho;
+      sn[j] = hnext / rho;
+      h(j, j) = rho;
+      h(j + 1, j) = 0.0;
+      gv[j + 1] = -sn[j] * gv[j];
+      gv[j] = cs[j] * gv[j];
+      const int k = j + 1;
+      for (int i = k - 1; i >= 0; --i) {
+        double sacc = gv[i];
+        for (int l = i + 1; l < k; ++l) sacc -= h(i, l) * y[l];
+        y[i] = sacc / h(i, i);
+      }
+      SMFG_CUDA(cudaMemcpyAsync(ydev.p, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, pl.stream));
+      k_lincomb<<<g, 256, 0, pl.stream>>>(xc.p, x0.p, Z.p, ydev.p, k, n);
+      double ce = INFINITY, co = INFINITY, cn[3] = {0, 0, 0};
+      device_residual(pl, b, xc.p, r_cand.p, 1, &ce, &co, cn);
+      if (cn[1] <= x_limit && std::isfinite(ce) && std::isfinite(co)) {
+        const double sc = gate_score(ce, co, tgt);
+        if (sc < best) {
+          best = sc;
+          eta_out = ce;
+          omega_out = co;
+          SMFG_CUDA(cudaMemcpyAsync(x, xc.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, pl.stream));
+          std::swap(r_best.p, r_cand.p);
+          improved = true;
+          if (ce <= 1e-10 && co <= tgt) {
+            done = true;
+            break;
+          }
+        }
+      }
+      if (hnext <= 0.0) break;
+      k_scale<<<g, 256, 0, pl.stream>>>(w, w, 1.0 / hnext, n);
+    }
+    if (stop || !improved) break;
+    SMFG_CUDA(cudaMemcpyAsync(x0.p, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, pl.stream));
+  }
+  SMFG_CUDA(cudaStreamSynchronize(pl.stream));
+  return used;
+}
+
+// db, dx: device, n x nrhs, leading dimension n; dx refined in place.
+int refine_core(smfg_plan_s *plan, double *db, double *dx, int nrhs, int method, int max_iters, int restart,
+                double omega_target, double *eta_inf, double *omega, int *iters) {
+  Plan &pl = plan->pl;
+  if (!pl.factored) return SMFG_ERR_SINGULAR;
+  const size_t len = (size_t)pl.n * nrhs;
+  const double tgt = omega_target > 0 ? omega_target : 1e-8;
+  DevVec r(pl, len), best(pl, len);
+  double be = 0, bo = 0;
+  bool stalled = false;
+  int used = 0;
+  if (method == SMFG_REFINE_CLASSICAL || method == SMFG_REFINE_AUTO)
+    used = classical_refine(plan, db, dx, r.p, best.p, nrhs, max_iters, tgt, method == SMFG_REFINE_AUTO,
+                            be, bo, stalled);
+  if (method == SMFG_REFINE_FGMRES || (method == SMFG_REFINE_AUTO && stalled && !(be <= 1e-10 && bo <= tgt))) {
+    int most = 0;
+    double emax = 0, omax = 0;
+    for (int c = 0; c < nrhs; ++c) {
+      double e = 0, o = 0;
+      const int u = fgmres_column(plan, db + (size_t)c * pl.n, dx + (size_t)c * pl.n, max_iters - used,
+                                  restart > 0 ? restart : 20, tgt, e, o);
+      most = std::max(most, u);
+      emax = std::max(emax, e);
+      omax = std::max(omax, o);
+    }
+    used += most;
+    be = emax;
+    bo = omax;
+  }
+  SMFG_CUDA(cudaStreamSynchronize(pl.stream));
+  if (eta_inf) *eta_inf = be;
+  if (omega) *omega = bo;
+  if (iters) *iters = used;
+  return SMFG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 SMFG_API int smfg_refine(smfg_plan_t plan, const double *b, double *x, int nrhs, int max_steps,
                          double omega_target, double *eta_inf, double *omega, int *steps) {
-  if (!plan || !b || !x || nrhs < 1) return SMFG_ERR_INVALID_ARG;
+  return smfg_refine_method(plan, b, x, nrhs, SMFG_REFINE_CLASSICAL, max_steps, 0, omega_target, eta_inf,
+                            omega, steps);
+}
+
+SMFG_API int smfg_refine_method(smfg_plan_t plan, const double *b, double *x, int nrhs, int method,
+                                int max_iters, int restart, double omega_target, double *eta_inf,
+                                double *omega, int *iters) {
+  if (!plan || !b || !x || nrhs < 1 || method < 0 || method > 2) return SMFG_ERR_INVALID_ARG;
   Plan &pl = plan->pl;
   if (!pl.factored) return SMFG_ERR_SINGULAR;
   try {
     SMFG_CUDA(cudaSetDevice(pl.device));
     clear_stale_error();
     const size_t len = (size_t)pl.n * nrhs;
-    double *d = nullptr;
-    SMFG_CUDA(cudaMallocAsync((void **)&d, sizeof(double) * len * 4, pl.stream));
-    double *db = d, *dx = d + len, *dr = d + 2 * len, *dbest = d + 3 * len;
-    SMFG_CUDA(cudaMemcpyAsync(db, b, sizeof(double) * len, cudaMemcpyHostToDevice, pl.stream));
-    SMFG_CUDA(cudaMemcpyAsync(dx, x, sizeof(double) * len, cudaMemcpyHostToDevice, pl.stream));
-    double e = 0, o = 0;
-    device_residual(pl, db, dx, dr, nrhs, &e, &o);
-    SMFG_CUDA(cudaMemcpyAsync(dbest, dx, sizeof(double) * len, cudaMemcpyDeviceToDevice, pl.stream));
-    double be = e, bo = o;
-    int it = 0;
-    const int sms = sm_count(pl.device);
-    const double tgt = omega_target > 0 ? omega_target : 1e-8;
-    while (it < max_steps && !(be <= 1e-10 && bo <= tgt)) {
-      LaunchCount lc;
-      enqueue_solve(pl, dr, nrhs, pl.n, SMFG_SOLVE_FULL, plan->has_scale, lc);
-      const int g = (int)std::max<int64_t>(1, std::min<int64_t>(4 * sms, ((int64_t)len + 255) / 256));
-      k_axpy<<<g, 256, 0, pl.stream>>>(dx, dr, (int64_t)len);
-      ++it;
-      device_residual(pl, db, dx, dr, nrhs, &e, &o);
-      const double sc = std::max(e / 1e-10, o / tgt), bsc = std::max(be / 1e-10, bo / tgt);
-      if (sc < bsc) {
-        be = e;
-        bo = o;
-        SMFG_CUDA(cudaMemcpyAsync(dbest, dx, sizeof(double) * len, cudaMemcpyDeviceToDevice, pl.stream));
-        if (sc / bsc > 0.85 && it >= 2) break;
-      } else {
-        break;
-      }
-    }
-    SMFG_CUDA(cudaMemcpyAsync(x, dbest, sizeof(double) * len, cudaMemcpyDeviceToHost, pl.stream));
-    SMFG_CUDA(cudaFreeAsync(d, pl.stream));
+    DevVec d(pl, 2 * len);
+    SMFG_CUDA(cudaMemcpyAsync(d.p, b, sizeof(double) * len, cudaMemcpyHostToDevice, pl.stream));
+    SMFG_CUDA(cudaMemcpyAsync(d.p + len, x, sizeof(double) * len, cudaMemcpyHostToDevice, pl.stream));
+    const int rc = refine_core(plan, d.p, d.p + len, nrhs, method, max_iters, restart, omega_target, eta_inf,
+                               omega, iters);
+    SMFG_CUDA(cudaMemcpyAsync(x, d.p + len, sizeof(double) * len, cudaMemcpyDeviceToHost, pl.stream));
     SMFG_CUDA(cudaStreamSynchronize(pl.stream));
-    if (eta_inf) *eta_inf = be;
-    if (omega) *omega = bo;
-    if (steps) *steps = it;
-    return SMFG_OK;
+    return rc;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return SMFG_ERR_CUDA;
+  }
+}
+
+SMFG_API int smfg_refine_device(smfg_plan_t plan, const double *d_b, double *d_x, int nrhs, int method,
+                                int max_iters, int restart, double omega_target, double *eta_inf,
+                                double *omega, int *iters) {
+  if (!plan || !d_b || !d_x || nrhs < 1 || method < 0 || method > 2) return SMFG_ERR_INVALID_ARG;
+  Plan &pl = plan->pl;
+  if (!pl.factored) return SMFG_ERR_SINGULAR;
+  try {
+    SMFG_CUDA(cudaSetDevice(pl.device));
+    clear_stale_error();
+    return refine_core(plan, const_cast<double *>(d_b), d_x, nrhs, method, max_iters, restart, omega_target,
+                       eta_inf, omega, iters);
   } catch (const std::exception &e) {
     set_last_error(e.what());
     return SMFG_ERR_CUDA;
@@ -1110,34 +1451,42 @@ SMFG_API int smfg_tc_update(double *d_C, int ldc, int n, const double *d_L, int 
     J.tiles = J.ntr * (J.ntr + 1) / 2;
     J.img = 0;
     const int64_t items = (int64_t)J.ntr * tc::kBM * 8 * J.nkb;
-    const int64_t ipref[2] = {0, items};
-    const int tpref[2] = {0, J.tiles};
+    // metadata block: job, item prefix, tile prefix, job count, error word
+    struct Meta {
+      tc::Job job;
+      int64_t ipref[2];
+      int tpref[2];
+      int njobs, pad;
+      unsigned long long err;
+    } hm{};
+    hm.job = J;
+    hm.ipref[1] = items;
+    hm.tpref[1] = J.tiles;
+    hm.njobs = 1;
     const int64_t img_bytes = tc::image_bytes(J.ntr, J.nkb);
-    const size_t meta = 256 + 2 * sizeof(int64_t) + 2 * sizeof(int) + 8;
+    const size_t meta = ((sizeof(Meta) + 255) / 256) * 256;
     uint8_t *buf = nullptr;
     cudaStream_t st = nullptr;
-    SMFG_CUDA(cudaMalloc((void **)&buf, meta + img_bytes + 256));
-    uint8_t *img = buf + ((meta + 255) / 256) * 256;
-    tc::Job *dj = reinterpret_cast<tc::Job *>(buf);
-    int64_t *dip = reinterpret_cast<int64_t *>(buf + sizeof(tc::Job) + 8);
-    int *dtp = reinterpret_cast<int *>(dip + 2);
-    unsigned long long *derr = reinterpret_cast<unsigned long long *>(dtp + 2);
-    static_assert(sizeof(tc::Job) + 8 + 2 * sizeof(int64_t) + 2 * sizeof(int) + 8 <= 256 + 2 * sizeof(int64_t) + 2 * sizeof(int) + 8, "meta");
-    SMFG_CUDA(cudaMemcpyAsync(dj, &J, sizeof(J), cudaMemcpyHostToDevice, st));
-    SMFG_CUDA(cudaMemcpyAsync(dip, ipref, sizeof(ipref), cudaMemcpyHostToDevice, st));
-    SMFG_CUDA(cudaMemcpyAsync(dtp, tpref, sizeof(tpref), cudaMemcpyHostToDevice, st));
-    SMFG_CUDA(cudaMemsetAsync(derr, 0, sizeof(unsigned long long), st));
+    SMFG_CUDA(cudaMalloc((void **)&buf, meta + img_bytes));
+    uint8_t *img = buf + meta;
+    Meta *dm = reinterpret_cast<Meta *>(buf);
+    SMFG_CUDA(cudaMemcpyAsync(dm, &hm, sizeof(Meta), cudaMemcpyHostToDevice, st));
+    const tc::Job *dj = &dm->job;
+    const int64_t *dip = dm->ipref;
+    const int *dtp = dm->tpref;
+    const int *dnj = &dm->njobs;
+    unsigned long long *derr = &dm->err;
     const int sg = (int)std::max<int64_t>(1, std::min<int64_t>(8 * sms, (items + 255) / 256));
     const int gg = std::max(1, std::min(J.tiles, sms));
     const int smem = (int)sizeof(tc::Smem);
     if (kind == SMFG_TC_TF32X3) {
       SMFG_CUDA(cudaFuncSetAttribute(tc::k_tc_syrk<tc::kTF32x3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-      tc::k_tc_split<tc::kTF32x3><<<sg, 256, 0, st>>>(dj, 1, dip, img);
-      tc::k_tc_syrk<tc::kTF32x3><<<gg, tc::kThreads, smem, st>>>(dj, 1, dtp, img, derr);
+      tc::k_tc_split<tc::kTF32x3><<<sg, 256, 0, st>>>(dj, dnj, dip, img);
+      tc::k_tc_syrk<tc::kTF32x3><<<gg, tc::kThreads, smem, st>>>(dj, dnj, dtp, img, derr, 1ull);
     } else {
       SMFG_CUDA(cudaFuncSetAttribute(tc::k_tc_syrk<tc::kBF16x3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-      tc::k_tc_split<tc::kBF16x3><<<sg, 256, 0, st>>>(dj, 1, dip, img);
-      tc::k_tc_syrk<tc::kBF16x3><<<gg, tc::kThreads, smem, st>>>(dj, 1, dtp, img, derr);
+      tc::k_tc_split<tc::kBF16x3><<<sg, 256, 0, st>>>(dj, dnj, dip, img);
+      tc::k_tc_syrk<tc::kBF16x3><<<gg, tc::kThreads, smem, st>>>(dj, dnj, dtp, img, derr, 1ull);
     }
     SMFG_CUDA(cudaGetLastError());
     unsigned long long herr = 0;

@@ -626,10 +626,15 @@ struct TppState {
   int post, ps, pl, stalled;
   int g_p0, g_p1, g_c0, g_e;  // the deferred update asked for
   int pad[4];
+  // mixed precision (outer blocks): the eligible columns [k, min(se, ne))
+  // are current; every column from there on has the pivots [0, tc_done)
+  // applied and waits for a tensor-core update by [tc_done, k)
+  int mixed, tc_done, se, flush;
   FrontStats st;
 };
 
-__device__ __forceinline__ void tpp_init(TppState &S, int ne, bool posdef) {
+__device__ __forceinline__ void tpp_init(TppState &S, int ne, bool posdef, bool mixed = false,
+                                         int nbo = 0) {
   S.phase = posdef ? 1 : 0;
   S.k = 0;
   S.live = ne;
@@ -637,7 +642,26 @@ __device__ __forceinline__ void tpp_init(TppState &S, int ne, bool posdef) {
   S.post = 0;
   S.ps = S.pl = S.stalled = 0;
   S.g_p0 = S.g_p1 = S.g_c0 = S.g_e = 0;
+  S.mixed = mixed ? 1 : 0;
+  S.tc_done = 0;
+  S.se = mixed ? nbo : (1 << 30);
+  S.flush = 0;
   S.st = FrontStats{0, 0, 0, 0, 0.0};
+}
+
+// End of the columns a deferred update may touch.
+__device__ __forceinline__ int tpp_upd_end(const TppState &S, int ne) {
+  return S.mixed ? min(ne, S.se) : ne;
+}
+
+// Mixed fronts: stops the step (returns true from tpp_step_blk with an
+// empty update) so that the caller applies the pending tensor-core update
+// before the step reads or swaps columns past the current outer block.
+__device__ __forceinline__ bool tpp_request_flush(TppState &S) {
+  S.flush = 1;
+  S.g_p0 = S.g_p1 = S.k;
+  S.g_c0 = S.g_e = S.k;
+  return true;
 }
 
 // Runs the blocked algorithm up to its next deferred update, which it leaves
@@ -648,8 +672,11 @@ template <int NT>
 __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontShared &sh, TppState &S) {
   const int f = v.f, ne = v.ne;
   const size_t sf = (size_t)v.ld;
+  // stale eligible columns past the outer block exist (mixed fronts)
+  auto stale = [&]() { return S.mixed && S.tc_done < S.k && min(S.se, ne) < ne; };
   for (int guard = 0; guard < 4 * (ne + 8); ++guard) {
     if (S.post == 1) {  // after a first-pass panel (ldlt_kernel.cpp:1047-1095)
+      if (S.stalled && stale()) return tpp_request_flush(S);
       S.post = 0;
       const int k = S.k, pl = S.pl;
       if (S.stalled && k != S.k_paired) {
@@ -704,6 +731,7 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
       continue;
     }
     if (S.post == 2) {  // after a main-loop panel (ldlt_kernel.cpp:1113-1127)
+      if (S.stalled && S.k < ne && stale()) return tpp_request_flush(S);
       S.post = 0;
       if (S.stalled && S.k < ne) {
         const int ss = S.k;
@@ -716,7 +744,7 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
         S.g_p0 = ss;
         S.g_p1 = S.k;
         S.g_c0 = S.k;
-        S.g_e = ne;
+        S.g_e = tpp_upd_end(S, ne);
         S.post = 3;
         return true;
       }
@@ -728,6 +756,8 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
     }
     if (S.phase == 0) {
       if (S.k < S.live) {
+        if (S.mixed && S.tc_done < S.k && min(S.live, S.k + prm.nb) > min(S.se, ne))
+          return tpp_request_flush(S);
         S.ps = S.k;
         S.pl = min(S.live, S.ps + prm.nb);
         S.stalled = 0;
@@ -742,7 +772,7 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
         S.g_p0 = S.ps;
         S.g_p1 = S.k;
         S.g_c0 = S.pl;
-        S.g_e = ne;
+        S.g_e = tpp_upd_end(S, ne);
         S.post = 1;
         return true;
       }
@@ -750,6 +780,8 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
     }
     if (S.phase == 1) {
       if (S.k < ne) {
+        if (S.mixed && S.tc_done < S.k && min(ne, S.k + prm.nb) > min(S.se, ne))
+          return tpp_request_flush(S);
         S.ps = S.k;
         S.pl = min(ne, S.ps + prm.nb);
         S.stalled = 0;
@@ -764,7 +796,7 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
         S.g_p0 = S.ps;
         S.g_p1 = S.k;
         S.g_c0 = S.pl;
-        S.g_e = ne;
+        S.g_e = tpp_upd_end(S, ne);
         S.post = 2;
         return true;
       }

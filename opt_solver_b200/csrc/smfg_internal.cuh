@@ -61,6 +61,14 @@ struct DevFactor {
   TppState *tpp = nullptr;    // per large front of a level: blocked-pivoting state
   double *work = nullptr;     // solve / refinement scratch
   int64_t work_cap = 0;
+  // mixed precision: fronts whose trailing updates run on the tensor cores
+  int8_t *sn_mixed = nullptr;    // per supernode, 0 / 1
+  void *tc_jobs = nullptr;       // tc::Job per large front of a level
+  int64_t *tc_ipref = nullptr;   // split work items, prefix over jobs
+  int *tc_tpref = nullptr;       // tiles, prefix over jobs
+  int *tc_njobs = nullptr;
+  uint8_t *tc_img = nullptr;     // operand images
+  int64_t tc_img_cap = 0;
 };
 
 struct Plan {
@@ -90,6 +98,10 @@ struct Plan {
   int factor_status = -1;
   smfg_info_t info{};
   std::vector<int> h_child_ptr, h_child_idx, h_sn_parent, h_postorder;
+  std::vector<int> h_fsym;             // symbolic front rows per supernode
+  std::vector<int8_t> front_mask;      // caller's per-front precision choice (empty: all may)
+  std::vector<int8_t> h_mixed;         // mixed fronts of the last factorization
+  int mixed_count = 0;
   std::vector<void *> allocs;
 };
 

@@ -3,15 +3,19 @@
 // supernodal solves and the residual.
 #pragma once
 #include "smfg_internal.cuh"
+#include "smfg_tc.cuh"
 
 namespace smfg {
 
 // counters[] slots
 enum : int { kCArena = 0, kCRows = 1, kCFlags = 2, kCMaxAbs = 3, kCAux = 4, kCEffSmall = 5,
-             kCActive = 6, kCGemmFlops = 7, kCCount = 8 };
+             kCActive = 6, kCGemmFlops = 7, kCTcFlops = 8, kCCount = 9 };
 // error flag bits (counters[kCFlags])
 enum : unsigned { kFArena = 1u, kFRows = 2u, kFNonfinite = 4u, kFNotPosdef = 8u, kFNonfiniteD = 16u,
-                  kFMap = 32u, kFInternal = 64u };
+                  kFMap = 32u, kFInternal = 64u, kFTcWait = 128u, kFTcCap = 256u };
+// flags after which the rest of a factorization is skipped (retried with
+// more room, or reported)
+constexpr unsigned kFAbort = kFArena | kFRows | kFTcWait | kFTcCap;
 
 __device__ __forceinline__ void set_flag(unsigned long long *cnt, unsigned bit) {
   atomicOr(cnt + kCFlags, (unsigned long long)bit);
@@ -136,7 +140,7 @@ __global__ void k_level_setup(DevPlan P, DevFactor X, int lo, int hi, int lvl, i
 // Rows of each front (children's delayed rows in child order, then its
 // symbolic rows) and each child's contribution-block row map into it.
 __global__ void k_level_rows(DevPlan P, DevFactor X, int lo, int hi) {
-  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  if (X.counters[kCFlags] & kFAbort) return;
   const int s = P.lvl_sn[lo + blockIdx.x];
   const int64_t roff = X.sn_roff[s];
   const int nd = X.sn_nd[s], f = X.sn_f[s], fsym = P.sn_fsym[s];
@@ -173,7 +177,7 @@ __global__ void k_level_rows(DevPlan P, DevFactor X, int lo, int hi) {
 // A child's block is read in place from its own front.
 __global__ void k_level_assemble(DevPlan P, DevFactor X, int lo, int hi, int lvl) {
   unsigned long long *cnt = X.counters;
-  if (cnt[kCFlags] & (kFArena | kFRows)) return;
+  if (cnt[kCFlags] & kFAbort) return;
   const int *pref = X.lvl_blk + lo + lvl;  // m + 1 prefix entries
   const int m = hi - lo;
   const int total = pref[m];
@@ -407,7 +411,7 @@ __device__ void store_front(DevPlan &P, DevFactor &X, int s, const FrontRef &v, 
 template <int NT, int FMIN, int FMAX, bool SMEM>
 __global__ void __launch_bounds__(NT) k_factor(DevPlan P, DevFactor X, int lo, int hi, PivotParams prm) {
   extern __shared__ __align__(16) double smem[];
-  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  if (X.counters[kCFlags] & kFAbort) return;
   const int s = P.lvl_sn[lo + blockIdx.x];
   const int f = X.sn_f[s];
   if (f < FMIN || f > FMAX || P.sn_fsym[s] >= kLargeMin) return;
@@ -435,15 +439,16 @@ __device__ __forceinline__ FrontRef large_view(DevPlan &P, DevFactor &X, int s) 
 }
 
 __global__ void k_large_init(DevPlan P, DevFactor X, const int *__restrict__ large, int nlarge,
-                             int posdef) {
-  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+                             int posdef, int nbo) {
+  if (X.counters[kCFlags] & kFAbort) return;
   const int s = large[blockIdx.x];
   const int f = X.sn_f[s];
   int *loc = X.ploc + X.sn_roff[s];
   for (int t = threadIdx.x; t < f; t += blockDim.x) loc[t] = t;
   if (threadIdx.x == 0) {
     TppState S;
-    tpp_init(S, X.sn_ne[s], posdef != 0);
+    const bool mixed = X.sn_mixed != nullptr && X.sn_mixed[s] != 0 && nbo > 0;
+    tpp_init(S, X.sn_ne[s], posdef != 0, mixed, nbo);
     S.pad[0] = 0;  // deferred update pending
     X.tpp[blockIdx.x] = S;
   }
@@ -453,7 +458,7 @@ template <int NT>
 __global__ void __launch_bounds__(NT) k_large_panel(DevPlan P, DevFactor X, const int *__restrict__ large,
                                                     PivotParams prm, int iter) {
   __shared__ FrontShared sh;
-  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  if (X.counters[kCFlags] & kFAbort) return;
   const int s = large[blockIdx.x];
   TppState S = X.tpp[blockIdx.x];
   if (S.phase == 2) {
@@ -644,7 +649,7 @@ __global__ void __launch_bounds__(256) k_large_gemm(DevPlan P, DevFactor X, cons
   extern __shared__ __align__(16) double dsm_g[];
   TileSmem &sm = *reinterpret_cast<TileSmem *>(dsm_g);
   __shared__ int pref[129];
-  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  if (X.counters[kCFlags] & kFAbort) return;
   for (int chunk = 0; chunk < nlarge; chunk += 128) {
     const int cnt = min(128, nlarge - chunk);
     __syncthreads();
@@ -688,7 +693,7 @@ __global__ void __launch_bounds__(256) k_large_schur(DevPlan P, DevFactor X, con
   extern __shared__ __align__(16) double dsm_g[];
   TileSmem &sm = *reinterpret_cast<TileSmem *>(dsm_g);
   __shared__ int pref[129];
-  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  if (X.counters[kCFlags] & kFAbort) return;
   for (int chunk = 0; chunk < nlarge; chunk += 128) {
     const int cnt = min(128, nlarge - chunk);
     __syncthreads();
@@ -697,7 +702,9 @@ __global__ void __launch_bounds__(256) k_large_schur(DevPlan P, DevFactor X, con
       for (int q = 0; q < cnt; ++q) {
         const int s = large[chunk + q];
         const int e = X.sn_ne[s], f = X.sn_f[s], k = tpp[chunk + q].k;
-        pref[q + 1] = pref[q] + ((f > e && k > 0) ? trap_tiles2(f - e, f - e) : 0);
+        // mixed fronts: the tensor-core updates covered the contribution block
+        const bool fp64 = !tpp[chunk + q].mixed;
+        pref[q + 1] = pref[q] + ((f > e && k > 0 && fp64) ? trap_tiles2(f - e, f - e) : 0);
       }
     }
     __syncthreads();
@@ -728,13 +735,13 @@ __global__ void __launch_bounds__(256) k_large_schur(DevPlan P, DevFactor X, con
 template <int NT>
 __global__ void __launch_bounds__(NT) k_large_finish(DevPlan P, DevFactor X, const int *__restrict__ large,
                                                      const TppState *__restrict__ tpp, PivotParams prm) {
-  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  if (X.counters[kCFlags] & kFAbort) return;
   const int s = large[blockIdx.x];
   const TppState S = tpp[blockIdx.x];
   const FrontRef v = large_view(P, X, s);
   const int f = v.f, ne = v.ne, p = S.k;
   const size_t sf = (size_t)f;
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && !S.mixed) {
     const double q = (double)(f - ne);
     if (q > 0 && p > 0)
       atomicAdd(reinterpret_cast<double *>(X.counters + kCGemmFlops), 2.0 * p * (q * (q + 1) / 2));
@@ -790,7 +797,7 @@ __global__ void __launch_bounds__(256) k_large_store(DevPlan P, DevFactor X, con
                                                      int nlarge, int posdef) {
   __shared__ int pref[65];
   __shared__ double sdv[32];
-  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  if (X.counters[kCFlags] & kFAbort) return;
   for (int chunk = 0; chunk < nlarge; chunk += 64) {
     const int cnt = min(64, nlarge - chunk);
     if (threadIdx.x == 0) {
@@ -862,7 +869,7 @@ __global__ void __launch_bounds__(256) k_large_panel_spd(DevPlan P, DevFactor X,
   __shared__ double lm[NB][NB];
   __shared__ double linv[NB];
   __shared__ int np_sh;
-  if (X.counters[kCFlags] & (kFArena | kFRows)) return;
+  if (X.counters[kCFlags] & kFAbort) return;
   const int q = blockIdx.y;
   const int s = large[q];
   const TppState S = cur[q];
@@ -950,18 +957,79 @@ __global__ void __launch_bounds__(256) k_large_panel_spd(DevPlan P, DevFactor X,
     o.g_p0 = ps;
     o.g_p1 = ps + np;
     o.g_c0 = pl;
-    o.g_e = ne;
+    o.g_e = tpp_upd_end(S, ne);
     o.pad[0] = np > 0 ? 1 : 0;
     if (np < nbp || o.k >= ne) o.phase = 2;
     nxt[q] = o;
     if (np > 0) {
       atomicMax(X.counters + kCActive, (unsigned long long)(iter + 1));
-      const long long m = ne - pl, h = f - pl;
+      const long long m = tpp_upd_end(S, ne) - pl, h = f - pl;
       if (m > 0)
         atomicAdd(reinterpret_cast<double *>(X.counters + kCGemmFlops),
                   2.0 * (double)np * (double)(m * h - m * (m - 1) / 2));
     }
   }
+}
+
+// Tensor-core updates due on a level's mixed large fronts (one thread): a
+// front whose outer block is used up (k reached min(se, ne)), that asked
+// for a flush, or that finished with pivots pending gets a job applying
+// the pivots [tc_done, k) to its columns from min(se, ne) on (the rows and
+// columns no deferred update of the block touched); its next outer block
+// then starts at k. Jobs, work-item and tile prefixes go to X.tc_*.
+__global__ void k_tc_jobs(DevPlan P, DevFactor X, const int *__restrict__ large, int nlarge,
+                          TppState *__restrict__ tpp, int nbo, int posdef, int ke) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  tc::Job *jobs = reinterpret_cast<tc::Job *>(X.tc_jobs);
+  int nj = 0, tiles = 0;
+  int64_t off = 0, items = 0;
+  double flops = 0.0;
+  X.tc_ipref[0] = 0;
+  X.tc_tpref[0] = 0;
+  const bool dead = (X.counters[kCFlags] & kFAbort) != 0;
+  for (int q = 0; q < nlarge && !dead; ++q) {
+    TppState &S = tpp[q];
+    if (!S.mixed) continue;
+    const int s = large[q];
+    const int f = X.sn_f[s], ne = X.sn_ne[s], k = S.k;
+    const int sep = min(S.se, ne);
+    if (S.tc_done < k && (S.flush || k >= sep || S.phase == 2)) {
+      const int n = f - sep, kc = k - S.tc_done;
+      if (n > 0) {
+        double *F = X.arena + X.sn_off[s];
+        tc::Job J;
+        J.C = F;
+        J.Ls = F + (int64_t)S.tc_done * f;
+        J.Ws = nullptr;
+        J.tags = posdef ? nullptr : X.tags + X.sn_roff[s];
+        J.ld = J.ldl = J.ldw = f;
+        J.r0 = J.lr0 = J.wr0 = sep;
+        J.n = n;
+        J.k0 = S.tc_done;
+        J.kc = kc;
+        J.ntr = (n + tc::kBM - 1) / tc::kBM;
+        J.nkb = (kc + ke - 1) / ke;
+        J.tiles = J.ntr * (J.ntr + 1) / 2;
+        J.img = off;
+        off += tc::image_bytes(J.ntr, J.nkb);
+        items += (int64_t)J.ntr * tc::kBM * 8 * J.nkb;
+        tiles += J.tiles;
+        jobs[nj++] = J;
+        X.tc_ipref[nj] = items;
+        X.tc_tpref[nj] = tiles;
+        flops += 2.0 * kc * ((double)n * (n + 1) / 2);
+      }
+      S.tc_done = k;
+      S.se = k + nbo;
+    }
+    S.flush = 0;
+  }
+  if (off > X.tc_img_cap) {
+    set_flag(X.counters, kFTcCap);
+    nj = 0;
+  }
+  *X.tc_njobs = nj;
+  if (flops > 0.0) atomicAdd(reinterpret_cast<double *>(X.counters + kCTcFlops), flops);
 }
 
 // Totals over all fronts, in supernode order (deterministic).
@@ -1578,6 +1646,80 @@ __global__ void k_axpy(double *__restrict__ x, const double *__restrict__ dx, in
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < len;
        t += (int64_t)gridDim.x * blockDim.x)
     x[t] += dx[t];
+}
+
+// ---------------------------------------------------------------------------
+// Krylov helpers of the FGMRES refinement (refinement.cpp:451-643): dot
+// products in a fixed order (per-block partials, then one block), vector
+// updates whose coefficient stays in device memory, the product with A.
+
+constexpr int kDotBlocks = 296;
+
+__global__ void __launch_bounds__(256) k_dot_part(const double *__restrict__ a, const double *__restrict__ b,
+                                                  int64_t n, double *__restrict__ part) {
+  __shared__ double red[8];
+  double s = 0.0;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+    s = fma(a[t], b[t], s);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_dot_fin(const double *__restrict__ part, int nparts, double *__restrict__ out) {
+  __shared__ double red[32];
+  double s = 0.0;
+  for (int t = threadIdx.x; t < nparts; t += blockDim.x) s += part[t];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    *out = t;
+  }
+}
+
+// y -= coef[0] * x
+__global__ void k_axpy_coef(double *__restrict__ y, const double *__restrict__ x, const double *__restrict__ coef,
+                            int64_t n) {
+  const double c = *coef;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+    y[t] = fma(-c, x[t], y[t]);
+}
+
+// y = x * alpha
+__global__ void k_scale(double *__restrict__ y, const double *__restrict__ x, double alpha, int64_t n) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+    y[t] = x[t] * alpha;
+}
+
+// xc = x0 + sum_l y[l] Z[l]
+__global__ void k_lincomb(double *__restrict__ xc, const double *__restrict__ x0, const double *__restrict__ Z,
+                          const double *__restrict__ y, int k, int64_t n) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    double v = x0[t];
+    for (int l = 0; l < k; ++l) v = fma(y[l], Z[(int64_t)l * n + t], v);
+    xc[t] = v;
+  }
+}
+
+// y = A x in the new numbering (the unscaled values), a warp per row
+__global__ void k_spmv(DevPlan P, const double *__restrict__ vals, const double *__restrict__ x,
+                       double *__restrict__ y, int n) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+    double s = 0.0;
+    for (int k = P.sptr[i] + lane; k < P.sptr[i + 1]; k += 32) s = fma(vals[P.sidx[k]], x[P.srow[k]], s);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) y[i] = s;
+  }
 }
 
 }  // namespace smfg

@@ -64,6 +64,9 @@ __host__ __device__ constexpr int64_t image_bytes(int ntr, int nkb) {
   return (int64_t)kOps * ntr * nkb * kBlkBytes;
 }
 
+// Elements of one 128-byte k-block row.
+__host__ __device__ constexpr int kblock_elems(int kind) { return kind == kTF32x3 ? 32 : 64; }
+
 // ---------------------------------------------------------------------------
 // PTX wrappers.
 
@@ -233,10 +236,11 @@ __device__ __forceinline__ double ld_value(const Job &J, int i, int t) {
 // core matrix (row group g, chunk q) at (g * 8 + q) * 128 bytes, row i & 7
 // at 16 (i & 7) bytes within it.
 template <int KIND>
-__global__ void __launch_bounds__(256) k_tc_split(const Job *__restrict__ jobs, int njobs,
+__global__ void __launch_bounds__(256) k_tc_split(const Job *__restrict__ jobs, const int *__restrict__ njobs_p,
                                                   const int64_t *__restrict__ item_pref, uint8_t *__restrict__ img) {
   constexpr int E = (KIND == kTF32x3) ? 4 : 8;  // elements per 16-byte chunk
   constexpr int KE = kRowBytes / ((KIND == kTF32x3) ? 4 : 2);  // elements per k-block row
+  const int njobs = *njobs_p;
   const int64_t total = item_pref[njobs];
   for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < total;
        w += (int64_t)gridDim.x * blockDim.x) {
@@ -334,10 +338,11 @@ __device__ __forceinline__ int find_job(const int *__restrict__ tile_pref, int n
 
 template <int KIND>
 __global__ void __launch_bounds__(kThreads, 1)
-    k_tc_syrk(const Job *__restrict__ jobs, int njobs, const int *__restrict__ tile_pref,
-              const uint8_t *__restrict__ img, unsigned long long *__restrict__ err) {
+    k_tc_syrk(const Job *__restrict__ jobs, const int *__restrict__ njobs_p, const int *__restrict__ tile_pref,
+              const uint8_t *__restrict__ img, unsigned long long *__restrict__ err, unsigned long long err_bit) {
   extern __shared__ __align__(1024) uint8_t tc_dsm[];
   Smem &sm = *reinterpret_cast<Smem *>(tc_dsm);
+  const int njobs = *njobs_p;
   const int total = tile_pref[njobs];
   if ((int)blockIdx.x >= total) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -474,7 +479,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   tc_fence_before();
   __syncthreads();
-  if (threadIdx.x == 0 && sm.abort) atomicOr(err, 1ull);
+  if (threadIdx.x == 0 && sm.abort) atomicOr(err, err_bit);
   if (warp == 1) {
     __syncwarp();
     tc_fence_after();

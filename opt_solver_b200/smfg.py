@@ -56,7 +56,8 @@ class Control(C.Structure):
     _fields_ = [("abi_version", C.c_int), ("posdef", C.c_int), ("u", C.c_double),
                 ("small_pivot", C.c_double), ("nb", C.c_int), ("blocked_min_front", C.c_int),
                 ("precision", C.c_int), ("max_negative_pivots", C.c_int),
-                ("scale", C.c_void_p), ("reserved_i", C.c_int * 8),
+                ("scale", C.c_void_p), ("profile", C.c_int), ("mixed_block", C.c_int),
+                ("mixed_kind", C.c_int), ("mixed_min_front", C.c_int), ("reserved_i", C.c_int * 4),
                 ("reserved_d", C.c_double * 8)]
 
 
@@ -121,6 +122,16 @@ def lib():
         L.smfg_residual_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                             C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.smfg_residual_noalloc.restype = C.c_int
+        L.smfg_refine_method.argtypes = [C.c_void_p, _f64p, _f64p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                         C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                         C.POINTER(C.c_int)]
+        L.smfg_refine_method.restype = C.c_int
+        L.smfg_refine_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                         C.c_int, C.c_double, C.POINTER(C.c_double),
+                                         C.POINTER(C.c_double), C.POINTER(C.c_int)]
+        L.smfg_refine_device.restype = C.c_int
+        L.smfg_set_front_precision.argtypes = [C.c_void_p, C.c_void_p]
+        L.smfg_set_front_precision.restype = C.c_int
         L.smfg_front_stats.argtypes = [C.c_void_p, _i32p]
         L.smfg_front_stats.restype = C.c_int
         L.smfg_error_string.argtypes = [C.c_int]
@@ -256,6 +267,7 @@ def analyse(n, col_ptr, row_idx, ordering: int = ORDER_ND, nemin: int = 8,
 
 
 TC_TF32X3, TC_BF16X3 = 0, 1
+REFINE_CLASSICAL, REFINE_FGMRES, REFINE_AUTO = 0, 1, 2
 
 
 def tc_update(C_t, L_t, W_t, kind: int = TC_TF32X3):
@@ -312,13 +324,33 @@ class Solver:
             pass
 
     # -- factor ------------------------------------------------------------
+    def set_front_precision(self, mask=None):
+        """Per-front choice for mixed factorizations (smfg_set_front_precision):
+        mask[s] = 1 lets supernode s use tensor-core updates; None: all may."""
+        if mask is None:
+            rc = lib().smfg_set_front_precision(self._h, None)
+        else:
+            m = np.ascontiguousarray(mask, dtype=np.int8)
+            if m.size != self.nsn:
+                raise ValueError(f"expected {self.nsn} entries")
+            rc = lib().smfg_set_front_precision(self._h, m.ctypes.data)
+        if rc != SMFG_OK:
+            raise SmfgError(rc, "smfg_set_front_precision")
+
     def factor(self, values, posdef: bool = False, u: float = 0.01, small: float = 1e-20,
                scale=None, precision: int = PREC_FP64, max_negative_pivots: int = -1,
-               raise_on_singular: bool = False) -> Info:
+               raise_on_singular: bool = False, mixed_block: int = 0, mixed_kind: int = 0,
+               mixed_min_front: int = 0) -> Info:
         """Factor new values (the caller's entry order). ``values`` is a
         numpy array, or any object with ``data_ptr()`` (a CUDA tensor) for
-        values already in device memory."""
+        values already in device memory. precision=PREC_MIXED: tensor-core
+        trailing updates on large fronts (mixed_block pivots per update,
+        mixed_kind TC_TF32X3 / TC_BF16X3, fronts of mixed_min_front rows or
+        more; 0 = the library's defaults)."""
         c = default_control(posdef, u, small, precision, max_negative_pivots)
+        c.mixed_block = mixed_block
+        c.mixed_kind = mixed_kind
+        c.mixed_min_front = mixed_min_front
         if scale is not None and len(scale):
             self._scale = np.ascontiguousarray(scale, dtype=np.float64)
             c.scale = self._scale.ctypes.data
@@ -345,7 +377,7 @@ class Solver:
         large-front GEMM kernels: their total device time, launch count and
         algorithmic flops (2 per fused multiply-add of the updates)."""
         c = default_control(posdef, 0.01, 1e-20, precision)
-        c.reserved_i[0] = 1
+        c.profile = 1
         if scale is not None and len(scale):
             self._scale = np.ascontiguousarray(scale, dtype=np.float64)
             c.scale = self._scale.ctypes.data
@@ -445,13 +477,28 @@ class Solver:
             raise SmfgError(rc, "smfg_residual_noalloc")
         return eta.value, om.value
 
-    def refine(self, b, x, max_steps: int = 10, omega_target: float = 1e-8):
+    def refine(self, b, x, max_steps: int = 10, omega_target: float = 1e-8,
+               method: int = REFINE_CLASSICAL, restart: int = 20):
+        """Iterative refinement of x for b (smfg_refine_method): classical,
+        FGMRES or auto; returns (x, eta_inf, omega, solves used)."""
         b = np.ascontiguousarray(b, dtype=np.float64)
         x = np.array(x, dtype=np.float64, copy=True, order="C")
         nrhs = 1 if b.ndim == 1 else b.shape[0]
         eta, om, st = C.c_double(), C.c_double(), C.c_int()
-        rc = lib().smfg_refine(self._h, b.reshape(-1), x.reshape(-1), nrhs, max_steps,
-                               omega_target, C.byref(eta), C.byref(om), C.byref(st))
+        rc = lib().smfg_refine_method(self._h, b.reshape(-1), x.reshape(-1), nrhs, method, max_steps,
+                                      restart, omega_target, C.byref(eta), C.byref(om), C.byref(st))
         if rc != SMFG_OK:
-            raise SmfgError(rc, "smfg_refine")
+            raise SmfgError(rc, "smfg_refine_method")
         return x, eta.value, om.value, st.value
+
+    def refine_device(self, d_b, d_x, nrhs: int = 1, max_steps: int = 10,
+                      omega_target: float = 1e-8, method: int = REFINE_AUTO, restart: int = 20):
+        """smfg_refine_device on CUDA tensors (n x nrhs, leading dimension
+        n); d_x refined in place. Returns (eta_inf, omega, solves used)."""
+        eta, om, st = C.c_double(), C.c_double(), C.c_int()
+        rc = lib().smfg_refine_device(self._h, C.c_void_p(d_b.data_ptr()), C.c_void_p(d_x.data_ptr()), nrhs,
+                                      method, max_steps, restart, omega_target, C.byref(eta),
+                                      C.byref(om), C.byref(st))
+        if rc != SMFG_OK:
+            raise SmfgError(rc, "smfg_refine_device")
+        return eta.value, om.value, st.value
