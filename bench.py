@@ -246,58 +246,89 @@ def dgemm_peak_tflops():
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+OMEGA_GATE = 1e-12  # the metric's scaled backward error bar
+
+
 def run_ours(args, rank, world, local):
+    """Both arms on the same workload: plain FP64 and mixed precision, each
+    step = factor + solve + refinement (auto: classical, then FGMRES) until
+    eta_inf <= 1e-10 and omega <= 1e-12, all on the device; per arm the
+    mean device time of K steps after W warm-up steps, max over ranks."""
     import torch
     from opt_solver_b200 import smfg
 
     torch.cuda.set_device(local)
     wl = _Workload(args.config, local, rank, world)
     sv, posdef = wl.sv, wl.posdef
-    prec = smfg.PREC_MIXED if args.precision == "mixed" else smfg.PREC_FP64
     d_vals = torch.from_numpy(np.ascontiguousarray(wl.values)).cuda()
     d_b0 = torch.from_numpy(np.ascontiguousarray(wl.b)).cuda()
-    d_b = d_b0.clone()
+    d_x = d_b0.clone()
+    arms = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    head = "mixed" if "mixed" in arms else "fp64"
+    res = {}
+    clocks = None
+    for arm in arms:
+        prec = smfg.PREC_MIXED if arm == "mixed" else smfg.PREC_FP64
 
-    def step():
-        info = sv.factor(d_vals, posdef=posdef, precision=prec)
-        d_b.copy_(d_b0)
-        sv.solve(d_b)
-        return info.factor_ms + sv.info.solve_ms, info
+        def step():
+            info = sv.factor(d_vals, posdef=posdef, precision=prec)
+            d_x.copy_(d_b0)
+            sv.solve(d_x)
+            eta, om, its = sv.refine_device(d_b0, d_x, nrhs=wl.nrhs, max_steps=args.refine_max,
+                                            omega_target=OMEGA_GATE, method=smfg.REFINE_AUTO)
+            f, so, rf = sv.last_times()
+            return f + so + rf, (f, so, rf), info, (eta, om, its)
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    barrier(world)
-    dev_ms = []
-    with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            ms, info = step()
-            dev_ms.append(ms)
-    torch.cuda.synchronize()
-    barrier(world)
-    ms_step = allmax(sum(dev_ms) / len(dev_ms), world)
-    inertia_ok = wl.inertia_ok()
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        barrier(world)
+        dev, parts = [], []
+        sampler = ClockSampler(local)
+        with sampler as clk:
+            for _ in range(args.steps):
+                ms, pr, info, acc = step()
+                dev.append(ms)
+                parts.append(pr)
+        torch.cuda.synchronize()
+        barrier(world)
+        if arm == head:
+            clocks = clk.summary()
+        ms_step = allmax(sum(dev) / len(dev), world)
+        fm = [p_[0] for p_ in parts]
+        sm_ = [p_[1] for p_ in parts]
+        rm = [p_[2] for p_ in parts]
+        res[arm] = {
+            "ms": ms_step, "factor_ms": sum(fm) / len(fm), "solve_ms": sum(sm_) / len(sm_),
+            "refine_ms": sum(rm) / len(rm), "eta_inf": acc[0], "omega": acc[1], "refine_solves": acc[2],
+            "inertia": list(info.inertia), "inertia_exact_per_system": wl.inertia_ok(),
+            "mixed_fronts": int(info.mixed_fronts), "kernel_launches": int(info.kernel_launches),
+            "flops": info.flops, "delayed": int(info.delayed_pivots),
+            "info": info,
+        }
+    # the arms agree on the inertia
+    if len(arms) == 2:
+        res["inertia_same"] = res["fp64"]["inertia"] == res["mixed"]["inertia"]
     # e2e: host buffers through the C ABI (copies inside the timed region)
+    prec = smfg.PREC_MIXED if head == "mixed" else smfg.PREC_FP64
     e2e = []
     for _ in range(max(2, min(args.steps, 5))):
         torch.cuda.synchronize()
         t = time.perf_counter()
         sv.factor(wl.values, posdef=posdef, precision=prec)
         x = sv.solve(wl.b)
+        x, _, _, _ = sv.refine(wl.b, x, max_steps=args.refine_max, omega_target=OMEGA_GATE,
+                               method=smfg.REFINE_AUTO)
         e2e.append((time.perf_counter() - t) * 1e3)
     e2e_ms = allmax(sum(e2e) / len(e2e), world)
     _, eta, om = sv.residual(wl.b, x)
-    out = {
-        "ms_per_step": ms_step, "info": sv.info, "eta": eta, "omega": om,
-        "analyse_s": wl.analyse_s, "e2e_ms": e2e_ms, "n": wl.n, "nnz": wl.nnz, "nrhs": wl.nrhs,
-        "desc": wl.desc, "clocks": clk.summary(), "nsn": wl.nsn, "systems": wl.systems,
-        "inertia_ok": inertia_ok,
-        "h2d": wl.nnz * 8 + wl.n * wl.nrhs * 8, "d2h": wl.n * wl.nrhs * 8,
-    }
     prof = sv.profile_factor(d_vals, posdef=posdef, precision=prec)
-    out["profile"] = prof
-    out["info"] = info
-    return out
+    return {
+        "arms": res, "head": head, "e2e_ms": e2e_ms, "e2e_eta": eta, "e2e_omega": om,
+        "analyse_s": wl.analyse_s, "n": wl.n, "nnz": wl.nnz, "nrhs": wl.nrhs, "desc": wl.desc,
+        "clocks": clocks, "nsn": wl.nsn, "systems": wl.systems,
+        "h2d": wl.nnz * 8 + wl.n * wl.nrhs * 8, "d2h": wl.n * wl.nrhs * 8, "profile": prof,
+    }
 
 
 def cpu_reference_ms(cfg, threads):
@@ -379,7 +410,7 @@ def ncu_step(args):
     import torch
     from opt_solver_b200 import smfg
     wl = _Workload(args.config, 0)
-    prec = smfg.PREC_MIXED if args.precision == "mixed" else smfg.PREC_FP64
+    prec = smfg.PREC_FP64 if args.precision == "fp64" else smfg.PREC_MIXED
     d_vals = torch.from_numpy(np.ascontiguousarray(wl.values)).cuda()
     d_b = torch.from_numpy(np.ascontiguousarray(wl.b)).cuda()
     info = wl.sv.factor(d_vals, posdef=wl.posdef, precision=prec)
@@ -397,7 +428,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="spd3d", choices=sorted(CONFIGS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
+                    help="both: time the plain FP64 and the mixed arm; the value is the mixed one")
+    ap.add_argument("--refine-max", type=int, default=30, help="refinement solves per step, at most")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ncu-step", action="store_true",
                     help="one factorization + solve and exit (for an ncu launch list)")
@@ -415,10 +448,28 @@ def main():
     r = run_ours(args, rank, world, local)
     if rank != 0:
         return
-    info = r["info"]
+    head = r["head"]
+    A = r["arms"][head]
+    info = A["info"]
     peaks = measured_peaks()
     prof = r["profile"]
-    if prof["gemm_ms"] > 0:
+    if head == "mixed" and prof.get("tc_ms", 0) > 0:
+        # the tensor-core trailing updates (split + product kernels) against
+        # the tensor pipe's rate for TF32 (half the measured BF16 dense
+        # rate) divided by the 3 split products each algorithmic product costs
+        bf = peaks.get("bf16_tflops") or 1590.0
+        peak = bf / 2.0 / 3.0
+        achieved = prof["tc_flops"] / (prof["tc_ms"] * 1e-3) / 1e12
+        roof = {
+            "kernel": "k_tc_split + k_tc_syrk (tcgen05 TF32x3 trailing updates of the mixed fronts)",
+            "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "traffic": None,
+            "peak_source": ("MEASURED_PEAKS.json bf16_tflops" if peaks.get("bf16_tflops") else "fallback 1590")
+            + " / 2 (TF32 rate) / 3 (split products per algorithmic product)",
+            "launches": prof["tc_passes"], "avg_launch_ms": prof["tc_ms"] / max(prof["tc_passes"], 1),
+            "algorithmic_flops_per_launch": prof["tc_flops"] / max(prof["tc_passes"], 1),
+        }
+    elif prof["gemm_ms"] > 0:
         dpeak = dgemm_peak_tflops()
         achieved = prof["gemm_flops"] / (prof["gemm_ms"] * 1e-3) / 1e12
         roof = {
@@ -434,7 +485,7 @@ def main():
         # whole against HBM, its algorithmic bytes the front arena written by
         # assembly and read + written by the front kernels (3 passes)
         hbm = peaks.get("hbm_gbs") or 6650.0
-        achieved = 3.0 * prof.get("arena_bytes", 0.0) / (info.factor_ms * 1e-3) / 1e9 if info.factor_ms else 0.0
+        achieved = 3.0 * prof.get("arena_bytes", 0.0) / (A["factor_ms"] * 1e-3) / 1e9 if A["factor_ms"] else 0.0
         roof = {
             "kernel": "whole factorization (level kernels of small fronts)", "bound": "hbm",
             "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
@@ -453,25 +504,35 @@ def main():
         except Exception as exc:  # noqa: BLE001
             cpu = {"value": None, "unit": "ms", "cores": 0, "kind": "reference", "sample": f"failed: {exc}"}
     batch = args.config == "batch"
+    arms = {}
+    for k, v in r["arms"].items():
+        if isinstance(v, dict):
+            arms[k] = {kk: vv for kk, vv in v.items() if kk != "info"}
     line = {
-        "metric": "factor+solve ms", "value": r["ms_per_step"], "unit": "ms", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+        "metric": "factor+solve ms", "value": A["ms"], "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": A["ms"],
         "higher_is_better": False, "scaling": "strong" if batch else "weak", "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "f64" if head == "fp64" else "f64 (tf32x3 tensor-core trailing updates)",
         "data": "synthetic (seeded generator of the configuration)",
         "config": {"workload": r["desc"], "n": r["n"], "nnz_lower": r["nnz"], "nrhs": r["nrhs"],
                    "supernodes": r["nsn"], "systems_this_rank": r["systems"],
                    "analysis": "engine nested dissection (smfg_analyse)",
-                   "precision": args.precision,
+                   "precision": head, "omega_gate": OMEGA_GATE,
+                   "step": "factor + solve + refinement (auto) to eta_inf <= 1e-10, omega <= 1e-12",
                    "parallelism": ("systems sharded over ranks" if batch else "replicas") if world > 1 else "1 GPU",
                    "l2": "inputs larger than L2 (front arena %.1f GB)" % (prof.get("arena_bytes", 0) / 1e9)},
         "e2e": {"value": r["e2e_ms"], "unit": "ms", "h2d_bytes_per_step": r["h2d"],
-                "d2h_bytes_per_step": r["d2h"]},
-        "gpu_launches": int(info.kernel_launches),
-        "factor_ms": info.factor_ms, "solve_ms": info.solve_ms, "flops": info.flops,
-        "gflops": info.flops / (info.factor_ms * 1e-3) / 1e9 if info.factor_ms else None,
-        "inertia": list(info.inertia), "inertia_exact_per_system": r["inertia_ok"],
-        "eta_inf": r["eta"], "omega": r["omega"],
+                "d2h_bytes_per_step": r["d2h"], "omega": r["e2e_omega"]},
+        "gpu_launches": int(A["kernel_launches"]),
+        "factor_ms": A["factor_ms"], "solve_ms": A["solve_ms"], "refine_ms": A["refine_ms"],
+        "flops": A["flops"],
+        "gflops": A["flops"] / (A["factor_ms"] * 1e-3) / 1e9 if A["factor_ms"] else None,
+        "inertia": A["inertia"], "inertia_exact_per_system": A["inertia_exact_per_system"],
+        "eta_inf": A["eta_inf"], "omega": A["omega"],
+        "arms": arms,
+        "mixed_speedup_vs_plain": (r["arms"]["fp64"]["ms"] / r["arms"]["mixed"]["ms"])
+        if len(arms) == 2 else None,
+        "inertia_same_both_arms": r["arms"].get("inertia_same"),
         "roofline": roof, "cpu_baseline": cpu, "clocks": r["clocks"],
         "measured_peaks": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops")},
     }

@@ -10,6 +10,11 @@
  * diagonal / backward passes (solver/src/solve.cpp:858-1075), on one GPU.
  *
  * All indices are 0-based int32; dense blocks are column-major.
+ *
+ * Calls taking device pointers run on the plan's own stream after the work
+ * the calling thread has queued on the legacy default stream (where a
+ * caller's copies or torch kernels wrote the inputs), and return once their
+ * own work is done.
  */
 #ifndef SMFG_H
 #define SMFG_H
@@ -130,9 +135,10 @@ typedef struct {
   int levels;
   int kernel_launches;    /* kernels launched by the last call */
   int mixed_fronts;       /* fronts whose trailing updates ran on the tensor cores */
-  int reserved_i[7];      /* [0]: profiled launches */
-  double reserved_d[8];   /* [0] profiled ms, [1] FP64 update flops, [2] arena bytes,
-                             [3] tensor-core update flops (2 per multiply-add) */
+  int reserved_i[7];      /* [0] profiled FP64 update launches, [1] tensor-core update passes */
+  double reserved_d[8];   /* [0] profiled FP64 update ms, [1] FP64 update flops, [2] arena bytes,
+                             [3] tensor-core update flops (2 per multiply-add), [4] profiled
+                             tensor-core update ms (split + product kernels) */
 } smfg_info_t;
 
 typedef struct smfg_plan_s *smfg_plan_t;
@@ -234,6 +240,11 @@ SMFG_API int smfg_refine_method(smfg_plan_t plan, const double *b, double *x, in
 SMFG_API int smfg_refine_device(smfg_plan_t plan, const double *d_b, double *d_x, int nrhs, int method,
                                 int max_iters, int restart, double omega_target, double *eta_inf,
                                 double *omega, int *iters);
+
+/* Device times (CUDA events on the plan's stream) of the last factor, solve
+ * and refinement; a refinement's time includes its waits for the host's
+ * small Hessenberg work between iterations. */
+SMFG_API int smfg_last_times(smfg_plan_t plan, double *factor_ms, double *solve_ms, double *refine_ms);
 
 /* A symbolic analysis of the engine's own (host code, no GPU needed),
  * producing the smfg_analysis_t contract above when smf's analyse

@@ -59,6 +59,14 @@ void set_last_error(const char *what) { g_last_error = what ? what : ""; }
 // ones, which keep failing), so that it is not reported as this call's.
 void clear_stale_error() { (void)cudaGetLastError(); }
 
+// Device-pointer calls: the plan's (non-blocking) stream waits for the work
+// the caller queued on the legacy default stream, where the inputs were
+// written (torch's default stream, a cudaMemcpy).
+void follow_caller(Plan &pl) {
+  SMFG_CUDA(cudaEventRecord(pl.ev_in, cudaStreamLegacy));
+  SMFG_CUDA(cudaStreamWaitEvent(pl.stream, pl.ev_in, 0));
+}
+
 int sm_count(int dev) {
   int v = 0;
   cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
@@ -316,23 +324,31 @@ struct LaunchCount {
 struct GemmProfile {
   bool on = false;
   std::vector<cudaEvent_t> ev;
+  std::vector<int> cls;  // class of each mark: 0 FP64 updates, 1 tensor-core updates
   size_t used = 0;
-  void mark(cudaStream_t st) {
+  void mark(cudaStream_t st, int c = 0) {
     if (!on) return;
     if (used == ev.size()) {
       cudaEvent_t e;
       SMFG_CUDA(cudaEventCreate(&e));
       ev.push_back(e);
+      cls.push_back(0);
     }
+    cls[used] = c;
     SMFG_CUDA(cudaEventRecord(ev[used++], st));
   }
-  double total_ms() {
+  // time between the marks of each pair (i, i + 1) whose first mark is of class c
+  double total_ms(int c = 0, int *pairs = nullptr) {
     double t = 0.0;
+    int np = 0;
     for (size_t i = 0; i + 1 < used; i += 2) {
+      if (cls[i] != c) continue;
       float ms = 0.0f;
       cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
       t += ms;
+      ++np;
     }
+    if (pairs) *pairs = np;
     return t;
   }
   ~GemmProfile() {
@@ -366,7 +382,7 @@ static void enqueue_tc(Plan &pl, const MixedCfg &mc, const int *lg, int nL, TppS
   const int smem = (int)sizeof(tc::Smem);
   k_tc_jobs<<<1, 32, 0, st>>>(pl.d, x, lg, nL, states, mc.nbo, posdef, tc::kblock_elems(mc.kind));
   const tc::Job *jobs = static_cast<const tc::Job *>(x.tc_jobs);
-  gp.mark(st);
+  gp.mark(st, 1);
   if (mc.kind == tc::kTF32x3) {
     tc::k_tc_split<tc::kTF32x3><<<4 * sms, 256, 0, st>>>(jobs, x.tc_njobs, x.tc_ipref, x.tc_img);
     tc::k_tc_syrk<tc::kTF32x3><<<sms, tc::kThreads, smem, st>>>(jobs, x.tc_njobs, x.tc_tpref, x.tc_img,
@@ -376,7 +392,7 @@ static void enqueue_tc(Plan &pl, const MixedCfg &mc, const int *lg, int nL, TppS
     tc::k_tc_syrk<tc::kBF16x3><<<sms, tc::kThreads, smem, st>>>(jobs, x.tc_njobs, x.tc_tpref, x.tc_img,
                                                                  x.counters + kCFlags, kFTcWait);
   }
-  gp.mark(st);
+  gp.mark(st, 1);
   lc.n += 3;
 }
 
@@ -598,10 +614,13 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
   inf.kernel_launches = lc.n;
   // profile (ctrl.profile): large-front GEMM device time, launches,
   // algorithmic flops; arena bytes in use
-  inf.reserved_d[0] = gp.on ? gp.total_ms() : 0.0;
+  int fp64_pairs = 0, tc_pairs = 0;
+  inf.reserved_d[0] = gp.on ? gp.total_ms(0, &fp64_pairs) : 0.0;
+  inf.reserved_d[4] = gp.on ? gp.total_ms(1, &tc_pairs) : 0.0;
+  inf.reserved_i[1] = tc_pairs;
   std::memcpy(&inf.reserved_d[1], &h_cnt[kCGemmFlops], sizeof(double));
   inf.reserved_d[2] = (double)h_cnt[kCArena] * 8.0;
-  inf.reserved_i[0] = (int)(gp.used / 2);
+  inf.reserved_i[0] = fp64_pairs;
   std::memcpy(&inf.reserved_d[3], &h_cnt[kCTcFlops], sizeof(double));
   inf.mixed_fronts = pl.mixed_count;
   int rc = SMFG_OK;
@@ -781,6 +800,7 @@ SMFG_API int smfg_plan_create(const smfg_analysis_t *a, int device, smfg_plan_t 
     SMFG_CUDA(cudaStreamCreateWithFlags(&h->pl.stream, cudaStreamNonBlocking));
     SMFG_CUDA(cudaEventCreate(&h->pl.ev0));
     SMFG_CUDA(cudaEventCreate(&h->pl.ev1));
+    SMFG_CUDA(cudaEventCreateWithFlags(&h->pl.ev_in, cudaEventDisableTiming));
     h->pl.nb = 16;
     build_plan(h->pl, *a);
     SMFG_CUDA(cudaStreamSynchronize(h->pl.stream));
@@ -809,6 +829,7 @@ SMFG_API void smfg_plan_destroy(smfg_plan_t *plan) {
   for (void *p : pl.allocs) cudaFree(p);
   if (pl.ev0) cudaEventDestroy(pl.ev0);
   if (pl.ev1) cudaEventDestroy(pl.ev1);
+  if (pl.ev_in) cudaEventDestroy(pl.ev_in);
   if (pl.stream) cudaStreamDestroy(pl.stream);
   delete *plan;
   *plan = nullptr;
@@ -828,6 +849,7 @@ static int factor_common(smfg_plan_t plan, const double *values, bool on_device,
     clear_stale_error();
     const double *dv = values;
     double *tmp = nullptr;
+    if (on_device) follow_caller(pl);
     if (!on_device) {
       tmp = pl.x.work;  // staged through the work buffer
       ensure_work(pl, std::max<int64_t>(pl.nnz_in, 1) + 16);
@@ -868,6 +890,7 @@ static int solve_common(smfg_plan_t plan, double *b, bool on_device, int nrhs, i
     double *db = b;
     double *staged = nullptr;
     const size_t bytes = sizeof(double) * ((size_t)ldb * (nrhs - 1) + pl.n);
+    if (on_device) follow_caller(pl);
     if (!on_device) {
       SMFG_CUDA(cudaMallocAsync((void **)&staged, bytes, pl.stream));
       SMFG_CUDA(cudaMemcpyAsync(staged, b, bytes, cudaMemcpyHostToDevice, pl.stream));
@@ -1078,6 +1101,7 @@ SMFG_API int smfg_residual_noalloc(smfg_plan_t plan, const double *d_b, const do
   try {
     SMFG_CUDA(cudaSetDevice(pl.device));
     clear_stale_error();
+    follow_caller(pl);
     double *sc = noalloc_scratch(pl.device);
     const size_t n = (size_t)pl.n;
     double *xp = sc, *bp = sc + n, *rp = sc + 2 * n;
@@ -1342,6 +1366,10 @@ int refine_core(smfg_plan_s *plan, double *db, double *dx, int nrhs, int method,
   if (!pl.factored) return SMFG_ERR_SINGULAR;
   const size_t len = (size_t)pl.n * nrhs;
   const double tgt = omega_target > 0 ? omega_target : 1e-8;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  SMFG_CUDA(cudaEventCreate(&t0));
+  SMFG_CUDA(cudaEventCreate(&t1));
+  SMFG_CUDA(cudaEventRecord(t0, pl.stream));
   DevVec r(pl, len), best(pl, len);
   double be = 0, bo = 0;
   bool stalled = false;
@@ -1364,7 +1392,13 @@ int refine_core(smfg_plan_s *plan, double *db, double *dx, int nrhs, int method,
     be = emax;
     bo = omax;
   }
+  SMFG_CUDA(cudaEventRecord(t1, pl.stream));
   SMFG_CUDA(cudaStreamSynchronize(pl.stream));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, t0, t1);
+  pl.refine_ms = ms;
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
   if (eta_inf) *eta_inf = be;
   if (omega) *omega = bo;
   if (iters) *iters = used;
@@ -1374,6 +1408,15 @@ int refine_core(smfg_plan_s *plan, double *db, double *dx, int nrhs, int method,
 }  // namespace
 
 extern "C" {
+
+SMFG_API int smfg_last_times(smfg_plan_t plan, double *factor_ms, double *solve_ms, double *refine_ms) {
+  if (!plan) return SMFG_ERR_INVALID_ARG;
+  const Plan &pl = plan->pl;
+  if (factor_ms) *factor_ms = pl.info.factor_ms;
+  if (solve_ms) *solve_ms = pl.info.solve_ms;
+  if (refine_ms) *refine_ms = pl.refine_ms;
+  return SMFG_OK;
+}
 
 SMFG_API int smfg_refine(smfg_plan_t plan, const double *b, double *x, int nrhs, int max_steps,
                          double omega_target, double *eta_inf, double *omega, int *steps) {
@@ -1414,6 +1457,7 @@ SMFG_API int smfg_refine_device(smfg_plan_t plan, const double *d_b, double *d_x
   try {
     SMFG_CUDA(cudaSetDevice(pl.device));
     clear_stale_error();
+    follow_caller(pl);
     return refine_core(plan, const_cast<double *>(d_b), d_x, nrhs, method, max_iters, restart, omega_target,
                        eta_inf, omega, iters);
   } catch (const std::exception &e) {

@@ -46,6 +46,10 @@ struct FrontShared {
   int np;
   double vals[8];
   int ivals[8];
+  // per-warp results of the parallel candidate tests / pairing scans
+  int ckind[32], ca[32], cb[32];
+  double pin[64], pout[64];
+  int pr[64];
   FrontStats st;
 };
 
@@ -396,6 +400,106 @@ __device__ __forceinline__ bool two_by_two_ok_s(double d00, double d10, double d
 }
 
 // select_pivot (ldlt_kernel.cpp:127-275). Result in sh.kind / sh.a / sh.b.
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__device__ __forceinline__ Top2 warp_top2(Top2 t) {
+  for (int o = 16; o > 0; o >>= 1) {
+    Top2 u;
+    u.m1 = __shfl_xor_sync(0xffffffffu, t.m1, o);
+    u.m2 = __shfl_xor_sync(0xffffffffu, t.m2, o);
+    u.r = __shfl_xor_sync(0xffffffffu, t.r, o);
+    t = top2_merge(t, u);
+  }
+  return t;
+}
+
+// The test of one candidate column of select_pivot's search loop
+// (ldlt_kernel.cpp:150-270) by one warp: 0 when the candidate gives no
+// pivot, else 1 (pivot a) or 2 (pivot pair a, b). The candidates' tests are
+// independent and the search takes the first candidate that gives one, so
+// warps may test consecutive candidates at once; maxima are exact in any
+// order, ties go to the lowest row as in the reference's scan.
+__device__ int cand_eval_warp(const FrontRef &v, int k, int limit, int cand, const PivotParams &prm, int &pa,
+                              int &pb) {
+  const int lane = threadIdx.x & 31;
+  const size_t sf = (size_t)v.ld;
+  const double *F = v.F;
+  const int f = v.f, ne = v.ne;
+  const double *col = F + (size_t)cand * sf;
+  const double a_cand = fabs(col[cand]);
+  Top2 t{0.0, 0.0, -1};
+  for (int i = k + lane; i < cand; i += 32) top2_add(t, fabs(F[(size_t)i * sf + cand]), i);
+#pragma unroll 4
+  for (int i = cand + 1 + lane; i < ne; i += 32) top2_add(t, fabs(col[i]), i);
+  t = warp_top2(t);
+  const int ext0 = ne > cand + 1 ? ne : cand + 1;
+  double ext = 0.0;
+#pragma unroll 4
+  for (int i = ext0 + lane; i < f; i += 32) ext = fmax(ext, fabs(col[i]));
+  ext = warp_max(ext);
+  const double m1 = t.m1, m2 = t.m2;
+  const int r_best = t.r;
+  bool weak_1x1 = false;
+  double weak_growth = 0.0;
+  pa = pb = -1;
+  if (a_cand >= prm.eff_small && !(__dmul_rn(prm.u, m1) > a_cand)) {
+    if (!(__dmul_rn(prm.u, ext) > a_cand)) {
+      const double colmax = dmax_ref(m1, ext);
+      if (!(a_cand < __dmul_rn(kWeakPivotRatio, colmax))) {
+        pa = cand;
+        return 1;
+      }
+      weak_1x1 = true;
+      weak_growth = colmax / a_cand;
+    }
+  }
+  if (r_best < k || r_best >= limit || m1 <= 0.0) {
+    if (weak_1x1) {
+      pa = cand;
+      return 1;
+    }
+    return 0;
+  }
+  const double *col_r = F + (size_t)r_best * sf;
+  double om2 = 0.0, off1 = 0.0;
+  for (int i = k + lane; i < r_best; i += 32) {
+    const double x = fabs(F[(size_t)i * sf + r_best]);
+    om2 = fmax(om2, x);
+    if (i != cand) off1 = fmax(off1, x);
+  }
+#pragma unroll 4
+  for (int i = r_best + 1 + lane; i < f; i += 32) {
+    const double x = fabs(col_r[i]);
+    om2 = fmax(om2, x);
+    if (i != cand) off1 = fmax(off1, x);
+  }
+  om2 = warp_max(om2);
+  off1 = warp_max(off1);
+  double growth2 = 0.0;
+  const double d00 = col[cand];
+  const double d10 = (r_best >= cand) ? F[(size_t)cand * sf + r_best] : F[(size_t)r_best * sf + cand];
+  const double d11 = col_r[r_best];
+  if (k + 1 < limit && two_by_two_ok_s(d00, d10, d11, dmax_ref(m2, ext), off1, prm, growth2) &&
+      (!weak_1x1 || growth2 < weak_growth)) {
+    pa = cand;
+    pb = r_best;
+    return 2;
+  }
+  if (weak_1x1) {
+    pa = cand;
+    return 1;
+  }
+  const double a_r = fabs(d11);
+  if (a_r >= prm.eff_small && (om2 == 0.0 || a_r >= __dmul_rn(prm.u, om2))) {
+    pa = r_best;
+    return 1;
+  }
+  return 0;
+}
+
 template <int NT>
 __device__ void select_pivot_blk(const FrontRef &v, int k, int limit, const PivotParams &prm,
                                  FrontShared &sh) {
@@ -433,81 +537,38 @@ __device__ void select_pivot_blk(const FrontRef &v, int k, int limit, const Pivo
       }
     }
   }
-  for (int cand = k; cand < limit && !done; ++cand) {
-    const double *col = F + (size_t)cand * sf;
-    const double a_cand = fabs(col[cand]);
-    Top2 t{0.0, 0.0, -1};
-    for (int i = k + threadIdx.x; i < cand; i += NT) top2_add(t, fabs(F[(size_t)i * sf + cand]), i);
-    for (int i = cand + 1 + threadIdx.x; i < ne; i += NT) top2_add(t, fabs(col[i]), i);
-    t = Block<NT>::top2(t, sh);
-    const int ext0 = ne > cand + 1 ? ne : cand + 1;
-    double ext = 0.0;
-    for (int i = ext0 + threadIdx.x; i < f; i += NT) ext = fmax(ext, fabs(col[i]));
-    ext = Block<NT>::max(ext, sh);
-    const double m1 = t.m1, m2 = t.m2;
-    const int r_best = t.r;
-    bool weak_1x1 = false;
-    double weak_growth = 0.0;
-    if (a_cand >= prm.eff_small && !(__dmul_rn(prm.u, m1) > a_cand)) {
-      if (!(__dmul_rn(prm.u, ext) > a_cand)) {
-        const double colmax = dmax_ref(m1, ext);
-        if (!(a_cand < __dmul_rn(kWeakPivotRatio, colmax))) {
-          kind = 1;
-          pa = cand;
-          done = true;
-          break;
-        }
-        weak_1x1 = true;
-        weak_growth = colmax / a_cand;
-      }
-    }
-    if (r_best < k || r_best >= limit || m1 <= 0.0) {
-      if (weak_1x1) {
-        kind = 1;
-        pa = cand;
+  // the search loop, NT / 32 candidates at a time (one warp each)
+  constexpr int NW = NT / 32;
+  const int warp = threadIdx.x >> 5;
+  for (int c0 = k; c0 < limit && !done; c0 += NW) {
+    const int cand = c0 + warp;
+    int wk = 0, wa = -1, wb = -1;
+    if (cand < limit) wk = cand_eval_warp(v, k, limit, cand, prm, wa, wb);
+    if (NW == 1) {
+      if (wk) {
+        kind = wk;
+        pa = wa;
+        pb = wb;
         done = true;
-        break;
       }
       continue;
     }
-    const double *col_r = F + (size_t)r_best * sf;
-    double om2 = 0.0, off1 = 0.0;
-    for (int i = k + threadIdx.x; i < r_best; i += NT) {
-      const double x = fabs(F[(size_t)i * sf + r_best]);
-      om2 = fmax(om2, x);
-      if (i != cand) off1 = fmax(off1, x);
+    if ((threadIdx.x & 31) == 0) {
+      sh.ckind[warp] = wk;
+      sh.ca[warp] = wa;
+      sh.cb[warp] = wb;
     }
-    for (int i = r_best + 1 + threadIdx.x; i < f; i += NT) {
-      const double x = fabs(col_r[i]);
-      om2 = fmax(om2, x);
-      if (i != cand) off1 = fmax(off1, x);
+    __syncthreads();
+    for (int w = 0; w < NW; ++w) {
+      if (sh.ckind[w]) {
+        kind = sh.ckind[w];
+        pa = sh.ca[w];
+        pb = sh.cb[w];
+        done = true;
+        break;
+      }
     }
-    Block<NT>::max2(om2, off1, sh);
-    double growth2 = 0.0;
-    const double d00 = col[cand];
-    const double d10 = (r_best >= cand) ? F[(size_t)cand * sf + r_best] : F[(size_t)r_best * sf + cand];
-    const double d11 = col_r[r_best];
-    if (k + 1 < limit && two_by_two_ok_s(d00, d10, d11, dmax_ref(m2, ext), off1, prm, growth2) &&
-        (!weak_1x1 || growth2 < weak_growth)) {
-      kind = 2;
-      pa = cand;
-      pb = r_best;
-      done = true;
-      break;
-    }
-    if (weak_1x1) {
-      kind = 1;
-      pa = cand;
-      done = true;
-      break;
-    }
-    const double a_r = fabs(d11);
-    if (a_r >= prm.eff_small && (om2 == 0.0 || a_r >= __dmul_rn(prm.u, om2))) {
-      kind = 1;
-      pa = r_best;
-      done = true;
-      break;
-    }
+    __syncthreads();
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -683,23 +744,42 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
         if (threadIdx.x == 0) sh.np = 0;
         __syncthreads();
         const int max_pairs = min(prm.nb / 2, 64);
-        for (int pos = k; pos < pl; ++pos) {
-          if (sh.np / 2 >= max_pairs) break;
-          const double *col = v.F + (size_t)pos * sf;
-          double in_max = 0.0;
-          for (int i = k + threadIdx.x; i < pos; i += NT) in_max = fmax(in_max, fabs(v.F[(size_t)i * sf + pos]));
-          for (int i = pos + 1 + threadIdx.x; i < pl; i += NT) in_max = fmax(in_max, fabs(col[i]));
-          in_max = Block<NT>::max(in_max, sh);
-          double out_max;
-          int r;
-          Block<NT>::argmax(col, pl, ne, out_max, r, sh);
+        // the scans of the panel's columns are independent of the pairing
+        // decisions: warps scan positions in parallel, thread 0 then takes
+        // the decisions in position order
+        constexpr int NWP = NT / 32;
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        for (int p0 = k; p0 < pl; p0 += 64) {
+          const int pend = min(pl, p0 + 64);
+          for (int pos = p0 + warp; pos < pend; pos += NWP) {
+            const double *col = v.F + (size_t)pos * sf;
+            double in_max = 0.0;
+            for (int i = k + lane; i < pos; i += 32) in_max = fmax(in_max, fabs(v.F[(size_t)i * sf + pos]));
+            for (int i = pos + 1 + lane; i < pl; i += 32) in_max = fmax(in_max, fabs(col[i]));
+            in_max = warp_max(in_max);
+            Top2 t{0.0, 0.0, -1};
+#pragma unroll 4
+            for (int i = pl + lane; i < ne; i += 32) top2_add(t, fabs(col[i]), i);
+            t = warp_top2(t);
+            if (lane == 0) {
+              sh.pin[pos - p0] = in_max;
+              sh.pout[pos - p0] = t.m1;
+              sh.pr[pos - p0] = t.r;
+            }
+          }
           __syncthreads();
-          if (threadIdx.x == 0 && r >= 0 && out_max > in_max) {
-            bool taken = false;
-            for (int t = 1; t < sh.np; t += 2) taken = taken || sh.order[t] == v.rows[r];
-            if (!taken) {
-              sh.order[sh.np++] = v.rows[pos];
-              sh.order[sh.np++] = v.rows[r];
+          if (threadIdx.x == 0) {
+            for (int pos = p0; pos < pend; ++pos) {
+              if (sh.np / 2 >= max_pairs) break;
+              const int r = sh.pr[pos - p0];
+              if (r >= 0 && sh.pout[pos - p0] > sh.pin[pos - p0]) {
+                bool taken = false;
+                for (int t = 1; t < sh.np; t += 2) taken = taken || sh.order[t] == v.rows[r];
+                if (!taken) {
+                  sh.order[sh.np++] = v.rows[pos];
+                  sh.order[sh.np++] = v.rows[r];
+                }
+              }
             }
           }
           __syncthreads();
@@ -707,11 +787,13 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
         const int np = sh.np;
         if (np > 0) {
           for (int t = 0; t < np; ++t) {
-            if (threadIdx.x == 0) {
-              int qq = k + t;
-              while (qq < f - 1 && v.rows[qq] != sh.order[t]) ++qq;
-              sh.ivals[0] = qq;
-            }
+            // the position of row id order[t] from k + t on (the first
+            // match, else f - 1), searched by the whole block
+            if (threadIdx.x == 0) sh.ivals[0] = f - 1;
+            __syncthreads();
+            const int want = sh.order[t];
+            for (int i = k + t + threadIdx.x; i < f - 1; i += NT)
+              if (v.rows[i] == want) atomicMin(&sh.ivals[0], i);
             __syncthreads();
             const int qq = sh.ivals[0];
             __syncthreads();

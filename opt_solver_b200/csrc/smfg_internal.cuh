@@ -91,6 +91,7 @@ struct Plan {
   DevFactor x;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev_in = nullptr;  // orders the stream after the caller's default-stream work
   // last factorization
   bool factored = false;
   int posdef = 0;
@@ -102,6 +103,7 @@ struct Plan {
   std::vector<int8_t> front_mask;      // caller's per-front precision choice (empty: all may)
   std::vector<int8_t> h_mixed;         // mixed fronts of the last factorization
   int mixed_count = 0;
+  double refine_ms = 0.0;  // device time of the last refinement
   std::vector<void *> allocs;
 };
 

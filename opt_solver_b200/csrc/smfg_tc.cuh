@@ -462,14 +462,16 @@ __global__ void __launch_bounds__(kThreads, 1)
         tmem_ld32(tmem + ((uint32_t)slice << 16) + (uint32_t)(buf * kBN + ch * 32), v);
         const int j0 = tj * kBN + ch * 32;
         if (i < J.n) {
+          // all 32 loads in flight before the stores (a warp covers 32
+          // consecutive rows of each column: coalesced)
+          const int jn = min(32, i - j0 + 1);  // columns j0 .. j0 + jn - 1 are <= i
+          double cv[32];
 #pragma unroll
-          for (int c = 0; c < 32; ++c) {
-            const int j = j0 + c;
-            if (j <= i) {
-              double *p = Ccol + (int64_t)j * J.ld;
-              *p -= (double)v[c];
-            }
-          }
+          for (int c = 0; c < 32; ++c)
+            cv[c] = (c < jn) ? __ldcg(Ccol + (int64_t)(j0 + c) * J.ld) : 0.0;
+#pragma unroll
+          for (int c = 0; c < 32; ++c)
+            if (c < jn) Ccol[(int64_t)(j0 + c) * J.ld] = cv[c] - (double)v[c];
         }
       }
       tc_fence_before();

@@ -130,6 +130,9 @@ def lib():
                                          C.c_int, C.c_double, C.POINTER(C.c_double),
                                          C.POINTER(C.c_double), C.POINTER(C.c_int)]
         L.smfg_refine_device.restype = C.c_int
+        L.smfg_last_times.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                      C.POINTER(C.c_double)]
+        L.smfg_last_times.restype = C.c_int
         L.smfg_set_front_precision.argtypes = [C.c_void_p, C.c_void_p]
         L.smfg_set_front_precision.restype = C.c_int
         L.smfg_front_stats.argtypes = [C.c_void_p, _i32p]
@@ -372,12 +375,16 @@ class Solver:
         return info
 
     def profile_factor(self, values, posdef: bool = False, precision: int = PREC_FP64,
-                       scale=None) -> dict:
+                       scale=None, **mixed) -> dict:
         """One factorization with CUDA events around every launch of the
-        large-front GEMM kernels: their total device time, launch count and
-        algorithmic flops (2 per fused multiply-add of the updates)."""
+        large-front update kernels: FP64 GEMMs and tensor-core passes (split
+        + product), their device times, launch counts and algorithmic flops
+        (2 per multiply-add of the updates)."""
         c = default_control(posdef, 0.01, 1e-20, precision)
         c.profile = 1
+        c.mixed_block = mixed.get("mixed_block", 0)
+        c.mixed_kind = mixed.get("mixed_kind", 0)
+        c.mixed_min_front = mixed.get("mixed_min_front", 0)
         if scale is not None and len(scale):
             self._scale = np.ascontiguousarray(scale, dtype=np.float64)
             c.scale = self._scale.ctypes.data
@@ -393,7 +400,8 @@ class Solver:
         self.info = info
         return {"gemm_ms": info.reserved_d[0], "gemm_flops": info.reserved_d[1],
                 "gemm_launches": info.reserved_i[0], "arena_bytes": info.reserved_d[2],
-                "factor_ms": info.factor_ms}
+                "tc_ms": info.reserved_d[4], "tc_flops": info.reserved_d[3],
+                "tc_passes": info.reserved_i[1], "factor_ms": info.factor_ms}
 
     # -- solve -------------------------------------------------------------
     def solve(self, b, job: int = SOLVE_FULL):
@@ -490,6 +498,12 @@ class Solver:
         if rc != SMFG_OK:
             raise SmfgError(rc, "smfg_refine_method")
         return x, eta.value, om.value, st.value
+
+    def last_times(self):
+        """(factor_ms, solve_ms, refine_ms) of the last calls, device time."""
+        f, s_, r = C.c_double(), C.c_double(), C.c_double()
+        lib().smfg_last_times(self._h, C.byref(f), C.byref(s_), C.byref(r))
+        return f.value, s_.value, r.value
 
     def refine_device(self, d_b, d_x, nrhs: int = 1, max_steps: int = 10,
                       omega_target: float = 1e-8, method: int = REFINE_AUTO, restart: int = 20):
