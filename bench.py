@@ -8,7 +8,7 @@ analysis, one right-hand side uniform in [-1, 1]. One step = numeric
 factorization of the values + one solve.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--config spd3d|spd3d40|lap2d|traj|kkt|batch] [--precision fp64|mixed]
+                  [--config spd3d|spd3d40|lap2d|traj|kkt|kkt3|batch] [--precision fp64|mixed|both]
 
 `value` is device time (CUDA events on the engine's stream) with the
 inputs already in HBM; `e2e` is the same step through the C ABI with host
@@ -36,7 +36,12 @@ CONFIGS = {
     "spd3d": ("SPD variable-coefficient 7-point 64^3 (n=262,144), 1 RHS", "varcoef_3d(64)", True, 1),
     "lap2d": ("2D 5-point Laplacian 150x150 (n=22,500), 1 RHS", "laplacian_2d(150)", True, 1),
     "traj": ("trajectory KKT T=200 (n=5,612), 8 RHS", "traj200", False, 8),
-    "kkt": ("IPM KKT 20^3 + 4,000 constraints (n=12,000), 1 RHS", "kkt_ipm(20, 4000)", False, 1),
+    "kkt": ("IPM KKT 20^3 + 4,000 constraints (n=12,000), smf's METIS ordering, 1 RHS N(0,1)",
+            "kkt_ipm(20, 4000)", False, 1),
+    # configuration 3 at full size: the analysis on smf's own METIS ordering
+    # (tests/golden/kkt40_32000_metis_perm.npz, made by the reference)
+    "kkt3": ("IPM KKT 40^3 + 32,000 constraints (n=96,000), Sigma 10^U[-8,8], delta 1e-8, smf's METIS "
+             "ordering, u=0.01, 1 RHS N(0,1)", "kkt_ipm(40, 32000)", False, 1),
     # the same generator as spd3d at 40^3: the small case of the ncu captures
     "spd3d40": ("SPD variable-coefficient 7-point 40^3 (n=64,000), 1 RHS", "varcoef_3d(40)", True, 1),
     # configuration 4: 1,024 trajectory KKTs (T uniform in 10..200) in one batch
@@ -81,12 +86,15 @@ class _Workload:
             self.expected = [(16 * ((m[0] - 12) // 28) + 12, 12 * ((m[0] - 12) // 28), 0) for m in mats]
         else:
             n, cp, ri, v = build_matrix(cfg)
-            a = smfg.analyse(n, cp, ri)
+            perm = given_ordering(cfg)
+            a = smfg.analyse(n, cp, ri, perm=perm)
+            self.ordering = "smf's METIS ordering (committed fixture)" if perm is not None else \
+                "engine nested dissection (smfg_analyse)"
             self.analyse_s = time.time() - t0
             self.sv = smfg.Solver(a, device=device)
             self.solver = self.sv
             self.values = v
-            self.b = W.rhs(n, self.nrhs, seed=1)
+            self.b = W.rhs(n, self.nrhs, seed=1, kind="normal" if cfg.startswith("kkt") else "uniform")
             self.n = n
             self.nnz = int(cp[-1])
             self.nsn = a.nsn
@@ -99,6 +107,16 @@ class _Workload:
         return [s[:3] for s in self.solver.system_stats()] == self.expected
 
 
+def given_ordering(cfg: str):
+    """smf's own fill-reducing ordering of the KKT workloads (perm[new] =
+    old), committed under tests/golden/ by make_kkt_orderings.py; None: the
+    engine's analysis orders the matrix itself."""
+    name = {"kkt": "kkt20_4000", "kkt3": "kkt40_32000"}.get(cfg)
+    if name is None:
+        return None
+    return np.load(os.path.join(ROOT, "tests", "golden", f"{name}_metis_perm.npz"))["perm"]
+
+
 def build_matrix(cfg: str):
     from opt_solver_b200 import workloads as W
     if cfg == "spd3d":
@@ -109,6 +127,8 @@ def build_matrix(cfg: str):
         return W.trajectory_kkt(200, np.random.default_rng(0))
     if cfg == "kkt":
         return W.kkt_ipm(20, 4000, seed=0)
+    if cfg == "kkt3":
+        return W.kkt_ipm(40, 32000, seed=0)
     if cfg == "spd3d40":
         return W.varcoef_3d(40, seed=0)
     raise ValueError(cfg)
@@ -124,6 +144,9 @@ def sample_matrix(cfg: str):
     if cfg == "batch":
         mats = batch_systems()[:64]
         return mats, "the first 64 of the 1,024 systems, one smf analyse/factor/solve each", BATCH_COUNT / 64
+    if cfg == "kkt3":
+        # smf refuses the full size (its largest front exceeds its storage cap)
+        return [W.kkt_ipm(20, 4000, seed=0)], "kkt_ipm(20, 4000) (n=12,000), same generator", None
     return [build_matrix(cfg)], "the full workload", 1.0
 
 
@@ -326,6 +349,7 @@ def run_ours(args, rank, world, local):
     return {
         "arms": res, "head": head, "e2e_ms": e2e_ms, "e2e_eta": eta, "e2e_omega": om,
         "analyse_s": wl.analyse_s, "n": wl.n, "nnz": wl.nnz, "nrhs": wl.nrhs, "desc": wl.desc,
+        "ordering": getattr(wl, "ordering", "engine nested dissection (smfg_analyse)"),
         "clocks": clocks, "nsn": wl.nsn, "systems": wl.systems,
         "h2d": wl.nnz * 8 + wl.n * wl.nrhs * 8, "d2h": wl.n * wl.nrhs * 8, "profile": prof,
     }
@@ -342,7 +366,7 @@ def cpu_reference_ms(cfg, threads):
     mats, sample, scale = sample_matrix(cfg)
     posdef = CONFIGS[cfg][2]
     nrhs = CONFIGS[cfg][3]
-    ordering = O.ORDER_METIS if cfg.startswith("spd3d") else O.ORDER_AUTO_PARALLEL
+    ordering = O.ORDER_METIS if (cfg.startswith("spd3d") or cfg.startswith("kkt")) else O.ORDER_AUTO_PARALLEL
     total = 0.0
     analyses = []
     for i, (n, cp, ri, v) in enumerate(mats):
@@ -516,7 +540,7 @@ def main():
         "data": "synthetic (seeded generator of the configuration)",
         "config": {"workload": r["desc"], "n": r["n"], "nnz_lower": r["nnz"], "nrhs": r["nrhs"],
                    "supernodes": r["nsn"], "systems_this_rank": r["systems"],
-                   "analysis": "engine nested dissection (smfg_analyse)",
+                   "analysis": r["ordering"],
                    "precision": head, "omega_gate": OMEGA_GATE,
                    "step": "factor + solve + refinement (auto) to eta_inf <= 1e-10, omega <= 1e-12",
                    "parallelism": ("systems sharded over ranks" if batch else "replicas") if world > 1 else "1 GPU",

@@ -116,7 +116,8 @@ typedef struct {
   int mixed_block;
   int mixed_kind;
   int mixed_min_front;
-  int reserved_i[4];
+  int panel_team;         /* CTAs per indefinite large front's pivoting (1, 2, 4, 8); 0: by front size */
+  int reserved_i[3];
   double reserved_d[8];
 } smfg_control_t;
 
@@ -138,7 +139,8 @@ typedef struct {
   int reserved_i[7];      /* [0] profiled FP64 update launches, [1] tensor-core update passes */
   double reserved_d[8];   /* [0] profiled FP64 update ms, [1] FP64 update flops, [2] arena bytes,
                              [3] tensor-core update flops (2 per multiply-add), [4] profiled
-                             tensor-core update ms (split + product kernels) */
+                             tensor-core update ms (split + product kernels), [5] profiled
+                             large-front pivoting panel ms */
 } smfg_info_t;
 
 typedef struct smfg_plan_s *smfg_plan_t;
@@ -245,6 +247,18 @@ SMFG_API int smfg_refine_device(smfg_plan_t plan, const double *d_b, double *d_x
  * and refinement; a refinement's time includes its waits for the host's
  * small Hessenberg work between iterations. */
 SMFG_API int smfg_last_times(smfg_plan_t plan, double *factor_ms, double *solve_ms, double *refine_ms);
+
+/* Symmetric max-product matching scaling (host code): the scaling smf
+ * applies before an indefinite factorization when matching scaling is on
+ * (solver/src/scaling_matching.cpp): a minimum-cost perfect matching on
+ * c_ij = log max_k |a_kj| - log |a_ij| (MC64 job 5) and scale[i] =
+ * exp((u_i + v_i) / 2) / sqrt(max_k |a_ki|) from its dual potentials, so
+ * that |s_i a_ij s_j| <= 1 with equality on the matched entries. Input:
+ * lower CSC (original numbering); scale: n doubles, to pass as
+ * smfg_control_t.scale. *unmatched: columns left without a match
+ * (structurally singular). SMFG_ERR_SINGULAR for an all-zero row. */
+SMFG_API int smfg_matching_scale(int n, const int *col_ptr, const int *row_idx, const double *values,
+                                 double *scale, int *unmatched);
 
 /* A symbolic analysis of the engine's own (host code, no GPU needed),
  * producing the smfg_analysis_t contract above when smf's analyse

@@ -279,6 +279,9 @@ static void build_plan(Plan &pl, const smfg_analysis_t &a) {
   x.lvl_blk = dalloc<int>(pl, (size_t)ns + nl + 1);
   x.counters = dalloc<unsigned long long>(pl, kCCount + 8);
   x.tpp = dalloc<TppState>(pl, 2 * (size_t)std::max(1, pl.max_large));  // two buffers (SPD panels)
+  x.team_bar = dalloc<unsigned>(pl, 2 * (size_t)std::max(1, pl.max_large));
+  SMFG_CUDA(cudaMemsetAsync(x.team_bar, 0, sizeof(unsigned) * 2 * std::max(1, pl.max_large), pl.stream));
+  x.team_red = dalloc<double>(pl, (size_t)kTeamRedDoubles * std::max(1, pl.max_large));
   x.sn_mixed = dalloc<int8_t>(pl, ns);
   SMFG_CUDA(cudaMemsetAsync(x.sn_mixed, 0, ns, pl.stream));
   x.tc_jobs = dalloc<tc::Job>(pl, std::max(1, pl.max_large));
@@ -373,6 +376,41 @@ static MixedCfg mixed_cfg(const smfg_control_t &c) {
   return m;
 }
 
+// Team size (CTAs per front) of a level's indefinite large-front panels, by
+// the largest symbolic front: the swaps and eliminations of a panel stream
+// its columns (16 x f doubles per pivot), which one SM's bandwidth bounds.
+static int panel_team(int maxf) { return maxf >= 3072 ? 8 : maxf >= 1536 ? 4 : maxf >= 768 ? 2 : 1; }
+
+template <int C>
+static void launch_panel_c(Plan &pl, const int *lg, int nL, const PivotParams &prm, int it) {
+  if constexpr (C == 1) {
+    k_large_panel<512, 1><<<nL, 512, 0, pl.stream>>>(pl.d, pl.x, lg, prm, it, pl.x.team_bar);
+  } else {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(nL * C), 1, 1);
+    cfg.blockDim = dim3(512, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = pl.stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = C;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    SMFG_CUDA(cudaLaunchKernelEx(&cfg, k_large_panel<512, C>, pl.d, pl.x, lg, prm, it, pl.x.team_bar));
+  }
+}
+
+static void launch_panel(Plan &pl, int team, const int *lg, int nL, const PivotParams &prm, int it) {
+  switch (team) {
+    case 8: launch_panel_c<8>(pl, lg, nL, prm, it); break;
+    case 4: launch_panel_c<4>(pl, lg, nL, prm, it); break;
+    case 2: launch_panel_c<2>(pl, lg, nL, prm, it); break;
+    default: launch_panel_c<1>(pl, lg, nL, prm, it); break;
+  }
+}
+
 // The tensor-core updates due on a level's large fronts (states `states`).
 static void enqueue_tc(Plan &pl, const MixedCfg &mc, const int *lg, int nL, TppState *states, int posdef,
                        LaunchCount &lc, GemmProfile &gp) {
@@ -438,6 +476,9 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
         for (int i = pl.lvl_large_ptr[l]; i < pl.lvl_large_ptr[l + 1] && !lvl_mixed; ++i)
           lvl_mixed = pl.h_mixed[pl.h_lvl_large[i]] != 0;
       k_large_init<<<nL, 256, 0, st>>>(d, x, lg, nL, c.posdef, lvl_mixed ? mc.nbo : 0);
+      const int team = (c.panel_team == 1 || c.panel_team == 2 || c.panel_team == 4 || c.panel_team == 8)
+                           ? c.panel_team
+                           : panel_team(pl.lvl_large_maxf[l]);
       SMFG_CUDA(cudaMemsetAsync(x.counters + kCActive, 0, sizeof(unsigned long long), st));
       const int ggrid = 2 * sms;
       int it = 0;
@@ -450,7 +491,9 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
         for (; it < steps; ++it) {
           TppState *cur = x.tpp + (size_t)(it & 1) * pl.max_large;
           TppState *nxt = x.tpp + (size_t)((it + 1) & 1) * pl.max_large;
+          gp.mark(st, 2);
           k_large_panel_spd<16><<<pgrid, 256, 0, st>>>(d, x, lg, cur, nxt, it);
+          gp.mark(st, 2);
           gp.mark(st);
           k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, nxt);
           gp.mark(st);
@@ -462,7 +505,9 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
       } else if (c.posdef) {
         const int steps = (pl.lvl_large_maxw[l] + c.nb - 1) / c.nb + 1;
         for (; it < steps; ++it) {
-          k_large_panel<512><<<nL, 512, 0, st>>>(d, x, lg, prm, it);
+          gp.mark(st, 2);
+          launch_panel(pl, team, lg, nL, prm, it);
+          gp.mark(st, 2);
           gp.mark(st);
           k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, x.tpp);
           gp.mark(st);
@@ -475,7 +520,9 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
         const int batch = 32;
         for (int guard = 0; guard < 1 << 20; guard += batch) {
           for (int b = 0; b < batch; ++b, ++it) {
-            k_large_panel<512><<<nL, 512, 0, st>>>(d, x, lg, prm, it);
+            gp.mark(st, 2);
+            launch_panel(pl, team, lg, nL, prm, it);
+            gp.mark(st, 2);
             gp.mark(st);
             k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, x.tpp);
             gp.mark(st);
@@ -617,6 +664,7 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
   int fp64_pairs = 0, tc_pairs = 0;
   inf.reserved_d[0] = gp.on ? gp.total_ms(0, &fp64_pairs) : 0.0;
   inf.reserved_d[4] = gp.on ? gp.total_ms(1, &tc_pairs) : 0.0;
+  inf.reserved_d[5] = gp.on ? gp.total_ms(2) : 0.0;
   inf.reserved_i[1] = tc_pairs;
   std::memcpy(&inf.reserved_d[1], &h_cnt[kCGemmFlops], sizeof(double));
   inf.reserved_d[2] = (double)h_cnt[kCArena] * 8.0;

@@ -50,6 +50,7 @@ struct FrontShared {
   int ckind[32], ca[32], cb[32];
   double pin[64], pout[64];
   int pr[64];
+  int tr_seq;  // team reductions so far (alike in every CTA of a team)
   FrontStats st;
 };
 
@@ -195,13 +196,77 @@ struct FrontRef {
   int8_t *tags;
   double *W;
   int *loc;  // assembly position of the row now at each position (null: untracked)
+  // teams of several CTAs: the team's barrier words {count, generation},
+  // the error word a timed-out barrier sets, this CTA's abort flag
+  unsigned *team_bar = nullptr;
+  unsigned long long *err = nullptr;
+  int *abort = nullptr;
+  double *team_red = nullptr;  // the team's reduction scratch: 2 buffers x C ranks x 4
 };
+
+// A team of C CTAs (a thread-block cluster; C = 1: the CTA alone) that runs
+// one front's threshold pivoting: every CTA takes the same pivot decisions
+// from the same data (its own block reductions, so the decisions are the
+// one-CTA decisions bit for bit), and the memory-heavy updates (row and
+// column swaps, eliminations of the panel) are split by rows over the team,
+// each followed by a team barrier (the cluster's hardware barrier, release
+// / acquire at cluster scope).
+template <int C>
+__device__ __forceinline__ int team_rank() {
+  if constexpr (C == 1) {
+    return 0;
+  } else {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return (int)r;
+  }
+}
+
+// Team barrier (C > 1): a sense-reversing barrier on two words in global
+// memory, the spin bounded by the global timer (2 s): a team whose CTAs
+// did not all arrive sets bit 128 of *err, and the CTA stops waiting at its
+// later barriers (its remaining work is then discarded by the host, which
+// reports the timeout). The team's CTAs are co-scheduled (one cluster), so
+// the wait only runs out if they took different paths.
+template <int C>
+__device__ __forceinline__ void team_sync(const FrontRef &v) {
+  if constexpr (C == 1) {
+    __syncthreads();
+  } else {
+    __syncthreads();
+    if (threadIdx.x == 0 && !*v.abort) {
+      volatile unsigned *gen_p = v.team_bar + 1;
+      __threadfence();
+      const unsigned gen = *gen_p;
+      const unsigned arrived = atomicAdd(v.team_bar, 1u) + 1u;
+      if (arrived == (unsigned)C) {
+        atomicExch(v.team_bar, 0u);
+        __threadfence();
+        atomicAdd(v.team_bar + 1, 1u);
+      } else {
+        unsigned long long t0;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+        while (*gen_p == gen) {
+          unsigned long long t;
+          asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+          if (t - t0 > 2000000000ull) {
+            *v.abort = 1;
+            atomicOr(v.err, 128ull);
+            break;
+          }
+        }
+      }
+      __threadfence();
+    }
+    __syncthreads();
+  }
+}
 
 __device__ __forceinline__ double fat(const FrontRef &v, int i, int j) {  // element (i, j), i >= j
   return v.F[(size_t)j * v.ld + i];
 }
 
-template <int NT>
+template <int NT, int C = 1>
 __device__ void sym_swap_blk(const FrontRef &v, int p, int q, int w_cols) {
   if (p == q) return;
   if (p > q) {
@@ -209,13 +274,15 @@ __device__ void sym_swap_blk(const FrontRef &v, int p, int q, int w_cols) {
     p = q;
     q = t;
   }
+  // no CTA of the team writes while another still reads (C > 1)
+  if constexpr (C > 1) team_sync<C>(v);
   const size_t sf = (size_t)v.ld;
   double *F = v.F;
   const int f = v.f;
   // Pairs: diagonal; m < p; p < m < q; m > q; rows; W rows. All disjoint.
   const int n1 = p, n2 = q - p - 1, n3 = f - q - 1;
   const int total = 1 + n1 + n2 + n3 + 1 + w_cols;
-  for (int t = threadIdx.x; t < total; t += NT) {
+  for (int t = team_rank<C>() * NT + (int)threadIdx.x; t < total; t += C * NT) {
     if (t == 0) {
       const double x = F[p * sf + p];
       F[p * sf + p] = F[q * sf + q];
@@ -252,7 +319,7 @@ __device__ void sym_swap_blk(const FrontRef &v, int p, int q, int w_cols) {
       W[q] = x;
     }
   }
-  __syncthreads();
+  team_sync<C>(v);
 }
 
 __device__ __forceinline__ void inertia_1x1(double d, double small, FrontStats &st) {
@@ -314,19 +381,22 @@ struct Lay {
   static __device__ __forceinline__ int g() { return threadIdx.x / RB; }
 };
 
-template <int NT>
+
+template <int NT, int C = 1>
 __device__ void eliminate_1x1_blk(const FrontRef &v, int k, int ucol_end, bool useW, int w_col) {
   using LY = Lay<NT>;
+  const int rk = team_rank<C>();
+  if constexpr (C > 1) team_sync<C>(v);
   const size_t sf = (size_t)v.ld;
   const int f = v.f;
   double *ck = v.F + k * sf;
   const double inv_d = 1.0 / ck[k];
   if (useW) {
     double *w = v.W + (size_t)w_col * f;
-    for (int i = k + 1 + threadIdx.x; i < f; i += NT) w[i] = ck[i];
+    for (int i = k + 1 + rk * NT + (int)threadIdx.x; i < f; i += C * NT) w[i] = ck[i];
   }
   // column j of (k, ucol_end), row i >= j: F(i, j) -= F(i, k) * l_j
-  for (int i = k + 1 + LY::r(); i < f; i += LY::RB) {
+  for (int i = k + 1 + rk * LY::RB + LY::r(); i < f; i += C * LY::RB) {
     const double cki = ck[i];
     const int jend = min(ucol_end, i + 1);
     for (int j = k + 1 + LY::g(); j < jend; j += LY::G) {
@@ -336,14 +406,18 @@ __device__ void eliminate_1x1_blk(const FrontRef &v, int k, int ucol_end, bool u
       cj[i] = __dsub_rn(cj[i], __dmul_rn(cki, lj));
     }
   }
-  __syncthreads();
-  for (int i = k + 1 + threadIdx.x; i < f; i += NT) ck[i] = __dmul_rn(ck[i], inv_d);
-  __syncthreads();
+  team_sync<C>(v);
+  for (int i = k + 1 + rk * NT + (int)threadIdx.x; i < f; i += C * NT) ck[i] = __dmul_rn(ck[i], inv_d);
+  // no barrier after the scaling for a team: the next pivot search reads
+  // only later columns, and the next swap or elimination starts with one
+  if constexpr (C == 1) __syncthreads();
 }
 
-template <int NT>
+template <int NT, int C = 1>
 __device__ void eliminate_2x2_blk(const FrontRef &v, int k, int ucol_end, bool useW, int w_col) {
   using LY = Lay<NT>;
+  const int rk = team_rank<C>();
+  if constexpr (C > 1) team_sync<C>(v);
   const size_t sf = (size_t)v.ld;
   const int f = v.f;
   double *c0 = v.F + k * sf;
@@ -353,12 +427,12 @@ __device__ void eliminate_2x2_blk(const FrontRef &v, int k, int ucol_end, bool u
   if (useW) {
     double *w0 = v.W + (size_t)w_col * f;
     double *w1 = w0 + f;
-    for (int i = k + 2 + threadIdx.x; i < f; i += NT) {
+    for (int i = k + 2 + rk * NT + (int)threadIdx.x; i < f; i += C * NT) {
       w0[i] = c0[i];
       w1[i] = c1[i];
     }
   }
-  for (int i = k + 2 + LY::r(); i < f; i += LY::RB) {
+  for (int i = k + 2 + rk * LY::RB + LY::r(); i < f; i += C * LY::RB) {
     const double c0i = c0[i], c1i = c1[i];
     const int jend = min(ucol_end, i + 1);
     for (int j = k + 2 + LY::g(); j < jend; j += LY::G) {
@@ -370,13 +444,15 @@ __device__ void eliminate_2x2_blk(const FrontRef &v, int k, int ucol_end, bool u
       d0[i] = __dsub_rn(d0[i], __dadd_rn(__dmul_rn(c0i, l0), __dmul_rn(c1i, l1)));
     }
   }
-  __syncthreads();
-  for (int i = k + 2 + threadIdx.x; i < f; i += NT) {
+  team_sync<C>(v);
+  for (int i = k + 2 + rk * NT + (int)threadIdx.x; i < f; i += C * NT) {
     const double a0 = c0[i], a1 = c1[i];
     c0[i] = __dadd_rn(__dmul_rn(i00, a0), __dmul_rn(i10, a1));
     c1[i] = __dadd_rn(__dmul_rn(i10, a0), __dmul_rn(i11, a1));
   }
-  __syncthreads();
+  // no barrier after the scaling for a team: the next pivot search reads
+  // only later columns, and the next swap or elimination starts with one
+  if constexpr (C == 1) __syncthreads();
 }
 
 // two_by_two_ok (ldlt_kernel.cpp:97-122); off0 = max(m2, max_{i>=ext0} |col|).
@@ -414,6 +490,139 @@ __device__ __forceinline__ Top2 warp_top2(Top2 t) {
     t = top2_merge(t, u);
   }
   return t;
+}
+
+// fn(|col[i]|, i) for i = start, start + S, ... < end, eight loads in
+// flight per thread (the scans are latency-bound otherwise).
+template <class Fn>
+__device__ __forceinline__ void scan8(const double *__restrict__ col, int start, int end, int S, Fn fn) {
+  int i = start;
+  for (; i + 7 * S < end; i += 8 * S) {
+    double x[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) x[u] = fabs(col[i + u * S]);
+#pragma unroll
+    for (int u = 0; u < 8; ++u) fn(x[u], i + u * S);
+  }
+  for (; i < end; i += S) fn(fabs(col[i]), i);
+}
+
+// Team-wide reduction of a bundle (a Top2 and two maxima): the block's
+// reduction, then for a team of C > 1 CTAs each CTA's partial to the team's
+// scratch, a team barrier and the C partials merged in rank order by every
+// CTA (the merges are exact and order-independent, so every CTA holds the
+// one-CTA result). Two buffers alternate: a buffer is rewritten only after
+// the barrier of the next reduction, which every CTA reaches after reading.
+template <int NT, int C>
+__device__ void team_bundle(const FrontRef &v, FrontShared &sh, Top2 &t, double &x1, double &x2) {
+  t = Block<NT>::top2(t, sh);
+  Block<NT>::max2(x1, x2, sh);
+  if constexpr (C > 1) {
+    const int buf = sh.tr_seq & 1;
+    double *slot = v.team_red + (size_t)buf * C * 6;  // per rank: Top2 (4), maxima (2)
+    const int rank = team_rank<C>();
+    if (threadIdx.x == 0) {
+      slot[rank * 4 + 0] = t.m1;
+      slot[rank * 4 + 1] = t.m2;
+      slot[rank * 4 + 2] = __longlong_as_double((long long)t.r);
+      slot[rank * 4 + 3] = 0.0;
+      slot[C * 4 + rank * 2 + 0] = x1;
+      slot[C * 4 + rank * 2 + 1] = x2;
+    }
+    team_sync<C>(v);
+    Top2 o{0.0, 0.0, -1};
+    double a = 0.0, b = 0.0;
+    for (int q = 0; q < C; ++q) {
+      Top2 u{__ldcg(slot + q * 4 + 0), __ldcg(slot + q * 4 + 1),
+             (int)__double_as_longlong(__ldcg(slot + q * 4 + 2))};
+      o = top2_merge(o, u);
+      a = fmax(a, __ldcg(slot + C * 4 + q * 2 + 0));
+      b = fmax(b, __ldcg(slot + C * 4 + q * 2 + 1));
+    }
+    t = o;
+    x1 = a;
+    x2 = b;
+    __syncthreads();
+    if (threadIdx.x == 0) sh.tr_seq += 1;
+    __syncthreads();
+  }
+}
+
+// One candidate's test (as cand_eval_warp) by the whole team: its scans
+// split by rows over every thread of every CTA, two team reductions.
+template <int NT, int C>
+__device__ int cand_eval_team(const FrontRef &v, int k, int limit, int cand, const PivotParams &prm,
+                              FrontShared &sh, int &pa, int &pb) {
+  const int tid = team_rank<C>() * NT + (int)threadIdx.x;
+  constexpr int NTT = C * NT;
+  const size_t sf = (size_t)v.ld;
+  const double *F = v.F;
+  const int f = v.f, ne = v.ne;
+  const double *col = F + (size_t)cand * sf;
+  const double a_cand = fabs(col[cand]);
+  Top2 t{0.0, 0.0, -1};
+  for (int i = k + tid; i < cand; i += NTT) top2_add(t, fabs(F[(size_t)i * sf + cand]), i);
+  scan8(col, cand + 1 + tid, ne, NTT, [&](double x, int i) { top2_add(t, x, i); });
+  const int ext0 = ne > cand + 1 ? ne : cand + 1;
+  double ext = 0.0, unused = 0.0;
+  scan8(col, ext0 + tid, f, NTT, [&](double x, int) { ext = fmax(ext, x); });
+  team_bundle<NT, C>(v, sh, t, ext, unused);
+  const double m1 = t.m1, m2 = t.m2;
+  const int r_best = t.r;
+  bool weak_1x1 = false;
+  double weak_growth = 0.0;
+  pa = pb = -1;
+  if (a_cand >= prm.eff_small && !(__dmul_rn(prm.u, m1) > a_cand)) {
+    if (!(__dmul_rn(prm.u, ext) > a_cand)) {
+      const double colmax = dmax_ref(m1, ext);
+      if (!(a_cand < __dmul_rn(kWeakPivotRatio, colmax))) {
+        pa = cand;
+        return 1;
+      }
+      weak_1x1 = true;
+      weak_growth = colmax / a_cand;
+    }
+  }
+  if (r_best < k || r_best >= limit || m1 <= 0.0) {
+    if (weak_1x1) {
+      pa = cand;
+      return 1;
+    }
+    return 0;
+  }
+  const double *col_r = F + (size_t)r_best * sf;
+  double om2 = 0.0, off1 = 0.0;
+  for (int i = k + tid; i < r_best; i += NTT) {
+    const double x = fabs(F[(size_t)i * sf + r_best]);
+    om2 = fmax(om2, x);
+    if (i != cand) off1 = fmax(off1, x);
+  }
+  scan8(col_r, r_best + 1 + tid, f, NTT, [&](double x, int i) {
+    om2 = fmax(om2, x);
+    if (i != cand) off1 = fmax(off1, x);
+  });
+  Top2 none{0.0, 0.0, -1};
+  team_bundle<NT, C>(v, sh, none, om2, off1);
+  double growth2 = 0.0;
+  const double d00 = col[cand];
+  const double d10 = (r_best >= cand) ? F[(size_t)cand * sf + r_best] : F[(size_t)r_best * sf + cand];
+  const double d11 = col_r[r_best];
+  if (k + 1 < limit && two_by_two_ok_s(d00, d10, d11, dmax_ref(m2, ext), off1, prm, growth2) &&
+      (!weak_1x1 || growth2 < weak_growth)) {
+    pa = cand;
+    pb = r_best;
+    return 2;
+  }
+  if (weak_1x1) {
+    pa = cand;
+    return 1;
+  }
+  const double a_r = fabs(d11);
+  if (a_r >= prm.eff_small && (om2 == 0.0 || a_r >= __dmul_rn(prm.u, om2))) {
+    pa = r_best;
+    return 1;
+  }
+  return 0;
 }
 
 // The test of one candidate column of select_pivot's search loop
@@ -500,7 +709,7 @@ __device__ int cand_eval_warp(const FrontRef &v, int k, int limit, int cand, con
   return 0;
 }
 
-template <int NT>
+template <int NT, int C = 1>
 __device__ void select_pivot_blk(const FrontRef &v, int k, int limit, const PivotParams &prm,
                                  FrontShared &sh) {
   const size_t sf = (size_t)v.ld;
@@ -528,8 +737,16 @@ __device__ void select_pivot_blk(const FrontRef &v, int k, int limit, const Pivo
     const double a0 = fabs(col0[k]);
     if (a0 >= prm.eff_small) {
       double cm = 0.0;
-      for (int i = k + 1 + threadIdx.x; i < f; i += NT) cm = fmax(cm, fabs(col0[i]));
-      cm = Block<NT>::max(cm, sh);
+      if constexpr (C == 1) {
+        scan8(col0, k + 1 + (int)threadIdx.x, f, NT, [&](double x, int) { cm = fmax(cm, x); });
+        cm = Block<NT>::max(cm, sh);
+      } else {
+        scan8(col0, k + 1 + team_rank<C>() * NT + (int)threadIdx.x, f, C * NT,
+              [&](double x, int) { cm = fmax(cm, x); });
+        Top2 none{0.0, 0.0, -1};
+        double unused = 0.0;
+        team_bundle<NT, C>(v, sh, none, cm, unused);
+      }
       if (!(__dmul_rn(prm.u, cm) > a0) && !(a0 < __dmul_rn(kWeakPivotRatio, cm))) {
         kind = 1;
         pa = k;
@@ -537,10 +754,52 @@ __device__ void select_pivot_blk(const FrontRef &v, int k, int limit, const Pivo
       }
     }
   }
-  // the search loop, NT / 32 candidates at a time (one warp each)
+  // the search loop: long columns (and teams) one candidate at a time on
+  // all threads; short ones NT / 32 candidates at a time (one warp each)
+  if constexpr (C > 1) {
+    // C candidates per round, one per CTA (its own block scans), then one
+    // team exchange: the first candidate in order that gives a pivot wins
+    const int rank = team_rank<C>();
+    for (int c0 = k; c0 < limit && !done; c0 += C) {
+      const int cand = c0 + rank;
+      int tk = 0, ta = -1, tb = -1;
+      if (cand < limit) tk = cand_eval_team<NT, 1>(v, k, limit, cand, prm, sh, ta, tb);
+      double *slot = v.team_red + (size_t)(sh.tr_seq & 1) * C * 6;
+      if (threadIdx.x == 0) {
+        slot[rank * 4 + 0] = (double)tk;
+        slot[rank * 4 + 1] = (double)ta;
+        slot[rank * 4 + 2] = (double)tb;
+      }
+      team_sync<C>(v);
+      for (int q = 0; q < C; ++q) {
+        const int qk = (int)__ldcg(slot + q * 4 + 0);
+        if (qk) {
+          kind = qk;
+          pa = (int)__ldcg(slot + q * 4 + 1);
+          pb = (int)__ldcg(slot + q * 4 + 2);
+          done = true;
+          break;
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) sh.tr_seq += 1;
+      __syncthreads();
+    }
+  } else if (f > 2048) {
+    for (int cand = k; cand < limit && !done; ++cand) {
+      int ta, tb;
+      const int tk = cand_eval_team<NT, 1>(v, k, limit, cand, prm, sh, ta, tb);
+      if (tk) {
+        kind = tk;
+        pa = ta;
+        pb = tb;
+        done = true;
+      }
+    }
+  }
   constexpr int NW = NT / 32;
   const int warp = threadIdx.x >> 5;
-  for (int c0 = k; c0 < limit && !done; c0 += NW) {
+  for (int c0 = k; c0 < limit && !done && !(C > 1 || f > 2048); c0 += NW) {
     const int cand = c0 + warp;
     int wk = 0, wa = -1, wb = -1;
     if (cand < limit) wk = cand_eval_warp(v, k, limit, cand, prm, wa, wb);
@@ -580,30 +839,30 @@ __device__ void select_pivot_blk(const FrontRef &v, int k, int limit, const Pivo
 }
 
 // apply_pivot (ldlt_kernel.cpp:666-698). The pivot choice is in sh.
-template <int NT>
+template <int NT, int C = 1>
 __device__ void apply_pivot_blk(const FrontRef &v, int &k, bool useW, int w_cols, int ucol_end,
                                 const PivotParams &prm, FrontShared &sh) {
   const size_t sf = (size_t)v.ld;
   const int f = v.f;
   const int kind = sh.kind, pa = sh.a, pb = sh.b;
   if (kind == 1) {
-    sym_swap_blk<NT>(v, k, pa, useW ? w_cols : 0);
+    sym_swap_blk<NT, C>(v, k, pa, useW ? w_cols : 0);
     if (threadIdx.x == 0) {
       inertia_1x1(v.F[k * sf + k], prm.eff_small, sh.st);
       v.tags[k] = 1;
       const double rem = (double)(f - (k + 1));
       sh.st.flops += rem + rem * (rem + 1.0);
     }
-    eliminate_1x1_blk<NT>(v, k, ucol_end, useW, w_cols);
+    eliminate_1x1_blk<NT, C>(v, k, ucol_end, useW, w_cols);
     k += 1;
     return;
   }
   int partner = pb;
   if (pa != k) {
-    sym_swap_blk<NT>(v, k, pa, useW ? w_cols : 0);
+    sym_swap_blk<NT, C>(v, k, pa, useW ? w_cols : 0);
     if (partner == k) partner = pa;
   }
-  if (partner != k + 1) sym_swap_blk<NT>(v, k + 1, partner, useW ? w_cols : 0);
+  if (partner != k + 1) sym_swap_blk<NT, C>(v, k + 1, partner, useW ? w_cols : 0);
   if (threadIdx.x == 0) {
     inertia_2x2(v.F[k * sf + k], v.F[k * sf + k + 1], v.F[(k + 1) * sf + k + 1], prm.small_pivot,
                 sh.st);
@@ -613,7 +872,7 @@ __device__ void apply_pivot_blk(const FrontRef &v, int &k, bool useW, int w_cols
     sh.st.flops += 6.0 * rem + 2.0 * rem * (rem + 1.0);
     ++sh.st.two_by_two;
   }
-  eliminate_2x2_blk<NT>(v, k, ucol_end, useW, w_cols);
+  eliminate_2x2_blk<NT, C>(v, k, ucol_end, useW, w_cols);
   k += 2;
 }
 
@@ -729,7 +988,7 @@ __device__ __forceinline__ bool tpp_request_flush(TppState &S) {
 // in S.g_* (returns true), or to its end (returns false: the Schur update of
 // the pivots [0, S.k) remains). The caller applies F[c0:f, c0:e] -=
 // L[c0:f, p0:p1] W[c0:e, :]^T between two calls.
-template <int NT>
+template <int NT, int C = 1>
 __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontShared &sh, TppState &S) {
   const int f = v.f, ne = v.ne;
   const size_t sf = (size_t)v.ld;
@@ -797,7 +1056,7 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
             __syncthreads();
             const int qq = sh.ivals[0];
             __syncthreads();
-            sym_swap_blk<NT>(v, k + t, qq, 0);
+            sym_swap_blk<NT, C>(v, k + t, qq, 0);
           }
           S.live = max(S.live, k + np);
           S.k_paired = k;
@@ -807,7 +1066,7 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
       if (S.stalled) {
         const int m = pl - k;
         const int mv = min(m, S.live - pl);
-        for (int t = 0; t < mv; ++t) sym_swap_blk<NT>(v, k + t, S.live - mv + t, 0);
+        for (int t = 0; t < mv; ++t) sym_swap_blk<NT, C>(v, k + t, S.live - mv + t, 0);
         S.live -= m;
       }
       continue;
@@ -817,12 +1076,12 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
       S.post = 0;
       if (S.stalled && S.k < ne) {
         const int ss = S.k;
-        select_pivot_blk<NT>(v, S.k, ne, prm, sh);
+        select_pivot_blk<NT, C>(v, S.k, ne, prm, sh);
         if (sh.kind == 0) {
           S.phase = 2;
           return false;
         }
-        apply_pivot_blk<NT>(v, S.k, true, 0, ss, prm, sh);
+        apply_pivot_blk<NT, C>(v, S.k, true, 0, ss, prm, sh);
         S.g_p0 = ss;
         S.g_p1 = S.k;
         S.g_c0 = S.k;
@@ -844,12 +1103,12 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
         S.pl = min(S.live, S.ps + prm.nb);
         S.stalled = 0;
         while (S.k < S.pl) {
-          select_pivot_blk<NT>(v, S.k, S.pl, prm, sh);
+          select_pivot_blk<NT, C>(v, S.k, S.pl, prm, sh);
           if (sh.kind == 0) {
             S.stalled = 1;
             break;
           }
-          apply_pivot_blk<NT>(v, S.k, true, S.k - S.ps, S.pl, prm, sh);
+          apply_pivot_blk<NT, C>(v, S.k, true, S.k - S.ps, S.pl, prm, sh);
         }
         S.g_p0 = S.ps;
         S.g_p1 = S.k;
@@ -868,12 +1127,12 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
         S.pl = min(ne, S.ps + prm.nb);
         S.stalled = 0;
         while (S.k < S.pl) {
-          select_pivot_blk<NT>(v, S.k, S.pl, prm, sh);
+          select_pivot_blk<NT, C>(v, S.k, S.pl, prm, sh);
           if (sh.kind == 0) {
             S.stalled = 1;
             break;
           }
-          apply_pivot_blk<NT>(v, S.k, true, S.k - S.ps, S.pl, prm, sh);
+          apply_pivot_blk<NT, C>(v, S.k, true, S.k - S.ps, S.pl, prm, sh);
         }
         S.g_p0 = S.ps;
         S.g_p1 = S.k;

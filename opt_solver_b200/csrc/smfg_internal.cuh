@@ -59,6 +59,8 @@ struct DevFactor {
   int64_t rows_cap = 0;
   unsigned long long *counters = nullptr;  // [0] arena base, [1] rows base, [2] error flags, [3] max|A| bits, [4] blocks
   TppState *tpp = nullptr;    // per large front of a level: blocked-pivoting state
+  unsigned *team_bar = nullptr;  // per large front of a level: its CTA team's barrier words
+  double *team_red = nullptr;    // per large front of a level: its team's reduction scratch
   double *work = nullptr;     // solve / refinement scratch
   int64_t work_cap = 0;
   // mixed precision: fronts whose trailing updates run on the tensor cores

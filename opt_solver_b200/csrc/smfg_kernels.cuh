@@ -13,6 +13,8 @@ enum : int { kCArena = 0, kCRows = 1, kCFlags = 2, kCMaxAbs = 3, kCAux = 4, kCEf
 // error flag bits (counters[kCFlags])
 enum : unsigned { kFArena = 1u, kFRows = 2u, kFNonfinite = 4u, kFNotPosdef = 8u, kFNonfiniteD = 16u,
                   kFMap = 32u, kFInternal = 64u, kFTcWait = 128u, kFTcCap = 256u };
+// team reduction scratch per large front (2 buffers x 8 CTAs x 6 doubles)
+constexpr int kTeamRedDoubles = 128;
 // flags after which the rest of a factorization is skipped (retried with
 // more room, or reported)
 constexpr unsigned kFAbort = kFArena | kFRows | kFTcWait | kFTcCap;
@@ -442,6 +444,7 @@ __global__ void k_large_init(DevPlan P, DevFactor X, const int *__restrict__ lar
                              int posdef, int nbo) {
   if (X.counters[kCFlags] & kFAbort) return;
   const int s = large[blockIdx.x];
+  if (threadIdx.x == 0) X.team_bar[2 * blockIdx.x] = 0u;  // arrivals of the front's team
   const int f = X.sn_f[s];
   int *loc = X.ploc + X.sn_roff[s];
   for (int t = threadIdx.x; t < f; t += blockDim.x) loc[t] = t;
@@ -454,27 +457,44 @@ __global__ void k_large_init(DevPlan P, DevFactor X, const int *__restrict__ lar
   }
 }
 
-template <int NT>
+// One blocked-TPP step (tpp_step_blk) of each large front of a level; a
+// front is taken by a team of C CTAs launched as one thread-block cluster
+// (blockIdx.x / C = the front), the pivot decisions taken by every CTA of
+// the team alike and the swaps and panel eliminations split over it.
+template <int NT, int C>
 __global__ void __launch_bounds__(NT) k_large_panel(DevPlan P, DevFactor X, const int *__restrict__ large,
-                                                    PivotParams prm, int iter) {
+                                                    PivotParams prm, int iter, unsigned *__restrict__ team_bar) {
   __shared__ FrontShared sh;
+  __shared__ int s_abort;
   if (X.counters[kCFlags] & kFAbort) return;
-  const int s = large[blockIdx.x];
-  TppState S = X.tpp[blockIdx.x];
+  const int q = blockIdx.x / C;
+  const bool lead = team_rank<C>() == 0 && threadIdx.x == 0;
+  const int s = large[q];
+  TppState S = X.tpp[q];
   if (S.phase == 2) {
-    if (threadIdx.x == 0) X.tpp[blockIdx.x].pad[0] = 0;
+    if (lead) X.tpp[q].pad[0] = 0;
     return;
   }
   prm.eff_small = __longlong_as_double((long long)X.counters[kCEffSmall]);
-  const FrontRef v = large_view(P, X, s);
-  if (threadIdx.x == 0) sh.st = S.st;
-  __syncthreads();
-  const bool more = tpp_step_blk<NT>(v, prm, sh, S);
-  __syncthreads();
+  FrontRef v = large_view(P, X, s);
+  v.team_bar = team_bar + 2 * q;
+  v.err = X.counters + kCFlags;
+  v.abort = &s_abort;
+  v.team_red = X.team_red + (size_t)q * kTeamRedDoubles;
   if (threadIdx.x == 0) {
+    sh.st = S.st;
+    sh.tr_seq = 0;
+    s_abort = 0;
+  }
+  __syncthreads();
+  // every CTA has read the state before the leader may write it back
+  if constexpr (C > 1) team_sync<C>(v);
+  const bool more = tpp_step_blk<NT, C>(v, prm, sh, S);
+  __syncthreads();
+  if (lead) {
     S.st = sh.st;
     S.pad[0] = more ? 1 : 0;
-    X.tpp[blockIdx.x] = S;
+    X.tpp[q] = S;
     if (more) {
       atomicMax(X.counters + kCActive, (unsigned long long)(iter + 1));
       // algorithmic flops of the deferred update asked for (2 per FMA)

@@ -57,7 +57,8 @@ class Control(C.Structure):
                 ("small_pivot", C.c_double), ("nb", C.c_int), ("blocked_min_front", C.c_int),
                 ("precision", C.c_int), ("max_negative_pivots", C.c_int),
                 ("scale", C.c_void_p), ("profile", C.c_int), ("mixed_block", C.c_int),
-                ("mixed_kind", C.c_int), ("mixed_min_front", C.c_int), ("reserved_i", C.c_int * 4),
+                ("mixed_kind", C.c_int), ("mixed_min_front", C.c_int), ("panel_team", C.c_int),
+                ("reserved_i", C.c_int * 3),
                 ("reserved_d", C.c_double * 8)]
 
 
@@ -150,6 +151,8 @@ def lib():
                                          C.POINTER(C.c_int64)]
         L.smfg_symbolic_view.restype = C.c_int
         L.smfg_symbolic_free.argtypes = [C.POINTER(C.c_void_p)]
+        L.smfg_matching_scale.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, C.POINTER(C.c_int)]
+        L.smfg_matching_scale.restype = C.c_int
         L.smfg_tc_update.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                      C.c_int, C.c_int, C.c_int]
         L.smfg_tc_update.restype = C.c_int
@@ -269,6 +272,19 @@ def analyse(n, col_ptr, row_idx, ordering: int = ORDER_ND, nemin: int = 8,
         L.smfg_symbolic_free(C.byref(h))
 
 
+def matching_scale(n, col_ptr, row_idx, values):
+    """smfg_matching_scale: symmetric max-product matching scaling (n
+    doubles, original numbering) and the count of unmatched columns."""
+    s = np.zeros(n, dtype=np.float64)
+    um = C.c_int()
+    rc = lib().smfg_matching_scale(int(n), np.ascontiguousarray(col_ptr, dtype=np.int32),
+                                   np.ascontiguousarray(row_idx, dtype=np.int32),
+                                   np.ascontiguousarray(values, dtype=np.float64), s, C.byref(um))
+    if rc != SMFG_OK:
+        raise SmfgError(rc, "smfg_matching_scale")
+    return s, um.value
+
+
 TC_TF32X3, TC_BF16X3 = 0, 1
 REFINE_CLASSICAL, REFINE_FGMRES, REFINE_AUTO = 0, 1, 2
 
@@ -343,7 +359,7 @@ class Solver:
     def factor(self, values, posdef: bool = False, u: float = 0.01, small: float = 1e-20,
                scale=None, precision: int = PREC_FP64, max_negative_pivots: int = -1,
                raise_on_singular: bool = False, mixed_block: int = 0, mixed_kind: int = 0,
-               mixed_min_front: int = 0) -> Info:
+               mixed_min_front: int = 0, panel_team: int = 0) -> Info:
         """Factor new values (the caller's entry order). ``values`` is a
         numpy array, or any object with ``data_ptr()`` (a CUDA tensor) for
         values already in device memory. precision=PREC_MIXED: tensor-core
@@ -354,6 +370,7 @@ class Solver:
         c.mixed_block = mixed_block
         c.mixed_kind = mixed_kind
         c.mixed_min_front = mixed_min_front
+        c.panel_team = panel_team
         if scale is not None and len(scale):
             self._scale = np.ascontiguousarray(scale, dtype=np.float64)
             c.scale = self._scale.ctypes.data
@@ -401,7 +418,8 @@ class Solver:
         return {"gemm_ms": info.reserved_d[0], "gemm_flops": info.reserved_d[1],
                 "gemm_launches": info.reserved_i[0], "arena_bytes": info.reserved_d[2],
                 "tc_ms": info.reserved_d[4], "tc_flops": info.reserved_d[3],
-                "tc_passes": info.reserved_i[1], "factor_ms": info.factor_ms}
+                "tc_passes": info.reserved_i[1], "panel_ms": info.reserved_d[5],
+                "factor_ms": info.factor_ms}
 
     # -- solve -------------------------------------------------------------
     def solve(self, b, job: int = SOLVE_FULL):

@@ -470,6 +470,19 @@ static int ldlt_factor_front(double *F, int f, int num_elig, int *rows, const mf
   return k;
 }
 
+void mfo_factor_front(double *F, int f, int ne, int *rows, const mfo_params *prm, int8_t *tags,
+                      int64_t *out) {
+  mfo_factor o;
+  memset(&o, 0, sizeof(o));
+  double *work = (double *)malloc(sizeof(double) * ((size_t)f * (prm->nb + 2) + (size_t)f * f + 1));
+  const int k = ldlt_factor_front(F, f, ne, rows, prm, tags, work, &o);
+  free(work);
+  out[0] = o.pos;
+  out[1] = o.neg;
+  out[2] = o.zero;
+  out[3] = k;
+}
+
 int mfo_factorize(const mfo_analysis *a, const double *pv, const mfo_params *prm, mfo_factor *o) {
   const int n = a->n, ns = a->nsn;
   o->pos = o->neg = o->zero = o->delayed = o->two_by_two = o->max_front = 0;

@@ -53,6 +53,14 @@ typedef struct {
 
 int mfo_factorize(const mfo_analysis *a, const double *pvals, const mfo_params *prm, mfo_factor *out);
 
+/* One dense front through the front kernel alone (ldlt_factor_front with
+ * first = 0, solver/src/ldlt_kernel.cpp:970-1139): F f x f column-major
+ * (lower triangle), the first ne columns eligible; rows, tags (f) updated in
+ * place. out[0..3] = positive, negative, zero pivots, accepted pivots. For
+ * the known-answer tests of the dense kernel. */
+void mfo_factor_front(double *F, int f, int ne, int *rows, const mfo_params *prm, int8_t *tags,
+                      int64_t *out);
+
 /* In-place full solve of A x = b on the permuted, scaled system:
  * x (n, new numbering) overwritten. */
 void mfo_solve_permuted(const mfo_analysis *a, const mfo_factor *fac, int posdef, double *x);

@@ -274,7 +274,27 @@ def _oracle_lib():
         _olib.mfo_solve_permuted.argtypes = [C.c_void_p, C.c_void_p, C.c_int, _f64p]
         _olib.mfo_residual.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, _f64p,
                                        C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        _olib.mfo_factor_front.argtypes = [_f64p, C.c_int, C.c_int, _i32p, C.c_void_p,
+                                           np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS"), _i64p]
     return _olib
+
+
+def factor_front(A, ne: int, u: float = 0.01, small: float = 1e-20, nb: int = 16,
+                 blocked_min_front: int = 96, posdef: bool = False):
+    """One dense front (f x f symmetric, lower triangle used, first ne columns
+    eligible) through the restated front kernel: (F, rows, tags, (pos, neg,
+    zero, accepted))."""
+    F = np.array(A, dtype=np.float64, order="F")
+    f = F.shape[0]
+    flat = np.ascontiguousarray(F.T.reshape(-1))  # column-major storage
+    rows = np.arange(f, dtype=np.int32)
+    tags = np.zeros(f, dtype=np.int8)
+    out = np.zeros(4, dtype=np.int64)
+    m = float(np.max(np.abs(F))) if F.size else 0.0
+    eff = small * m if 0.0 < m < small else small
+    prm = _MfoParams(u, eff, small, nb, blocked_min_front, int(posdef), 0, 0)
+    _oracle_lib().mfo_factor_front(flat, f, ne, rows, C.byref(prm), tags, out)
+    return flat.reshape(f, f).T, rows, tags, tuple(int(x) for x in out)
 
 
 def permuted_values(a: Analysis, values, scale=None):

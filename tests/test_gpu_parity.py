@@ -134,3 +134,28 @@ def test_not_posdef_and_nonfinite(ref_lib):
         sv.factor(nanv, posdef=True)
     gi = sv.factor(v, posdef=True)
     assert gi.status == 0 and gi.inertia == (n, 0, 0)
+
+
+@pytest.mark.parametrize("team", [2, 4, 8])
+def test_panel_teams_bitwise(team, oracle_lib):
+    """The indefinite large-front pivoting on a team of CTAs (a thread-block
+    cluster splitting the swaps and eliminations by rows) gives the one-CTA
+    factor bit for bit, and both the oracle's."""
+    O = oracle_lib
+    from opt_solver_b200 import smfg
+    from opt_solver_b200 import workloads as W
+    n, cp, ri, v = W.kkt_ipm(12, 800, seed=11)
+    a = smfg.analyse(n, cp, ri)
+    ox = O.restated_factorize(a, O.permuted_values(a, v), False)
+    sv = smfg.Solver(a, device=0)
+    g1 = sv.factor(v, posdef=False, panel_team=1)
+    e1 = sv.export()
+    gt = sv.factor(v, posdef=False, panel_team=team)
+    et = sv.export()
+    assert gt.inertia == g1.inertia == ox.inertia == (12 ** 3, 800, 0)
+    assert gt.delayed_pivots == g1.delayed_pivots == ox.delayed > 0
+    assert np.array_equal(et.blocks, e1.blocks)
+    assert np.array_equal(et.rows, e1.rows)
+    for s in range(a.nsn):
+        assert np.array_equal(et.block(s), ox.block(s)), s
+    sv.close()
