@@ -964,7 +964,11 @@ __device__ __forceinline__ void tpp_init(TppState &S, int ne, bool posdef, bool 
   S.g_p0 = S.g_p1 = S.g_c0 = S.g_e = 0;
   S.mixed = mixed ? 1 : 0;
   S.tc_done = 0;
-  S.se = mixed ? nbo : (1 << 30);
+  // SPD: outer blocks of nbo pivots; indefinite: every eligible column
+  // stays in the FP64 deferred updates (the pivot search and its swaps
+  // never meet a stale column) and the tensor cores take the contribution
+  // block, nbo pivots at a time
+  S.se = (mixed && posdef) ? nbo : (1 << 30);
   S.flush = 0;
   S.st = FrontStats{0, 0, 0, 0, 0.0};
 }

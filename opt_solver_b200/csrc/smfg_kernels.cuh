@@ -1013,7 +1013,9 @@ __global__ void k_tc_jobs(DevPlan P, DevFactor X, const int *__restrict__ large,
     const int s = large[q];
     const int f = X.sn_f[s], ne = X.sn_ne[s], k = S.k;
     const int sep = min(S.se, ne);
-    if (S.tc_done < k && (S.flush || k >= sep || S.phase == 2)) {
+    const bool cb_only = S.se >= ne;  // the contribution block only (indefinite fronts)
+    const bool due = cb_only ? (k - S.tc_done >= nbo) : (k >= sep);
+    if (S.tc_done < k && (S.flush || due || S.phase == 2)) {
       const int n = f - sep, kc = k - S.tc_done;
       if (n > 0) {
         double *F = X.arena + X.sn_off[s];
@@ -1040,7 +1042,7 @@ __global__ void k_tc_jobs(DevPlan P, DevFactor X, const int *__restrict__ large,
         flops += 2.0 * kc * ((double)n * (n + 1) / 2);
       }
       S.tc_done = k;
-      S.se = k + nbo;
+      if (!cb_only) S.se = k + nbo;
     }
     S.flush = 0;
   }
