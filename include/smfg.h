@@ -260,6 +260,23 @@ SMFG_API int smfg_last_times(smfg_plan_t plan, double *factor_ms, double *solve_
 SMFG_API int smfg_matching_scale(int n, const int *col_ptr, const int *row_idx, const double *values,
                                  double *scale, int *unmatched);
 
+/* The learned per-front precision selector's network (no reference
+ * counterpart: smf has no learned component). A one-hidden-layer MLP in
+ * FP32, d features (<= 32) -> h ReLU units (<= 64) -> one logit, its
+ * parameters packed as W1 (h x d, row-major), b1 (h), w2 (h), b2 (1):
+ * smfg_mlp_params(d, h) floats. All pointers are device memory; the calls
+ * are synchronous on the legacy default stream. forward: out[s] =
+ * sigmoid(logit(X[s, :])). backward: grad (params + 1 floats, the last
+ * the loss) of sum_s w_s BCE(p_s, y_s) / n (w NULL: 1), scratch holding
+ * ceil(n / 128) * (params + 1) floats; the sum is taken in a fixed order.
+ * adam: one Adam step (step >= 1 for the bias corrections). */
+SMFG_API int smfg_mlp_params(int d, int h);
+SMFG_API int smfg_mlp_forward(const float *d_X, int n, int d, const float *d_params, int h, float *d_out);
+SMFG_API int smfg_mlp_backward(const float *d_X, const float *d_y, const float *d_w, int n, int d,
+                               const float *d_params, int h, float *d_scratch, float *d_grad);
+SMFG_API int smfg_mlp_adam(float *d_params, const float *d_grad, float *d_m, float *d_v, int np, float lr,
+                           float beta1, float beta2, float eps, int step);
+
 /* A symbolic analysis of the engine's own (host code, no GPU needed),
  * producing the smfg_analysis_t contract above when smf's analyse
  * (solver/src/symbolic_analysis.cpp:434, out of this library's scope) is not

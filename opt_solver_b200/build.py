@@ -18,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsmfg.so")
-SOURCES = ["smfg_engine.cu", "smfg_analyse.cpp", "smfg_scaling.cpp"]
+SOURCES = ["smfg_engine.cu", "smfg_analyse.cpp", "smfg_scaling.cpp", "smfg_mlp.cu"]
 DEPS = ["smfg_front.cuh", "smfg_kernels.cuh", "smfg_internal.cuh", "smfg_tc.cuh"]
 
 

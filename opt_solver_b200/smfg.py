@@ -151,6 +151,16 @@ def lib():
                                          C.POINTER(C.c_int64)]
         L.smfg_symbolic_view.restype = C.c_int
         L.smfg_symbolic_free.argtypes = [C.POINTER(C.c_void_p)]
+        L.smfg_mlp_params.argtypes = [C.c_int, C.c_int]
+        L.smfg_mlp_params.restype = C.c_int
+        L.smfg_mlp_forward.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]
+        L.smfg_mlp_forward.restype = C.c_int
+        L.smfg_mlp_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                        C.c_void_p, C.c_void_p]
+        L.smfg_mlp_backward.restype = C.c_int
+        L.smfg_mlp_adam.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float,
+                                    C.c_float, C.c_float, C.c_float, C.c_int]
+        L.smfg_mlp_adam.restype = C.c_int
         L.smfg_matching_scale.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, C.POINTER(C.c_int)]
         L.smfg_matching_scale.restype = C.c_int
         L.smfg_tc_update.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
