@@ -117,7 +117,14 @@ typedef struct {
   int mixed_kind;
   int mixed_min_front;
   int panel_team;         /* CTAs per indefinite large front's pivoting (1, 2, 4, 8); 0: by front size */
-  int reserved_i[3];
+  /* 1: replay the factorization as one CUDA graph. The first call with a
+   * given configuration (control, precision mask, value pointer) factors
+   * normally and captures the launch sequence; later calls with the same
+   * configuration replay it (the refactor of an interior-point iteration).
+   * A replay that finds a front needing more pivoting steps than captured,
+   * or an arena too small, falls back to the normal path. */
+  int graph;
+  int reserved_i[2];
   double reserved_d[8];
 } smfg_control_t;
 

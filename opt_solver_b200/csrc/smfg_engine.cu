@@ -435,7 +435,7 @@ static void enqueue_tc(Plan &pl, const MixedCfg &mc, const int *lg, int nL, TppS
 }
 
 static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_t &c, LaunchCount &lc,
-                           GemmProfile &gp) {
+                           GemmProfile &gp, bool fixed = false) {
   DevPlan &d = pl.d;
   DevFactor &x = pl.x;
   cudaStream_t st = pl.stream;
@@ -444,7 +444,8 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
   SMFG_CUDA(cudaMemsetAsync(x.sn_dout, 0, sizeof(int) * pl.nsn, st));
   const double *scale = nullptr;
   if (c.scale) {
-    SMFG_CUDA(cudaMemcpyAsync(x.scale, c.scale, sizeof(double) * pl.n, cudaMemcpyHostToDevice, st));
+    // a graph reads the scale the host put in x.scale before the replay
+    if (!fixed) SMFG_CUDA(cudaMemcpyAsync(x.scale, c.scale, sizeof(double) * pl.n, cudaMemcpyHostToDevice, st));
     scale = x.scale;
   }
   const int *pcol = d.pcol;
@@ -514,6 +515,17 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
           if (lvl_mixed) enqueue_tc(pl, mc, lg, nL, x.tpp, c.posdef, lc, gp);
         }
         lc.n += 2 * steps;
+      } else if (fixed) {
+        // graph capture: a fixed number of steps (finished fronts return at
+        // once), checked on the device
+        const int steps = 2 * ((pl.lvl_large_maxw[l] + c.nb - 1) / c.nb) + 16;
+        for (; it < steps; ++it) {
+          launch_panel(pl, team, lg, nL, prm, it);
+          k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, x.tpp);
+          if (lvl_mixed) enqueue_tc(pl, mc, lg, nL, x.tpp, c.posdef, lc, gp);
+        }
+        k_steps_check<<<1, 32, 0, st>>>(x.counters, steps);
+        lc.n += 2 * steps + 1;
       } else {
         // data-dependent: batches, then a look at the last step that
         // still asked for an update
@@ -596,14 +608,47 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
     }
   }
   SMFG_CUDA(cudaMemcpyAsync(pl.x.sn_mixed, pl.h_mixed.data(), pl.nsn, cudaMemcpyHostToDevice, pl.stream));
-  FactorTotals *d_tot = nullptr;
+  FactorTotals *d_tot = reinterpret_cast<FactorTotals *>(pl.x.counters + kCCount);
   unsigned long long h_cnt[kCCount];
   FactorTotals tot{};
   LaunchCount lc;
   GemmProfile gp;
   gp.on = c.profile != 0;
   float ms = 0.0f;
-  for (int attempt = 0; attempt < 4; ++attempt) {
+  // the graph's configuration: everything its launches captured
+  std::vector<unsigned char> key;
+  auto put = [&](const void *p, size_t n) {
+    const unsigned char *b = static_cast<const unsigned char *>(p);
+    key.insert(key.end(), b, b + n);
+  };
+  bool replayed = false;
+  const bool use_graph = c.graph != 0 && !gp.on;
+  if (use_graph) {
+    smfg_control_t kc = c;
+    kc.scale = c.scale ? reinterpret_cast<const double *>(1) : nullptr;  // the scale's values are copied per call
+    put(&kc, sizeof(kc));
+    put(&d_values, sizeof(d_values));
+    put(pl.h_mixed.data(), pl.h_mixed.size());
+    put(&pl.x.arena, sizeof(pl.x.arena));
+    put(&pl.x.arena_cap, sizeof(int64_t));
+    put(&pl.x.rows_cap, sizeof(int64_t));
+    put(&pl.x.tc_img, sizeof(pl.x.tc_img));
+    if (pl.graph_exec && key == pl.graph_key) {
+      if (c.scale)
+        SMFG_CUDA(cudaMemcpyAsync(pl.x.scale, c.scale, sizeof(double) * pl.n, cudaMemcpyHostToDevice, pl.stream));
+      SMFG_CUDA(cudaEventRecord(pl.ev0, pl.stream));
+      SMFG_CUDA(cudaGraphLaunch(pl.graph_exec, pl.stream));
+      SMFG_CUDA(cudaEventRecord(pl.ev1, pl.stream));
+      SMFG_CUDA(cudaMemcpyAsync(h_cnt, pl.x.counters, sizeof(h_cnt), cudaMemcpyDeviceToHost, pl.stream));
+      SMFG_CUDA(cudaMemcpyAsync(&tot, d_tot, sizeof(tot), cudaMemcpyDeviceToHost, pl.stream));
+      SMFG_CUDA(cudaStreamSynchronize(pl.stream));
+      SMFG_CUDA(cudaEventElapsedTime(&ms, pl.ev0, pl.ev1));
+      const unsigned fl = (unsigned)h_cnt[kCFlags];
+      replayed = !(fl & (kFArena | kFRows | kFTcCap | kFSteps));
+      lc.n = pl.graph_launches;
+    }
+  }
+  for (int attempt = 0; attempt < 4 && !replayed; ++attempt) {
     ensure_arena(pl, std::max(need_a, pl.x.arena_cap), std::max(need_r, pl.x.rows_cap));
     if (pl.x.tc_img_cap < tc_need) {
       dfree(pl, pl.x.tc_img);
@@ -614,7 +659,6 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
     gp.used = 0;
     SMFG_CUDA(cudaEventRecord(pl.ev0, pl.stream));
     enqueue_factor(pl, d_values, c, lc, gp);
-    if (!d_tot) d_tot = reinterpret_cast<FactorTotals *>(pl.x.counters + kCCount);
     static_assert(sizeof(FactorTotals) <= 8 * sizeof(unsigned long long), "totals slot");
     k_finish<<<1, 1024, 0, pl.stream>>>(pl.d, pl.x, d_tot);
     lc.n += 1;
@@ -634,6 +678,38 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
       continue;
     }
     break;
+  }
+  if (use_graph && !replayed && !((unsigned)h_cnt[kCFlags] & (kFArena | kFRows | kFTcCap))) {
+    // capture the sequence for the next call with this configuration
+    key.clear();
+    smfg_control_t kc = c;
+    kc.scale = c.scale ? reinterpret_cast<const double *>(1) : nullptr;
+    put(&kc, sizeof(kc));
+    put(&d_values, sizeof(d_values));
+    put(pl.h_mixed.data(), pl.h_mixed.size());
+    put(&pl.x.arena, sizeof(pl.x.arena));
+    put(&pl.x.arena_cap, sizeof(int64_t));
+    put(&pl.x.rows_cap, sizeof(int64_t));
+    put(&pl.x.tc_img, sizeof(pl.x.tc_img));
+    if (pl.graph_exec) {
+      cudaGraphExecDestroy(pl.graph_exec);
+      pl.graph_exec = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    LaunchCount glc;
+    GemmProfile none;
+    SMFG_CUDA(cudaStreamBeginCapture(pl.stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_factor(pl, d_values, c, glc, none, true);
+    k_finish<<<1, 1024, 0, pl.stream>>>(pl.d, pl.x, d_tot);
+    const cudaError_t ce = cudaStreamEndCapture(pl.stream, &g);
+    if (ce == cudaSuccess && g) {
+      if (cudaGraphInstantiate(&pl.graph_exec, g, 0) != cudaSuccess) pl.graph_exec = nullptr;
+      cudaGraphDestroy(g);
+      pl.graph_key = key;
+      pl.graph_launches = glc.n + 1;
+    } else {
+      clear_stale_error();
+    }
   }
   const unsigned flags = (unsigned)h_cnt[kCFlags];
   // stored pivots of the large fronts by level (the solves' block counts)
@@ -878,6 +954,7 @@ SMFG_API void smfg_plan_destroy(smfg_plan_t *plan) {
   if (pl.ev0) cudaEventDestroy(pl.ev0);
   if (pl.ev1) cudaEventDestroy(pl.ev1);
   if (pl.ev_in) cudaEventDestroy(pl.ev_in);
+  if (pl.graph_exec) cudaGraphExecDestroy(pl.graph_exec);
   if (pl.stream) cudaStreamDestroy(pl.stream);
   delete *plan;
   *plan = nullptr;

@@ -12,7 +12,7 @@ enum : int { kCArena = 0, kCRows = 1, kCFlags = 2, kCMaxAbs = 3, kCAux = 4, kCEf
              kCActive = 6, kCGemmFlops = 7, kCTcFlops = 8, kCCount = 9 };
 // error flag bits (counters[kCFlags])
 enum : unsigned { kFArena = 1u, kFRows = 2u, kFNonfinite = 4u, kFNotPosdef = 8u, kFNonfiniteD = 16u,
-                  kFMap = 32u, kFInternal = 64u, kFTcWait = 128u, kFTcCap = 256u };
+                  kFMap = 32u, kFInternal = 64u, kFTcWait = 128u, kFTcCap = 256u, kFSteps = 512u };
 // team reduction scratch per large front (2 buffers x 8 CTAs x 6 doubles)
 constexpr int kTeamRedDoubles = 128;
 // flags after which the rest of a factorization is skipped (retried with
@@ -1052,6 +1052,13 @@ __global__ void k_tc_jobs(DevPlan P, DevFactor X, const int *__restrict__ large,
   }
   *X.tc_njobs = nj;
   if (flops > 0.0) atomicAdd(reinterpret_cast<double *>(X.counters + kCTcFlops), flops);
+}
+
+// Graph replays run a fixed number of pivoting steps per level: a front
+// still asking for an update at the last one did not finish (the host then
+// factors without the graph).
+__global__ void k_steps_check(unsigned long long *cnt, int steps) {
+  if (threadIdx.x == 0 && cnt[kCActive] >= (unsigned long long)steps) set_flag(cnt, kFSteps);
 }
 
 // Totals over all fronts, in supernode order (deterministic).

@@ -58,7 +58,7 @@ class Control(C.Structure):
                 ("precision", C.c_int), ("max_negative_pivots", C.c_int),
                 ("scale", C.c_void_p), ("profile", C.c_int), ("mixed_block", C.c_int),
                 ("mixed_kind", C.c_int), ("mixed_min_front", C.c_int), ("panel_team", C.c_int),
-                ("reserved_i", C.c_int * 3),
+                ("graph", C.c_int), ("reserved_i", C.c_int * 2),
                 ("reserved_d", C.c_double * 8)]
 
 
@@ -369,7 +369,7 @@ class Solver:
     def factor(self, values, posdef: bool = False, u: float = 0.01, small: float = 1e-20,
                scale=None, precision: int = PREC_FP64, max_negative_pivots: int = -1,
                raise_on_singular: bool = False, mixed_block: int = 0, mixed_kind: int = 0,
-               mixed_min_front: int = 0, panel_team: int = 0) -> Info:
+               mixed_min_front: int = 0, panel_team: int = 0, graph: bool = False) -> Info:
         """Factor new values (the caller's entry order). ``values`` is a
         numpy array, or any object with ``data_ptr()`` (a CUDA tensor) for
         values already in device memory. precision=PREC_MIXED: tensor-core
@@ -381,6 +381,7 @@ class Solver:
         c.mixed_kind = mixed_kind
         c.mixed_min_front = mixed_min_front
         c.panel_team = panel_team
+        c.graph = int(graph)
         if scale is not None and len(scale):
             self._scale = np.ascontiguousarray(scale, dtype=np.float64)
             c.scale = self._scale.ctypes.data
