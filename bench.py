@@ -49,6 +49,15 @@ CONFIGS = {
               "trajectory_batch(1024)", False, 8),
 }
 BATCH_COUNT = 1024
+# configuration 5: interior-point refactor streams, the analysis reused
+STREAMS = {
+    # the 64^3 pattern with the barrier diagonal Sigma_k added (SPD)
+    "stream": ("refactor stream: 64^3 SPD pattern + Sigma_k on the diagonal, 60 refactors, 1 RHS", "spd3d", True),
+    # the KKT at the size the reference factors, Sigma_k on the primal block
+    "kktstream": ("refactor stream: IPM KKT 20^3 + 4,000 (n=12,000), Sigma_k on the primal diagonal, "
+                  "60 refactors, 1 RHS", "kkt", False),
+}
+STREAM_LEN = 60
 
 
 def batch_systems(rank: int = 0, world: int = 1):
@@ -355,6 +364,114 @@ def run_ours(args, rank, world, local):
     }
 
 
+SELECTOR_FILE = os.path.join(ROOT, "opt_solver_b200", "data", "selector.npz")
+
+
+def run_stream(args, rank, world, local):
+    """Configuration 5: one analysis, then refactors of a barrier-parameter
+    stream; per step factor + solve + refinement (auto) to omega <= 1e-12,
+    device time. Arms: plain FP64; and graph replay + mixed precision +
+    the learned selector's mask (decided once from the stream's first, plain
+    factorization) with the FP64 judge (fronts whose counts changed against
+    the previous step are refactored in FP64 and leave the mask)."""
+    import torch
+    from opt_solver_b200 import selector as S
+    from opt_solver_b200 import smfg
+    from opt_solver_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    desc, base, posdef = STREAMS[args.config]
+    n, cp, ri, v = build_matrix(base)
+    t0 = time.time()
+    a = smfg.analyse(n, cp, ri, perm=given_ordering(base))
+    analyse_s = time.time() - t0
+    dslot = W.diagonal_slots(n, cp, ri)
+    base_vals = np.array(v, dtype=np.float64)
+    if posdef:
+        sig_idx = np.arange(n)
+        expected = (n, 0, 0)
+    else:
+        nh = 20 ** 3
+        sig_idx = np.arange(nh)
+        base_vals[dslot[:nh]] = 6.0  # H's diagonal without the barrier term
+        expected = (nh, n - nh, 0)
+    sig = W.sigma_stream(sig_idx.size, STREAM_LEN, seed=5)
+    vals = np.repeat(base_vals[None, :], STREAM_LEN, axis=0)
+    vals[:, dslot[sig_idx]] += sig
+    scale = None if posdef else smfg.matching_scale(n, cp, ri, vals[0])[0]
+    d_all = torch.from_numpy(vals).cuda()
+    d_vals = torch.empty(vals.shape[1], dtype=torch.float64, device="cuda")
+    b = W.rhs(n, 1, seed=1, kind="normal")
+    d_b0 = torch.from_numpy(b).cuda()
+    d_x = d_b0.clone()
+    sv = smfg.Solver(a, device=local)
+    sel = S.load(SELECTOR_FILE, device=local) if os.path.exists(SELECTOR_FILE) else None
+    res = {}
+    clocks = None
+    for arm in ("fp64", "mixed"):
+        lat, fac, sol, ref_ms, solves, inertia_ok, fallbacks = [], [], [], [], [], 0, 0
+        prev = None
+        mask = None
+        sampler = ClockSampler(local)
+        with sampler as clk:
+            for it in range(args.warmup + args.steps):
+                k = it % STREAM_LEN
+                d_vals.copy_(d_all[k])
+                nbad = 0
+                if arm == "fp64" or prev is None:
+                    info = sv.factor(d_vals, posdef=posdef, scale=scale)
+                    f_ms = info.factor_ms
+                else:
+                    if mask is None:
+                        X = S.front_features(a, vals[k], posdef, prev, scale)
+                        mask = sel.mask(a, X) if sel is not None else S.candidates(a).astype(np.int8)
+                    info, mask, nbad = S.factor_checked(sv, a, d_vals, posdef, mask, prev, expected, scale,
+                                                        graph=True)
+                    f_ms = info.reserved_d[6]
+                if arm == "mixed":
+                    prev = sv.front_stats()
+                d_x.copy_(d_b0)
+                sv.solve(d_x)
+                eta, om, its = sv.refine_device(d_b0, d_x, nrhs=1, max_steps=args.refine_max,
+                                                omega_target=OMEGA_GATE, method=smfg.REFINE_AUTO)
+                _, s_ms, r_ms = sv.last_times()
+                if it >= args.warmup:
+                    lat.append(f_ms + s_ms + r_ms)
+                    fac.append(f_ms)
+                    sol.append(s_ms)
+                    ref_ms.append(r_ms)
+                    solves.append(its)
+                    inertia_ok += int(tuple(info.inertia) == expected and om <= OMEGA_GATE)
+                    fallbacks += nbad
+        if arm == "mixed":
+            clocks = clk.summary()
+        res[arm] = {
+            "ms_mean": float(np.mean(lat)), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "factor_ms_mean": float(np.mean(fac)),
+            "solve_ms_mean": float(np.mean(sol)), "refine_ms_mean": float(np.mean(ref_ms)),
+            "refine_solves_mean": float(np.mean(solves)), "refine_solves_max": int(np.max(solves)),
+            "steps_inertia_exact_and_omega_met": inertia_ok, "steps": len(lat),
+            "fp64_fallback_fronts": fallbacks,
+            "mixed_fronts": int(mask.sum()) if (arm == "mixed" and mask is not None) else 0,
+        }
+    sv.close()
+    M, P = res["mixed"], res["fp64"]
+    return {
+        "metric": "factor+solve ms", "value": allmax(M["ms_mean"], world), "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": allmax(M["ms_mean"], world),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (tf32x3 tensor-core updates on the selected fronts)",
+        "data": "synthetic (seeded generator of the configuration)",
+        "config": {"workload": desc, "n": n, "nnz_lower": int(cp[-1]), "stream_length": STREAM_LEN,
+                   "analysis_s": analyse_s, "selector": "trained (opt_solver_b200/data/selector.npz)"
+                   if sel is not None else "none (every large front mixed)",
+                   "step": "refactor + solve + refinement (auto) to eta_inf <= 1e-10, omega <= 1e-12",
+                   "l2": "inputs larger than L2" if vals.shape[1] * 8 > 126e6 else "per-step values fit L2"},
+        "arms": res, "mixed_speedup_vs_plain": P["ms_mean"] / M["ms_mean"],
+        "gpu_launches": None, "clocks": clocks,
+    }
+
+
 def cpu_reference_ms(cfg, threads):
     """The reference smf solver (oracle/_ref, compiled from its sources) on
     the host cores, fastest host mode (non-deterministic, `threads` threads,
@@ -410,12 +527,13 @@ def run_reference_arm(args, rank, world):
     threads = os.cpu_count() or 1
     times = []
     sample = ""
+    cfg = STREAMS[args.config][1] if args.config in STREAMS else args.config
     for i in range(args.warmup + args.steps):
-        ms, sample = cpu_reference_ms(args.config, threads)
+        ms, sample = cpu_reference_ms(cfg, threads)
         if i >= args.warmup:
             times.append(ms)
     ms_step = statistics.median(times)
-    desc = CONFIGS[args.config][0]
+    desc = STREAMS[args.config][0] if args.config in STREAMS else CONFIGS[args.config][0]
     return {
         "impl": "reference", "metric": "factor+solve ms", "value": ms_step, "unit": "ms",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
@@ -451,7 +569,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="spd3d", choices=sorted(CONFIGS))
+    ap.add_argument("--config", default="spd3d", choices=sorted(list(CONFIGS) + list(STREAMS)))
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
                     help="both: time the plain FP64 and the mixed arm; the value is the mixed one")
     ap.add_argument("--refine-max", type=int, default=30, help="refinement solves per step, at most")
@@ -467,6 +585,11 @@ def main():
     if args.impl == "reference":
         line = run_reference_arm(args, rank, world)
         if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    if args.config in STREAMS:
+        line = run_stream(args, rank, world, local)
+        if rank == 0:
             print(json.dumps(line), flush=True)
         return
     r = run_ours(args, rank, world, local)

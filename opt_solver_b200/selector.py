@@ -235,10 +235,12 @@ def factor_checked(sv, a, values, posdef, mask, stats_plain, expected_inertia=No
     last plain factorization's per-front counts: fronts whose own or
     parent's counts changed (or all mixed fronts, when the inertia is not
     the expected one) are set to FP64 and the matrix is refactored.
-    Returns (info, mask used last, misjudged fronts)."""
+    Returns (info, mask used last, misjudged fronts); info.reserved_d[6]
+    holds the device time of all factorizations of the call."""
     parent = np.asarray(a.sn_parent)
     sv.set_front_precision(mask)
     info = sv.factor(values, posdef=posdef, precision=smfg.PREC_MIXED, scale=scale, **kw)
+    total_ms = info.factor_ms
     st = sv.front_stats()
     bad = np.zeros(a.nsn, dtype=bool)
     if stats_plain is not None:
@@ -254,6 +256,8 @@ def factor_checked(sv, a, values, posdef, mask, stats_plain, expected_inertia=No
         mask[bad] = 0
         sv.set_front_precision(mask)
         info = sv.factor(values, posdef=posdef, precision=smfg.PREC_MIXED, scale=scale, **kw)
+        total_ms += info.factor_ms
+    info.reserved_d[6] = total_ms
     return info, mask, nbad
 
 
@@ -304,3 +308,41 @@ def load(path: str, device: int = 0) -> "Selector":
     sel.sd = t.as_tensor(z["sd"])
     sel.threshold = float(z["threshold"])
     return sel
+
+
+def training_problems(count: int = 36, seed: int = 0):
+    """The synthetic training families: interior-point KKTs of several sizes,
+    constraint counts and barrier ranges, and SPD variable-coefficient grids
+    (workloads.py's generators)."""
+    from . import workloads as W
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        if i % 4 == 3:
+            out.append(W.varcoef_3d(int(rng.integers(16, 25)), seed=1000 + i) + (True,))
+        else:
+            m = int(rng.integers(10, 17))
+            ncon = int(rng.integers(m ** 3 // 4, m ** 3 // 2))
+            lo = float(rng.uniform(-10, -4))
+            out.append(W.kkt_ipm(m, ncon, seed=2000 + i, sigma_range=(lo, -lo)) + (False,))
+    return out
+
+
+def main(argv=None):
+    """python -m opt_solver_b200.selector OUT.npz: train the selector on the
+    solver's outcomes over the synthetic families and save it."""
+    import sys
+    argv = sys.argv[1:] if argv is None else argv
+    out = argv[0] if argv else "selector.npz"
+    X, y, _ = collect_outcomes(training_problems(), runs=4, seed=1)
+    sel = Selector(N_FEATURES, 16, seed=0)
+    hist = sel.fit(X, y, epochs=500, lr=0.02)
+    p = sel.predict(X)
+    acc = float(np.mean((p >= sel.threshold) == (y > 0.5)))
+    print(f"samples {len(y)}, positive share {y.mean():.3f}, loss {hist[0]:.4f} -> {hist[-1]:.4f}, "
+          f"training accuracy {acc:.3f}")
+    save(sel, out)
+
+
+if __name__ == "__main__":
+    main()

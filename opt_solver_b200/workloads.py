@@ -139,3 +139,31 @@ def rhs(n: int, nrhs: int = 1, seed: int = 0, kind: str = "uniform"):
     # nrhs > 1: shape (nrhs, n), i.e. the column-major n x nrhs block with
     # leading dimension n that smf's solve takes.
     return b if nrhs > 1 else b[0].copy()
+
+
+def sigma_stream(n_sigma: int, count: int = 60, seed: int = 0, mu0: float = 1e-1, mu1: float = 1e-10,
+                 sigma_range=(-8.0, 8.0)):
+    """The barrier diagonals of an interior-point refactor stream
+    (configuration 5): Sigma_k = Sigma_0 mu_k / mu_0 with mu geometric from
+    mu0 to mu1 over `count` steps and per-entry multiplicative noise
+    log-uniform in [0.5, 2]; Sigma_0 log-uniform in 10^sigma_range. Returns
+    a (count, n_sigma) array."""
+    rng = np.random.default_rng(seed)
+    sigma0 = 10.0 ** rng.uniform(sigma_range[0], sigma_range[1], size=n_sigma)
+    mus = np.geomspace(mu0, mu1, count)
+    out = np.empty((count, n_sigma))
+    for k in range(count):
+        noise = 10.0 ** rng.uniform(np.log10(0.5), np.log10(2.0), size=n_sigma)
+        out[k] = sigma0 * (mus[k] / mu0) * noise
+    return out
+
+
+def diagonal_slots(n, col_ptr, row_idx):
+    """Positions of the diagonal entries in a lower CSC (one per column)."""
+    cp = np.asarray(col_ptr, dtype=np.int64)
+    ri = np.asarray(row_idx)
+    cols = np.repeat(np.arange(n), np.diff(cp))
+    pos = np.nonzero(ri == cols)[0]
+    out = np.full(n, -1, dtype=np.int64)
+    out[cols[pos]] = pos
+    return out
