@@ -63,9 +63,9 @@ STREAM_LEN = 60
 def batch_systems(rank: int = 0, world: int = 1):
     """This rank's contiguous share of configuration 4's systems."""
     from opt_solver_b200 import workloads as W
+    from opt_solver_b200.batch import shard
     mats = W.trajectory_batch(BATCH_COUNT, seed=0)
-    lo = rank * BATCH_COUNT // world
-    hi = (rank + 1) * BATCH_COUNT // world
+    lo, hi = shard(BATCH_COUNT, rank, world)
     return mats[lo:hi]
 
 

@@ -121,3 +121,37 @@ class BatchSolver:
             out.append(x[..., o:o + n])
             o += n
         return out
+
+
+def shard(count: int, rank: int, world: int):
+    """This rank's contiguous slice [lo, hi) of `count` independent systems
+    (configuration 4 on N GPUs: no data-path collective)."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank / world")
+    return rank * count // world, (rank + 1) * count // world
+
+
+def gather_system_stats(local_stats, lo: int, count: int, world: int):
+    """Every rank's per-system (pos, neg, zero, 2x2, delays) rows gathered in
+    system order over torch.distributed (any backend). Returns the
+    (count, 5) array on every rank; raises if the slices do not tile
+    [0, count)."""
+    import torch
+    import torch.distributed as dist
+    mine = (int(lo), [tuple(int(v) for v in r) for r in local_stats])
+    if world == 1:
+        parts = [mine]
+    else:
+        parts = [None] * world
+        dist.all_gather_object(parts, mine)
+    parts.sort(key=lambda p: p[0])
+    out, nxt = [], 0
+    for lo_r, rows in parts:
+        if lo_r != nxt:
+            raise RuntimeError(f"system slices do not tile: expected {nxt}, got {lo_r}")
+        out.extend(rows)
+        nxt += len(rows)
+    if nxt != count:
+        raise RuntimeError(f"{nxt} of {count} systems gathered")
+    del torch
+    return np.asarray(out, dtype=np.int64).reshape(count, 5)
