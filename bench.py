@@ -92,6 +92,7 @@ class _Workload:
             self.nsn = self.solver.merged.nsn
             self.systems = len(mats)
             self.sv = self.solver.solver
+            self.scale = None
             self.expected = [(16 * ((m[0] - 12) // 28) + 12, 12 * ((m[0] - 12) // 28), 0) for m in mats]
         else:
             n, cp, ri, v = build_matrix(cfg)
@@ -104,6 +105,8 @@ class _Workload:
             self.solver = self.sv
             self.values = v
             self.b = W.rhs(n, self.nrhs, seed=1, kind="normal" if cfg.startswith("kkt") else "uniform")
+            # the KKT configurations run with max-product matching scaling on
+            self.scale = smfg.matching_scale(n, cp, ri, v)[0] if cfg.startswith("kkt") else None
             self.n = n
             self.nnz = int(cp[-1])
             self.nsn = a.nsn
@@ -303,7 +306,7 @@ def run_ours(args, rank, world, local):
         prec = smfg.PREC_MIXED if arm == "mixed" else smfg.PREC_FP64
 
         def step():
-            info = sv.factor(d_vals, posdef=posdef, precision=prec)
+            info = sv.factor(d_vals, posdef=posdef, precision=prec, scale=wl.scale)
             d_x.copy_(d_b0)
             sv.solve(d_x)
             eta, om, its = sv.refine_device(d_b0, d_x, nrhs=wl.nrhs, max_steps=args.refine_max,
@@ -347,14 +350,14 @@ def run_ours(args, rank, world, local):
     for _ in range(max(2, min(args.steps, 5))):
         torch.cuda.synchronize()
         t = time.perf_counter()
-        sv.factor(wl.values, posdef=posdef, precision=prec)
+        sv.factor(wl.values, posdef=posdef, precision=prec, scale=wl.scale)
         x = sv.solve(wl.b)
         x, _, _, _ = sv.refine(wl.b, x, max_steps=args.refine_max, omega_target=OMEGA_GATE,
                                method=smfg.REFINE_AUTO)
         e2e.append((time.perf_counter() - t) * 1e3)
     e2e_ms = allmax(sum(e2e) / len(e2e), world)
     _, eta, om = sv.residual(wl.b, x)
-    prof = sv.profile_factor(d_vals, posdef=posdef, precision=prec)
+    prof = sv.profile_factor(d_vals, posdef=posdef, precision=prec, scale=wl.scale)
     return {
         "arms": res, "head": head, "e2e_ms": e2e_ms, "e2e_eta": eta, "e2e_omega": om,
         "analyse_s": wl.analyse_s, "n": wl.n, "nnz": wl.nnz, "nrhs": wl.nrhs, "desc": wl.desc,
@@ -555,7 +558,7 @@ def ncu_step(args):
     prec = smfg.PREC_FP64 if args.precision == "fp64" else smfg.PREC_MIXED
     d_vals = torch.from_numpy(np.ascontiguousarray(wl.values)).cuda()
     d_b = torch.from_numpy(np.ascontiguousarray(wl.b)).cuda()
-    info = wl.sv.factor(d_vals, posdef=wl.posdef, precision=prec)
+    info = wl.sv.factor(d_vals, posdef=wl.posdef, precision=prec, scale=getattr(wl, "scale", None))
     fl = info.kernel_launches
     wl.sv.solve(d_b)
     torch.cuda.synchronize()

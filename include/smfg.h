@@ -187,6 +187,14 @@ SMFG_API int smfg_inertia(smfg_plan_t plan, int *pos, int *neg, int *zero);
  * Kept for later factorizations until changed. */
 SMFG_API int smfg_set_front_precision(smfg_plan_t plan, const int8_t *mask);
 
+/* Tuned team sizes of the indefinite large-front pivoting (an autotuner's
+ * choice; no reference counterpart): teams[b] CTAs (1, 2, 4, 8; 0 = the
+ * built-in rule) for levels whose largest front has [384, 768), [768,
+ * 1536), [1536, 3072), >= 3072 symbolic rows (b = 0..3). NULL resets.
+ * smfg_control_t.panel_team, when set, overrides the table. Kept for later
+ * factorizations. */
+SMFG_API int smfg_set_panel_teams(smfg_plan_t plan, const int *teams);
+
 /* Per-front export of the last factor, in the FactorKeep layout
  * (factor_posdef.hpp:43-220): for supernode s, f[s] realized rows, p[s]
  * stored pivots, its L block (f x p, leading dimension f, D inline for the

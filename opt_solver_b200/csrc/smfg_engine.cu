@@ -376,10 +376,24 @@ static MixedCfg mixed_cfg(const smfg_control_t &c) {
   return m;
 }
 
+// Pivoting steps between two tensor-core passes of indefinite mixed fronts.
+constexpr int kTcEvery = 16;
+
 // Team size (CTAs per front) of a level's indefinite large-front panels, by
 // the largest symbolic front: the swaps and eliminations of a panel stream
 // its columns (16 x f doubles per pivot), which one SM's bandwidth bounds.
 static int panel_team(int maxf) { return maxf >= 3072 ? 8 : maxf >= 1536 ? 4 : maxf >= 768 ? 2 : 1; }
+
+// Size bucket of a level's largest large front: [384, 768), [768, 1536),
+// [1536, 3072), [3072, ...).
+static int team_bucket(int maxf) { return maxf >= 3072 ? 3 : maxf >= 1536 ? 2 : maxf >= 768 ? 1 : 0; }
+
+static int level_team(const Plan &pl, const smfg_control_t &c, int maxf) {
+  auto ok = [](int t) { return t == 1 || t == 2 || t == 4 || t == 8; };
+  if (ok(c.panel_team)) return c.panel_team;
+  const int tuned = pl.panel_teams[team_bucket(maxf)];
+  return ok(tuned) ? tuned : panel_team(maxf);
+}
 
 template <int C>
 static void launch_panel_c(Plan &pl, const int *lg, int nL, const PivotParams &prm, int it) {
@@ -477,9 +491,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
         for (int i = pl.lvl_large_ptr[l]; i < pl.lvl_large_ptr[l + 1] && !lvl_mixed; ++i)
           lvl_mixed = pl.h_mixed[pl.h_lvl_large[i]] != 0;
       k_large_init<<<nL, 256, 0, st>>>(d, x, lg, nL, c.posdef, lvl_mixed ? mc.nbo : 0);
-      const int team = (c.panel_team == 1 || c.panel_team == 2 || c.panel_team == 4 || c.panel_team == 8)
-                           ? c.panel_team
-                           : panel_team(pl.lvl_large_maxf[l]);
+      const int team = level_team(pl, c, pl.lvl_large_maxf[l]);
       SMFG_CUDA(cudaMemsetAsync(x.counters + kCActive, 0, sizeof(unsigned long long), st));
       const int ggrid = 2 * sms;
       int it = 0;
@@ -522,7 +534,9 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
         for (; it < steps; ++it) {
           launch_panel(pl, team, lg, nL, prm, it);
           k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, x.tpp);
-          if (lvl_mixed) enqueue_tc(pl, mc, lg, nL, x.tpp, c.posdef, lc, gp);
+          // contribution-block updates: at most 16 steps (256 pivots) apart
+          if (lvl_mixed && ((it + 1) % kTcEvery == 0 || it == steps - 1))
+            enqueue_tc(pl, mc, lg, nL, x.tpp, c.posdef, lc, gp);
         }
         k_steps_check<<<1, 32, 0, st>>>(x.counters, steps);
         lc.n += 2 * steps + 1;
@@ -538,7 +552,8 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
             gp.mark(st);
             k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, x.tpp);
             gp.mark(st);
-            if (lvl_mixed) enqueue_tc(pl, mc, lg, nL, x.tpp, c.posdef, lc, gp);
+            // contribution-block updates: at most 16 steps (256 pivots) apart
+            if (lvl_mixed && (it + 1) % kTcEvery == 0) enqueue_tc(pl, mc, lg, nL, x.tpp, c.posdef, lc, gp);
           }
           lc.n += 2 * batch;
           unsigned long long act = 0;
@@ -546,6 +561,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
           SMFG_CUDA(cudaStreamSynchronize(st));
           if (act < (unsigned long long)it) break;
         }
+        if (lvl_mixed) enqueue_tc(pl, mc, lg, nL, x.tpp, c.posdef, lc, gp);
       }
       gp.mark(st);
       k_large_schur<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, fin);
@@ -601,7 +617,8 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
         // rows grow with delays: room for a quarter more, regrown on overflow
         const int f = pl.h_fsym[s] + pl.h_fsym[s] / 4 + 64;
         const int ntr = (f + tc::kBM - 1) / tc::kBM;
-        const int nkb = (mc.nbo + c.nb + tc::kblock_elems(mc.kind) - 1) / tc::kblock_elems(mc.kind);
+        const int kmax = c.posdef ? mc.nbo + c.nb : mc.nbo + kTcEvery * c.nb;
+        const int nkb = (kmax + tc::kblock_elems(mc.kind) - 1) / tc::kblock_elems(mc.kind);
         lvl_bytes += tc::image_bytes(ntr, nkb);
       }
       tc_need = std::max(tc_need, lvl_bytes);
@@ -1052,6 +1069,17 @@ SMFG_API int smfg_solve(smfg_plan_t plan, double *b, int nrhs, int ldb, int job,
 SMFG_API int smfg_solve_device(smfg_plan_t plan, double *d_b, int nrhs, int ldb, int job,
                                smfg_info_t *info) {
   return solve_common(plan, d_b, true, nrhs, ldb, job, info);
+}
+
+SMFG_API int smfg_set_panel_teams(smfg_plan_t plan, const int *teams) {
+  if (!plan) return SMFG_ERR_INVALID_ARG;
+  Plan &pl = plan->pl;
+  for (int b = 0; b < 4; ++b) {
+    const int t = teams ? teams[b] : 0;
+    if (t != 0 && t != 1 && t != 2 && t != 4 && t != 8) return SMFG_ERR_INVALID_ARG;
+    pl.panel_teams[b] = t;
+  }
+  return SMFG_OK;
 }
 
 SMFG_API int smfg_set_front_precision(smfg_plan_t plan, const int8_t *mask) {

@@ -106,6 +106,7 @@ struct Plan {
   std::vector<int8_t> h_mixed;         // mixed fronts of the last factorization
   int mixed_count = 0;
   double refine_ms = 0.0;  // device time of the last refinement
+  int panel_teams[4] = {0, 0, 0, 0};  // tuned CTAs per size bucket of a level's largest front (0: rule)
   // CUDA graph of the factorization (smfg_control_t.graph)
   cudaGraphExec_t graph_exec = nullptr;
   std::vector<unsigned char> graph_key;

@@ -134,6 +134,8 @@ def lib():
         L.smfg_last_times.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                       C.POINTER(C.c_double)]
         L.smfg_last_times.restype = C.c_int
+        L.smfg_set_panel_teams.argtypes = [C.c_void_p, C.c_void_p]
+        L.smfg_set_panel_teams.restype = C.c_int
         L.smfg_set_front_precision.argtypes = [C.c_void_p, C.c_void_p]
         L.smfg_set_front_precision.restype = C.c_int
         L.smfg_front_stats.argtypes = [C.c_void_p, _i32p]
@@ -365,6 +367,18 @@ class Solver:
             rc = lib().smfg_set_front_precision(self._h, m.ctypes.data)
         if rc != SMFG_OK:
             raise SmfgError(rc, "smfg_set_front_precision")
+
+    def set_panel_teams(self, teams=None):
+        """smfg_set_panel_teams: CTAs per front-size bucket (4 ints, 0 = rule)."""
+        if teams is None:
+            rc = lib().smfg_set_panel_teams(self._h, None)
+        else:
+            t = np.ascontiguousarray(teams, dtype=np.int32)
+            if t.size != 4:
+                raise ValueError("four buckets")
+            rc = lib().smfg_set_panel_teams(self._h, t.ctypes.data)
+        if rc != SMFG_OK:
+            raise SmfgError(rc, "smfg_set_panel_teams")
 
     def factor(self, values, posdef: bool = False, u: float = 0.01, small: float = 1e-20,
                scale=None, precision: int = PREC_FP64, max_negative_pivots: int = -1,
