@@ -430,7 +430,7 @@ def run_stream(args, rank, world, local):
                         mask = sel.mask(a, X) if sel is not None else S.candidates(a).astype(np.int8)
                     info, mask, nbad = S.factor_checked(sv, a, d_vals, posdef, mask, prev, expected, scale,
                                                         graph=True)
-                    f_ms = info.reserved_d[6]
+                    f_ms = info.total_ms
                 if arm == "mixed":
                     prev = sv.front_stats()
                 d_x.copy_(d_b0)

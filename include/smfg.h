@@ -143,11 +143,14 @@ typedef struct {
   int levels;
   int kernel_launches;    /* kernels launched by the last call */
   int mixed_fronts;       /* fronts whose trailing updates ran on the tensor cores */
-  int reserved_i[7];      /* [0] profiled FP64 update launches, [1] tensor-core update passes */
-  double reserved_d[8];   /* [0] profiled FP64 update ms, [1] FP64 update flops, [2] arena bytes,
-                             [3] tensor-core update flops (2 per multiply-add), [4] profiled
-                             tensor-core update ms (split + product kernels), [5] profiled
-                             large-front pivoting panel ms */
+  int reserved_i[7];      /* [0] profiled FP64 update launches, [1] tensor-core update passes,
+                             [2] deferred front updates, [3] those of at most 2 pivots */
+  double reserved_d[8];   /* [0] profiled FP64 update ms (deferred + Schur), [1] FP64 update
+                             flops, [2] arena bytes, [3] tensor-core update flops (2 per
+                             multiply-add), [4] profiled tensor-core update ms (split + product
+                             kernels), [5] profiled large-front pivoting panel ms, [6] deferred
+                             update bytes (each element read and written once), [7] profiled
+                             Schur update ms (part of [0]) */
 } smfg_info_t;
 
 typedef struct smfg_plan_s *smfg_plan_t;

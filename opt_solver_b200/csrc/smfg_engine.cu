@@ -327,7 +327,8 @@ struct LaunchCount {
 struct GemmProfile {
   bool on = false;
   std::vector<cudaEvent_t> ev;
-  std::vector<int> cls;  // class of each mark: 0 FP64 updates, 1 tensor-core updates
+  std::vector<int> cls;  // class of each mark: 0 FP64 deferred updates, 1 tensor-core updates,
+                         // 2 pivoting panels, 3 FP64 Schur updates
   size_t used = 0;
   void mark(cudaStream_t st, int c = 0) {
     if (!on) return;
@@ -378,6 +379,15 @@ static MixedCfg mixed_cfg(const smfg_control_t &c) {
 
 // Pivoting steps between two tensor-core passes of indefinite mixed fronts.
 constexpr int kTcEvery = 16;
+
+// Deferred updates of a level's large fronts: the streamed kernel for
+// panels of up to 16 pivots, the general tiled one beyond.
+static void launch_defer(Plan &pl, const int *lg, int nL, const TppState *states, int ggrid) {
+  if (pl.nb <= kDK)
+    k_large_defer<<<kDBlocksPerSM * sm_count(pl.device), 256, 0, pl.stream>>>(pl.d, pl.x, lg, nL, states);
+  else
+    k_large_gemm<<<ggrid, 256, sizeof(TileSmem), pl.stream>>>(pl.d, pl.x, lg, nL, states);
+}
 
 // Team size (CTAs per front) of a level's indefinite large-front panels, by
 // the largest symbolic front: the swaps and eliminations of a panel stream
@@ -508,7 +518,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
           k_large_panel_spd<16><<<pgrid, 256, 0, st>>>(d, x, lg, cur, nxt, it);
           gp.mark(st, 2);
           gp.mark(st);
-          k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, nxt);
+          launch_defer(pl, lg, nL, nxt, ggrid);
           gp.mark(st);
           if (lvl_mixed && ((it + 1) * c.nb % mc.nbo == 0 || it == steps - 1))
             enqueue_tc(pl, mc, lg, nL, nxt, c.posdef, lc, gp);
@@ -522,7 +532,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
           launch_panel(pl, team, lg, nL, prm, it);
           gp.mark(st, 2);
           gp.mark(st);
-          k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, x.tpp);
+          launch_defer(pl, lg, nL, x.tpp, ggrid);
           gp.mark(st);
           if (lvl_mixed) enqueue_tc(pl, mc, lg, nL, x.tpp, c.posdef, lc, gp);
         }
@@ -533,7 +543,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
         const int steps = 2 * ((pl.lvl_large_maxw[l] + c.nb - 1) / c.nb) + 16;
         for (; it < steps; ++it) {
           launch_panel(pl, team, lg, nL, prm, it);
-          k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, x.tpp);
+          launch_defer(pl, lg, nL, x.tpp, ggrid);
           // contribution-block updates: at most 16 steps (256 pivots) apart
           if (lvl_mixed && ((it + 1) % kTcEvery == 0 || it == steps - 1))
             enqueue_tc(pl, mc, lg, nL, x.tpp, c.posdef, lc, gp);
@@ -550,7 +560,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
             launch_panel(pl, team, lg, nL, prm, it);
             gp.mark(st, 2);
             gp.mark(st);
-            k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, x.tpp);
+            launch_defer(pl, lg, nL, x.tpp, ggrid);
             gp.mark(st);
             // contribution-block updates: at most 16 steps (256 pivots) apart
             if (lvl_mixed && (it + 1) % kTcEvery == 0) enqueue_tc(pl, mc, lg, nL, x.tpp, c.posdef, lc, gp);
@@ -563,9 +573,9 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
         }
         if (lvl_mixed) enqueue_tc(pl, mc, lg, nL, x.tpp, c.posdef, lc, gp);
       }
-      gp.mark(st);
+      gp.mark(st, 3);
       k_large_schur<<<ggrid, 256, sizeof(TileSmem), st>>>(d, x, lg, nL, fin);
-      gp.mark(st);
+      gp.mark(st, 3);
       k_large_finish<512><<<nL, 512, 0, st>>>(d, x, lg, fin, prm);
       k_large_store<<<ggrid, 256, 0, st>>>(d, x, lg, nL, c.posdef);
       lc.n += 4;
@@ -755,7 +765,13 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
   // profile (ctrl.profile): large-front GEMM device time, launches,
   // algorithmic flops; arena bytes in use
   int fp64_pairs = 0, tc_pairs = 0;
-  inf.reserved_d[0] = gp.on ? gp.total_ms(0, &fp64_pairs) : 0.0;
+  int schur_pairs = 0;
+  inf.reserved_d[0] = gp.on ? gp.total_ms(0, &fp64_pairs) + gp.total_ms(3, &schur_pairs) : 0.0;
+  inf.reserved_d[7] = gp.on ? gp.total_ms(3) : 0.0;
+  fp64_pairs += schur_pairs;
+  std::memcpy(&inf.reserved_d[6], &h_cnt[kCDeferBytes], sizeof(double));
+  inf.reserved_i[2] = (int)h_cnt[kCDeferUpd];
+  inf.reserved_i[3] = (int)h_cnt[kCDeferSmall];
   inf.reserved_d[4] = gp.on ? gp.total_ms(1, &tc_pairs) : 0.0;
   inf.reserved_d[5] = gp.on ? gp.total_ms(2) : 0.0;
   inf.reserved_i[1] = tc_pairs;

@@ -196,11 +196,12 @@ struct FrontRef {
   int8_t *tags;
   double *W;
   int *loc;  // assembly position of the row now at each position (null: untracked)
-  // teams of several CTAs: the team's barrier words {count, generation},
-  // the error word a timed-out barrier sets, this CTA's abort flag
-  unsigned *team_bar = nullptr;
+  // teams of several CTAs: the team's barrier counter, the error word a
+  // timed-out barrier sets, this CTA's abort flag
+  unsigned *team_bar = nullptr;  // this launch's arrival counter (monotone within the launch)
   unsigned long long *err = nullptr;
   int *abort = nullptr;
+  unsigned *bar_seq = nullptr;    // this CTA's barriers so far in the launch (shared memory)
   double *team_red = nullptr;  // the team's reduction scratch: 2 buffers x C ranks x 4
 };
 
@@ -222,12 +223,16 @@ __device__ __forceinline__ int team_rank() {
   }
 }
 
-// Team barrier (C > 1): a sense-reversing barrier on two words in global
-// memory, the spin bounded by the global timer (2 s): a team whose CTAs
-// did not all arrive sets bit 128 of *err, and the CTA stops waiting at its
-// later barriers (its remaining work is then discarded by the host, which
-// reports the timeout). The team's CTAs are co-scheduled (one cluster), so
-// the wait only runs out if they took different paths.
+// Team barrier (C > 1): an arrival counter in global memory that only grows
+// during a launch (the launch's own slot, reset by the previous launch): the
+// i-th barrier adds 1 (acquire-release: the last arrival reads the others'
+// writes through it) and waits, with acquire loads, until the counter
+// reaches C (i + 1). The spin is bounded by the
+// global timer (2 s): a team whose CTAs did not all arrive sets bit 128 of
+// *err, and the CTA stops waiting at its later barriers (the host then
+// discards the factorization and reports the timeout). The team's CTAs are
+// co-scheduled (one cluster), so the wait only runs out if they took
+// different paths.
 template <int C>
 __device__ __forceinline__ void team_sync(const FrontRef &v) {
   if constexpr (C == 1) {
@@ -235,18 +240,17 @@ __device__ __forceinline__ void team_sync(const FrontRef &v) {
   } else {
     __syncthreads();
     if (threadIdx.x == 0 && !*v.abort) {
-      volatile unsigned *gen_p = v.team_bar + 1;
-      __threadfence();
-      const unsigned gen = *gen_p;
-      const unsigned arrived = atomicAdd(v.team_bar, 1u) + 1u;
-      if (arrived == (unsigned)C) {
-        atomicExch(v.team_bar, 0u);
-        __threadfence();
-        atomicAdd(v.team_bar + 1, 1u);
-      } else {
+      const unsigned target = (unsigned)C * (*v.bar_seq + 1u);
+      *v.bar_seq += 1u;
+      unsigned seen;
+      asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], 1;" : "=r"(seen) : "l"(v.team_bar) : "memory");
+      seen += 1u;
+      if (seen < target) {
         unsigned long long t0;
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-        while (*gen_p == gen) {
+        while (true) {
+          asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(seen) : "l"(v.team_bar) : "memory");
+          if (seen >= target) break;
           unsigned long long t;
           asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
           if (t - t0 > 2000000000ull) {
@@ -256,7 +260,6 @@ __device__ __forceinline__ void team_sync(const FrontRef &v) {
           }
         }
       }
-      __threadfence();
     }
     __syncthreads();
   }
@@ -383,10 +386,14 @@ struct Lay {
 
 
 template <int NT, int C = 1>
-__device__ void eliminate_1x1_blk(const FrontRef &v, int k, int ucol_end, bool useW, int w_col) {
+__device__ void eliminate_1x1_blk(const FrontRef &v, int k, int ucol_end, bool useW, int w_col,
+                                  bool synced = false) {
   using LY = Lay<NT>;
   const int rk = team_rank<C>();
-  if constexpr (C > 1) team_sync<C>(v);
+  // (a swap that just ended with a team barrier needs no second one)
+  if constexpr (C > 1) {
+    if (!synced) team_sync<C>(v);
+  }
   const size_t sf = (size_t)v.ld;
   const int f = v.f;
   double *ck = v.F + k * sf;
@@ -414,10 +421,14 @@ __device__ void eliminate_1x1_blk(const FrontRef &v, int k, int ucol_end, bool u
 }
 
 template <int NT, int C = 1>
-__device__ void eliminate_2x2_blk(const FrontRef &v, int k, int ucol_end, bool useW, int w_col) {
+__device__ void eliminate_2x2_blk(const FrontRef &v, int k, int ucol_end, bool useW, int w_col,
+                                  bool synced = false) {
   using LY = Lay<NT>;
   const int rk = team_rank<C>();
-  if constexpr (C > 1) team_sync<C>(v);
+  // (a swap that just ended with a team barrier needs no second one)
+  if constexpr (C > 1) {
+    if (!synced) team_sync<C>(v);
+  }
   const size_t sf = (size_t)v.ld;
   const int f = v.f;
   double *c0 = v.F + k * sf;
@@ -846,6 +857,7 @@ __device__ void apply_pivot_blk(const FrontRef &v, int &k, bool useW, int w_cols
   const int f = v.f;
   const int kind = sh.kind, pa = sh.a, pb = sh.b;
   if (kind == 1) {
+    const bool swapped = pa != k;
     sym_swap_blk<NT, C>(v, k, pa, useW ? w_cols : 0);
     if (threadIdx.x == 0) {
       inertia_1x1(v.F[k * sf + k], prm.eff_small, sh.st);
@@ -853,16 +865,21 @@ __device__ void apply_pivot_blk(const FrontRef &v, int &k, bool useW, int w_cols
       const double rem = (double)(f - (k + 1));
       sh.st.flops += rem + rem * (rem + 1.0);
     }
-    eliminate_1x1_blk<NT, C>(v, k, ucol_end, useW, w_cols);
+    eliminate_1x1_blk<NT, C>(v, k, ucol_end, useW, w_cols, swapped);
     k += 1;
     return;
   }
   int partner = pb;
+  bool swapped = false;
   if (pa != k) {
     sym_swap_blk<NT, C>(v, k, pa, useW ? w_cols : 0);
     if (partner == k) partner = pa;
+    swapped = true;
   }
-  if (partner != k + 1) sym_swap_blk<NT, C>(v, k + 1, partner, useW ? w_cols : 0);
+  if (partner != k + 1) {
+    sym_swap_blk<NT, C>(v, k + 1, partner, useW ? w_cols : 0);
+    swapped = true;
+  }
   if (threadIdx.x == 0) {
     inertia_2x2(v.F[k * sf + k], v.F[k * sf + k + 1], v.F[(k + 1) * sf + k + 1], prm.small_pivot,
                 sh.st);
@@ -872,7 +889,7 @@ __device__ void apply_pivot_blk(const FrontRef &v, int &k, bool useW, int w_cols
     sh.st.flops += 6.0 * rem + 2.0 * rem * (rem + 1.0);
     ++sh.st.two_by_two;
   }
-  eliminate_2x2_blk<NT, C>(v, k, ucol_end, useW, w_cols);
+  eliminate_2x2_blk<NT, C>(v, k, ucol_end, useW, w_cols, swapped);
   k += 2;
 }
 

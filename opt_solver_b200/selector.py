@@ -235,8 +235,8 @@ def factor_checked(sv, a, values, posdef, mask, stats_plain, expected_inertia=No
     last plain factorization's per-front counts: fronts whose own or
     parent's counts changed (or all mixed fronts, when the inertia is not
     the expected one) are set to FP64 and the matrix is refactored.
-    Returns (info, mask used last, misjudged fronts); info.reserved_d[6]
-    holds the device time of all factorizations of the call."""
+    Returns (info, mask used last, misjudged fronts); info.total_ms holds
+    the device time of all factorizations of the call."""
     parent = np.asarray(a.sn_parent)
     sv.set_front_precision(mask)
     info = sv.factor(values, posdef=posdef, precision=smfg.PREC_MIXED, scale=scale, **kw)
@@ -257,7 +257,7 @@ def factor_checked(sv, a, values, posdef, mask, stats_plain, expected_inertia=No
         sv.set_front_precision(mask)
         info = sv.factor(values, posdef=posdef, precision=smfg.PREC_MIXED, scale=scale, **kw)
         total_ms += info.factor_ms
-    info.reserved_d[6] = total_ms
+    info.total_ms = total_ms
     return info, mask, nbad
 
 

@@ -444,6 +444,8 @@ class Solver:
                 "gemm_launches": info.reserved_i[0], "arena_bytes": info.reserved_d[2],
                 "tc_ms": info.reserved_d[4], "tc_flops": info.reserved_d[3],
                 "tc_passes": info.reserved_i[1], "panel_ms": info.reserved_d[5],
+                "schur_ms": info.reserved_d[7], "defer_bytes": info.reserved_d[6],
+                "defer_updates": info.reserved_i[2], "defer_small": info.reserved_i[3],
                 "factor_ms": info.factor_ms}
 
     # -- solve -------------------------------------------------------------
