@@ -40,9 +40,10 @@ struct FrontShared {
   double red[32];
   int redi[32];
   double red2[32];
+  double red3[32], red4[32];
   int kind, a, b;        // pivot choice
   int k;                 // next pivot position
-  int order[128];        // stall partner pairs (row ids)
+  int order[128];        // stall partner pairs (row ids, or assembly positions)
   int np;
   double vals[8];
   int ivals[8];
@@ -138,6 +139,52 @@ struct Block {
     }
   }
 
+  // A Top2 and two maxima in one pass (one shared-memory round).
+  static __device__ void bundle(Top2 &t, double &a, double &b, FrontShared &sh) {
+    for (int o = 16; o > 0; o >>= 1) {
+      Top2 u;
+      u.m1 = __shfl_xor_sync(0xffffffffu, t.m1, o);
+      u.m2 = __shfl_xor_sync(0xffffffffu, t.m2, o);
+      u.r = __shfl_xor_sync(0xffffffffu, t.r, o);
+      t = top2_merge(t, u);
+      a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+      b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+    }
+    if (NW == 1) return;
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) {
+      sh.red[w] = t.m1;
+      sh.red2[w] = t.m2;
+      sh.redi[w] = t.r;
+      sh.red3[w] = a;
+      sh.red4[w] = b;
+    }
+    __syncthreads();
+    if (l < NW) {
+      t.m1 = sh.red[l];
+      t.m2 = sh.red2[l];
+      t.r = sh.redi[l];
+      a = sh.red3[l];
+      b = sh.red4[l];
+    } else {
+      t.m1 = 0.0;
+      t.m2 = 0.0;
+      t.r = -1;
+      a = 0.0;
+      b = 0.0;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      Top2 u;
+      u.m1 = __shfl_xor_sync(0xffffffffu, t.m1, o);
+      u.m2 = __shfl_xor_sync(0xffffffffu, t.m2, o);
+      u.r = __shfl_xor_sync(0xffffffffu, t.r, o);
+      t = top2_merge(t, u);
+      a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+      b = fmax(b, __shfl_xor_sync(0xffffffffu, b, o));
+    }
+  }
+
   static __device__ Top2 top2(Top2 t, FrontShared &sh) {
     for (int o = 16; o > 0; o >>= 1) {
       Top2 u;
@@ -189,6 +236,15 @@ struct Block {
 // The front: F f x f column-major with leading dimension ld (lower triangle
 // used), its row ids, pivot tags, and W (f x nb, leading dimension f) for the
 // blocked path's unscaled pivot columns.
+// The pairing swaps' targets and their play-through on the position maps
+// (moved rows -> positions, moved positions -> rows; the latest entry wins).
+constexpr int kPairMax = 64;
+struct PairScratch {
+  int qq[kPairMax];
+  int row_key[2 * kPairMax], row_pos[2 * kPairMax];
+  int pos_key[2 * kPairMax], pos_row[2 * kPairMax];
+};
+
 struct FrontRef {
   double *F;
   int ld, f, ne;
@@ -196,6 +252,8 @@ struct FrontRef {
   int8_t *tags;
   double *W;
   int *loc;  // assembly position of the row now at each position (null: untracked)
+  int *inv = nullptr;  // position of each assembly position (kept with loc; null: untracked)
+  PairScratch *pair = nullptr;  // shared-memory scratch of the tracked pairing swaps
   // teams of several CTAs: the team's barrier counter, the error word a
   // timed-out barrier sets, this CTA's abort flag
   unsigned *team_bar = nullptr;  // this launch's arrival counter (monotone within the launch)
@@ -210,8 +268,7 @@ struct FrontRef {
 // from the same data (its own block reductions, so the decisions are the
 // one-CTA decisions bit for bit), and the memory-heavy updates (row and
 // column swaps, eliminations of the panel) are split by rows over the team,
-// each followed by a team barrier (the cluster's hardware barrier, release
-// / acquire at cluster scope).
+// each followed by a team barrier (team_sync below).
 template <int C>
 __device__ __forceinline__ int team_rank() {
   if constexpr (C == 1) {
@@ -269,16 +326,20 @@ __device__ __forceinline__ double fat(const FrontRef &v, int i, int j) {  // ele
   return v.F[(size_t)j * v.ld + i];
 }
 
+// Returns whether it swapped (and so ended with a team barrier).
 template <int NT, int C = 1>
-__device__ void sym_swap_blk(const FrontRef &v, int p, int q, int w_cols) {
-  if (p == q) return;
+__device__ bool sym_swap_blk(const FrontRef &v, int p, int q, int w_cols, bool synced = false) {
+  if (p == q) return false;
   if (p > q) {
     const int t = p;
     p = q;
     q = t;
   }
-  // no CTA of the team writes while another still reads (C > 1)
-  if constexpr (C > 1) team_sync<C>(v);
+  // no CTA of the team writes while another still reads (C > 1); a swap
+  // that follows a team barrier (the previous swap's) needs no other
+  if constexpr (C > 1) {
+    if (!synced) team_sync<C>(v);
+  }
   const size_t sf = (size_t)v.ld;
   double *F = v.F;
   const int f = v.f;
@@ -313,6 +374,10 @@ __device__ void sym_swap_blk(const FrontRef &v, int p, int q, int w_cols) {
         const int a = v.loc[p];
         v.loc[p] = v.loc[q];
         v.loc[q] = a;
+        if (v.inv) {
+          v.inv[v.loc[p]] = p;
+          v.inv[a] = q;
+        }
       }
     } else {
       const int c = t - (n1 + n2 + n3 + 2);
@@ -323,6 +388,7 @@ __device__ void sym_swap_blk(const FrontRef &v, int p, int q, int w_cols) {
     }
   }
   team_sync<C>(v);
+  return true;
 }
 
 __device__ __forceinline__ void inertia_1x1(double d, double small, FrontStats &st) {
@@ -385,6 +451,11 @@ struct Lay {
 };
 
 
+// Panels of up to this many columns right of the pivot take the
+// row-at-a-time elimination path.
+constexpr int kElimCols = 16;
+constexpr int kElimGroup = 8;  // loads in flight per thread
+
 template <int NT, int C = 1>
 __device__ void eliminate_1x1_blk(const FrontRef &v, int k, int ucol_end, bool useW, int w_col,
                                   bool synced = false) {
@@ -402,15 +473,39 @@ __device__ void eliminate_1x1_blk(const FrontRef &v, int k, int ucol_end, bool u
     double *w = v.W + (size_t)w_col * f;
     for (int i = k + 1 + rk * NT + (int)threadIdx.x; i < f; i += C * NT) w[i] = ck[i];
   }
-  // column j of (k, ucol_end), row i >= j: F(i, j) -= F(i, k) * l_j
-  for (int i = k + 1 + rk * LY::RB + LY::r(); i < f; i += C * LY::RB) {
-    const double cki = ck[i];
-    const int jend = min(ucol_end, i + 1);
-    for (int j = k + 1 + LY::g(); j < jend; j += LY::G) {
-      const double lj = __dmul_rn(ck[j], inv_d);
-      if (lj == 0.0) continue;
-      double *cj = v.F + (size_t)j * sf;
-      cj[i] = __dsub_rn(cj[i], __dmul_rn(cki, lj));
+  const int nj = ucol_end - (k + 1);
+  if (nj <= kElimCols) {
+    // a panel: the multipliers once in shared memory, then each thread
+    // one row of every column at a time (all loads of the row in flight)
+    __shared__ double s_l[kElimCols];
+    for (int jj = threadIdx.x; jj < nj; jj += NT) s_l[jj] = __dmul_rn(ck[k + 1 + jj], inv_d);
+    __syncthreads();
+    for (int i = k + 1 + rk * NT + (int)threadIdx.x; i < f; i += C * NT) {
+      const double cki = ck[i];
+      const int jn = min(nj, i - k);  // columns j = k + 1 + jj <= i
+      double *row = v.F + (size_t)(k + 1) * sf + i;
+      for (int j0 = 0; j0 < jn; j0 += kElimGroup) {
+        double x[kElimGroup];
+#pragma unroll
+        for (int u = 0; u < kElimGroup; ++u) x[u] = (j0 + u < jn) ? row[(size_t)(j0 + u) * sf] : 0.0;
+#pragma unroll
+        for (int u = 0; u < kElimGroup; ++u) {
+          const double lj = s_l[j0 + u];
+          if (j0 + u < jn && lj != 0.0) row[(size_t)(j0 + u) * sf] = __dsub_rn(x[u], __dmul_rn(cki, lj));
+        }
+      }
+    }
+  } else {
+    // column j of (k, ucol_end), row i >= j: F(i, j) -= F(i, k) * l_j
+    for (int i = k + 1 + rk * LY::RB + LY::r(); i < f; i += C * LY::RB) {
+      const double cki = ck[i];
+      const int jend = min(ucol_end, i + 1);
+      for (int j = k + 1 + LY::g(); j < jend; j += LY::G) {
+        const double lj = __dmul_rn(ck[j], inv_d);
+        if (lj == 0.0) continue;
+        double *cj = v.F + (size_t)j * sf;
+        cj[i] = __dsub_rn(cj[i], __dmul_rn(cki, lj));
+      }
     }
   }
   team_sync<C>(v);
@@ -443,16 +538,44 @@ __device__ void eliminate_2x2_blk(const FrontRef &v, int k, int ucol_end, bool u
       w1[i] = c1[i];
     }
   }
-  for (int i = k + 2 + rk * LY::RB + LY::r(); i < f; i += C * LY::RB) {
-    const double c0i = c0[i], c1i = c1[i];
-    const int jend = min(ucol_end, i + 1);
-    for (int j = k + 2 + LY::g(); j < jend; j += LY::G) {
-      const double a0 = c0[j], a1 = c1[j];
-      const double l0 = __dadd_rn(__dmul_rn(i00, a0), __dmul_rn(i10, a1));
-      const double l1 = __dadd_rn(__dmul_rn(i10, a0), __dmul_rn(i11, a1));
-      if (l0 == 0.0 && l1 == 0.0) continue;
-      double *d0 = v.F + (size_t)j * sf;
-      d0[i] = __dsub_rn(d0[i], __dadd_rn(__dmul_rn(c0i, l0), __dmul_rn(c1i, l1)));
+  const int nj = ucol_end - (k + 2);
+  if (nj <= kElimCols) {
+    // as eliminate_1x1_blk: multipliers in shared memory, rows in flight
+    __shared__ double s_l0[kElimCols], s_l1[kElimCols];
+    for (int jj = threadIdx.x; jj < nj; jj += NT) {
+      const double a0 = c0[k + 2 + jj], a1 = c1[k + 2 + jj];
+      s_l0[jj] = __dadd_rn(__dmul_rn(i00, a0), __dmul_rn(i10, a1));
+      s_l1[jj] = __dadd_rn(__dmul_rn(i10, a0), __dmul_rn(i11, a1));
+    }
+    __syncthreads();
+    for (int i = k + 2 + rk * NT + (int)threadIdx.x; i < f; i += C * NT) {
+      const double c0i = c0[i], c1i = c1[i];
+      const int jn = min(nj, i - k - 1);  // columns j = k + 2 + jj <= i
+      double *row = v.F + (size_t)(k + 2) * sf + i;
+      for (int j0 = 0; j0 < jn; j0 += kElimGroup) {
+        double x[kElimGroup];
+#pragma unroll
+        for (int u = 0; u < kElimGroup; ++u) x[u] = (j0 + u < jn) ? row[(size_t)(j0 + u) * sf] : 0.0;
+#pragma unroll
+        for (int u = 0; u < kElimGroup; ++u) {
+          const double l0 = s_l0[j0 + u], l1 = s_l1[j0 + u];
+          if (j0 + u < jn && !(l0 == 0.0 && l1 == 0.0))
+            row[(size_t)(j0 + u) * sf] = __dsub_rn(x[u], __dadd_rn(__dmul_rn(c0i, l0), __dmul_rn(c1i, l1)));
+        }
+      }
+    }
+  } else {
+    for (int i = k + 2 + rk * LY::RB + LY::r(); i < f; i += C * LY::RB) {
+      const double c0i = c0[i], c1i = c1[i];
+      const int jend = min(ucol_end, i + 1);
+      for (int j = k + 2 + LY::g(); j < jend; j += LY::G) {
+        const double a0 = c0[j], a1 = c1[j];
+        const double l0 = __dadd_rn(__dmul_rn(i00, a0), __dmul_rn(i10, a1));
+        const double l1 = __dadd_rn(__dmul_rn(i10, a0), __dmul_rn(i11, a1));
+        if (l0 == 0.0 && l1 == 0.0) continue;
+        double *d0 = v.F + (size_t)j * sf;
+        d0[i] = __dsub_rn(d0[i], __dadd_rn(__dmul_rn(c0i, l0), __dmul_rn(c1i, l1)));
+      }
     }
   }
   team_sync<C>(v);
@@ -503,19 +626,38 @@ __device__ __forceinline__ Top2 warp_top2(Top2 t) {
   return t;
 }
 
-// fn(|col[i]|, i) for i = start, start + S, ... < end, eight loads in
-// flight per thread (the scans are latency-bound otherwise).
-template <class Fn>
-__device__ __forceinline__ void scan8(const double *__restrict__ col, int start, int end, int S, Fn fn) {
-  int i = start;
-  for (; i + 7 * S < end; i += 8 * S) {
-    double x[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) x[u] = fabs(col[i + u * S]);
-#pragma unroll
-    for (int u = 0; u < 8; ++u) fn(x[u], i + u * S);
+// |col[i]| for i in [lo, hi), thread tid of nth: 16-byte loads of aligned
+// pairs, eight pairs in flight; each thread visits its indexes in increasing
+// order (the head element before its pairs, the tail after), so fn sees a
+// thread's share in scan order.
+template <typename Fn>
+__device__ __forceinline__ void scanv(const double *__restrict__ col, int lo, int hi, int tid, int nth, Fn fn) {
+  if (lo >= hi) return;
+  int a = lo;
+  if (reinterpret_cast<uintptr_t>(col + a) & 15) {
+    if (tid == 0) fn(fabs(col[a]), a);
+    ++a;
   }
-  for (; i < end; i += S) fn(fabs(col[i]), i);
+  const int npair = (hi - a) >> 1;
+  const double2 *p2 = reinterpret_cast<const double2 *>(col + a);
+  int m = tid;
+  for (; m + 7 * nth < npair; m += 8 * nth) {
+    double2 x[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) x[u] = p2[m + u * nth];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int i = a + 2 * (m + u * nth);
+      fn(fabs(x[u].x), i);
+      fn(fabs(x[u].y), i + 1);
+    }
+  }
+  for (; m < npair; m += nth) {
+    const double2 x = p2[m];
+    fn(fabs(x.x), a + 2 * m);
+    fn(fabs(x.y), a + 2 * m + 1);
+  }
+  if (((hi - a) & 1) && tid == npair % nth) fn(fabs(col[hi - 1]), hi - 1);
 }
 
 // Team-wide reduction of a bundle (a Top2 and two maxima): the block's
@@ -526,8 +668,7 @@ __device__ __forceinline__ void scan8(const double *__restrict__ col, int start,
 // the barrier of the next reduction, which every CTA reaches after reading.
 template <int NT, int C>
 __device__ void team_bundle(const FrontRef &v, FrontShared &sh, Top2 &t, double &x1, double &x2) {
-  t = Block<NT>::top2(t, sh);
-  Block<NT>::max2(x1, x2, sh);
+  Block<NT>::bundle(t, x1, x2, sh);
   if constexpr (C > 1) {
     const int buf = sh.tr_seq & 1;
     double *slot = v.team_red + (size_t)buf * C * 6;  // per rank: Top2 (4), maxima (2)
@@ -573,10 +714,12 @@ __device__ int cand_eval_team(const FrontRef &v, int k, int limit, int cand, con
   const double a_cand = fabs(col[cand]);
   Top2 t{0.0, 0.0, -1};
   for (int i = k + tid; i < cand; i += NTT) top2_add(t, fabs(F[(size_t)i * sf + cand]), i);
-  scan8(col, cand + 1 + tid, ne, NTT, [&](double x, int i) { top2_add(t, x, i); });
-  const int ext0 = ne > cand + 1 ? ne : cand + 1;
+  // rows (cand, ne) into the top two, rows [max(ne, cand + 1), f) into ext
   double ext = 0.0, unused = 0.0;
-  scan8(col, ext0 + tid, f, NTT, [&](double x, int) { ext = fmax(ext, x); });
+  scanv(col, cand + 1, f, tid, NTT, [&](double x, int i) {
+    if (i < ne) top2_add(t, x, i);
+    else ext = fmax(ext, x);
+  });
   team_bundle<NT, C>(v, sh, t, ext, unused);
   const double m1 = t.m1, m2 = t.m2;
   const int r_best = t.r;
@@ -608,7 +751,7 @@ __device__ int cand_eval_team(const FrontRef &v, int k, int limit, int cand, con
     om2 = fmax(om2, x);
     if (i != cand) off1 = fmax(off1, x);
   }
-  scan8(col_r, r_best + 1 + tid, f, NTT, [&](double x, int i) {
+  scanv(col_r, r_best + 1, f, tid, NTT, [&](double x, int i) {
     om2 = fmax(om2, x);
     if (i != cand) off1 = fmax(off1, x);
   });
@@ -749,10 +892,10 @@ __device__ void select_pivot_blk(const FrontRef &v, int k, int limit, const Pivo
     if (a0 >= prm.eff_small) {
       double cm = 0.0;
       if constexpr (C == 1) {
-        scan8(col0, k + 1 + (int)threadIdx.x, f, NT, [&](double x, int) { cm = fmax(cm, x); });
+        scanv(col0, k + 1, f, (int)threadIdx.x, NT, [&](double x, int) { cm = fmax(cm, x); });
         cm = Block<NT>::max(cm, sh);
       } else {
-        scan8(col0, k + 1 + team_rank<C>() * NT + (int)threadIdx.x, f, C * NT,
+        scanv(col0, k + 1, f, team_rank<C>() * NT + (int)threadIdx.x, C * NT,
               [&](double x, int) { cm = fmax(cm, x); });
         Top2 none{0.0, 0.0, -1};
         double unused = 0.0;
@@ -877,7 +1020,7 @@ __device__ void apply_pivot_blk(const FrontRef &v, int &k, bool useW, int w_cols
     swapped = true;
   }
   if (partner != k + 1) {
-    sym_swap_blk<NT, C>(v, k + 1, partner, useW ? w_cols : 0);
+    sym_swap_blk<NT, C>(v, k + 1, partner, useW ? w_cols : 0, swapped);
     swapped = true;
   }
   if (threadIdx.x == 0) {
@@ -1005,6 +1148,42 @@ __device__ __forceinline__ bool tpp_request_flush(TppState &S) {
   return true;
 }
 
+// The targets of the pairing swaps (ldlt_kernel.cpp:1047-1095: the row
+// order[t] goes to position k + t from the first position >= k + t that
+// holds it, else from f - 1) when the front tracks positions (v.inv): the
+// swaps are played on the maps, their moves kept in v.pair's override lists.
+// One thread; np <= kPairMax.
+__device__ __forceinline__ void pairing_targets(const FrontRef &v, int k, int f, int np, const FrontShared &sh) {
+  PairScratch &ps = *v.pair;
+  int nr = 0, npos = 0;
+  auto pos_of = [&](int id) {
+    for (int m = nr - 1; m >= 0; --m)
+      if (ps.row_key[m] == id) return ps.row_pos[m];
+    return v.inv[id];
+  };
+  auto id_at = [&](int pos) {
+    for (int m = npos - 1; m >= 0; --m)
+      if (ps.pos_key[m] == pos) return ps.pos_row[m];
+    return v.loc[pos];
+  };
+  for (int t = 0; t < np; ++t) {
+    const int at = pos_of(sh.order[t]);
+    const int qq = (at >= k + t && at < f - 1) ? at : f - 1;
+    ps.qq[t] = qq;
+    if (qq != k + t) {
+      const int idp = id_at(k + t), idq = id_at(qq);
+      ps.row_key[nr] = idp;
+      ps.row_pos[nr++] = qq;
+      ps.row_key[nr] = idq;
+      ps.row_pos[nr++] = k + t;
+      ps.pos_key[npos] = k + t;
+      ps.pos_row[npos++] = idq;
+      ps.pos_key[npos] = qq;
+      ps.pos_row[npos++] = idp;
+    }
+  }
+}
+
 // Runs the blocked algorithm up to its next deferred update, which it leaves
 // in S.g_* (returns true), or to its end (returns false: the Schur update of
 // the pivots [0, S.k) remains). The caller applies F[c0:f, c0:e] -=
@@ -1024,6 +1203,10 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
         if (threadIdx.x == 0) sh.np = 0;
         __syncthreads();
         const int max_pairs = min(prm.nb / 2, 64);
+        // rows named by assembly position (one to one with the row ids)
+        // where the front tracks positions: the swap targets then come from
+        // the position maps, not from a search
+        const bool tracked = v.inv && v.pair && max_pairs <= kPairMax / 2;
         // the scans of the panel's columns are independent of the pairing
         // decisions: warps scan positions in parallel, thread 0 then takes
         // the decisions in position order
@@ -1053,11 +1236,12 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
               if (sh.np / 2 >= max_pairs) break;
               const int r = sh.pr[pos - p0];
               if (r >= 0 && sh.pout[pos - p0] > sh.pin[pos - p0]) {
+                const int id_r = tracked ? v.loc[r] : v.rows[r];
                 bool taken = false;
-                for (int t = 1; t < sh.np; t += 2) taken = taken || sh.order[t] == v.rows[r];
+                for (int t = 1; t < sh.np; t += 2) taken = taken || sh.order[t] == id_r;
                 if (!taken) {
-                  sh.order[sh.np++] = v.rows[pos];
-                  sh.order[sh.np++] = v.rows[r];
+                  sh.order[sh.np++] = tracked ? v.loc[pos] : v.rows[pos];
+                  sh.order[sh.np++] = id_r;
                 }
               }
             }
@@ -1066,18 +1250,28 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
         }
         const int np = sh.np;
         if (np > 0) {
-          for (int t = 0; t < np; ++t) {
-            // the position of row id order[t] from k + t on (the first
-            // match, else f - 1), searched by the whole block
-            if (threadIdx.x == 0) sh.ivals[0] = f - 1;
+          if (tracked) {
+            // positions tracked: thread 0 plays the swaps on the position
+            // maps first (the maps as they stand, plus the moves so far),
+            // so the swaps then run back to back
+            if (threadIdx.x == 0) pairing_targets(v, k, f, np, sh);
             __syncthreads();
-            const int want = sh.order[t];
-            for (int i = k + t + threadIdx.x; i < f - 1; i += NT)
-              if (v.rows[i] == want) atomicMin(&sh.ivals[0], i);
-            __syncthreads();
-            const int qq = sh.ivals[0];
-            __syncthreads();
-            sym_swap_blk<NT, C>(v, k + t, qq, 0);
+            bool sy = false;
+            for (int t = 0; t < np; ++t) sy = sym_swap_blk<NT, C>(v, k + t, v.pair->qq[t], 0, sy) || sy;
+          } else {
+            for (int t = 0; t < np; ++t) {
+              // the position of row id order[t] from k + t on (the first
+              // match, else f - 1), searched by the whole block
+              if (threadIdx.x == 0) sh.ivals[0] = f - 1;
+              __syncthreads();
+              const int want = sh.order[t];
+              for (int i = k + t + threadIdx.x; i < f - 1; i += NT)
+                if (v.rows[i] == want) atomicMin(&sh.ivals[0], i);
+              __syncthreads();
+              const int qq = sh.ivals[0];
+              __syncthreads();
+              sym_swap_blk<NT, C>(v, k + t, qq, 0);
+            }
           }
           S.live = max(S.live, k + np);
           S.k_paired = k;
@@ -1087,7 +1281,8 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
       if (S.stalled) {
         const int m = pl - k;
         const int mv = min(m, S.live - pl);
-        for (int t = 0; t < mv; ++t) sym_swap_blk<NT, C>(v, k + t, S.live - mv + t, 0);
+        bool sy = false;
+        for (int t = 0; t < mv; ++t) sy = sym_swap_blk<NT, C>(v, k + t, S.live - mv + t, 0, sy) || sy;
         S.live -= m;
       }
       continue;

@@ -438,6 +438,7 @@ __device__ __forceinline__ FrontRef large_view(DevPlan &P, DevFactor &X, int s) 
   v.tags = X.tags + X.sn_roff[s];
   v.W = v.F + (size_t)f * f;
   v.loc = X.ploc + X.sn_roff[s];
+  v.inv = X.ploc + X.rows_cap + X.sn_roff[s];
   return v;
 }
 
@@ -451,7 +452,11 @@ __global__ void k_large_init(DevPlan P, DevFactor X, const int *__restrict__ lar
   }
   const int f = X.sn_f[s];
   int *loc = X.ploc + X.sn_roff[s];
-  for (int t = threadIdx.x; t < f; t += blockDim.x) loc[t] = t;
+  int *inv = X.ploc + X.rows_cap + X.sn_roff[s];
+  for (int t = threadIdx.x; t < f; t += blockDim.x) {
+    loc[t] = t;
+    inv[t] = t;
+  }
   if (threadIdx.x == 0) {
     TppState S;
     const bool mixed = X.sn_mixed != nullptr && X.sn_mixed[s] != 0 && nbo > 0;
@@ -471,6 +476,7 @@ __global__ void __launch_bounds__(NT) k_large_panel(DevPlan P, DevFactor X, cons
   __shared__ FrontShared sh;
   __shared__ int s_abort;
   __shared__ unsigned s_bar_seq;
+  __shared__ PairScratch s_pair;
   if (X.counters[kCFlags] & kFAbort) return;
   const int q = blockIdx.x / C;
   const bool lead = team_rank<C>() == 0 && threadIdx.x == 0;
@@ -489,6 +495,7 @@ __global__ void __launch_bounds__(NT) k_large_panel(DevPlan P, DevFactor X, cons
   v.err = X.counters + kCFlags;
   v.abort = &s_abort;
   v.bar_seq = &s_bar_seq;
+  v.pair = &s_pair;
   v.team_red = X.team_red + (size_t)q * kTeamRedDoubles;
   if (threadIdx.x == 0) {
     sh.st = S.st;
