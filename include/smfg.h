@@ -116,7 +116,7 @@ typedef struct {
   int mixed_block;
   int mixed_kind;
   int mixed_min_front;
-  int panel_team;         /* CTAs per indefinite large front's pivoting (1, 2, 4, 8); 0: by front size */
+  int panel_team;         /* CTAs per indefinite large front's pivoting (1, 2, 4, 8, 16); 0: by front size */
   /* 1: replay the factorization as one CUDA graph. The first call with a
    * given configuration (control, precision mask, value pointer) factors
    * normally and captures the launch sequence; later calls with the same
@@ -191,7 +191,7 @@ SMFG_API int smfg_inertia(smfg_plan_t plan, int *pos, int *neg, int *zero);
 SMFG_API int smfg_set_front_precision(smfg_plan_t plan, const int8_t *mask);
 
 /* Tuned team sizes of the indefinite large-front pivoting (an autotuner's
- * choice; no reference counterpart): teams[b] CTAs (1, 2, 4, 8; 0 = the
+ * choice; no reference counterpart): teams[b] CTAs (1, 2, 4, 8, 16; 0 = the
  * built-in rule) for levels whose largest front has [384, 768), [768,
  * 1536), [1536, 3072), >= 3072 symbolic rows (b = 0..3). NULL resets.
  * smfg_control_t.panel_team, when set, overrides the table. Kept for later

@@ -19,7 +19,7 @@ import numpy as np
 from . import smfg
 
 BUCKETS = ((384, 768), (768, 1536), (1536, 3072), (3072, 1 << 30))
-TEAMS = (1, 2, 4, 8)
+TEAMS = (1, 2, 4, 8, 16)
 BLOCKS = (128, 256, 512)
 
 

@@ -392,17 +392,47 @@ static void launch_defer(Plan &pl, const int *lg, int nL, const TppState *states
 // Team size (CTAs per front) of a level's indefinite large-front panels, by
 // the largest symbolic front: the swaps and eliminations of a panel stream
 // its columns (16 x f doubles per pivot), which one SM's bandwidth bounds.
-static int panel_team(int maxf) { return maxf >= 3072 ? 8 : maxf >= 1536 ? 4 : maxf >= 768 ? 2 : 1; }
+static int panel_team(int maxf) { return maxf >= 3072 ? 16 : maxf >= 1536 ? 4 : maxf >= 768 ? 2 : 1; }
 
 // Size bucket of a level's largest large front: [384, 768), [768, 1536),
 // [1536, 3072), [3072, ...).
 static int team_bucket(int maxf) { return maxf >= 3072 ? 3 : maxf >= 1536 ? 2 : maxf >= 768 ? 1 : 0; }
 
+// Whether a 16-CTA cluster of the pivoting kernel fits on the device
+// (a non-portable cluster size; 8 is the portable limit).
+static bool team16_ok(int dev) {
+  static int cached[64];
+  static bool done[64];
+  if (dev < 0 || dev >= 64) return false;
+  if (!done[dev]) {
+    done[dev] = true;
+    cached[dev] = 0;
+    if (cudaFuncSetAttribute(k_large_panel<512, 16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+        cudaSuccess) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(16, 1, 1);
+      cfg.blockDim = dim3(512, 1, 1);
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = 16;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      int n = 0;
+      if (cudaOccupancyMaxActiveClusters(&n, k_large_panel<512, 16>, &cfg) == cudaSuccess) cached[dev] = n;
+    }
+    cudaGetLastError();
+  }
+  return cached[dev] > 0;
+}
+
 static int level_team(const Plan &pl, const smfg_control_t &c, int maxf) {
-  auto ok = [](int t) { return t == 1 || t == 2 || t == 4 || t == 8; };
+  auto ok = [&](int t) { return t == 1 || t == 2 || t == 4 || t == 8 || (t == 16 && team16_ok(pl.device)); };
   if (ok(c.panel_team)) return c.panel_team;
   const int tuned = pl.panel_teams[team_bucket(maxf)];
-  return ok(tuned) ? tuned : panel_team(maxf);
+  const int t = ok(tuned) ? tuned : panel_team(maxf);
+  return ok(t) ? t : 8;  // 16 where the device cannot place a 16-CTA cluster
 }
 
 template <int C>
@@ -428,6 +458,7 @@ static void launch_panel_c(Plan &pl, const int *lg, int nL, const PivotParams &p
 
 static void launch_panel(Plan &pl, int team, const int *lg, int nL, const PivotParams &prm, int it) {
   switch (team) {
+    case 16: launch_panel_c<16>(pl, lg, nL, prm, it); break;
     case 8: launch_panel_c<8>(pl, lg, nL, prm, it); break;
     case 4: launch_panel_c<4>(pl, lg, nL, prm, it); break;
     case 2: launch_panel_c<2>(pl, lg, nL, prm, it); break;
@@ -604,6 +635,7 @@ static void set_kernel_attrs(int nb) {
 
 static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c, smfg_info_t *info) {
   SMFG_CUDA(cudaSetDevice(pl.device));
+  (void)team16_ok(pl.device);  // queried here, outside any stream capture
   pl.nb = std::max(2, c.nb);
   set_kernel_attrs(pl.nb);
   // arena: exact for SPD (no delays); head-room for delays, regrown on overflow
@@ -1092,7 +1124,7 @@ SMFG_API int smfg_set_panel_teams(smfg_plan_t plan, const int *teams) {
   Plan &pl = plan->pl;
   for (int b = 0; b < 4; ++b) {
     const int t = teams ? teams[b] : 0;
-    if (t != 0 && t != 1 && t != 2 && t != 4 && t != 8) return SMFG_ERR_INVALID_ARG;
+    if (t != 0 && t != 1 && t != 2 && t != 4 && t != 8 && t != 16) return SMFG_ERR_INVALID_ARG;
     pl.panel_teams[b] = t;
   }
   return SMFG_OK;

@@ -14,8 +14,8 @@ enum : int { kCArena = 0, kCRows = 1, kCFlags = 2, kCMaxAbs = 3, kCAux = 4, kCEf
 // error flag bits (counters[kCFlags])
 enum : unsigned { kFArena = 1u, kFRows = 2u, kFNonfinite = 4u, kFNotPosdef = 8u, kFNonfiniteD = 16u,
                   kFMap = 32u, kFInternal = 64u, kFTcWait = 128u, kFTcCap = 256u, kFSteps = 512u };
-// team reduction scratch per large front (2 buffers x 8 CTAs x 6 doubles)
-constexpr int kTeamRedDoubles = 128;
+// team reduction scratch per large front (2 buffers x 16 CTAs x 6 doubles)
+constexpr int kTeamRedDoubles = 256;
 // flags after which the rest of a factorization is skipped (retried with
 // more room, or reported)
 constexpr unsigned kFAbort = kFArena | kFRows | kFTcWait | kFTcCap;

@@ -369,7 +369,8 @@ class Solver:
             raise SmfgError(rc, "smfg_set_front_precision")
 
     def set_panel_teams(self, teams=None):
-        """smfg_set_panel_teams: CTAs per front-size bucket (4 ints, 0 = rule)."""
+        """smfg_set_panel_teams: CTAs per front-size bucket (4 ints of 0, 1, 2, 4,
+        8, 16; 0 = rule)."""
         if teams is None:
             rc = lib().smfg_set_panel_teams(self._h, None)
         else:

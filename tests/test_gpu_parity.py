@@ -136,7 +136,7 @@ def test_not_posdef_and_nonfinite(ref_lib):
     assert gi.status == 0 and gi.inertia == (n, 0, 0)
 
 
-@pytest.mark.parametrize("team", [2, 4, 8])
+@pytest.mark.parametrize("team", [2, 4, 8, 16])
 def test_panel_teams_bitwise(team, oracle_lib):
     """The indefinite large-front pivoting on a team of CTAs (a thread-block
     cluster splitting the swaps and eliminations by rows) gives the one-CTA
