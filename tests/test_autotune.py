@@ -34,7 +34,7 @@ def test_autotune_teams():
     e0 = sv.export()
     res = autotune.tune(sv, a, v, False, scale=scale)
     print(res["panel_teams"], round(res["default_ms"], 1), "->", round(res["best_ms"], 1))
-    assert all(t in (0, 1, 2, 4, 8) for t in res["panel_teams"])
+    assert all(t in (0, 1, 2, 4, 8, 16) for t in res["panel_teams"])
     assert res["best_ms"] <= res["default_ms"]
     sv.factor(v, posdef=False, scale=scale)   # with the tuned table on the plan
     e1 = sv.export()
