@@ -976,6 +976,15 @@ SMFG_API const char *smfg_error_string(int code) {
   }
 }
 
+// Scratch that the plan's pool keeps between calls (above it, freed blocks
+// go back to the device at the next synchronization).
+constexpr uint64_t kPoolKeepBytes = 4ull << 30;
+
+static cudaError_t plan_malloc_async(Plan &pl, void **p, size_t bytes) {
+  if (pl.pool) return cudaMallocFromPoolAsync(p, bytes, pl.pool, pl.stream);
+  return cudaMallocAsync(p, bytes, pl.stream);
+}
+
 SMFG_API int smfg_plan_create(const smfg_analysis_t *a, int device, smfg_plan_t *out) {
   if (!a || !out || a->n < 0 || a->nsn < 0) return SMFG_ERR_INVALID_ARG;
   *out = nullptr;
@@ -990,6 +999,19 @@ SMFG_API int smfg_plan_create(const smfg_analysis_t *a, int device, smfg_plan_t 
     SMFG_CUDA(cudaEventCreate(&h->pl.ev0));
     SMFG_CUDA(cudaEventCreate(&h->pl.ev1));
     SMFG_CUDA(cudaEventCreateWithFlags(&h->pl.ev_in, cudaEventDisableTiming));
+    {
+      cudaMemPoolProps props = {};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = device;
+      if (cudaMemPoolCreate(&h->pl.pool, &props) == cudaSuccess) {
+        uint64_t keep = kPoolKeepBytes;
+        cudaMemPoolSetAttribute(h->pl.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      } else {
+        h->pl.pool = nullptr;  // the device's default pool then
+        cudaGetLastError();
+      }
+    }
     h->pl.nb = 16;
     build_plan(h->pl, *a);
     SMFG_CUDA(cudaStreamSynchronize(h->pl.stream));
@@ -1021,6 +1043,7 @@ SMFG_API void smfg_plan_destroy(smfg_plan_t *plan) {
   if (pl.ev_in) cudaEventDestroy(pl.ev_in);
   if (pl.graph_exec) cudaGraphExecDestroy(pl.graph_exec);
   if (pl.stream) cudaStreamDestroy(pl.stream);
+  if (pl.pool) cudaMemPoolDestroy(pl.pool);
   delete *plan;
   *plan = nullptr;
 }
@@ -1082,7 +1105,7 @@ static int solve_common(smfg_plan_t plan, double *b, bool on_device, int nrhs, i
     const size_t bytes = sizeof(double) * ((size_t)ldb * (nrhs - 1) + pl.n);
     if (on_device) follow_caller(pl);
     if (!on_device) {
-      SMFG_CUDA(cudaMallocAsync((void **)&staged, bytes, pl.stream));
+      SMFG_CUDA(plan_malloc_async(pl, (void **)&staged, bytes));
       SMFG_CUDA(cudaMemcpyAsync(staged, b, bytes, cudaMemcpyHostToDevice, pl.stream));
       db = staged;
     }
@@ -1217,27 +1240,32 @@ SMFG_API int smfg_factor_export(smfg_plan_t plan, int *f, int *p, int64_t *blk_o
 // Device residual of x for b (both n x nrhs, leading dimension n, device).
 static void device_residual(Plan &pl, const double *db, const double *dx, double *dr, int nrhs,
                             double *eta, double *omega, double *norms = nullptr) {
+  // the five maxima of every column, read back with one synchronization
   unsigned long long *mx = nullptr;
-  SMFG_CUDA(cudaMallocAsync((void **)&mx, sizeof(unsigned long long) * 8, pl.stream));
+  SMFG_CUDA(plan_malloc_async(pl, (void **)&mx, sizeof(unsigned long long) * 8 * nrhs));
+  SMFG_CUDA(cudaMemsetAsync(mx, 0, sizeof(unsigned long long) * 8 * nrhs, pl.stream));
   // permuted copies: the residual works in the new numbering
   double *xp = nullptr, *bp = nullptr, *rp = nullptr;
   const size_t len = (size_t)pl.n;
-  SMFG_CUDA(cudaMallocAsync((void **)&xp, sizeof(double) * len * 3, pl.stream));
+  SMFG_CUDA(plan_malloc_async(pl, (void **)&xp, sizeof(double) * len * 3));
   bp = xp + len;
   rp = bp + len;
   const int sms = sm_count(pl.device);
   double e_max = 0.0, o_max = 0.0;
   for (int r = 0; r < nrhs; ++r) {
-    SMFG_CUDA(cudaMemsetAsync(mx, 0, sizeof(unsigned long long) * 8, pl.stream));
     const int g = (int)std::max<int64_t>(1, std::min<int64_t>(4 * sms, (pl.n + 255) / 256));
     k_solve_gather<<<g, 256, 0, pl.stream>>>(dx + (size_t)r * pl.n, pl.n, 1, pl.n, pl.d.perm, nullptr, xp);
     k_solve_gather<<<g, 256, 0, pl.stream>>>(db + (size_t)r * pl.n, pl.n, 1, pl.n, pl.d.perm, nullptr, bp);
-    const int rg = (int)std::max<int64_t>(1, std::min<int64_t>(8 * sms, (pl.n + 7) / 8));
-    k_residual<<<rg, 256, 0, pl.stream>>>(pl.d, pl.x.pv_raw, xp, bp, rp, pl.n, mx);
+    const int rg = (int)std::max<int64_t>(1, std::min<int64_t>(8 * sms, (pl.n + 31) / 32));
+    k_residual<<<rg, 256, 0, pl.stream>>>(pl.d, pl.x.pv_raw, xp, bp, rp, pl.n, mx + 8 * r);
     k_solve_scatter<<<g, 256, 0, pl.stream>>>(dr + (size_t)r * pl.n, pl.n, 1, pl.n, pl.d.perm, nullptr, rp);
-    unsigned long long h[8];
-    SMFG_CUDA(cudaMemcpyAsync(h, mx, sizeof(h), cudaMemcpyDeviceToHost, pl.stream));
-    SMFG_CUDA(cudaStreamSynchronize(pl.stream));
+  }
+  std::vector<unsigned long long> hv((size_t)8 * nrhs);
+  SMFG_CUDA(cudaMemcpyAsync(hv.data(), mx, sizeof(unsigned long long) * 8 * nrhs, cudaMemcpyDeviceToHost,
+                            pl.stream));
+  SMFG_CUDA(cudaStreamSynchronize(pl.stream));
+  for (int r = 0; r < nrhs; ++r) {
+    const unsigned long long *h = hv.data() + 8 * r;
     double v[5];
     for (int i = 0; i < 5; ++i) std::memcpy(&v[i], &h[i], 8);
     const double den = v[1] * v[2] + v[3];
@@ -1309,7 +1337,7 @@ SMFG_API int smfg_residual_noalloc(smfg_plan_t plan, const double *d_b, const do
     unsigned long long *mx = reinterpret_cast<unsigned long long *>(sc + 3 * (size_t)kNoAllocMaxN);
     const int sms = sm_count(pl.device);
     const int g = (int)std::max<int64_t>(1, std::min<int64_t>(4 * sms, ((int64_t)n + 255) / 256));
-    const int rg = (int)std::max<int64_t>(1, std::min<int64_t>(8 * sms, ((int64_t)n + 7) / 8));
+    const int rg = (int)std::max<int64_t>(1, std::min<int64_t>(8 * sms, ((int64_t)n + 31) / 32));
     double e_max = 0.0, o_max = 0.0;
     for (int r = 0; r < nrhs; ++r) {
       // the maxima start from zero on every call (the array keeps the last
@@ -1347,7 +1375,7 @@ SMFG_API int smfg_residual(smfg_plan_t plan, const double *b, const double *x, i
     clear_stale_error();
     const size_t len = (size_t)pl.n * nrhs;
     double *d = nullptr;
-    SMFG_CUDA(cudaMallocAsync((void **)&d, sizeof(double) * len * 3, pl.stream));
+    SMFG_CUDA(plan_malloc_async(pl, (void **)&d, sizeof(double) * len * 3));
     SMFG_CUDA(cudaMemcpyAsync(d, b, sizeof(double) * len, cudaMemcpyHostToDevice, pl.stream));
     SMFG_CUDA(cudaMemcpyAsync(d + len, x, sizeof(double) * len, cudaMemcpyHostToDevice, pl.stream));
     double e = 0, o = 0;
@@ -1386,7 +1414,7 @@ struct DevVec {
   Plan &pl;
   double *p = nullptr;
   DevVec(Plan &pl_, size_t n) : pl(pl_) {
-    SMFG_CUDA(cudaMallocAsync((void **)&p, sizeof(double) * std::max<size_t>(1, n), pl.stream));
+    SMFG_CUDA(plan_malloc_async(pl, (void **)&p, sizeof(double) * std::max<size_t>(1, n)));
   }
   ~DevVec() { cudaFreeAsync(p, pl.stream); }
 };
@@ -1403,7 +1431,7 @@ void dev_spmv(Plan &pl, const double *x, double *y, double *tmp2n) {
   const int g = (int)std::max<int64_t>(1, std::min<int64_t>(4 * sms, (pl.n + 255) / 256));
   double *xp = tmp2n, *yp = tmp2n + pl.n;
   k_solve_gather<<<g, 256, 0, pl.stream>>>(x, pl.n, 1, pl.n, pl.d.perm, nullptr, xp);
-  const int rg = (int)std::max<int64_t>(1, std::min<int64_t>(8 * sms, (pl.n + 7) / 8));
+  const int rg = (int)std::max<int64_t>(1, std::min<int64_t>(8 * sms, (pl.n + 31) / 32));
   k_spmv<<<rg, 256, 0, pl.stream>>>(pl.d, pl.x.pv_raw, xp, yp, pl.n);
   k_solve_scatter<<<g, 256, 0, pl.stream>>>(y, pl.n, 1, pl.n, pl.d.perm, nullptr, yp);
 }

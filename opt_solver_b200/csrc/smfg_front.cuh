@@ -40,7 +40,6 @@ struct FrontShared {
   double red[32];
   int redi[32];
   double red2[32];
-  double red3[32], red4[32];
   int kind, a, b;        // pivot choice
   int k;                 // next pivot position
   int order[128];        // stall partner pairs (row ids, or assembly positions)
@@ -157,16 +156,16 @@ struct Block {
       sh.red[w] = t.m1;
       sh.red2[w] = t.m2;
       sh.redi[w] = t.r;
-      sh.red3[w] = a;
-      sh.red4[w] = b;
+      sh.pin[w] = a;  // (the pairing scans' arrays: never in use at the same time)
+      sh.pout[w] = b;
     }
     __syncthreads();
     if (l < NW) {
       t.m1 = sh.red[l];
       t.m2 = sh.red2[l];
       t.r = sh.redi[l];
-      a = sh.red3[l];
-      b = sh.red4[l];
+      a = sh.pin[l];
+      b = sh.pout[l];
     } else {
       t.m1 = 0.0;
       t.m2 = 0.0;
@@ -452,7 +451,7 @@ struct Lay {
 
 
 // Panels of up to this many columns right of the pivot take the
-// row-at-a-time elimination path.
+// row-at-a-time elimination path (global-memory fronts: blocks of 512).
 constexpr int kElimCols = 16;
 constexpr int kElimGroup = 8;  // loads in flight per thread
 
@@ -474,7 +473,7 @@ __device__ void eliminate_1x1_blk(const FrontRef &v, int k, int ucol_end, bool u
     for (int i = k + 1 + rk * NT + (int)threadIdx.x; i < f; i += C * NT) w[i] = ck[i];
   }
   const int nj = ucol_end - (k + 1);
-  if (nj <= kElimCols) {
+  if (NT >= 512 && nj <= kElimCols) {
     // a panel: the multipliers once in shared memory, then each thread
     // one row of every column at a time (all loads of the row in flight)
     __shared__ double s_l[kElimCols];
@@ -539,7 +538,7 @@ __device__ void eliminate_2x2_blk(const FrontRef &v, int k, int ucol_end, bool u
     }
   }
   const int nj = ucol_end - (k + 2);
-  if (nj <= kElimCols) {
+  if (NT >= 512 && nj <= kElimCols) {
     // as eliminate_1x1_blk: multipliers in shared memory, rows in flight
     __shared__ double s_l0[kElimCols], s_l1[kElimCols];
     for (int jj = threadIdx.x; jj < nj; jj += NT) {
@@ -633,6 +632,10 @@ __device__ __forceinline__ Top2 warp_top2(Top2 t) {
 template <typename Fn>
 __device__ __forceinline__ void scanv(const double *__restrict__ col, int lo, int hi, int tid, int nth, Fn fn) {
   if (lo >= hi) return;
+  if (nth < 512) {  // small blocks (fronts in shared memory): one element at a time
+    for (int i = lo + tid; i < hi; i += nth) fn(fabs(col[i]), i);
+    return;
+  }
   int a = lo;
   if (reinterpret_cast<uintptr_t>(col + a) & 15) {
     if (tid == 0) fn(fabs(col[a]), a);

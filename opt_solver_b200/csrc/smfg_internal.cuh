@@ -92,6 +92,10 @@ struct Plan {
   DevPlan d;
   DevFactor x;
   cudaStream_t stream = nullptr;
+  // the plan's own stream-ordered pool (refinement, residual and staging
+  // scratch): keeps up to kPoolKeepBytes between calls instead of unmapping
+  // them at each synchronization
+  cudaMemPool_t pool = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t ev_in = nullptr;  // orders the stream after the caller's default-stream work
   // last factorization

@@ -1777,27 +1777,35 @@ __device__ __forceinline__ void two_sum(double a, double b, double &s, double &e
   e = (a - (s - bb)) + (b - bb);
 }
 
+// kResLanes lanes per row (rows hold a few entries of the symmetric
+// pattern: a warp takes 32 / kResLanes rows at a time).
+constexpr int kResLanes = 8;
+
 __global__ void k_residual(DevPlan P, const double *__restrict__ vals, const double *__restrict__ x,
                            const double *__restrict__ b, double *__restrict__ r, int n,
                            unsigned long long *mx /* [0] |r|max [1] row |A| sum max [2] |x| max [3] |b| max [4] omega */) {
-  const int lane = threadIdx.x & 31;
+  constexpr int RPW = 32 / kResLanes;
+  const int lane = threadIdx.x & 31, sub = lane % kResLanes, grp = lane / kResLanes;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   double m_r = 0.0, m_a = 0.0, m_x = 0.0, m_b = 0.0, m_o = 0.0;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+  for (int i0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * RPW; i0 < n; i0 += warps * RPW) {
+    const int i = i0 + grp;
     double s = 0.0, c = 0.0, as = 0.0, ra = 0.0;
-    for (int k = P.sptr[i] + lane; k < P.sptr[i + 1]; k += 32) {
-      const double a = vals[P.sidx[k]];
-      const double xj = x[P.srow[k]];
-      const double pr = a * xj;
-      const double pe = fma(a, xj, -pr);
-      double t, e;
-      two_sum(s, pr, t, e);
-      s = t;
-      c += e + pe;
-      as = fma(fabs(a), fabs(xj), as);
-      ra += fabs(a);
+    if (i < n) {
+      for (int k = P.sptr[i] + sub; k < P.sptr[i + 1]; k += kResLanes) {
+        const double a = vals[P.sidx[k]];
+        const double xj = x[P.srow[k]];
+        const double pr = a * xj;
+        const double pe = fma(a, xj, -pr);
+        double t, e;
+        two_sum(s, pr, t, e);
+        s = t;
+        c += e + pe;
+        as = fma(fabs(a), fabs(xj), as);
+        ra += fabs(a);
+      }
     }
-    for (int o = 16; o > 0; o >>= 1) {
+    for (int o = kResLanes / 2; o > 0; o >>= 1) {  // within the row's lanes
       const double s2 = __shfl_xor_sync(0xffffffffu, s, o);
       const double c2 = __shfl_xor_sync(0xffffffffu, c, o);
       double t, e;
@@ -1807,7 +1815,7 @@ __global__ void k_residual(DevPlan P, const double *__restrict__ vals, const dou
       as += __shfl_xor_sync(0xffffffffu, as, o);
       ra += __shfl_xor_sync(0xffffffffu, ra, o);
     }
-    if (lane == 0) {
+    if (sub == 0 && i < n) {
       const double bi = b[i];
       double t, e;
       two_sum(bi, -s, t, e);
@@ -1821,6 +1829,13 @@ __global__ void k_residual(DevPlan P, const double *__restrict__ vals, const dou
       const double om = den > 0.0 ? fabs(res) / den : (res == 0.0 ? 0.0 : INFINITY);
       m_o = fmax(m_o, om);
     }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    m_r = fmax(m_r, __shfl_xor_sync(0xffffffffu, m_r, o));
+    m_a = fmax(m_a, __shfl_xor_sync(0xffffffffu, m_a, o));
+    m_x = fmax(m_x, __shfl_xor_sync(0xffffffffu, m_x, o));
+    m_b = fmax(m_b, __shfl_xor_sync(0xffffffffu, m_b, o));
+    m_o = fmax(m_o, __shfl_xor_sync(0xffffffffu, m_o, o));
   }
   if (lane == 0) {
     atomicMax(mx + 0, (unsigned long long)__double_as_longlong(m_r));
@@ -1901,13 +1916,16 @@ __global__ void k_lincomb(double *__restrict__ xc, const double *__restrict__ x0
 // y = A x in the new numbering (the unscaled values), a warp per row
 __global__ void k_spmv(DevPlan P, const double *__restrict__ vals, const double *__restrict__ x,
                        double *__restrict__ y, int n) {
-  const int lane = threadIdx.x & 31;
+  constexpr int RPW = 32 / kResLanes;  // rows per warp, as k_residual
+  const int lane = threadIdx.x & 31, sub = lane % kResLanes, grp = lane / kResLanes;
   const int warps = (gridDim.x * blockDim.x) >> 5;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+  for (int i0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * RPW; i0 < n; i0 += warps * RPW) {
+    const int i = i0 + grp;
     double s = 0.0;
-    for (int k = P.sptr[i] + lane; k < P.sptr[i + 1]; k += 32) s = fma(vals[P.sidx[k]], x[P.srow[k]], s);
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) y[i] = s;
+    if (i < n)
+      for (int k = P.sptr[i] + sub; k < P.sptr[i + 1]; k += kResLanes) s = fma(vals[P.sidx[k]], x[P.srow[k]], s);
+    for (int o = kResLanes / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (sub == 0 && i < n) y[i] = s;
   }
 }
 
