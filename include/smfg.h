@@ -235,6 +235,14 @@ SMFG_API int smfg_residual(smfg_plan_t plan, const double *b, const double *x, i
  * one array: calls that overlap on the GPU (other threads or streams) race,
  * so serialize them. Synchronizes the plan's stream. */
 #define SMFG_NOALLOC_MAX_N 262144
+/* Kernel self-benchmark (no reference counterpart): the streamed deferred
+ * update on one synthetic front of f rows, ne eligible columns, a pending
+ * panel of k <= 16 pivots; best device time of reps launches (ms), the
+ * update's algorithmic bytes, and the entries whose bits differ from the
+ * tiled kernel's result (0 expected). Allocates 3 (f^2 + 16 f) doubles. */
+SMFG_API int smfg_kernel_bench_defer(int f, int ne, int k, int reps, double *ms, double *bytes,
+                                     long long *mismatches);
+
 SMFG_API int smfg_residual_noalloc(smfg_plan_t plan, const double *d_b, const double *d_x, double *d_r,
                                    int nrhs, double *eta_inf, double *omega);
 

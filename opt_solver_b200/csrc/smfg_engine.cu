@@ -1778,3 +1778,113 @@ SMFG_API int smfg_tc_update(double *d_C, int ldc, int n, const double *d_L, int 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Kernel self-benchmark (no reference counterpart): the streamed deferred
+// update (k_large_defer) on one synthetic large front of f rows, its first
+// ne columns eligible, one panel of k pivots pending (the rows [16, f) x
+// columns [16, ne) trapezoid), timed with CUDA events over reps launches
+// after one warm-up, each on freshly restored values; then the tiled kernel
+// (k_large_gemm) on the same input, and the two results compared bit for
+// bit. Sized for profiler captures and self-checks, not for a factorization.
+namespace smfg {
+__global__ void k_kbench_fill(double *a, size_t n, unsigned long long seed) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    unsigned long long h = (i + 1) * 0x9E3779B97F4A7C15ull ^ seed;
+    h ^= h >> 29;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 32;
+    a[i] = (double)(h & 0xFFFFF) / 1048576.0 - 0.5;
+  }
+}
+__global__ void k_kbench_diff(const double *a, const double *b, size_t n, unsigned long long *cnt) {
+  unsigned long long c = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    c += (__double_as_longlong(a[i]) != __double_as_longlong(b[i])) ? 1ull : 0ull;
+  if (c) atomicAdd(cnt, c);
+}
+}  // namespace smfg
+
+extern "C" SMFG_API int smfg_kernel_bench_defer(int f, int ne, int k, int reps, double *ms, double *bytes,
+                                                long long *mismatches) {
+  if (f < 64 || ne < 32 || ne > f || k < 1 || k > kDK || reps < 1 || !ms || !bytes || !mismatches)
+    return SMFG_ERR_INVALID_ARG;
+  const size_t nel = (size_t)f * f + (size_t)kDK * f;
+  std::vector<void *> mem;
+  auto take = [&](size_t b) {
+    void *p = nullptr;
+    SMFG_CUDA(cudaMalloc(&p, b));
+    mem.push_back(p);
+    return p;
+  };
+  int rc = SMFG_OK;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  try {
+    double *arena = static_cast<double *>(take(nel * 8));
+    double *orig = static_cast<double *>(take(nel * 8));
+    double *out = static_cast<double *>(take(nel * 8));
+    auto *cnt = static_cast<unsigned long long *>(take(32 * 8));
+    int *sn_f = static_cast<int *>(take(4));
+    int *large = static_cast<int *>(take(4));
+    auto *sn_off = static_cast<int64_t *>(take(8));
+    auto *tpp = static_cast<TppState *>(take(sizeof(TppState)));
+    k_kbench_fill<<<1184, 256>>>(orig, nel, 0x5EEDull);
+    SMFG_CUDA(cudaMemset(cnt, 0, 32 * 8));
+    const int zero = 0;
+    const int64_t zero8 = 0;
+    SMFG_CUDA(cudaMemcpy(sn_f, &f, 4, cudaMemcpyHostToDevice));
+    SMFG_CUDA(cudaMemcpy(large, &zero, 4, cudaMemcpyHostToDevice));
+    SMFG_CUDA(cudaMemcpy(sn_off, &zero8, 8, cudaMemcpyHostToDevice));
+    TppState S{};
+    S.pad[0] = 1;
+    S.g_p0 = 0;
+    S.g_p1 = k;
+    S.g_c0 = 16;
+    S.g_e = ne;
+    SMFG_CUDA(cudaMemcpy(tpp, &S, sizeof S, cudaMemcpyHostToDevice));
+    DevPlan P{};
+    DevFactor X{};
+    X.counters = cnt;
+    X.sn_f = sn_f;
+    X.sn_off = sn_off;
+    X.arena = arena;
+    X.arena_cap = (int64_t)nel;
+    int dev = 0;
+    SMFG_CUDA(cudaGetDevice(&dev));
+    const int sms = sm_count(dev);
+    SMFG_CUDA(cudaFuncSetAttribute(k_large_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem)));
+    SMFG_CUDA(cudaEventCreate(&e0));
+    SMFG_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    for (int r = 0; r <= reps; ++r) {
+      SMFG_CUDA(cudaMemcpy(arena, orig, nel * 8, cudaMemcpyDeviceToDevice));
+      SMFG_CUDA(cudaEventRecord(e0));
+      k_large_defer<<<kDBlocksPerSM * sms, 256>>>(P, X, large, 1, tpp);
+      SMFG_CUDA(cudaEventRecord(e1));
+      SMFG_CUDA(cudaEventSynchronize(e1));
+      SMFG_CUDA(cudaGetLastError());
+      float t = 0.0f;
+      SMFG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+      if (r > 0) best = std::min(best, t);
+    }
+    SMFG_CUDA(cudaMemcpy(out, arena, nel * 8, cudaMemcpyDeviceToDevice));
+    SMFG_CUDA(cudaMemcpy(arena, orig, nel * 8, cudaMemcpyDeviceToDevice));
+    k_large_gemm<<<2 * sms, 256, sizeof(TileSmem)>>>(P, X, large, 1, tpp);
+    SMFG_CUDA(cudaMemset(cnt + 16, 0, 8));
+    k_kbench_diff<<<1184, 256>>>(out, arena, (size_t)f * f, cnt + 16);
+    unsigned long long h[17];
+    SMFG_CUDA(cudaMemcpy(h, cnt, sizeof h, cudaMemcpyDeviceToHost));
+    const long long m = ne - 16, hh = f - 16;
+    *ms = best;
+    *bytes = 16.0 * (double)(m * hh - m * (m - 1) / 2);
+    *mismatches = (long long)h[16];
+    if (h[kCFlags] & kFAbort) rc = SMFG_ERR_INTERNAL;
+  } catch (const std::exception &ex) {
+    set_last_error(ex.what());
+    rc = SMFG_ERR_CUDA;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  for (void *p : mem) cudaFree(p);
+  return rc;
+}

@@ -301,6 +301,21 @@ TC_TF32X3, TC_BF16X3 = 0, 1
 REFINE_CLASSICAL, REFINE_FGMRES, REFINE_AUTO = 0, 1, 2
 
 
+def kernel_bench_defer(f: int = 8000, ne: int = 4000, k: int = 16, reps: int = 5) -> dict:
+    """smfg_kernel_bench_defer: the streamed deferred-update kernel on one
+    synthetic front (f rows, ne eligible columns, k pending pivots): best
+    device ms, algorithmic bytes, GB/s, and entries differing bitwise from
+    the tiled kernel (0 expected)."""
+    L = lib()
+    L.smfg_kernel_bench_defer.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double),
+                                          C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
+    ms, by, mm = C.c_double(), C.c_double(), C.c_longlong()
+    rc = L.smfg_kernel_bench_defer(f, ne, k, reps, C.byref(ms), C.byref(by), C.byref(mm))
+    if rc != SMFG_OK:
+        raise SmfgError(rc, "smfg_kernel_bench_defer")
+    return {"ms": ms.value, "bytes": by.value, "gbs": by.value / (ms.value * 1e6), "mismatches": mm.value}
+
+
 def tc_update(C_t, L_t, W_t, kind: int = TC_TF32X3):
     """smfg_tc_update on CUDA float64 tensors given TRANSPOSED (row-major
     (k, n) / (n, n) tensors are the column-major n x k / n x n matrices):
