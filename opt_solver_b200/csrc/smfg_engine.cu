@@ -893,7 +893,7 @@ static void enqueue_solve(Plan &pl, double *d_b, int nrhs, int ldb, int job, boo
         const int *lg = d.lvl_large + pl.lvl_large_ptr[l];
         const int nb = (large_pmax(pl, l) + kSB - 1) / kSB;
         for (int b = 0; b < nb; ++b) {
-          k_fwd_tri<<<nL, kSolveNT, 0, st>>>(d, x, lg, b, pl.posdef, xv, wk, rows_total, nrhs);
+          k_fwd_tri<<<nL, kTriNT, 0, st>>>(d, x, lg, b, pl.posdef, xv, wk, rows_total, nrhs);
           k_fwd_gemv<<<lgrid, 256, 0, st>>>(d, x, lg, nL, b, wk, rows_total, nrhs);
         }
         lc.n += 2 * nb;
@@ -916,7 +916,7 @@ static void enqueue_solve(Plan &pl, double *d_b, int nrhs, int ldb, int job, boo
         const int nb = (large_pmax(pl, l) + kSB - 1) / kSB;
         for (int b = nb - 1; b >= 0; --b) {
           k_bwd_dots<<<lgrid, 256, 0, st>>>(d, x, lg, nL, b, wk, rows_total, nrhs);
-          k_bwd_tri<<<nL, kSolveNT, 0, st>>>(d, x, lg, b, pl.posdef, xv, wk, rows_total, nrhs);
+          k_bwd_tri<<<nL, kTriNT, 0, st>>>(d, x, lg, b, pl.posdef, xv, wk, rows_total, nrhs);
         }
         lc.n += 2 * nb;
       }

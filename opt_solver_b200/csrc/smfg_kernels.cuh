@@ -1600,12 +1600,36 @@ __global__ void __launch_bounds__(kSolveNT) k_bwd_front(DevPlan P, DevFactor X, 
 // Large fronts' L11 solves in blocks of kSB columns: one block of threads
 // per front solves the block's triangle (32-column steps), then all blocks
 // of the GPU update the rows below it (forward) or the dot products of the
-// next block's columns with the solved rows (backward).
+// next block's columns with the solved rows (backward). The loops are
+// latency-bound (each front's block waits for the one before it), so every
+// thread keeps its loads of L in flight together: a warp takes 32 rows of
+// one 32-column strip (32 loads a lane), and partial sums over strips or
+// row ranges meet in shared memory in a fixed order (deterministic).
 constexpr int kSB = 256;
+constexpr int kTriNT = 256;  // threads of the triangle kernels
 
-__global__ void __launch_bounds__(kSolveNT) k_fwd_tri(DevPlan P, DevFactor X, const int *__restrict__ large,
-                                                      int b, int posdef, double *x, double *wk,
-                                                      int64_t rows_total, int nrhs) {
+// acc over the 32 columns [jb, jb + nb) of row i: sum of L(i, j) w[j]
+// (w in shared memory, indexed from wb), all loads issued first.
+__device__ __forceinline__ double strip_dot32(const double *L, size_t sf, int i, int jb, int nb,
+                                              const double *w, int wb) {
+  // (L is only read while the solves run: the read-only path)
+  const double *li = L + (size_t)jb * sf + i;
+  double acc = 0.0;
+  if (nb == 32) {
+    double l[32];
+#pragma unroll
+    for (int u = 0; u < 32; ++u) l[u] = __ldg(li + (size_t)u * sf);
+#pragma unroll
+    for (int u = 0; u < 32; ++u) acc = fma(l[u], w[jb + u - wb], acc);
+  } else {
+    for (int u = 0; u < nb; ++u) acc = fma(__ldg(li + (size_t)u * sf), w[jb + u - wb], acc);
+  }
+  return acc;
+}
+
+__global__ void __launch_bounds__(kTriNT) k_fwd_tri(DevPlan P, DevFactor X, const int *__restrict__ large,
+                                                    int b, int posdef, double *x, double *wk,
+                                                    int64_t rows_total, int nrhs) {
   const int s = large[blockIdx.x];
   const int f = X.sn_f[s], p = X.sn_pstore[s];
   const int j0 = b * kSB;
@@ -1615,42 +1639,60 @@ __global__ void __launch_bounds__(kSolveNT) k_fwd_tri(DevPlan P, DevFactor X, co
   const int *rows = X.rows + roff;
   const double *L = X.arena + X.sn_off[s];
   const size_t sf = (size_t)f;
-  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   __shared__ double Ls[32][33];
+  __shared__ double ws[kSB];
   for (int r = 0; r < nrhs; ++r) {
     double *w = wk + (int64_t)r * rows_total + roff;
+    for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) ws[t] = w[j0 + t];
     for (int jb = j0; jb < j1; jb += 32) {
       const int nb = min(32, j1 - jb);
-      load_tri32<kSolveNT>(L, sf, jb, nb, Ls);
-      if (warp == 0) tri_fwd_warp(w, jb, nb, posdef, Ls);
+      load_tri32<kTriNT>(L, sf, jb, nb, Ls);
+      if (warp == 0) {
+        // the 32 x 32 triangle on the block's values in shared memory
+        double wi = (lane < nb) ? ws[jb - j0 + lane] : 0.0;
+        for (int j = 0; j < nb; ++j) {
+          double wj = __shfl_sync(0xffffffffu, wi, j);
+          if (posdef) wj = wj / Ls[j][j];
+          if (lane == j) wi = wj;
+          if (lane > j && lane < nb) wi = fma(-Ls[lane][j], wj, wi);
+        }
+        if (lane < nb) ws[jb - j0 + lane] = wi;
+      }
       __syncthreads();
-      for (int i = jb + nb + threadIdx.x; i < j1; i += kSolveNT) {
-        double acc = w[i];
-        for (int j = jb; j < jb + nb; ++j) acc = fma(-L[(size_t)j * sf + i], w[j], acc);
-        w[i] = acc;
+      // the block's rows below this strip: a warp per 32 rows
+      for (int i = jb + nb + warp * 32 + lane; i - lane < j1; i += kTriNT) {
+        const double acc = (i < j1) ? strip_dot32(L, sf, i, jb, nb, ws, j0) : 0.0;
+        if (i < j1) ws[i - j0] -= acc;
       }
       __syncthreads();
     }
+    for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) w[j0 + t] = ws[t];
     double *xr = x + (int64_t)r * P.n;
-    for (int j = j0 + threadIdx.x; j < j1; j += kSolveNT) xr[rows[j]] = w[j];
+    for (int j = j0 + threadIdx.x; j < j1; j += kTriNT) xr[rows[j]] = ws[j - j0];
     __syncthreads();
   }
 }
 
-// w[j1:f) -= L[j1:f, j0:j1) w[j0:j1) of each large front, rows over blocks.
+// w[j1:f) -= L[j1:f, j0:j1) w[j0:j1) of each large front: a work item is 32
+// rows; its 8 warps take 32-column strips of the block, lane = row, and the
+// strips' partial sums are added in strip order.
 __global__ void __launch_bounds__(256) k_fwd_gemv(DevPlan P, DevFactor X, const int *__restrict__ large,
                                                   int nlarge, int b, double *wk, int64_t rows_total,
                                                   int nrhs) {
   __shared__ double ws[kSB];
+  __shared__ double part[8][33];
   __shared__ int pref[65];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int chunk = 0; chunk < nlarge; chunk += 64) {
     const int cnt = min(64, nlarge - chunk);
+    __syncthreads();
     if (threadIdx.x == 0) {
       pref[0] = 0;
       for (int q = 0; q < cnt; ++q) {
         const int s = large[chunk + q];
         const int f = X.sn_f[s], p = X.sn_pstore[s], j1 = min(p, (b + 1) * kSB);
-        pref[q + 1] = pref[q] + ((b * kSB < p && f > j1) ? (f - j1 + 255) / 256 * nrhs : 0);
+        pref[q + 1] = pref[q] + ((b * kSB < p && f > j1) ? (f - j1 + 31) / 32 * nrhs : 0);
       }
     }
     __syncthreads();
@@ -1665,7 +1707,7 @@ __global__ void __launch_bounds__(256) k_fwd_gemv(DevPlan P, DevFactor X, const 
       const int s = large[chunk + a];
       const int f = X.sn_f[s], p = X.sn_pstore[s];
       const int j0 = b * kSB, j1 = min(p, j0 + kSB);
-      const int nchunks = (f - j1 + 255) / 256;
+      const int nchunks = (f - j1 + 31) / 32;
       const int item = wi - pref[a];
       const int r = item / nchunks, rc = item % nchunks;
       double *w = wk + (int64_t)r * rows_total + X.sn_roff[s];
@@ -1674,32 +1716,41 @@ __global__ void __launch_bounds__(256) k_fwd_gemv(DevPlan P, DevFactor X, const 
       __syncthreads();
       for (int t = threadIdx.x; t < j1 - j0; t += 256) ws[t] = w[j0 + t];
       __syncthreads();
-      const int i = j1 + rc * 256 + threadIdx.x;
-      if (i < f) {
-        double acc = w[i];
-        for (int j = j0; j < j1; ++j) acc = fma(-L[(size_t)j * sf + i], ws[j - j0], acc);
-        w[i] = acc;
+      const int i = j1 + rc * 32 + lane;
+      const int jb = j0 + warp * 32;
+      double acc = 0.0;
+      if (i < f && jb < j1) acc = strip_dot32(L, sf, i, jb, min(32, j1 - jb), ws, j0);
+      part[warp][lane] = acc;
+      __syncthreads();
+      if (warp == 0 && i < f) {
+        double sum = 0.0;
+#pragma unroll
+        for (int g = 0; g < 8; ++g) sum += part[g][lane];
+        w[i] -= sum;
       }
     }
-    __syncthreads();
   }
 }
 
 // v[j] -= sum_{i in [j1, p)} L(i, j) v[i] for the columns j of block b of
-// each large front (warp per column; the rows below are solved).
+// each large front: a work item is one column, its rows split over the
+// block's threads (all loads of a thread in flight), partial sums added in
+// thread order.
 __global__ void __launch_bounds__(256) k_bwd_dots(DevPlan P, DevFactor X, const int *__restrict__ large,
                                                   int nlarge, int b, double *wk, int64_t rows_total,
                                                   int nrhs) {
   __shared__ int pref[65];
+  __shared__ double red[8];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int chunk = 0; chunk < nlarge; chunk += 64) {
     const int cnt = min(64, nlarge - chunk);
+    __syncthreads();
     if (threadIdx.x == 0) {
       pref[0] = 0;
       for (int q = 0; q < cnt; ++q) {
         const int s = large[chunk + q];
         const int p = X.sn_pstore[s], j0 = b * kSB, j1 = min(p, j0 + kSB);
-        pref[q + 1] = pref[q] + ((j0 < p && j1 < p) ? (j1 - j0 + 7) / 8 * nrhs : 0);
+        pref[q + 1] = pref[q] + ((j0 < p && j1 < p) ? (j1 - j0) * nrhs : 0);
       }
     }
     __syncthreads();
@@ -1714,26 +1765,39 @@ __global__ void __launch_bounds__(256) k_bwd_dots(DevPlan P, DevFactor X, const 
       const int s = large[chunk + a];
       const int f = X.sn_f[s], p = X.sn_pstore[s];
       const int j0 = b * kSB, j1 = min(p, j0 + kSB);
-      const int ncc = (j1 - j0 + 7) / 8;
       const int item = wi - pref[a];
-      const int r = item / ncc, cc = item % ncc;
-      const int j = j0 + cc * 8 + warp;
-      if (j < j1) {
-        double *v = wk + (int64_t)r * rows_total + X.sn_roff[s];
-        const double *Lj = X.arena + X.sn_off[s] + (size_t)j * f;
-        double acc = 0.0;
-        for (int i = j1 + lane; i < p; i += 32) acc = fma(Lj[i], v[i], acc);
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) v[j] -= acc;
+      const int r = item / (j1 - j0), j = j0 + item % (j1 - j0);
+      double *v = wk + (int64_t)r * rows_total + X.sn_roff[s];
+      const double *Lj = X.arena + X.sn_off[s] + (size_t)j * f;
+      double acc = 0.0;
+      int i = j1 + (int)threadIdx.x;
+      for (; i + 7 * 256 < p; i += 8 * 256) {
+        double l[8], y[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          l[u] = __ldg(Lj + i + u * 256);
+          y[u] = v[i + u * 256];
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) acc = fma(l[u], y[u], acc);
+      }
+      for (; i < p; i += 256) acc = fma(Lj[i], v[i], acc);
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      __syncthreads();
+      if (lane == 0) red[warp] = acc;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double sum = 0.0;
+        for (int g = 0; g < 8; ++g) sum += red[g];
+        v[j] -= sum;
       }
     }
-    __syncthreads();
   }
 }
 
-__global__ void __launch_bounds__(kSolveNT) k_bwd_tri(DevPlan P, DevFactor X, const int *__restrict__ large,
-                                                      int b, int posdef, double *x, double *wk,
-                                                      int64_t rows_total, int nrhs) {
+__global__ void __launch_bounds__(kTriNT) k_bwd_tri(DevPlan P, DevFactor X, const int *__restrict__ large,
+                                                    int b, int posdef, double *x, double *wk,
+                                                    int64_t rows_total, int nrhs) {
   const int s = large[blockIdx.x];
   const int f = X.sn_f[s], p = X.sn_pstore[s];
   const int j0 = b * kSB;
@@ -1745,30 +1809,53 @@ __global__ void __launch_bounds__(kSolveNT) k_bwd_tri(DevPlan P, DevFactor X, co
   const size_t sf = (size_t)f;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   __shared__ double Ls[32][33];
+  __shared__ double vs[kSB];
   for (int r = 0; r < nrhs; ++r) {
     double *v = wk + (int64_t)r * rows_total + roff;
+    for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) vs[t] = v[j0 + t];
+    __syncthreads();
     for (int je = j1; je > j0; je -= 32) {
       const int jb = max(j0, je - 32), nb = je - jb;
-      for (int j = jb + warp; j < je; j += kSolveNT / 32) {
+      // v[j] -= sum over the block's solved rows [je, j1) of L(i, j) v[i]:
+      // a warp per column, its lanes' rows (at most 7 a lane) loaded at once
+      for (int j = jb + warp; j < je; j += kTriNT / 32) {
         const double *Lj = L + (size_t)j * sf;
+        double l[7], y[7];
+#pragma unroll
+        for (int u = 0; u < 7; ++u) {
+          const int i = je + lane + 32 * u;
+          l[u] = (i < j1) ? Lj[i] : 0.0;
+          y[u] = (i < j1) ? vs[i - j0] : 0.0;
+        }
         double acc = 0.0;
-        for (int i = je + lane; i < j1; i += 32) acc = fma(Lj[i], v[i], acc);
+#pragma unroll
+        for (int u = 0; u < 7; ++u) acc = fma(l[u], y[u], acc);
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) v[j] -= acc;
+        if (lane == 0) vs[j - j0] -= acc;
       }
-      load_tri32<kSolveNT>(L, sf, jb, nb, Ls);
-      if (warp == 0) tri_bwd_warp(v, jb, nb, posdef, Ls);
+      load_tri32<kTriNT>(L, sf, jb, nb, Ls);
+      if (warp == 0) {
+        double vi = (lane < nb) ? vs[jb - j0 + lane] : 0.0;
+        for (int j = nb - 1; j >= 0; --j) {
+          double xj = __shfl_sync(0xffffffffu, vi, j);
+          if (posdef) xj = xj / Ls[j][j];
+          if (lane == j) vi = xj;
+          if (lane < j) vi = fma(-Ls[j][lane], xj, vi);
+        }
+        if (lane < nb) vs[jb - j0 + lane] = vi;
+      }
       __syncthreads();
     }
+    for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) v[j0 + t] = vs[t];
     double *xr = x + (int64_t)r * P.n;
-    for (int j = j0 + threadIdx.x; j < j1; j += kSolveNT) xr[rows[j]] = v[j];
+    for (int j = j0 + threadIdx.x; j < j1; j += kTriNT) xr[rows[j]] = vs[j - j0];
     __syncthreads();
   }
 }
 
 // ---------------------------------------------------------------------------
 // Residual r = b - A x and backward errors (refinement.cpp:39-130), on the
-// full symmetric pattern, one warp per row, compensated dot products
+// full symmetric pattern, eight lanes per row, compensated dot products
 // (Ogita, Rump & Oishi, "Accurate sum and dot product", SIAM J. Sci.
 // Comput. 26(6), 2005: TwoProduct via fma, TwoSum) in the new numbering.
 __device__ __forceinline__ void two_sum(double a, double b, double &s, double &e) {
