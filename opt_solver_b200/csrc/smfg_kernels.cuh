@@ -1355,7 +1355,7 @@ __device__ __forceinline__ void tri_bwd_warp(double *v, int jb, int nb, int posd
 // Forward sweep of one level: gather, children's update vectors in child
 // order, blocked unit (indefinite) or non-unit (SPD) L11 solve, then
 // w[p:f) -= L21 w[0:p) unless the front is large.
-__global__ void __launch_bounds__(kSolveNT) k_fwd_front(DevPlan P, DevFactor X, int lo, int posdef,
+__global__ void __launch_bounds__(kSolveNT, 4) k_fwd_front(DevPlan P, DevFactor X, int lo, int posdef,
                                                         double *x, double *wk, int64_t rows_total,
                                                         int nrhs) {
   const int s = P.lvl_sn[lo + blockIdx.x];
@@ -1367,35 +1367,49 @@ __global__ void __launch_bounds__(kSolveNT) k_fwd_front(DevPlan P, DevFactor X, 
   const bool large = P.sn_fsym[s] >= kLargeMin;
   __shared__ double Ls[32][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int r = 0; r < nrhs; ++r) {
-    double *w = wk + (int64_t)r * rows_total + roff;
-    double *xr = x + (int64_t)r * P.n;
-    for (int i = threadIdx.x; i < f; i += kSolveNT) w[i] = (i < p) ? xr[rows[i]] : 0.0;
-    __syncthreads();
-    for (int t = P.child_ptr[s]; t < P.child_ptr[s + 1]; ++t) {
-      const int c = P.child_idx[t];
-      const int pc = X.sn_pstore[c], q = X.sn_f[c] - pc;
-      const int *cmap = X.cbmap + X.sn_roff[c] + pc;
-      const double *u = wk + (int64_t)r * rows_total + X.sn_roff[c] + pc;
-      for (int i = threadIdx.x; i < q; i += kSolveNT) w[cmap[i]] += u[i];
-      __syncthreads();
+  // every right-hand side at once: gather, children's update vectors in
+  // child order, then per 32-column strip the triangle (a warp per
+  // right-hand side) and the rows below (each L entry loaded once for all)
+  for (int64_t t = threadIdx.x; t < (int64_t)f * nrhs; t += kSolveNT) {
+    const int r = (int)(t / f), i = (int)(t % f);
+    wk[(int64_t)r * rows_total + roff + i] = (i < p) ? x[(int64_t)r * P.n + rows[i]] : 0.0;
+  }
+  __syncthreads();
+  for (int t = P.child_ptr[s]; t < P.child_ptr[s + 1]; ++t) {
+    const int c = P.child_idx[t];
+    const int pc = X.sn_pstore[c], q = X.sn_f[c] - pc;
+    const int *cmap = X.cbmap + X.sn_roff[c] + pc;
+    for (int64_t u = threadIdx.x; u < (int64_t)q * nrhs; u += kSolveNT) {
+      const int r = (int)(u / q), i = (int)(u % q);
+      wk[(int64_t)r * rows_total + roff + cmap[i]] += wk[(int64_t)r * rows_total + X.sn_roff[c] + pc + i];
     }
-    if (large) continue;  // the block kernels (k_fwd_tri / k_fwd_gemv) go on
-    const int rend = f;
-    for (int jb = 0; jb < p; jb += 32) {
-      const int nb = min(32, p - jb);
-      load_tri32<kSolveNT>(L, sf, jb, nb, Ls);
-      if (warp == 0) tri_fwd_warp(w, jb, nb, posdef, Ls);
-      __syncthreads();
-      for (int i = jb + nb + threadIdx.x; i < rend; i += kSolveNT) {
-        double acc = w[i];
-        for (int j = jb; j < jb + nb; ++j) acc = fma(-L[(size_t)j * sf + i], w[j], acc);
-        w[i] = acc;
+    __syncthreads();
+  }
+  if (large) return;  // the block kernels (k_fwd_tri / k_fwd_gemv) go on
+  for (int jb = 0; jb < p; jb += 32) {
+    const int nb = min(32, p - jb);
+    load_tri32<kSolveNT>(L, sf, jb, nb, Ls);
+    for (int r = warp; r < nrhs; r += kSolveNT / 32) tri_fwd_warp(wk + (int64_t)r * rows_total + roff, jb, nb, posdef, Ls);
+    __syncthreads();
+    for (int i = jb + nb + threadIdx.x; i < f; i += kSolveNT) {
+      const double *li = L + (size_t)jb * sf + i;
+      double l[32];
+#pragma unroll
+      for (int u = 0; u < 32; ++u) l[u] = (u < nb) ? __ldg(li + (size_t)u * sf) : 0.0;
+      for (int r = 0; r < nrhs; ++r) {
+        double *w = wk + (int64_t)r * rows_total + roff;
+        double acc = 0.0;
+#pragma unroll
+        for (int u = 0; u < 32; ++u)
+          if (u < nb) acc = fma(l[u], w[jb + u], acc);
+        w[i] -= acc;
       }
-      __syncthreads();
     }
-    for (int i = threadIdx.x; i < p; i += kSolveNT) xr[rows[i]] = w[i];
     __syncthreads();
+  }
+  for (int64_t t = threadIdx.x; t < (int64_t)p * nrhs; t += kSolveNT) {
+    const int r = (int)(t / p), i = (int)(t % p);
+    x[(int64_t)r * P.n + rows[i]] = wk[(int64_t)r * rows_total + roff + i];
   }
 }
 
@@ -1499,8 +1513,6 @@ __global__ void __launch_bounds__(256) k_bwd_l21(DevPlan P, DevFactor X, const i
 __global__ void __launch_bounds__(kSolveNT) k_bwd_front(DevPlan P, DevFactor X, int lo, int posdef,
                                                         double *x, double *wk, int64_t rows_total,
                                                         int nrhs, int apply_d, int apply_lt) {
-  __shared__ double vs_small[1];
-  (void)vs_small;
   const int s = P.lvl_sn[lo + blockIdx.x];
   const int f = X.sn_f[s], p = X.sn_pstore[s];
   const int64_t roff = X.sn_roff[s];
@@ -1510,90 +1522,124 @@ __global__ void __launch_bounds__(kSolveNT) k_bwd_front(DevPlan P, DevFactor X, 
   const bool large = P.sn_fsym[s] >= kLargeMin;
   __shared__ double Ls[32][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int r = 0; r < nrhs; ++r) {
-    double *v = wk + (int64_t)r * rows_total + roff;  // large: v[0:p) holds L21^T x_ext
-    double *xr = x + (int64_t)r * P.n;
-    // D^-1 of each pivot block; 2x2 blocks start where the upper slot
-    // (c, c+1) is nonzero
-    for (int c = threadIdx.x; c < p; c += kSolveNT) {
-      const bool second = apply_d && !posdef && (c > 0) && L[(size_t)c * sf + c - 1] != 0.0;
-      if (second) continue;
-      double y0 = xr[rows[c]];
-      if (!posdef && apply_d) {
-        const double d00 = L[(size_t)c * sf + c];
-        const double d10 = (c + 1 < p) ? L[(size_t)(c + 1) * sf + c] : 0.0;
-        if (d10 != 0.0) {
-          const double d11 = L[(size_t)(c + 1) * sf + c + 1];
-          const double r0 = y0, r1 = xr[rows[c + 1]];
-          const double s2 = max3_ref(fabs(d00), fabs(d10), fabs(d11));
-          double z0 = 0.0, z1 = 0.0;
-          if (isfinite(s2) && s2 != 0.0) {
-            const double a = d00 / s2, bb = d10 / s2, cc = d11 / s2;
-            const double det = __dsub_rn(__dmul_rn(a, cc), __dmul_rn(bb, bb));
-            if (isfinite(det) && det != 0.0) {
-              if (!isfinite(r0) || !isfinite(r1)) {
-                z0 = r0;
-                z1 = r1;
-              } else {
-                const double rs = fmax(fabs(r0), fabs(r1));
-                if (rs != 0.0) {
-                  const double q0 = r0 / rs, q1 = r1 / rs;
-                  const double u0 = __dsub_rn(__dmul_rn(cc, q0), __dmul_rn(bb, q1)) / det;
-                  const double u1 = __dadd_rn(__dmul_rn(-bb, q0), __dmul_rn(a, q1)) / det;
-                  const double ratio = rs / s2;
-                  z0 = __dmul_rn(u0, ratio);
-                  z1 = __dmul_rn(u1, ratio);
-                }
+  // every right-hand side at once. D^-1 of each pivot block; 2x2 blocks
+  // start where the upper slot (c, c+1) is nonzero. (large: v[0:p) holds
+  // L21^T x_ext)
+  for (int64_t t = threadIdx.x; t < (int64_t)p * nrhs; t += kSolveNT) {
+    const int r = (int)(t / p), c = (int)(t % p);
+    double *v = wk + (int64_t)r * rows_total + roff;
+    const double *xr = x + (int64_t)r * P.n;
+    const bool second = apply_d && !posdef && (c > 0) && L[(size_t)c * sf + c - 1] != 0.0;
+    if (second) continue;
+    double y0 = xr[rows[c]];
+    if (!posdef && apply_d) {
+      const double d00 = L[(size_t)c * sf + c];
+      const double d10 = (c + 1 < p) ? L[(size_t)(c + 1) * sf + c] : 0.0;
+      if (d10 != 0.0) {
+        const double d11 = L[(size_t)(c + 1) * sf + c + 1];
+        const double r0 = y0, r1 = xr[rows[c + 1]];
+        const double s2 = max3_ref(fabs(d00), fabs(d10), fabs(d11));
+        double z0 = 0.0, z1 = 0.0;
+        if (isfinite(s2) && s2 != 0.0) {
+          const double a = d00 / s2, bb = d10 / s2, cc = d11 / s2;
+          const double det = __dsub_rn(__dmul_rn(a, cc), __dmul_rn(bb, bb));
+          if (isfinite(det) && det != 0.0) {
+            if (!isfinite(r0) || !isfinite(r1)) {
+              z0 = r0;
+              z1 = r1;
+            } else {
+              const double rs = fmax(fabs(r0), fabs(r1));
+              if (rs != 0.0) {
+                const double q0 = r0 / rs, q1 = r1 / rs;
+                const double u0 = __dsub_rn(__dmul_rn(cc, q0), __dmul_rn(bb, q1)) / det;
+                const double u1 = __dadd_rn(__dmul_rn(-bb, q0), __dmul_rn(a, q1)) / det;
+                const double ratio = rs / s2;
+                z0 = __dmul_rn(u0, ratio);
+                z1 = __dmul_rn(u1, ratio);
               }
             }
           }
-          if (apply_lt && large) {
-            z0 -= v[c];
-            z1 -= v[c + 1];
-          }
-          v[c] = z0;
-          v[c + 1] = z1;
-          continue;
         }
-        y0 = (d00 == 0.0 || !isfinite(d00)) ? 0.0 : y0 / d00;
+        if (apply_lt && large) {
+          z0 -= v[c];
+          z1 -= v[c + 1];
+        }
+        v[c] = z0;
+        v[c + 1] = z1;
+        continue;
       }
-      if (apply_lt && large) y0 -= v[c];
-      v[c] = y0;
+      y0 = (d00 == 0.0 || !isfinite(d00)) ? 0.0 : y0 / d00;
     }
-    __syncthreads();
-    if (!apply_lt) {
-      for (int i = threadIdx.x; i < p; i += kSolveNT) xr[rows[i]] = v[i];
-      __syncthreads();
-      continue;
+    if (apply_lt && large) y0 -= v[c];
+    v[c] = y0;
+  }
+  __syncthreads();
+  if (!apply_lt) {
+    for (int64_t t = threadIdx.x; t < (int64_t)p * nrhs; t += kSolveNT) {
+      const int r = (int)(t / p), i = (int)(t % p);
+      x[(int64_t)r * P.n + rows[i]] = wk[(int64_t)r * rows_total + roff + i];
     }
-    if (large) continue;  // the block kernels (k_bwd_dots / k_bwd_tri) go on
-    {  // v -= L21^T x_ext, warp per column
-      for (int j = warp; j < p; j += kSolveNT / 32) {
-        const double *Lj = L + (size_t)j * sf;
+    return;
+  }
+  if (large) return;  // the block kernels (k_bwd_dots / k_bwd_tri) go on
+  // v -= L21^T x_ext: a warp per column, its lanes' rows loaded once for
+  // every right-hand side
+  for (int j = warp; j < p; j += kSolveNT / 32) {
+    const double *Lj = L + (size_t)j * sf;
+    for (int i0 = p; i0 < f; i0 += 32 * 4) {
+      double l[4];
+      int ri[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + lane + 32 * u;
+        l[u] = (i < f) ? __ldg(Lj + i) : 0.0;
+        ri[u] = (i < f) ? rows[i] : -1;
+      }
+      for (int r = 0; r < nrhs; ++r) {
+        const double *xr = x + (int64_t)r * P.n;
         double acc = 0.0;
-        for (int i = p + lane; i < f; i += 32) acc = fma(Lj[i], xr[rows[i]], acc);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (ri[u] >= 0) acc = fma(l[u], xr[ri[u]], acc);
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) v[j] -= acc;
+        if (lane == 0) wk[(int64_t)r * rows_total + roff + j] -= acc;
       }
-      __syncthreads();
     }
-    // blocked L11^-T: blocks from the end; dots with the solved part, then
-    // the 32 x 32 triangle by one warp
-    for (int je = p; je > 0; je -= 32) {
-      const int jb = max(0, je - 32), nb = je - jb;
-      for (int j = jb + warp; j < je; j += kSolveNT / 32) {
-        const double *Lj = L + (size_t)j * sf;
-        double acc = 0.0;
-        for (int i = je + lane; i < p; i += 32) acc = fma(Lj[i], v[i], acc);
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) v[j] -= acc;
+  }
+  __syncthreads();
+  // blocked L11^-T: blocks from the end; dots with the solved part, then
+  // the 32 x 32 triangle (a warp per right-hand side)
+  for (int je = p; je > 0; je -= 32) {
+    const int jb = max(0, je - 32), nb = je - jb;
+    for (int j = jb + warp; j < je; j += kSolveNT / 32) {
+      const double *Lj = L + (size_t)j * sf;
+      for (int i0 = je; i0 < p; i0 += 32 * 4) {
+        double l[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int i = i0 + lane + 32 * u;
+          l[u] = (i < p) ? __ldg(Lj + i) : 0.0;
+        }
+        for (int r = 0; r < nrhs; ++r) {
+          double *v = wk + (int64_t)r * rows_total + roff;
+          double acc = 0.0;
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int i = i0 + lane + 32 * u;
+            if (i < p) acc = fma(l[u], v[i], acc);
+          }
+          for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+          if (lane == 0) v[j] -= acc;
+        }
       }
-      load_tri32<kSolveNT>(L, sf, jb, nb, Ls);
-      if (warp == 0) tri_bwd_warp(v, jb, nb, posdef, Ls);
-      __syncthreads();
     }
-    for (int i = threadIdx.x; i < p; i += kSolveNT) xr[rows[i]] = v[i];
+    load_tri32<kSolveNT>(L, sf, jb, nb, Ls);
+    for (int r = warp; r < nrhs; r += kSolveNT / 32) tri_bwd_warp(wk + (int64_t)r * rows_total + roff, jb, nb, posdef, Ls);
     __syncthreads();
+  }
+  for (int64_t t = threadIdx.x; t < (int64_t)p * nrhs; t += kSolveNT) {
+    const int r = (int)(t / p), i = (int)(t % p);
+    x[(int64_t)r * P.n + rows[i]] = wk[(int64_t)r * rows_total + roff + i];
   }
 }
 
