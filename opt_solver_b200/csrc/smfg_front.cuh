@@ -1041,11 +1041,98 @@ __device__ void apply_pivot_blk(const FrontRef &v, int &k, bool useW, int w_cols
 
 // deferred_update (ldlt_kernel.cpp:705-761): F[c0:f, c0:e] -= L[c0:f, p0:p1]
 // W[c0:e, :]^T, one fused multiply-add per pivot in order, zero W skipped.
+// (L D)(j, c) as fill_ld_column computes it (ldlt_kernel.cpp:764-818).
+__device__ __forceinline__ double ld_entry(const FrontRef &v, int c, int j) {
+  const size_t sf = (size_t)v.ld;
+  const double *Lc = v.F + (size_t)c * sf;
+  const int8_t tag = v.tags[c];
+  if (tag == 1) return __dmul_rn(Lc[j], Lc[c]);
+  if (tag == 2) return __dadd_rn(__dmul_rn(Lc[j], Lc[c]), __dmul_rn(Lc[sf + j], Lc[c + 1]));
+  if (tag == -1) {
+    const double *L0 = Lc - sf;
+    return __dadd_rn(__dmul_rn(L0[j], L0[c]), __dmul_rn(Lc[j], Lc[c]));
+  }
+  return 0.0;
+}
+
+// The update F[i, j] -= sum over pivots c in [p0, p0 + kk), in order, of
+// L(i, c) B(c, j) on the lower part of rows [c0, f) x columns [c0, cend),
+// B = W (deferred updates) or (L D)^T (Schur), by one block of 512
+// threads on a front in global memory: 64 x 64 tiles one after the other,
+// 16 pivots of L and B staged in shared memory at a time (B computed once
+// per tile column and chunk instead of once per entry), 8 entries a thread.
+// Every entry keeps its chain c = fma(-l, b, c) over the pivots in order
+// (b = 0 skipped): the loops it replaces give the same bits.
+template <bool SCHUR>
+__device__ void front_update_tiles(const FrontRef &v, int c0, int cend, int p0, int kk) {
+  constexpr int T = 64, KC = 16;
+  __shared__ double As[KC][T], Bs[KC][T];
+  const int f = v.f;
+  const size_t sf = (size_t)v.ld;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;  // rows tx + 16 r, columns ty + 32 q
+  const int rt = (f - c0 + T - 1) / T, ct = (cend - c0 + T - 1) / T;
+  for (int tj = 0; tj < ct; ++tj) {
+    for (int ti = tj; ti < rt; ++ti) {
+      const int i0 = c0 + ti * T, j0 = c0 + tj * T;
+      double c[4][2];
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int i = i0 + tx + 16 * r, j = j0 + ty + 32 * q;
+          c[r][q] = (i < f && j < cend && i >= j) ? v.F[(size_t)j * sf + i] : 0.0;
+        }
+      for (int k0 = 0; k0 < kk; k0 += KC) {
+        const int kc = min(KC, kk - k0);
+        __syncthreads();  // the previous chunk's readers are done
+#pragma unroll
+        for (int u = 0; u < KC * T / 512; ++u) {
+          const int t = tid + 512 * u, pp = t >> 6, x = t & 63;
+          As[pp][x] = (pp < kc && i0 + x < f) ? v.F[(size_t)(p0 + k0 + pp) * sf + i0 + x] : 0.0;
+          double bval = 0.0;
+          if (pp < kc && j0 + x < cend) {
+            if constexpr (SCHUR) bval = ld_entry(v, p0 + k0 + pp, j0 + x);
+            else bval = v.W[(size_t)(k0 + pp) * f + j0 + x];
+          }
+          Bs[pp][x] = bval;
+        }
+        __syncthreads();
+        for (int pp = 0; pp < kc; ++pp) {
+          double av[4], bv[2];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) av[r] = As[pp][tx + 16 * r];
+#pragma unroll
+          for (int q = 0; q < 2; ++q) bv[q] = Bs[pp][ty + 32 * q];
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            if (bv[q] != 0.0) {
+#pragma unroll
+              for (int r = 0; r < 4; ++r) c[r][q] = fma(-av[r], bv[q], c[r][q]);
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int i = i0 + tx + 16 * r, j = j0 + ty + 32 * q;
+          if (i < f && j < cend && i >= j) v.F[(size_t)j * sf + i] = c[r][q];
+        }
+    }
+  }
+  __syncthreads();
+}
+
 template <int NT>
 __device__ void deferred_update_blk(const FrontRef &v, int p0, int p1, int c0, int e) {
   using LY = Lay<NT>;
   const int jb = p1 - p0;
   if (jb <= 0 || e - c0 <= 0) return;
+  if constexpr (NT == 512) {  // fronts in global memory: tiles staged in shared memory
+    front_update_tiles<false>(v, c0, e, p0, jb);
+    return;
+  }
   const size_t sf = (size_t)v.ld;
   const int f = v.f;
   for (int i = c0 + LY::r(); i < f; i += LY::RB) {
@@ -1063,19 +1150,6 @@ __device__ void deferred_update_blk(const FrontRef &v, int p0, int p1, int c0, i
   __syncthreads();
 }
 
-// (L D)(j, c) as fill_ld_column computes it (ldlt_kernel.cpp:764-818).
-__device__ __forceinline__ double ld_entry(const FrontRef &v, int c, int j) {
-  const size_t sf = (size_t)v.ld;
-  const double *Lc = v.F + (size_t)c * sf;
-  const int8_t tag = v.tags[c];
-  if (tag == 1) return __dmul_rn(Lc[j], Lc[c]);
-  if (tag == 2) return __dadd_rn(__dmul_rn(Lc[j], Lc[c]), __dmul_rn(Lc[sf + j], Lc[c + 1]));
-  if (tag == -1) {
-    const double *L0 = Lc - sf;
-    return __dadd_rn(__dmul_rn(L0[j], L0[c]), __dmul_rn(Lc[j], Lc[c]));
-  }
-  return 0.0;
-}
 
 // schur_update (ldlt_kernel.cpp:820-933): F[e:f, e:f] -= L LD^T over the
 // pivots [p0, p) in order.
@@ -1084,6 +1158,10 @@ __device__ void schur_update_blk(const FrontRef &v, int p0, int p, int e) {
   using LY = Lay<NT>;
   const int f = v.f;
   if (p <= p0 || f - e <= 0) return;
+  if constexpr (NT == 512) {  // fronts in global memory: tiles staged in shared memory
+    front_update_tiles<true>(v, e, f, p0, p - p0);
+    return;
+  }
   const size_t sf = (size_t)v.ld;
   for (int i = e + LY::r(); i < f; i += LY::RB) {
     for (int j = e + LY::g(); j <= i; j += LY::G) {
