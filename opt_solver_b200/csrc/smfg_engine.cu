@@ -74,8 +74,12 @@ int sm_count(int dev) {
 }
 
 // Dynamic shared memory of the in-shared-memory front kernels.
-size_t front_smem_bytes(int fmax, int nb) {
-  return (size_t)fmax * fmax * 8 + (size_t)fmax * nb * 8 + (size_t)fmax * 12 + (size_t)fmax + 64;
+// Shared memory of a front of at most fmax rows factored in shared memory:
+// F, W (only when the blocked path can run: fmax >= blocked_min_front),
+// rows, positions and tags.
+size_t front_smem_bytes(int fmax, int nb, int blocked_min_front = 0) {
+  const size_t w = (fmax >= blocked_min_front) ? (size_t)fmax * nb * 8 : 0;
+  return (size_t)fmax * fmax * 8 + w + (size_t)fmax * 12 + (size_t)fmax + 64;
 }
 
 }  // namespace
@@ -512,18 +516,25 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
   lc.n += 2;
   PivotParams prm{c.u, c.small_pivot, c.small_pivot, c.nb, c.blocked_min_front, c.posdef};
   const MixedCfg mc = mixed_cfg(c);
-  const size_t smem_s = front_smem_bytes(kSmallMax, c.nb);
-  const size_t smem_m = front_smem_bytes(kMediumMax, c.nb);
+  // the shared-memory front kernels by size bucket: each launch's shared
+  // memory sized to its bucket (more blocks per SM for the many small fronts)
+  const int bmf = c.blocked_min_front;
+  const size_t smem_s32 = front_smem_bytes(32, c.nb, bmf), smem_s48 = front_smem_bytes(48, c.nb, bmf);
+  const size_t smem_s64 = front_smem_bytes(kSmallMax, c.nb, bmf);
+  const size_t smem_m96 = front_smem_bytes(96, c.nb, bmf), smem_m128 = front_smem_bytes(kMediumMax, c.nb, bmf);
   for (int l = 0; l < pl.nlevels; ++l) {
     const int lo = pl.lvl_ptr[l], hi = pl.lvl_ptr[l + 1], m = hi - lo;
     k_level_setup<1024><<<1, 1024, 0, st>>>(d, x, lo, hi, l, c.nb);
     k_level_rows<<<m, 128, 0, st>>>(d, x, lo, hi);
     const int asm_grid = std::max(1, std::min(4 * sms, m * 64));
     k_level_assemble<<<asm_grid, 256, 0, st>>>(d, x, lo, hi, l);
-    k_factor<32, 1, kSmallMax, true><<<m, 32, smem_s, st>>>(d, x, lo, hi, prm);
-    k_factor<128, kSmallMax + 1, kMediumMax, true><<<m, 128, smem_m, st>>>(d, x, lo, hi, prm);
+    k_factor<32, 1, 32, true><<<m, 32, smem_s32, st>>>(d, x, lo, hi, prm);
+    k_factor<32, 33, 48, true><<<m, 32, smem_s48, st>>>(d, x, lo, hi, prm);
+    k_factor<32, 49, kSmallMax, true><<<m, 32, smem_s64, st>>>(d, x, lo, hi, prm);
+    k_factor<128, kSmallMax + 1, 96, true><<<m, 128, smem_m96, st>>>(d, x, lo, hi, prm);
+    k_factor<128, 97, kMediumMax, true><<<m, 128, smem_m128, st>>>(d, x, lo, hi, prm);
     k_factor<512, kMediumMax + 1, 1 << 30, false><<<m, 512, 0, st>>>(d, x, lo, hi, prm);
-    lc.n += 6;
+    lc.n += 9;
     const int nL = pl.lvl_large_ptr[l + 1] - pl.lvl_large_ptr[l];
     if (nL > 0) {
       const int *lg = d.lvl_large + pl.lvl_large_ptr[l];
@@ -618,11 +629,16 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
 static void set_kernel_attrs(int nb) {
   static int done_nb = -1;
   if (done_nb == nb) return;
-  SMFG_CUDA(cudaFuncSetAttribute(k_factor<32, 1, kSmallMax, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+  // (the with-W sizes: launches ask for at most these)
+  SMFG_CUDA(cudaFuncSetAttribute(k_factor<32, 1, 32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)front_smem_bytes(32, nb)));
+  SMFG_CUDA(cudaFuncSetAttribute(k_factor<32, 33, 48, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)front_smem_bytes(48, nb)));
+  SMFG_CUDA(cudaFuncSetAttribute(k_factor<32, 49, kSmallMax, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)front_smem_bytes(kSmallMax, nb)));
-  SMFG_CUDA(cudaFuncSetAttribute(k_factor<128, kSmallMax + 1, kMediumMax, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+  SMFG_CUDA(cudaFuncSetAttribute(k_factor<128, kSmallMax + 1, 96, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_smem_bytes(96, nb)));
+  SMFG_CUDA(cudaFuncSetAttribute(k_factor<128, 97, kMediumMax, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)front_smem_bytes(kMediumMax, nb)));
   SMFG_CUDA(cudaFuncSetAttribute(k_large_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem)));
   SMFG_CUDA(cudaFuncSetAttribute(tc::k_tc_syrk<tc::kTF32x3>, cudaFuncAttributeMaxDynamicSharedMemorySize,

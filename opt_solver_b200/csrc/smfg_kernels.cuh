@@ -198,18 +198,25 @@ __global__ void k_level_assemble(DevPlan P, DevFactor X, int lo, int hi, int lvl
     const int j1 = min(j0 + kAsmCols, f);
     double *F = X.arena + X.sn_off[s];
     const size_t sf = (size_t)f;
+    // (the loops below run over (column, row) pairs of the item, so small
+    // fronts keep every thread busy)
     // 1. zero the lower part of columns [j0, j1)
-    for (int jj = j0; jj < j1; ++jj)
-      for (int i = jj + threadIdx.x; i < f; i += blockDim.x) F[jj * sf + i] = 0.0;
+    for (int t = threadIdx.x; t < (j1 - j0) * f; t += blockDim.x) {
+      const int jj = j0 + t / f, i = t % f;
+      if (i >= jj) F[jj * sf + i] = 0.0;
+    }
     __syncthreads();
-    // 2. original entries of the pivot columns in [j0, j1)
+    // 2. original entries of the pivot columns in [j0, j1): their slots are
+    // one contiguous range (consecutive columns), each slot a distinct entry
     const int cs = P.sn_start[s], wdt = P.sn_width[s];
     const int ca = max(j0 - nd, 0), cb = min(j1 - nd, wdt);
-    for (int c = ca; c < cb; ++c) {
-      const int jcol = cs + c;
-      const int colpos = nd + c;
-      for (int k = P.pcp[jcol] + threadIdx.x; k < P.pcp[jcol + 1]; k += blockDim.x)
-        F[colpos * sf + nd + P.amap[k]] += X.pv[k];
+    if (ca < cb) {
+      const int k0 = P.pcp[cs + ca], k1 = P.pcp[cs + cb];
+      for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+        int c = ca;  // the column of slot k (at most kAsmCols candidates)
+        while (c + 1 < cb && P.pcp[cs + c + 1] <= k) ++c;
+        F[(nd + c) * sf + nd + P.amap[k]] += X.pv[k];
+      }
     }
     __syncthreads();
     // 3. children in order
@@ -239,18 +246,16 @@ __global__ void k_level_assemble(DevPlan P, DevFactor X, int lo, int hi, int lvl
       const int ja = rng[0], jb = rng[1];
       const double *Fc = X.arena + X.sn_off[c];
       const size_t sfc = (size_t)fc;
-      for (int jj = ja; jj < jb; ++jj) {
-        const int lj = cmap[jj];
-        const double *src = Fc + (size_t)(pc + jj) * sfc + pc;
-        double *dst = F + (size_t)lj * sf;
-        for (int ii = jj + threadIdx.x; ii < q; ii += blockDim.x) {
-          const int li = cmap[ii];
-          if (li < lj) {
-            set_flag(cnt, kFMap);
-            continue;
-          }
-          dst[li] += src[ii];
+      // (column, row) pairs of the child's block; its targets are distinct
+      for (int t = threadIdx.x; t < (jb - ja) * q; t += blockDim.x) {
+        const int jj = ja + t / q, ii = t % q;
+        if (ii < jj) continue;
+        const int lj = cmap[jj], li = cmap[ii];
+        if (li < lj) {
+          set_flag(cnt, kFMap);
+          continue;
         }
+        F[(size_t)lj * sf + li] += Fc[(size_t)(pc + jj) * sfc + pc + ii];
       }
       __syncthreads();
     }
@@ -286,9 +291,12 @@ __device__ void factor_one_front(DevPlan &P, DevFactor &X, int s, const PivotPar
   v.ne = ne;
   int *inv;
   if (SMEM) {
+    // F, then W only where the blocked path runs (the launch's shared
+    // memory holds W only for buckets that can reach it), then the ints
+    const bool blocked = f >= prm0.blocked_min_front && nb > 1;
     double *F = smem;
     double *W = F + sf * sf;
-    int *rows = (int *)(W + sf * nb);
+    int *rows = (int *)(W + (blocked ? sf * nb : 0));
     int *loc = rows + f;
     inv = loc + f;
     int8_t *tags = (int8_t *)(inv + f);
