@@ -282,6 +282,7 @@ def dgemm_peak_tflops():
 
 
 OMEGA_GATE = 1e-12  # the metric's scaled backward error bar
+GRAPH_REPLAY = {"kkt3": False}  # configurations whose steps replay a CUDA graph (default: yes)
 
 
 def run_ours(args, rank, world, local):
@@ -299,6 +300,10 @@ def run_ours(args, rank, world, local):
     d_b0 = torch.from_numpy(np.ascontiguousarray(wl.b)).cuda()
     d_x = d_b0.clone()
     arms = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    # the refactor of an unchanged pattern replays the captured factor
+    # sequence (the first warm-up step captures); the 96,000-row KKT's
+    # pivoting runs too many data-dependent steps for a fixed-budget graph
+    use_graph = GRAPH_REPLAY.get(args.config, True)
     head = "mixed" if "mixed" in arms else "fp64"
     res = {}
     clocks = None
@@ -306,7 +311,7 @@ def run_ours(args, rank, world, local):
         prec = smfg.PREC_MIXED if arm == "mixed" else smfg.PREC_FP64
 
         def step():
-            info = sv.factor(d_vals, posdef=posdef, precision=prec, scale=wl.scale)
+            info = sv.factor(d_vals, posdef=posdef, precision=prec, scale=wl.scale, graph=use_graph)
             d_x.copy_(d_b0)
             sv.solve(d_x)
             eta, om, its = sv.refine_device(d_b0, d_x, nrhs=wl.nrhs, max_steps=args.refine_max,
@@ -347,10 +352,13 @@ def run_ours(args, rank, world, local):
     # e2e: host buffers through the C ABI (copies inside the timed region)
     prec = smfg.PREC_MIXED if head == "mixed" else smfg.PREC_FP64
     e2e = []
+    # one untimed call first: it captures the factor graph for the staged
+    # host values (the timed calls replay it, as a refactor loop would)
+    sv.factor(wl.values, posdef=posdef, precision=prec, scale=wl.scale, graph=use_graph)
     for _ in range(max(2, min(args.steps, 5))):
         torch.cuda.synchronize()
         t = time.perf_counter()
-        sv.factor(wl.values, posdef=posdef, precision=prec, scale=wl.scale)
+        sv.factor(wl.values, posdef=posdef, precision=prec, scale=wl.scale, graph=use_graph)
         x = sv.solve(wl.b)
         x, _, _, _ = sv.refine(wl.b, x, max_steps=args.refine_max, omega_target=OMEGA_GATE,
                                method=smfg.REFINE_AUTO)
@@ -361,6 +369,7 @@ def run_ours(args, rank, world, local):
     return {
         "arms": res, "head": head, "e2e_ms": e2e_ms, "e2e_eta": eta, "e2e_omega": om,
         "analyse_s": wl.analyse_s, "n": wl.n, "nnz": wl.nnz, "nrhs": wl.nrhs, "desc": wl.desc,
+        "graph": use_graph,
         "ordering": getattr(wl, "ordering", "engine nested dissection (smfg_analyse)"),
         "clocks": clocks, "nsn": wl.nsn, "systems": wl.systems,
         "h2d": wl.nnz * 8 + wl.n * wl.nrhs * 8, "d2h": wl.n * wl.nrhs * 8, "profile": prof,
@@ -707,6 +716,7 @@ def main():
                    "precision": head, "omega_gate": OMEGA_GATE,
                    "step": "factor + solve + refinement (auto) to eta_inf <= 1e-10, omega <= 1e-12",
                    "parallelism": ("systems sharded over ranks" if batch else "replicas") if world > 1 else "1 GPU",
+                   "factor_graph_replay": r["graph"],
                    "l2": "inputs larger than L2 (front arena %.1f GB)" % (prof.get("arena_bytes", 0) / 1e9)},
         "e2e": {"value": r["e2e_ms"], "unit": "ms", "h2d_bytes_per_step": r["h2d"],
                 "d2h_bytes_per_step": r["d2h"], "omega": r["e2e_omega"]},
