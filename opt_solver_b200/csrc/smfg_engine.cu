@@ -520,7 +520,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
   // memory sized to its bucket (more blocks per SM for the many small fronts)
   const int bmf = c.blocked_min_front;
   const size_t smem_s32 = front_smem_bytes(32, c.nb, bmf), smem_s48 = front_smem_bytes(48, c.nb, bmf);
-  const size_t smem_s64 = front_smem_bytes(kSmallMax, c.nb, bmf);
+  const size_t smem_s56 = front_smem_bytes(56, c.nb, bmf), smem_s64 = front_smem_bytes(kSmallMax, c.nb, bmf);
   const size_t smem_m96 = front_smem_bytes(96, c.nb, bmf), smem_m128 = front_smem_bytes(kMediumMax, c.nb, bmf);
   for (int l = 0; l < pl.nlevels; ++l) {
     const int lo = pl.lvl_ptr[l], hi = pl.lvl_ptr[l + 1], m = hi - lo;
@@ -530,11 +530,12 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
     k_level_assemble<<<asm_grid, 256, 0, st>>>(d, x, lo, hi, l);
     k_factor<32, 1, 32, true><<<m, 32, smem_s32, st>>>(d, x, lo, hi, prm);
     k_factor<32, 33, 48, true><<<m, 32, smem_s48, st>>>(d, x, lo, hi, prm);
-    k_factor<32, 49, kSmallMax, true><<<m, 32, smem_s64, st>>>(d, x, lo, hi, prm);
+    k_factor<32, 49, 56, true><<<m, 32, smem_s56, st>>>(d, x, lo, hi, prm);
+    k_factor<32, 57, kSmallMax, true><<<m, 32, smem_s64, st>>>(d, x, lo, hi, prm);
     k_factor<128, kSmallMax + 1, 96, true><<<m, 128, smem_m96, st>>>(d, x, lo, hi, prm);
     k_factor<128, 97, kMediumMax, true><<<m, 128, smem_m128, st>>>(d, x, lo, hi, prm);
     k_factor<512, kMediumMax + 1, 1 << 30, false><<<m, 512, 0, st>>>(d, x, lo, hi, prm);
-    lc.n += 9;
+    lc.n += 10;
     const int nL = pl.lvl_large_ptr[l + 1] - pl.lvl_large_ptr[l];
     if (nL > 0) {
       const int *lg = d.lvl_large + pl.lvl_large_ptr[l];
@@ -634,7 +635,9 @@ static void set_kernel_attrs(int nb) {
                                  (int)front_smem_bytes(32, nb)));
   SMFG_CUDA(cudaFuncSetAttribute(k_factor<32, 33, 48, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)front_smem_bytes(48, nb)));
-  SMFG_CUDA(cudaFuncSetAttribute(k_factor<32, 49, kSmallMax, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  SMFG_CUDA(cudaFuncSetAttribute(k_factor<32, 49, 56, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)front_smem_bytes(56, nb)));
+  SMFG_CUDA(cudaFuncSetAttribute(k_factor<32, 57, kSmallMax, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)front_smem_bytes(kSmallMax, nb)));
   SMFG_CUDA(cudaFuncSetAttribute(k_factor<128, kSmallMax + 1, 96, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_smem_bytes(96, nb)));

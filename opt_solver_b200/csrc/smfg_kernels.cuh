@@ -246,16 +246,37 @@ __global__ void k_level_assemble(DevPlan P, DevFactor X, int lo, int hi, int lvl
       const int ja = rng[0], jb = rng[1];
       const double *Fc = X.arena + X.sn_off[c];
       const size_t sfc = (size_t)fc;
-      // (column, row) pairs of the child's block; its targets are distinct
-      for (int t = threadIdx.x; t < (jb - ja) * q; t += blockDim.x) {
-        const int jj = ja + t / q, ii = t % q;
-        if (ii < jj) continue;
-        const int lj = cmap[jj], li = cmap[ii];
-        if (li < lj) {
-          set_flag(cnt, kFMap);
-          continue;
+      // (column, row) pairs of the child's block, four a thread in flight;
+      // its targets are distinct
+      const int np2 = (jb - ja) * q;
+      for (int t0 = threadIdx.x; t0 < np2; t0 += 4 * (int)blockDim.x) {
+        double sv[4], dv[4];
+        size_t di[4];
+        bool ok[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int t = t0 + u * (int)blockDim.x;
+          ok[u] = false;
+          di[u] = 0;
+          sv[u] = dv[u] = 0.0;
+          if (t < np2) {
+            const int jj = ja + t / q, ii = t % q;
+            if (ii >= jj) {
+              const int lj = cmap[jj], li = cmap[ii];
+              if (li < lj) {
+                set_flag(cnt, kFMap);
+              } else {
+                ok[u] = true;
+                di[u] = (size_t)lj * sf + li;
+                sv[u] = Fc[(size_t)(pc + jj) * sfc + pc + ii];
+                dv[u] = F[di[u]];
+              }
+            }
+          }
         }
-        F[(size_t)lj * sf + li] += Fc[(size_t)(pc + jj) * sfc + pc + ii];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (ok[u]) F[di[u]] = dv[u] + sv[u];
       }
       __syncthreads();
     }
@@ -1006,12 +1027,26 @@ __global__ void __launch_bounds__(256) k_large_store(DevPlan P, DevFactor X, con
       if (posdef) {
         if (threadIdx.x < c1 - c0) sdv[threadIdx.x] = sqrt(F[(size_t)(c0 + threadIdx.x) * sf + c0 + threadIdx.x]);
         __syncthreads();
-        for (int c = c0; c < c1; ++c) {
-          double *Lc = F + (size_t)c * sf;
-          const double sd = sdv[c - c0];
-          for (int i = threadIdx.x; i < f; i += 256) {
-            if (i < c) Lc[i] = 0.0;
-            else if (i > c) Lc[i] = __dmul_rn(Lc[i], sd);
+        // the item's columns as one run of (column, row) pairs (columns are
+        // contiguous, leading dimension f), eight entries a thread in flight
+        double *base = F + (size_t)c0 * sf;
+        const int64_t n = (int64_t)(c1 - c0) * f;
+        for (int64_t t0 = threadIdx.x; t0 < n; t0 += 8 * 256) {
+          double y[8];
+          int cc[8], ii[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int64_t t = t0 + 256 * u;
+            cc[u] = c0 + (int)(t / f);
+            ii[u] = (int)(t % f);
+            y[u] = (t < n && ii[u] > cc[u]) ? base[t] : 0.0;  // the strictly lower part is read
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int64_t t = t0 + 256 * u;
+            if (t >= n) continue;
+            if (ii[u] < cc[u]) base[t] = 0.0;
+            else if (ii[u] > cc[u]) base[t] = __dmul_rn(y[u], sdv[cc[u] - c0]);
           }
         }
         __syncthreads();
