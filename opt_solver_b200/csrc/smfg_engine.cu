@@ -386,11 +386,20 @@ constexpr int kTcEvery = 16;
 
 // Deferred updates of a level's large fronts: the streamed kernel for
 // panels of up to 16 pivots, the general tiled one beyond.
-static void launch_defer(Plan &pl, const int *lg, int nL, const TppState *states, int ggrid) {
+static void launch_defer(Plan &pl, const int *lg, int nL, const TppState *states, int ggrid, int mode = 0,
+                         cudaStream_t stream = nullptr) {
+  cudaStream_t st = stream ? stream : pl.stream;
   if (pl.nb <= kDK)
-    k_large_defer<<<kDBlocksPerSM * sm_count(pl.device), 256, 0, pl.stream>>>(pl.d, pl.x, lg, nL, states);
+    k_large_defer<<<kDBlocksPerSM * sm_count(pl.device), 256, 0, st>>>(pl.d, pl.x, lg, nL, states, mode);
   else
-    k_large_gemm<<<ggrid, 256, sizeof(TileSmem), pl.stream>>>(pl.d, pl.x, lg, nL, states);
+    k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(pl.d, pl.x, lg, nL, states);
+}
+
+// SPD large fronts factor with look-ahead (two streams, two W buffers per
+// front) when the panels are 16 wide, the plan has its second stream, and
+// no profile asks for per-kernel timing.
+static bool lookahead(const Plan &pl, const smfg_control_t &c, bool profiling) {
+  return c.posdef && c.nb == 16 && pl.stream2 != nullptr && !profiling;
 }
 
 // Team size (CTAs per front) of a level's indefinite large-front panels, by
@@ -516,6 +525,8 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
   lc.n += 2;
   PivotParams prm{c.u, c.small_pivot, c.small_pivot, c.nb, c.blocked_min_front, c.posdef};
   const MixedCfg mc = mixed_cfg(c);
+  // W columns per front in the arena: two buffers under look-ahead
+  const int wcols = lookahead(pl, c, gp.on) ? 2 * c.nb : c.nb;
   // the shared-memory front kernels by size bucket: each launch's shared
   // memory sized to its bucket (more blocks per SM for the many small fronts)
   const int bmf = c.blocked_min_front;
@@ -524,7 +535,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
   const size_t smem_m96 = front_smem_bytes(96, c.nb, bmf), smem_m128 = front_smem_bytes(kMediumMax, c.nb, bmf);
   for (int l = 0; l < pl.nlevels; ++l) {
     const int lo = pl.lvl_ptr[l], hi = pl.lvl_ptr[l + 1], m = hi - lo;
-    k_level_setup<1024><<<1, 1024, 0, st>>>(d, x, lo, hi, l, c.nb);
+    k_level_setup<1024><<<1, 1024, 0, st>>>(d, x, lo, hi, l, wcols);
     k_level_rows<<<m, 128, 0, st>>>(d, x, lo, hi);
     const int asm_grid = std::max(1, std::min(4 * sms, m * 64));
     k_level_assemble<<<asm_grid, 256, 0, st>>>(d, x, lo, hi, l);
@@ -554,18 +565,36 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
         // double-buffered; the closing step leaves phase 2
         const int steps = (pl.lvl_large_maxw[l] + c.nb - 1) / c.nb + 1;
         const dim3 pgrid((pl.lvl_large_maxf[l] + 255) / 256, nL);
+        // look-ahead (unless profiling): each panel's update of the next
+        // panel's 16 columns runs on the stream before the next panel, the
+        // rest on stream2 alongside it; every entry still takes its updates
+        // in pivot order (the next-columns update waits for the previous
+        // rest update), and the two W buffers alternate so that a panel
+        // never overwrites the W a running rest update reads
+        const bool ahead = lookahead(pl, c, gp.on);
         for (; it < steps; ++it) {
           TppState *cur = x.tpp + (size_t)(it & 1) * pl.max_large;
           TppState *nxt = x.tpp + (size_t)((it + 1) & 1) * pl.max_large;
           gp.mark(st, 2);
-          k_large_panel_spd<16><<<pgrid, 256, 0, st>>>(d, x, lg, cur, nxt, it);
+          k_large_panel_spd<16><<<pgrid, 256, 0, st>>>(d, x, lg, cur, nxt, it, ahead ? 1 : 0);
           gp.mark(st, 2);
-          gp.mark(st);
-          launch_defer(pl, lg, nL, nxt, ggrid);
-          gp.mark(st);
+          if (ahead) {
+            SMFG_CUDA(cudaEventRecord(pl.ev_panel, st));
+            if (it > 0) SMFG_CUDA(cudaStreamWaitEvent(st, pl.ev_rest, 0));
+            launch_defer(pl, lg, nL, nxt, ggrid, 1);
+            SMFG_CUDA(cudaStreamWaitEvent(pl.stream2, pl.ev_panel, 0));
+            launch_defer(pl, lg, nL, nxt, ggrid, 2, pl.stream2);
+            SMFG_CUDA(cudaEventRecord(pl.ev_rest, pl.stream2));
+            lc.n += 1;
+          } else {
+            gp.mark(st);
+            launch_defer(pl, lg, nL, nxt, ggrid);
+            gp.mark(st);
+          }
           if (lvl_mixed && ((it + 1) * c.nb % mc.nbo == 0 || it == steps - 1))
             enqueue_tc(pl, mc, lg, nL, nxt, c.posdef, lc, gp);
         }
+        if (ahead) SMFG_CUDA(cudaStreamWaitEvent(st, pl.ev_rest, 0));  // join before the Schur update
         fin = x.tpp + (size_t)(steps & 1) * pl.max_large;
         lc.n += 2 * steps;
       } else if (c.posdef) {
@@ -658,7 +687,9 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
   pl.nb = std::max(2, c.nb);
   set_kernel_attrs(pl.nb);
   // arena: exact for SPD (no delays); head-room for delays, regrown on overflow
-  const int64_t base_a = pl.sum_f2, base_r = pl.sum_f;
+  // (look-ahead: a second W buffer, nb columns more per front)
+  const int64_t base_a = pl.sum_f2 + (lookahead(pl, c, c.profile != 0) ? pl.sum_f * (int64_t)c.nb : 0),
+                base_r = pl.sum_f;
   int64_t need_a = c.posdef ? base_a : base_a + base_a / 4 + (int64_t)pl.max_fsym * pl.max_fsym * 2 + 4096;
   int64_t need_r = c.posdef ? base_r : base_r + base_r / 2 + 4096;
   // mixed fronts: large, at least min_front rows, allowed by the caller's mask
@@ -1018,6 +1049,9 @@ SMFG_API int smfg_plan_create(const smfg_analysis_t *a, int device, smfg_plan_t 
     SMFG_CUDA(cudaEventCreate(&h->pl.ev0));
     SMFG_CUDA(cudaEventCreate(&h->pl.ev1));
     SMFG_CUDA(cudaEventCreateWithFlags(&h->pl.ev_in, cudaEventDisableTiming));
+    SMFG_CUDA(cudaStreamCreateWithFlags(&h->pl.stream2, cudaStreamNonBlocking));
+    SMFG_CUDA(cudaEventCreateWithFlags(&h->pl.ev_panel, cudaEventDisableTiming));
+    SMFG_CUDA(cudaEventCreateWithFlags(&h->pl.ev_rest, cudaEventDisableTiming));
     {
       cudaMemPoolProps props = {};
       props.allocType = cudaMemAllocationTypePinned;
@@ -1061,6 +1095,10 @@ SMFG_API void smfg_plan_destroy(smfg_plan_t *plan) {
   if (pl.ev1) cudaEventDestroy(pl.ev1);
   if (pl.ev_in) cudaEventDestroy(pl.ev_in);
   if (pl.graph_exec) cudaGraphExecDestroy(pl.graph_exec);
+  if (pl.stream2) cudaStreamSynchronize(pl.stream2);
+  if (pl.ev_panel) cudaEventDestroy(pl.ev_panel);
+  if (pl.ev_rest) cudaEventDestroy(pl.ev_rest);
+  if (pl.stream2) cudaStreamDestroy(pl.stream2);
   if (pl.stream) cudaStreamDestroy(pl.stream);
   if (pl.pool) cudaMemPoolDestroy(pl.pool);
   delete *plan;
@@ -1878,7 +1916,7 @@ extern "C" SMFG_API int smfg_kernel_bench_defer(int f, int ne, int k, int reps, 
     for (int r = 0; r <= reps; ++r) {
       SMFG_CUDA(cudaMemcpy(arena, orig, nel * 8, cudaMemcpyDeviceToDevice));
       SMFG_CUDA(cudaEventRecord(e0));
-      k_large_defer<<<kDBlocksPerSM * sms, 256>>>(P, X, large, 1, tpp);
+      k_large_defer<<<kDBlocksPerSM * sms, 256>>>(P, X, large, 1, tpp, 0);
       SMFG_CUDA(cudaEventRecord(e1));
       SMFG_CUDA(cudaEventSynchronize(e1));
       SMFG_CUDA(cudaGetLastError());

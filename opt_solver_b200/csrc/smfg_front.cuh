@@ -1203,6 +1203,7 @@ __device__ __forceinline__ void tpp_init(TppState &S, int ne, bool posdef, bool 
   S.post = 0;
   S.ps = S.pl = S.stalled = 0;
   S.g_p0 = S.g_p1 = S.g_c0 = S.g_e = 0;
+  S.pad[0] = S.pad[1] = S.pad[2] = S.pad[3] = 0;  // [0] update pending, [1] its W buffer
   S.mixed = mixed ? 1 : 0;
   S.tc_done = 0;
   // SPD: outer blocks of nbo pivots; indefinite: every eligible column

@@ -98,6 +98,10 @@ struct Plan {
   cudaMemPool_t pool = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t ev_in = nullptr;  // orders the stream after the caller's default-stream work
+  // SPD look-ahead: the deferred updates past the next panel run on stream2
+  // while the next panel factors (events: a panel done, a rest update done)
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_panel = nullptr, ev_rest = nullptr;
   // last factorization
   bool factored = false;
   int posdef = 0;

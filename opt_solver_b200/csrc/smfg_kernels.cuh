@@ -792,14 +792,17 @@ __device__ __forceinline__ void defer_tile(int w, int rows, int &ti, int &tj) {
   ti = (int)(t + (w - S(t)));
 }
 
+// mode: 0 the whole update, 1 only the next panel's 16 columns [c0, c0 + 16),
+// 2 only the columns past them (look-ahead)
 __global__ void __launch_bounds__(256, kDBlocksPerSM) k_large_defer(DevPlan P, DevFactor X,
                                                                     const int *__restrict__ large, int nlarge,
-                                                                    const TppState *__restrict__ tpp) {
+                                                                    const TppState *__restrict__ tpp, int mode) {
   __shared__ double Ls[kDK][kDT];  // [pivot][row of the tile]
   __shared__ double Ws[kDK][kDT];  // [pivot][column of the tile]
   __shared__ int pref[kDFronts + 1];
   __shared__ int m_f[kDFronts], m_c0[kDFronts], m_e[kDFronts], m_p0[kDFronts], m_kk[kDFronts];
   __shared__ long long m_off[kDFronts];
+  __shared__ int m_wo[kDFronts];
   __shared__ int wsum[8];
   if (X.counters[kCFlags] & kFAbort) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -812,13 +815,18 @@ __global__ void __launch_bounds__(256, kDBlocksPerSM) k_large_defer(DevPlan P, D
       const TppState &S = tpp[chunk + tid];
       const int s = large[chunk + tid];
       const int f = X.sn_f[s];
-      if (S.pad[0] && S.g_p1 > S.g_p0 && S.g_e > S.g_c0) nt = defer_tiles(f - S.g_c0, S.g_e - S.g_c0);
+      // the columns of this launch's share of the update
+      const int split = min(S.g_e, S.g_c0 + kDK);
+      const int cs = mode == 2 ? split : S.g_c0, ce = mode == 1 ? split : S.g_e;
+      if (S.pad[0] && S.g_p1 > S.g_p0 && ce > cs) nt = defer_tiles(f - cs, ce - cs);
       m_f[tid] = f;
-      m_c0[tid] = S.g_c0;
-      m_e[tid] = S.g_e;
+      m_c0[tid] = cs;
+      m_e[tid] = ce;
       m_p0[tid] = S.g_p0;
       m_kk[tid] = S.g_p1 - S.g_p0;
+      // (W of the panel: the second buffer for odd look-ahead panels)
       m_off[tid] = (long long)X.sn_off[s];
+      m_wo[tid] = S.pad[1];
     }
     // inclusive block scan of the tile counts
     int v = nt;
@@ -848,7 +856,7 @@ __global__ void __launch_bounds__(256, kDBlocksPerSM) k_large_defer(DevPlan P, D
       const int f = m_f[a], e = m_e[a], kk = m_kk[a], p0 = m_p0[a];
       const size_t sf = (size_t)f;
       double *F = X.arena + m_off[a];
-      const double *Wp = F + sf * sf;
+      const double *Wp = F + sf * sf + (size_t)m_wo[a] * kDK * sf;
       const int i0 = m_c0[a] + ti * kDT, j0 = m_c0[a] + tj * kDT;
       double c[4][4];
 #pragma unroll
@@ -1083,7 +1091,7 @@ __global__ void __launch_bounds__(256) k_large_store(DevPlan P, DevFactor X, con
 template <int NB>
 __global__ void __launch_bounds__(256) k_large_panel_spd(DevPlan P, DevFactor X, const int *__restrict__ large,
                                                          const TppState *__restrict__ cur,
-                                                         TppState *__restrict__ nxt, int iter) {
+                                                         TppState *__restrict__ nxt, int iter, int w2) {
   __shared__ double T[NB][NB + 1];
   __shared__ double lm[NB][NB];
   __shared__ double linv[NB];
@@ -1107,7 +1115,9 @@ __global__ void __launch_bounds__(256) k_large_panel_spd(DevPlan P, DevFactor X,
   if (r0 >= f) return;
   const size_t sf = (size_t)f;
   double *F = X.arena + X.sn_off[s];
-  double *W = F + sf * sf;
+  // w2: two W buffers per front (look-ahead), alternating by panel
+  const int wpar = w2 ? (iter & 1) : 0;
+  double *W = F + sf * sf + (size_t)wpar * NB * sf;
   const double eff_small = __longlong_as_double((long long)X.counters[kCEffSmall]);
   for (int t = threadIdx.x; t < NB * NB; t += 256) {
     const int r = t / NB, c = t % NB;
@@ -1178,6 +1188,7 @@ __global__ void __launch_bounds__(256) k_large_panel_spd(DevPlan P, DevFactor X,
     o.g_c0 = pl;
     o.g_e = tpp_upd_end(S, ne);
     o.pad[0] = np > 0 ? 1 : 0;
+    o.pad[1] = wpar;  // the W buffer this panel's update reads
     if (np < nbp || o.k >= ne) o.phase = 2;
     nxt[q] = o;
     if (np > 0) {
