@@ -72,8 +72,11 @@ __global__ void k_eff_small(unsigned long long *cnt, double small_pivot) {
 // row list (multifrontal_serial.cpp:510-545), assembly work items.
 template <int NT>
 __global__ void k_level_setup(DevPlan P, DevFactor X, int lo, int hi, int lvl, int nb) {
-  __shared__ long long sa[NT], sr[NT], sb[NT];
+  static_assert(NT % 32 == 0 && NT <= 1024, "block size");
+  constexpr int NW = NT / 32;
+  __shared__ long long wa[NW], wr[NW], wb[NW];
   __shared__ long long base_a, base_r, run_a, run_r, run_b;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned long long *cnt = X.counters;
   if (threadIdx.x == 0) {
     base_a = (long long)cnt[kCArena];
@@ -100,33 +103,61 @@ __global__ void k_level_setup(DevPlan P, DevFactor X, int lo, int hi, int lvl, i
       fr = f;
       fb = (f + kAsmCols - 1) / kAsmCols;
     }
-    sa[threadIdx.x] = fa;
-    sr[threadIdx.x] = fr;
-    sb[threadIdx.x] = fb;
-    __syncthreads();
-    for (int o = 1; o < NT; o <<= 1) {  // inclusive scan (Hillis-Steele)
-      long long xa = 0, xr = 0, xb = 0;
-      if (threadIdx.x >= (unsigned)o) {
-        xa = sa[threadIdx.x - o];
-        xr = sr[threadIdx.x - o];
-        xb = sb[threadIdx.x - o];
+    // inclusive block scan of (fa, fr, fb): warp shuffles, then the warps'
+    // totals scanned by warp 0
+    long long va = fa, vr = fr, vb = fb;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long ya = __shfl_up_sync(0xffffffffu, va, o);
+      const long long yr = __shfl_up_sync(0xffffffffu, vr, o);
+      const long long yb = __shfl_up_sync(0xffffffffu, vb, o);
+      if (lane >= o) {
+        va += ya;
+        vr += yr;
+        vb += yb;
       }
-      __syncthreads();
-      sa[threadIdx.x] += xa;
-      sr[threadIdx.x] += xr;
-      sb[threadIdx.x] += xb;
-      __syncthreads();
+    }
+    if (lane == 31) {
+      wa[warp] = va;
+      wr[warp] = vr;
+      wb[warp] = vb;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      long long ta = lane < NW ? wa[lane] : 0, tr = lane < NW ? wr[lane] : 0, tb = lane < NW ? wb[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const long long ya = __shfl_up_sync(0xffffffffu, ta, o);
+        const long long yr = __shfl_up_sync(0xffffffffu, tr, o);
+        const long long yb = __shfl_up_sync(0xffffffffu, tb, o);
+        if (lane >= o) {
+          ta += ya;
+          tr += yr;
+          tb += yb;
+        }
+      }
+      if (lane < NW) {
+        wa[lane] = ta;
+        wr[lane] = tr;
+        wb[lane] = tb;
+      }
+    }
+    __syncthreads();
+    if (warp > 0) {
+      va += wa[warp - 1];
+      vr += wr[warp - 1];
+      vb += wb[warp - 1];
     }
     if (i < hi) {
-      X.sn_off[s] = base_a + run_a + sa[threadIdx.x] - fa;
-      X.sn_roff[s] = base_r + run_r + sr[threadIdx.x] - fr;
-      X.lvl_blk[i + lvl] = (int)(run_b + sb[threadIdx.x] - fb);
+      X.sn_off[s] = base_a + run_a + va - fa;
+      X.sn_roff[s] = base_r + run_r + vr - fr;
+      X.lvl_blk[i + lvl] = (int)(run_b + vb - fb);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      run_a += sa[NT - 1];
-      run_r += sr[NT - 1];
-      run_b += sb[NT - 1];
+      run_a += wa[NW - 1];
+      run_r += wr[NW - 1];
+      run_b += wb[NW - 1];
     }
     __syncthreads();
   }
