@@ -395,11 +395,18 @@ static void launch_defer(Plan &pl, const int *lg, int nL, const TppState *states
     k_large_gemm<<<ggrid, 256, sizeof(TileSmem), st>>>(pl.d, pl.x, lg, nL, states);
 }
 
-// SPD large fronts factor with look-ahead (two streams, two W buffers per
-// front) when the panels are 16 wide, the plan has its second stream, and
-// no profile asks for per-kernel timing.
+// SPD large fronts factor two 16-pivot panels a step (k_large_panel_spd2; W
+// of 32 rows per front), with look-ahead (two streams, two W buffers) when
+// the plan has its second stream and no profile asks for per-kernel timing.
+static bool spd_steps(const smfg_control_t &c) { return c.posdef && c.nb == 16; }
 static bool lookahead(const Plan &pl, const smfg_control_t &c, bool profiling) {
-  return c.posdef && c.nb == 16 && pl.stream2 != nullptr && !profiling;
+  return spd_steps(c) && pl.stream2 != nullptr && !profiling;
+}
+// W rows per front in the arena: 32 for the two-panel SPD steps, twice that
+// under look-ahead, else the panel width.
+static int w_rows(const Plan &pl, const smfg_control_t &c, bool profiling) {
+  if (!spd_steps(c)) return c.nb;
+  return lookahead(pl, c, profiling) ? 4 * c.nb : 2 * c.nb;
 }
 
 // Team size (CTAs per front) of a level's indefinite large-front panels, by
@@ -525,8 +532,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
   lc.n += 2;
   PivotParams prm{c.u, c.small_pivot, c.small_pivot, c.nb, c.blocked_min_front, c.posdef};
   const MixedCfg mc = mixed_cfg(c);
-  // W columns per front in the arena: two buffers under look-ahead
-  const int wcols = lookahead(pl, c, gp.on) ? 2 * c.nb : c.nb;
+  const int wcols = w_rows(pl, c, gp.on);
   // the shared-memory front kernels by size bucket: each launch's shared
   // memory sized to its bucket (more blocks per SM for the many small fronts)
   const int bmf = c.blocked_min_front;
@@ -563,20 +569,21 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
       if (c.posdef && c.nb == 16) {
         // no delays, no search: one multi-block step per panel, states
         // double-buffered; the closing step leaves phase 2
-        const int steps = (pl.lvl_large_maxw[l] + c.nb - 1) / c.nb + 1;
         const dim3 pgrid((pl.lvl_large_maxf[l] + 255) / 256, nL);
-        // look-ahead (unless profiling): each panel's update of the next
-        // panel's 16 columns runs on the stream before the next panel, the
+        // two panels (32 pivots) per step and one rank-32 deferred update.
+        // Look-ahead (unless profiling): the step's update of the next
+        // step's 32 columns runs on the stream before the next step, the
         // rest on stream2 alongside it; every entry still takes its updates
         // in pivot order (the next-columns update waits for the previous
-        // rest update), and the two W buffers alternate so that a panel
-        // never overwrites the W a running rest update reads
+        // rest update), and two W buffers alternate so that a step never
+        // overwrites the W a running rest update reads
         const bool ahead = lookahead(pl, c, gp.on);
+        const int steps = (pl.lvl_large_maxw[l] + 2 * c.nb - 1) / (2 * c.nb) + 1;
         for (; it < steps; ++it) {
           TppState *cur = x.tpp + (size_t)(it & 1) * pl.max_large;
           TppState *nxt = x.tpp + (size_t)((it + 1) & 1) * pl.max_large;
           gp.mark(st, 2);
-          k_large_panel_spd<16><<<pgrid, 256, 0, st>>>(d, x, lg, cur, nxt, it, ahead ? 1 : 0);
+          k_large_panel_spd2<16><<<pgrid, 256, 0, st>>>(d, x, lg, cur, nxt, it, ahead ? 1 : 0);
           gp.mark(st, 2);
           if (ahead) {
             SMFG_CUDA(cudaEventRecord(pl.ev_panel, st));
@@ -591,7 +598,7 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
             launch_defer(pl, lg, nL, nxt, ggrid);
             gp.mark(st);
           }
-          if (lvl_mixed && ((it + 1) * c.nb % mc.nbo == 0 || it == steps - 1))
+          if (lvl_mixed && ((it + 1) * 2 * c.nb % mc.nbo == 0 || it == steps - 1))
             enqueue_tc(pl, mc, lg, nL, nxt, c.posdef, lc, gp);
         }
         if (ahead) SMFG_CUDA(cudaStreamWaitEvent(st, pl.ev_rest, 0));  // join before the Schur update
@@ -688,7 +695,8 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
   set_kernel_attrs(pl.nb);
   // arena: exact for SPD (no delays); head-room for delays, regrown on overflow
   // (look-ahead: a second W buffer, nb columns more per front)
-  const int64_t base_a = pl.sum_f2 + (lookahead(pl, c, c.profile != 0) ? pl.sum_f * (int64_t)c.nb : 0),
+  // (the symbolic sizes hold nb W rows per front; the SPD steps need more)
+  const int64_t base_a = pl.sum_f2 + pl.sum_f * (int64_t)(w_rows(pl, c, c.profile != 0) - c.nb),
                 base_r = pl.sum_f;
   int64_t need_a = c.posdef ? base_a : base_a + base_a / 4 + (int64_t)pl.max_fsym * pl.max_fsym * 2 + 4096;
   int64_t need_r = c.posdef ? base_r : base_r + base_r / 2 + 4096;

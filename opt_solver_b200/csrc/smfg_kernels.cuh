@@ -800,7 +800,7 @@ __global__ void __launch_bounds__(256) k_large_gemm(DevPlan P, DevFactor X, cons
 // store phases overlap; the L and W slices of a tile are read once into
 // shared memory. Measured on one 16,000-row front (K = 16): 4.6 TB/s,
 // against 3.0 TB/s for the general tiled kernel.
-constexpr int kDT = 64, kDK = 16, kDFronts = 256, kDBlocksPerSM = 4;
+constexpr int kDT = 64, kDK = 32, kDFronts = 256, kDBlocksPerSM = 4;
 
 // Tiles of a lower trapezoid rows x cols (rows >= cols) in kDT squares:
 // column tile tj holds the row tiles [tj, rt).
@@ -823,8 +823,9 @@ __device__ __forceinline__ void defer_tile(int w, int rows, int &ti, int &tj) {
   ti = (int)(t + (w - S(t)));
 }
 
-// mode: 0 the whole update, 1 only the next panel's 16 columns [c0, c0 + 16),
-// 2 only the columns past them (look-ahead)
+// mode: 0 the whole update, 1 only the next step's kDK columns [c0, c0 +
+// kDK), 2 only the columns past them (look-ahead). At most kDK pivots; W
+// buffer pad[1] (kDK rows each).
 __global__ void __launch_bounds__(256, kDBlocksPerSM) k_large_defer(DevPlan P, DevFactor X,
                                                                     const int *__restrict__ large, int nlarge,
                                                                     const TppState *__restrict__ tpp, int mode) {
@@ -847,7 +848,7 @@ __global__ void __launch_bounds__(256, kDBlocksPerSM) k_large_defer(DevPlan P, D
       const int s = large[chunk + tid];
       const int f = X.sn_f[s];
       // the columns of this launch's share of the update
-      const int split = min(S.g_e, S.g_c0 + kDK);
+      const int split = min(S.g_e, S.g_c0 + kDK);  // the next step's 32 columns
       const int cs = mode == 2 ? split : S.g_c0, ce = mode == 1 ? split : S.g_e;
       if (S.pad[0] && S.g_p1 > S.g_p0 && ce > cs) nt = defer_tiles(f - cs, ce - cs);
       m_f[tid] = f;
@@ -874,6 +875,24 @@ __global__ void __launch_bounds__(256, kDBlocksPerSM) k_large_defer(DevPlan P, D
     if (tid == 0) pref[0] = 0;
     __syncthreads();
     const int total = pref[cnt];
+    // diagonal rows a two-panel SPD step staged in W: into F (block q of the
+    // grid takes front q; the tiles below never touch these rows)
+    if (mode != 2) {
+      for (int q = blockIdx.x; q < cnt; q += gridDim.x) {
+        const TppState &S = tpp[chunk + q];
+        const int nd = S.pad[2];
+        if (!S.pad[0] || nd <= 0) continue;
+        const int s = large[chunk + q];
+        const int f = X.sn_f[s];
+        const size_t sf = (size_t)f;
+        double *F = X.arena + X.sn_off[s];
+        const double *Wd = F + sf * sf + (size_t)S.pad[1] * kDK * sf;
+        for (int t = tid; t < nd * nd; t += 256) {
+          const int c = t / nd, r = t % nd;
+          if (r >= c) F[(size_t)(S.g_p0 + c) * sf + S.g_p0 + r] = Wd[(size_t)c * f + S.g_p0 + r];
+        }
+      }
+    }
     for (int w = blockIdx.x; w < total; w += gridDim.x) {
       int lo = 0, hi = cnt;
       while (hi - lo > 1) {
@@ -887,7 +906,7 @@ __global__ void __launch_bounds__(256, kDBlocksPerSM) k_large_defer(DevPlan P, D
       const int f = m_f[a], e = m_e[a], kk = m_kk[a], p0 = m_p0[a];
       const size_t sf = (size_t)f;
       double *F = X.arena + m_off[a];
-      const double *Wp = F + sf * sf + (size_t)m_wo[a] * kDK * sf;
+      const double *Wp = F + sf * sf + (size_t)m_wo[a] * kDK * sf;  // second W buffer: kDK rows on
       const int i0 = m_c0[a] + ti * kDT, j0 = m_c0[a] + tj * kDT;
       double c[4][4];
 #pragma unroll
@@ -1110,23 +1129,27 @@ __global__ void __launch_bounds__(256) k_large_store(DevPlan P, DevFactor X, con
   }
 }
 
-// The SPD panel of the large fronts on many blocks (the posdef case of
-// ldlt_factor_front's panel loop, ldlt_kernel.cpp:1100-1112 with
-// select_pivot's in-order test :130-134 and eliminate_1x1 :352-458). Every
-// block factors the panel's diagonal block in shared memory (the pivots'
-// multipliers l_j = F(j, k) / d... as ck[j] * inv_d), then takes its own
-// rows through the same pivots in registers: per entry the reference's
-// operations in the reference's order, with no synchronization between
-// blocks. Grid: (row blocks of 256 rows, large fronts). The state is read
-// from `cur` and the next one written to `nxt` (one block per front).
+// Two SPD panels per launch (32 pivots, then one rank-32 deferred update:
+// half the launches and half the deferred traffic of one panel at a time).
+// Per entry the operations and their order are the one-panel path's: the
+// second panel's columns take the first panel's update as the deferred
+// update would (c = fma(-l_p, w_p, c) over its pivots in order, w_p = 0
+// skipped) before the second panel's eliminations, and the columns past
+// both take one chain over the 32 pivots in order. Every block factors both
+// diagonal blocks itself: the first, then the first panel's pivots on the
+// second panel's 16 rows (their unscaled values w and multipliers l to
+// shared memory), the second block updated from them and factored. A
+// failing pivot in the first panel ends the front there (as the one-panel
+// path ends it).
 template <int NB>
-__global__ void __launch_bounds__(256) k_large_panel_spd(DevPlan P, DevFactor X, const int *__restrict__ large,
-                                                         const TppState *__restrict__ cur,
-                                                         TppState *__restrict__ nxt, int iter, int w2) {
-  __shared__ double T[NB][NB + 1];
-  __shared__ double lm[NB][NB];
-  __shared__ double linv[NB];
-  __shared__ int np_sh;
+__global__ void __launch_bounds__(256) k_large_panel_spd2(DevPlan P, DevFactor X, const int *__restrict__ large,
+                                                          const TppState *__restrict__ cur,
+                                                          TppState *__restrict__ nxt, int iter, int w2) {
+  __shared__ double T[NB][NB + 1], T2[NB][NB + 1];
+  __shared__ double lm[NB][NB], lm2[NB][NB];
+  __shared__ double linv[NB], linv2[NB];
+  __shared__ double Wr[NB][NB], Lr[NB][NB];  // [row of panel 2][pivot of panel 1]
+  __shared__ int np_sh, np2_sh;
   if (X.counters[kCFlags] & kFAbort) return;
   const int q = blockIdx.y;
   const int s = large[q];
@@ -1142,21 +1165,24 @@ __global__ void __launch_bounds__(256) k_large_panel_spd(DevPlan P, DevFactor X,
   }
   const int f = X.sn_f[s], ne = X.sn_ne[s];
   const int ps = S.k, pl = min(ne, ps + NB), nbp = pl - ps;
+  const int ps2 = pl, pl2 = min(ne, ps2 + NB), nbp2 = pl2 - ps2;
   const int r0 = ps + blockIdx.x * 256;
   if (r0 >= f) return;
   const size_t sf = (size_t)f;
   double *F = X.arena + X.sn_off[s];
-  // w2: two W buffers per front (look-ahead), alternating by panel
+  // W: rows [0, 16) panel 1, [16, 32) panel 2; w2 (look-ahead): two such
+  // buffers alternating by step
   const int wpar = w2 ? (iter & 1) : 0;
-  double *W = F + sf * sf + (size_t)wpar * NB * sf;
+  double *W = F + sf * sf + (size_t)wpar * 2 * NB * sf;
   const double eff_small = __longlong_as_double((long long)X.counters[kCEffSmall]);
+  const int lane = threadIdx.x & 31;
+  // panel 1's diagonal block
   for (int t = threadIdx.x; t < NB * NB; t += 256) {
     const int r = t / NB, c = t % NB;
     T[r][c] = (r < nbp && c <= r) ? F[(size_t)(ps + c) * sf + ps + r] : 0.0;
   }
   __syncthreads();
   if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
     int np = 0;
     for (int k = 0; k < nbp; ++k) {
       const double d = T[k][k];
@@ -1179,7 +1205,75 @@ __global__ void __launch_bounds__(256) k_large_panel_spd(DevPlan P, DevFactor X,
     if (lane == 0) np_sh = np;
   }
   __syncthreads();
-  const int np = np_sh;
+  const int np1 = np_sh;
+  const bool two = np1 == NB && nbp == NB && nbp2 > 0;
+  if (two) {
+    // panel 1's pivots on panel 2's rows (threads 0..15: one row each)
+    if (threadIdx.x < nbp2) {
+      const int i = ps2 + threadIdx.x;
+      double a[NB];
+#pragma unroll
+      for (int c = 0; c < NB; ++c) a[c] = F[(size_t)(ps + c) * sf + i];
+#pragma unroll
+      for (int k = 0; k < NB; ++k) {
+        const double w = a[k];
+        Wr[threadIdx.x][k] = w;
+#pragma unroll
+        for (int j = k + 1; j < NB; ++j) {
+          const double l = lm[k][j];
+          if (l != 0.0) a[j] = __dsub_rn(a[j], __dmul_rn(w, l));
+        }
+        a[k] = __dmul_rn(w, linv[k]);
+        Lr[threadIdx.x][k] = a[k];
+      }
+    }
+    // panel 2's diagonal block, panel 1's update applied as the deferred
+    // update applies it
+    for (int t = threadIdx.x; t < NB * NB; t += 256) {
+      const int r = t / NB, c = t % NB;
+      T2[r][c] = (r < nbp2 && c <= r) ? F[(size_t)(ps2 + c) * sf + ps2 + r] : 0.0;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < NB * NB; t += 256) {
+      const int r = t / NB, c = t % NB;
+      if (r < nbp2 && c <= r) {
+        double v = T2[r][c];
+#pragma unroll
+        for (int p = 0; p < NB; ++p) {
+          const double bw = Wr[c][p];
+          if (bw != 0.0) v = fma(-Lr[r][p], bw, v);
+        }
+        T2[r][c] = v;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      int np = 0;
+      for (int k = 0; k < nbp2; ++k) {
+        const double d = T2[k][k];
+        if (!(d > 0.0 && isfinite(d))) break;
+        const double inv = 1.0 / d;
+        if (lane == 0) linv2[k] = inv;
+        if (lane > k && lane < nbp2) lm2[k][lane] = __dmul_rn(T2[lane][k], inv);
+        __syncwarp();
+        if (lane > k && lane < nbp2) {
+          const double tik = T2[lane][k];
+          for (int j = k + 1; j <= lane; ++j) {
+            const double l = lm2[k][j];
+            if (l != 0.0) T2[lane][j] = __dsub_rn(T2[lane][j], __dmul_rn(tik, l));
+          }
+          T2[lane][k] = __dmul_rn(tik, inv);
+        }
+        __syncwarp();
+        ++np;
+      }
+      if (lane == 0) np2_sh = np;
+    }
+  } else if (threadIdx.x == 0) {
+    np2_sh = 0;
+  }
+  __syncthreads();
+  const int np2 = np2_sh;
   const int i = r0 + threadIdx.x;
   if (i < f) {
     double a[NB];
@@ -1187,7 +1281,7 @@ __global__ void __launch_bounds__(256) k_large_panel_spd(DevPlan P, DevFactor X,
     for (int c = 0; c < NB; ++c) a[c] = (c < nbp && ps + c <= i) ? F[(size_t)(ps + c) * sf + i] : 0.0;
 #pragma unroll
     for (int k = 0; k < NB; ++k) {
-      if (k < np && i > ps + k) {
+      if (k < np1 && i > ps + k) {
         const double w = a[k];
         W[(size_t)k * f + i] = w;
 #pragma unroll
@@ -1200,31 +1294,86 @@ __global__ void __launch_bounds__(256) k_large_panel_spd(DevPlan P, DevFactor X,
         a[k] = __dmul_rn(w, linv[k]);
       }
     }
+    // rows of the panels' diagonal blocks go to W (columns [ps, pend) at
+    // W rows c): other blocks read their original values in this launch;
+    // the deferred-update launch copies them into F
+    const bool stage = i < (two ? pl2 : pl);
 #pragma unroll
     for (int c = 0; c < NB; ++c)
-      if (c < nbp && ps + c <= i) F[(size_t)(ps + c) * sf + i] = a[c];
+      if (c < nbp && ps + c <= i) {
+        if (stage) W[(size_t)c * f + i] = a[c];
+        else F[(size_t)(ps + c) * sf + i] = a[c];
+      }
+    if (two && i >= ps2) {
+      // the second panel's columns of this row: panel 1's update, then
+      // panel 2's pivots
+      double b[NB];
+#pragma unroll
+      for (int c = 0; c < NB; ++c) {
+        b[c] = 0.0;
+        if (c < nbp2 && ps2 + c <= i) {
+          double v = F[(size_t)(ps2 + c) * sf + i];
+#pragma unroll
+          for (int p = 0; p < NB; ++p) {
+            const double bw = Wr[c][p];
+            if (bw != 0.0) v = fma(-a[p], bw, v);
+          }
+          b[c] = v;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < NB; ++k) {
+        if (k < np2 && i > ps2 + k) {
+          const double w = b[k];
+          W[(size_t)(NB + k) * f + i] = w;
+#pragma unroll
+          for (int j = k + 1; j < NB; ++j) {
+            if (j < nbp2 && ps2 + j <= i) {
+              const double l = lm2[k][j];
+              if (l != 0.0) b[j] = __dsub_rn(b[j], __dmul_rn(w, l));
+            }
+          }
+          b[k] = __dmul_rn(w, linv2[k]);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < NB; ++c)
+        if (c < nbp2 && ps2 + c <= i) {
+          if (stage) W[(size_t)(NB + c) * f + i] = b[c];
+          else F[(size_t)(ps2 + c) * sf + i] = b[c];
+        }
+    }
   }
   if (lead && threadIdx.x == 0) {
     TppState o = S;
     int8_t *tags = X.tags + X.sn_roff[s];
-    for (int k = 0; k < np; ++k) {
+    for (int k = 0; k < np1; ++k) {
       tags[ps + k] = 1;
       inertia_1x1(T[k][k], eff_small, o.st);
       const double rem = (double)(f - (ps + k + 1));
       o.st.flops += rem + rem * (rem + 1.0);
     }
+    for (int k = 0; k < np2; ++k) {
+      tags[ps2 + k] = 1;
+      inertia_1x1(T2[k][k], eff_small, o.st);
+      const double rem = (double)(f - (ps2 + k + 1));
+      o.st.flops += rem + rem * (rem + 1.0);
+    }
+    const int np = np1 + np2;
+    const int pend = two ? pl2 : pl;  // the deferred update starts past the panels done
     o.k = ps + np;
     o.g_p0 = ps;
     o.g_p1 = ps + np;
-    o.g_c0 = pl;
+    o.g_c0 = pend;
     o.g_e = tpp_upd_end(S, ne);
     o.pad[0] = np > 0 ? 1 : 0;
-    o.pad[1] = wpar;  // the W buffer this panel's update reads
-    if (np < nbp || o.k >= ne) o.phase = 2;
+    o.pad[1] = wpar;       // the W buffer of this step's update
+    o.pad[2] = pend - ps;  // diagonal rows [ps, pend) staged in W (copied by k_large_defer)
+    if (np1 < nbp || (two && np2 < nbp2) || o.k >= ne) o.phase = 2;
     nxt[q] = o;
     if (np > 0) {
       atomicMax(X.counters + kCActive, (unsigned long long)(iter + 1));
-      const long long m = tpp_upd_end(S, ne) - pl, h = f - pl;
+      const long long m = tpp_upd_end(S, ne) - pend, h = f - pend;
       if (m > 0) {
         const double elems = (double)(m * h - m * (m - 1) / 2);
         atomicAdd(reinterpret_cast<double *>(X.counters + kCGemmFlops), 2.0 * (double)np * elems);
