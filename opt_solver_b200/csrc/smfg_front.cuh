@@ -1186,7 +1186,7 @@ struct TppState {
   int phase, k, live, k_paired;
   int post, ps, pl, stalled;
   int g_p0, g_p1, g_c0, g_e;  // the deferred update asked for
-  int pad[4];
+  int pad[4];  // see tpp_init
   // mixed precision (outer blocks): the eligible columns [k, min(se, ne))
   // are current; every column from there on has the pivots [0, tc_done)
   // applied and waits for a tensor-core update by [tc_done, k)
@@ -1203,7 +1203,9 @@ __device__ __forceinline__ void tpp_init(TppState &S, int ne, bool posdef, bool 
   S.post = 0;
   S.ps = S.pl = S.stalled = 0;
   S.g_p0 = S.g_p1 = S.g_c0 = S.g_e = 0;
-  S.pad[0] = S.pad[1] = S.pad[2] = S.pad[3] = 0;  // [0] update pending, [1] its W buffer
+  // pad: [0] a deferred update pending, [1] the W buffer it reads, [2] rows
+  // of the panels' diagonal blocks staged in W (two-panel SPD steps)
+  S.pad[0] = S.pad[1] = S.pad[2] = S.pad[3] = 0;
   S.mixed = mixed ? 1 : 0;
   S.tc_done = 0;
   // SPD: outer blocks of nbo pivots; indefinite: every eligible column
