@@ -536,7 +536,7 @@ def run_reference_arm(args, rank, world):
         return None
     from oracle import oracle as O
     if not O.ref_available():
-        return {"impl": "reference", "unavailable": "oracle/_ref not built (no /root/reference at build time)"}
+        return {"impl": "reference", "unavailable": "oracle/_ref not built (the reference sources were absent at build time)"}
     threads = os.cpu_count() or 1
     times = []
     sample = ""
