@@ -1927,7 +1927,28 @@ __global__ void __launch_bounds__(kTriNT) k_fwd_tri(DevPlan P, DevFactor X, cons
     for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) ws[t] = w[j0 + t];
     for (int jb = j0; jb < j1; jb += 32) {
       const int nb = min(32, j1 - jb);
-      load_tri32<kTriNT>(L, sf, jb, nb, Ls);
+      // every load of the strip first (its triangle, and this thread's row
+      // below it: at most 224 rows, one a thread), so that they are in
+      // flight across the barriers and the triangle solve
+      double tv[1024 / kTriNT];
+#pragma unroll
+      for (int u = 0; u < 1024 / kTriNT; ++u) {
+        const int t = (int)threadIdx.x + kTriNT * u, r = t & 31, c = t >> 5;
+        tv[u] = (r < nb && c < nb && c <= r) ? __ldg(L + (size_t)(jb + c) * sf + jb + r) : 0.0;
+      }
+      const int i = jb + nb + warp * 32 + lane;
+      double l[32];
+      if (nb == 32 && i < j1) {
+#pragma unroll
+        for (int u = 0; u < 32; ++u) l[u] = __ldg(L + (size_t)(jb + u) * sf + i);
+      }
+      __syncthreads();  // the previous strip's readers of Ls and ws are done
+#pragma unroll
+      for (int u = 0; u < 1024 / kTriNT; ++u) {
+        const int t = (int)threadIdx.x + kTriNT * u;
+        Ls[t & 31][t >> 5] = tv[u];
+      }
+      __syncthreads();
       if (warp == 0) {
         // the 32 x 32 triangle on the block's values in shared memory
         double wi = (lane < nb) ? ws[jb - j0 + lane] : 0.0;
@@ -1941,12 +1962,18 @@ __global__ void __launch_bounds__(kTriNT) k_fwd_tri(DevPlan P, DevFactor X, cons
       }
       __syncthreads();
       // the block's rows below this strip: a warp per 32 rows
-      for (int i = jb + nb + warp * 32 + lane; i - lane < j1; i += kTriNT) {
-        const double acc = (i < j1) ? strip_dot32(L, sf, i, jb, nb, ws, j0) : 0.0;
-        if (i < j1) ws[i - j0] -= acc;
+      if (i < j1) {
+        double acc = 0.0;
+        if (nb == 32) {
+#pragma unroll
+          for (int u = 0; u < 32; ++u) acc = fma(l[u], ws[jb + u - j0], acc);
+        } else {
+          acc = strip_dot32(L, sf, i, jb, nb, ws, j0);
+        }
+        ws[i - j0] -= acc;
       }
-      __syncthreads();
     }
+    __syncthreads();
     for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) w[j0 + t] = ws[t];
     double *xr = x + (int64_t)r * P.n;
     for (int j = j0 + threadIdx.x; j < j1; j += kTriNT) xr[rows[j]] = ws[j - j0];
@@ -2096,6 +2123,13 @@ __global__ void __launch_bounds__(kTriNT) k_bwd_tri(DevPlan P, DevFactor X, cons
     __syncthreads();
     for (int je = j1; je > j0; je -= 32) {
       const int jb = max(j0, je - 32), nb = je - jb;
+      // the strip's triangle loaded first, in flight during the dots
+      double tv[1024 / kTriNT];
+#pragma unroll
+      for (int u = 0; u < 1024 / kTriNT; ++u) {
+        const int t = (int)threadIdx.x + kTriNT * u, r = t & 31, c = t >> 5;
+        tv[u] = (r < nb && c < nb && c <= r) ? __ldg(L + (size_t)(jb + c) * sf + jb + r) : 0.0;
+      }
       // v[j] -= sum over the block's solved rows [je, j1) of L(i, j) v[i]:
       // a warp per column, its lanes' rows (at most 7 a lane) loaded at once
       for (int j = jb + warp; j < je; j += kTriNT / 32) {
@@ -2113,7 +2147,13 @@ __global__ void __launch_bounds__(kTriNT) k_bwd_tri(DevPlan P, DevFactor X, cons
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (lane == 0) vs[j - j0] -= acc;
       }
-      load_tri32<kTriNT>(L, sf, jb, nb, Ls);
+      // (the previous strip's solve, the last reader of Ls, ended at a barrier)
+#pragma unroll
+      for (int u = 0; u < 1024 / kTriNT; ++u) {
+        const int t = (int)threadIdx.x + kTriNT * u;
+        Ls[t & 31][t >> 5] = tv[u];
+      }
+      __syncthreads();
       if (warp == 0) {
         double vi = (lane < nb) ? vs[jb - j0 + lane] : 0.0;
         for (int j = nb - 1; j >= 0; --j) {
