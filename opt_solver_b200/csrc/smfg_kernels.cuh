@@ -1560,6 +1560,23 @@ __device__ __forceinline__ void load_tri32(const double *L, size_t sf, int jb, i
   __syncthreads();
 }
 
+// The same triangle copied asynchronously (8-byte cp.async, zero fill
+// outside the lower triangle); the caller waits with cp_async_wait_all()
+// and a barrier before reading Ls.
+template <int NT>
+__device__ __forceinline__ void load_tri32_async(const double *L, size_t sf, int jb, int nb, double (*Ls)[33]) {
+  for (int t = threadIdx.x; t < 1024; t += NT) {
+    const int r = t & 31, c = t >> 5;
+    const bool in = r < nb && c < nb && c <= r;
+    const double *src = in ? L + (size_t)(jb + c) * sf + jb + r : L;
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(&Ls[r][c]);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(in ? 8 : 0) : "memory");
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // w[jb:jb+nb) <- L11^-1 w (unit, or non-unit for SPD): lane = row.
 __device__ __forceinline__ void tri_fwd_warp(double *w, int jb, int nb, int posdef, const double (*Ls)[33]) {
   const int lane = threadIdx.x & 31;
@@ -1622,14 +1639,33 @@ __global__ void __launch_bounds__(kSolveNT, 4) k_fwd_front(DevPlan P, DevFactor 
   if (large) return;  // the block kernels (k_fwd_tri / k_fwd_gemv) go on
   for (int jb = 0; jb < p; jb += 32) {
     const int nb = min(32, p - jb);
-    load_tri32<kSolveNT>(L, sf, jb, nb, Ls);
+    // the strip's triangle and this thread's first row below it loaded
+    // before the barriers and the triangle solves (in flight meanwhile)
+    double tv[1024 / kSolveNT];
+#pragma unroll
+    for (int u = 0; u < 1024 / kSolveNT; ++u) {
+      const int t = (int)threadIdx.x + kSolveNT * u, r = t & 31, c = t >> 5;
+      tv[u] = (r < nb && c < nb && c <= r) ? __ldg(L + (size_t)(jb + c) * sf + jb + r) : 0.0;
+    }
+    const int i1 = jb + nb + (int)threadIdx.x;
+    double l[32];
+#pragma unroll
+    for (int u = 0; u < 32; ++u) l[u] = (i1 < f && u < nb) ? __ldg(L + (size_t)(jb + u) * sf + i1) : 0.0;
+    __syncthreads();  // the previous strip's readers of Ls and the vectors are done
+#pragma unroll
+    for (int u = 0; u < 1024 / kSolveNT; ++u) {
+      const int t = (int)threadIdx.x + kSolveNT * u;
+      Ls[t & 31][t >> 5] = tv[u];
+    }
+    __syncthreads();
     for (int r = warp; r < nrhs; r += kSolveNT / 32) tri_fwd_warp(wk + (int64_t)r * rows_total + roff, jb, nb, posdef, Ls);
     __syncthreads();
-    for (int i = jb + nb + threadIdx.x; i < f; i += kSolveNT) {
-      const double *li = L + (size_t)jb * sf + i;
-      double l[32];
+    for (int i = i1; i < f; i += kSolveNT) {
+      if (i != i1) {
+        const double *li = L + (size_t)jb * sf + i;
 #pragma unroll
-      for (int u = 0; u < 32; ++u) l[u] = (u < nb) ? __ldg(li + (size_t)u * sf) : 0.0;
+        for (int u = 0; u < 32; ++u) l[u] = (u < nb) ? __ldg(li + (size_t)u * sf) : 0.0;
+      }
       for (int r = 0; r < nrhs; ++r) {
         double *w = wk + (int64_t)r * rows_total + roff;
         double acc = 0.0;
@@ -1639,8 +1675,8 @@ __global__ void __launch_bounds__(kSolveNT, 4) k_fwd_front(DevPlan P, DevFactor 
         w[i] -= acc;
       }
     }
-    __syncthreads();
   }
+  __syncthreads();
   for (int64_t t = threadIdx.x; t < (int64_t)p * nrhs; t += kSolveNT) {
     const int r = (int)(t / p), i = (int)(t % p);
     x[(int64_t)r * P.n + rows[i]] = wk[(int64_t)r * rows_total + roff + i];
@@ -1845,6 +1881,9 @@ __global__ void __launch_bounds__(kSolveNT) k_bwd_front(DevPlan P, DevFactor X, 
   // the 32 x 32 triangle (a warp per right-hand side)
   for (int je = p; je > 0; je -= 32) {
     const int jb = max(0, je - 32), nb = je - jb;
+    // the strip's triangle copied to Ls first, in flight during the dots
+    // (the previous strip's solves, the last readers of Ls, ended at a barrier)
+    load_tri32_async<kSolveNT>(L, sf, jb, nb, Ls);
     for (int j = jb + warp; j < je; j += kSolveNT / 32) {
       const double *Lj = L + (size_t)j * sf;
       for (int i0 = je; i0 < p; i0 += 32 * 4) {
@@ -1867,7 +1906,8 @@ __global__ void __launch_bounds__(kSolveNT) k_bwd_front(DevPlan P, DevFactor X, 
         }
       }
     }
-    load_tri32<kSolveNT>(L, sf, jb, nb, Ls);
+    cp_async_wait_all();
+    __syncthreads();
     for (int r = warp; r < nrhs; r += kSolveNT / 32) tri_bwd_warp(wk + (int64_t)r * rows_total + roff, jb, nb, posdef, Ls);
     __syncthreads();
   }
