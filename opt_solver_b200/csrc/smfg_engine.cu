@@ -1312,18 +1312,30 @@ static void device_residual(Plan &pl, const double *db, const double *dx, double
   // permuted copies: the residual works in the new numbering
   double *xp = nullptr, *bp = nullptr, *rp = nullptr;
   const size_t len = (size_t)pl.n;
-  SMFG_CUDA(plan_malloc_async(pl, (void **)&xp, sizeof(double) * len * 3));
-  bp = xp + len;
-  rp = bp + len;
   const int sms = sm_count(pl.device);
+  const int rg = (int)std::max<int64_t>(1, std::min<int64_t>(8 * sms, (pl.n + 31) / 32));
   double e_max = 0.0, o_max = 0.0;
-  for (int r = 0; r < nrhs; ++r) {
+  if (nrhs > 1) {
+    // several columns per pass: the matrix read once for up to kResLanes
+    // of them, x interleaved, b and r in the original numbering
+    const int cmax = std::min(nrhs, kResLanes);
+    SMFG_CUDA(plan_malloc_async(pl, (void **)&xp, sizeof(double) * len * cmax));
+    for (int r0 = 0; r0 < nrhs; r0 += kResLanes) {
+      const int cn = std::min(kResLanes, nrhs - r0);
+      const int g = (int)std::max<int64_t>(1, std::min<int64_t>(4 * sms, ((int64_t)pl.n * cn + 255) / 256));
+      k_gather_interleave<<<g, 256, 0, pl.stream>>>(dx + (size_t)r0 * pl.n, pl.n, cn, pl.d.perm, xp);
+      k_residual_rhs<<<rg, 256, 0, pl.stream>>>(pl.d, pl.x.pv_raw, xp, cn, db + (size_t)r0 * pl.n,
+                                                dr + (size_t)r0 * pl.n, pl.n, mx + 8 * r0);
+    }
+  } else {
+    SMFG_CUDA(plan_malloc_async(pl, (void **)&xp, sizeof(double) * len * 3));
+    bp = xp + len;
+    rp = bp + len;
     const int g = (int)std::max<int64_t>(1, std::min<int64_t>(4 * sms, (pl.n + 255) / 256));
-    k_solve_gather<<<g, 256, 0, pl.stream>>>(dx + (size_t)r * pl.n, pl.n, 1, pl.n, pl.d.perm, nullptr, xp);
-    k_solve_gather<<<g, 256, 0, pl.stream>>>(db + (size_t)r * pl.n, pl.n, 1, pl.n, pl.d.perm, nullptr, bp);
-    const int rg = (int)std::max<int64_t>(1, std::min<int64_t>(8 * sms, (pl.n + 31) / 32));
-    k_residual<<<rg, 256, 0, pl.stream>>>(pl.d, pl.x.pv_raw, xp, bp, rp, pl.n, mx + 8 * r);
-    k_solve_scatter<<<g, 256, 0, pl.stream>>>(dr + (size_t)r * pl.n, pl.n, 1, pl.n, pl.d.perm, nullptr, rp);
+    k_solve_gather<<<g, 256, 0, pl.stream>>>(dx, pl.n, 1, pl.n, pl.d.perm, nullptr, xp);
+    k_solve_gather<<<g, 256, 0, pl.stream>>>(db, pl.n, 1, pl.n, pl.d.perm, nullptr, bp);
+    k_residual<<<rg, 256, 0, pl.stream>>>(pl.d, pl.x.pv_raw, xp, bp, rp, pl.n, mx);
+    k_solve_scatter<<<g, 256, 0, pl.stream>>>(dr, pl.n, 1, pl.n, pl.d.perm, nullptr, rp);
   }
   std::vector<unsigned long long> hv((size_t)8 * nrhs);
   SMFG_CUDA(cudaMemcpyAsync(hv.data(), mx, sizeof(unsigned long long) * 8 * nrhs, cudaMemcpyDeviceToHost,

@@ -2293,6 +2293,121 @@ __global__ void k_residual(DevPlan P, const double *__restrict__ vals, const dou
   }
 }
 
+// Up to kResLanes right-hand sides at once: the pattern and the values read
+// once for all of them, x interleaved in the new numbering (xi[i * nr + q]),
+// b read and r written in the original numbering (column q at q * n). Each
+// column's sums take the same operations in the same order as k_residual;
+// after the row's reduction, lane sub keeps the maxima of column sub.
+__global__ void k_residual_rhs(DevPlan P, const double *__restrict__ vals, const double *__restrict__ xi, int nr,
+                               const double *__restrict__ b, double *__restrict__ r, int n,
+                               unsigned long long *mx /* 8 per column, as k_residual */) {
+  constexpr int RPW = 32 / kResLanes;
+  const int lane = threadIdx.x & 31, sub = lane % kResLanes, grp = lane / kResLanes;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  double m_r = 0.0, m_a = 0.0, m_x = 0.0, m_b = 0.0, m_o = 0.0;
+  for (int i0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * RPW; i0 < n; i0 += warps * RPW) {
+    const int i = i0 + grp;
+    double s[kResLanes], c[kResLanes], as[kResLanes], ra = 0.0;
+#pragma unroll
+    for (int q = 0; q < kResLanes; ++q) s[q] = c[q] = as[q] = 0.0;
+    if (i < n) {
+      for (int k = P.sptr[i] + sub; k < P.sptr[i + 1]; k += kResLanes) {
+        const double a = vals[P.sidx[k]];
+        const double *xj = xi + (int64_t)P.srow[k] * nr;
+#pragma unroll
+        for (int q = 0; q < kResLanes; ++q) {
+          if (q < nr) {
+            const double xv = xj[q];
+            const double pr = a * xv;
+            const double pe = fma(a, xv, -pr);
+            double t, e;
+            two_sum(s[q], pr, t, e);
+            s[q] = t;
+            c[q] += e + pe;
+            as[q] = fma(fabs(a), fabs(xv), as[q]);
+          }
+        }
+        ra += fabs(a);
+      }
+    }
+    for (int o = kResLanes / 2; o > 0; o >>= 1) {  // within the row's lanes
+#pragma unroll
+      for (int q = 0; q < kResLanes; ++q) {
+        if (q < nr) {
+          const double s2 = __shfl_xor_sync(0xffffffffu, s[q], o);
+          const double c2 = __shfl_xor_sync(0xffffffffu, c[q], o);
+          double t, e;
+          two_sum(s[q], s2, t, e);
+          s[q] = t;
+          c[q] += c2 + e;
+          as[q] += __shfl_xor_sync(0xffffffffu, as[q], o);
+        }
+      }
+      ra += __shfl_xor_sync(0xffffffffu, ra, o);
+    }
+    // the butterfly leaves the compensation term rounded differently on
+    // the row's lanes: every column takes the row's first lane's values,
+    // the ones k_residual uses
+    double S = 0.0, C = 0.0, AS = 0.0;
+    const int lead = grp * kResLanes;
+#pragma unroll
+    for (int q = 0; q < kResLanes; ++q) {
+      if (q < nr) {
+        const double s0 = __shfl_sync(0xffffffffu, s[q], lead);
+        const double c0 = __shfl_sync(0xffffffffu, c[q], lead);
+        const double a0 = __shfl_sync(0xffffffffu, as[q], lead);
+        if (q == sub) {
+          S = s0;
+          C = c0;
+          AS = a0;
+        }
+      }
+    }
+    if (sub < nr && i < n) {
+      const int64_t o = (int64_t)sub * n + P.perm[i];
+      const double bi = b[o];
+      double t, e;
+      two_sum(bi, -S, t, e);
+      const double res = t + (e - C);
+      r[o] = res;
+      m_r = fmax(m_r, fabs(res));
+      m_a = fmax(m_a, ra);
+      m_x = fmax(m_x, fabs(xi[(int64_t)i * nr + sub]));
+      m_b = fmax(m_b, fabs(bi));
+      const double den = AS + fabs(bi);
+      const double om = den > 0.0 ? fabs(res) / den : (res == 0.0 ? 0.0 : INFINITY);
+      m_o = fmax(m_o, om);
+    }
+  }
+  for (int o = 16; o >= kResLanes; o >>= 1) {  // across the rows, per column
+    m_r = fmax(m_r, __shfl_xor_sync(0xffffffffu, m_r, o));
+    m_a = fmax(m_a, __shfl_xor_sync(0xffffffffu, m_a, o));
+    m_x = fmax(m_x, __shfl_xor_sync(0xffffffffu, m_x, o));
+    m_b = fmax(m_b, __shfl_xor_sync(0xffffffffu, m_b, o));
+    m_o = fmax(m_o, __shfl_xor_sync(0xffffffffu, m_o, o));
+  }
+  if (grp == 0 && sub < nr) {
+    unsigned long long *m = mx + 8 * sub;
+    atomicMax(m + 0, (unsigned long long)__double_as_longlong(m_r));
+    atomicMax(m + 1, (unsigned long long)__double_as_longlong(m_a));
+    atomicMax(m + 2, (unsigned long long)__double_as_longlong(m_x));
+    atomicMax(m + 3, (unsigned long long)__double_as_longlong(m_b));
+    atomicMax(m + 4, (unsigned long long)__double_as_longlong(m_o));
+  }
+}
+
+// xi[i * nr + q] = x[q * n + perm[i]]: nr columns interleaved in the new
+// numbering, for k_residual_rhs.
+__global__ void k_gather_interleave(const double *__restrict__ x, int n, int nr, const int *__restrict__ perm,
+                                    double *__restrict__ xi) {
+  const int64_t tot = (int64_t)n * nr;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t / nr), q = (int)(t % nr);
+    xi[t] = x[(int64_t)q * n + perm[i]];
+  }
+}
+
 __global__ void k_axpy(double *__restrict__ x, const double *__restrict__ dx, int64_t len) {
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < len;
        t += (int64_t)gridDim.x * blockDim.x)

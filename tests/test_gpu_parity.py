@@ -95,6 +95,34 @@ def test_multi_rhs_and_jobs(ref_lib):
 
 
 @pytest.mark.gpu
+def test_multi_rhs_residual_bitwise(ref_lib):
+    """The residual of several columns per pass (8, then the rest) equals
+    the one-column residual column by column, bit for bit; eta and omega are
+    the columns' maxima."""
+    O = ref_lib
+    from opt_solver_b200.smfg import Solver
+    from opt_solver_b200 import workloads as W
+    n, cp, ri, v = W.trajectory_kkt(30, np.random.default_rng(4))
+    ref = reference_for(O, False, "amd", "none")
+    a = ref.analyse(n, cp, ri, v)
+    sv = Solver(a)
+    sv.factor(v, posdef=False)
+    B = W.rhs(n, 11, seed=6, kind="normal")
+    X = sv.solve(B)
+    X[3] *= 1.0 + 1e-9  # columns with different backward errors
+    R, eta, om = sv.residual(B, X)
+    etas, oms = [], []
+    for k in range(B.shape[0]):
+        r1, e1, o1 = sv.residual(B[k], X[k])
+        assert np.array_equal(R[k], r1), k
+        etas.append(e1)
+        oms.append(o1)
+    assert eta == max(etas) and om == max(oms)
+    _, _, om_o = O.residual(n, cp, ri, v, B[3], X[3])
+    assert oms[3] <= 4 * om_o + 1e-18
+
+
+@pytest.mark.gpu
 def test_refactor_reuses_plan(ref_lib):
     """IpmSession-style refactors of one analysis (ipm_session.cpp:147-243)."""
     O = ref_lib
