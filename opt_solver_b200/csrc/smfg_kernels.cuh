@@ -2298,9 +2298,15 @@ __global__ void k_residual(DevPlan P, const double *__restrict__ vals, const dou
 // b read and r written in the original numbering (column q at q * n). Each
 // column's sums take the same operations in the same order as k_residual;
 // after the row's reduction, lane sub keeps the maxima of column sub.
-__global__ void k_residual_rhs(DevPlan P, const double *__restrict__ vals, const double *__restrict__ xi, int nr,
-                               const double *__restrict__ b, double *__restrict__ r, int n,
-                               unsigned long long *mx /* 8 per column, as k_residual */) {
+// Latency: a lane's next kResAhead entries have their indices, then their
+// values, loaded together, the next entry's x while the current one is
+// summed, and the row's b and x ahead of the entries.
+constexpr int kResAhead = 4;
+
+__global__ void __launch_bounds__(256, 2)
+    k_residual_rhs(DevPlan P, const double *__restrict__ vals, const double *__restrict__ xi, int nr,
+                   const double *__restrict__ b, double *__restrict__ r, int n,
+                   unsigned long long *mx /* 8 per column, as k_residual */) {
   constexpr int RPW = 32 / kResLanes;
   const int lane = threadIdx.x & 31, sub = lane % kResLanes, grp = lane / kResLanes;
   const int warps = (gridDim.x * blockDim.x) >> 5;
@@ -2310,24 +2316,55 @@ __global__ void k_residual_rhs(DevPlan P, const double *__restrict__ vals, const
     double s[kResLanes], c[kResLanes], as[kResLanes], ra = 0.0;
 #pragma unroll
     for (int q = 0; q < kResLanes; ++q) s[q] = c[q] = as[q] = 0.0;
+    int64_t ob = 0;
+    double bi = 0.0, xs = 0.0;
+    if (sub < nr && i < n) {
+      ob = (int64_t)sub * n + P.perm[i];
+      bi = b[ob];
+      xs = xi[(int64_t)i * nr + sub];
+    }
     if (i < n) {
-      for (int k = P.sptr[i] + sub; k < P.sptr[i + 1]; k += kResLanes) {
-        const double a = vals[P.sidx[k]];
-        const double *xj = xi + (int64_t)P.srow[k] * nr;
+      const int ke = P.sptr[i + 1];
+      for (int k0 = P.sptr[i] + sub; k0 < ke; k0 += kResLanes * kResAhead) {
+        // entries past the row's end read index 0 and are not summed
+        int jx[kResAhead], ix[kResAhead];
 #pragma unroll
-        for (int q = 0; q < kResLanes; ++q) {
-          if (q < nr) {
-            const double xv = xj[q];
-            const double pr = a * xv;
-            const double pe = fma(a, xv, -pr);
-            double t, e;
-            two_sum(s[q], pr, t, e);
-            s[q] = t;
-            c[q] += e + pe;
-            as[q] = fma(fabs(a), fabs(xv), as[q]);
-          }
+        for (int u = 0; u < kResAhead; ++u) {
+          const int k = k0 + u * kResLanes;
+          jx[u] = k < ke ? P.srow[k] : 0;
+          ix[u] = k < ke ? P.sidx[k] : 0;
         }
-        ra += fabs(a);
+        double av[kResAhead], xc[kResLanes];
+#pragma unroll
+        for (int u = 0; u < kResAhead; ++u) av[u] = vals[ix[u]];
+#pragma unroll
+        for (int q = 0; q < kResLanes; ++q) xc[q] = q < nr ? xi[(int64_t)jx[0] * nr + q] : 0.0;
+#pragma unroll
+        for (int u = 0; u < kResAhead; ++u) {
+          double xn[kResLanes];
+#pragma unroll
+          for (int q = 0; q < kResLanes; ++q)
+            xn[q] = (u + 1 < kResAhead && q < nr) ? xi[(int64_t)jx[u + 1 < kResAhead ? u + 1 : u] * nr + q] : 0.0;
+          if (k0 + u * kResLanes < ke) {
+            const double a = av[u];
+#pragma unroll
+            for (int q = 0; q < kResLanes; ++q) {
+              if (q < nr) {
+                const double xv = xc[q];
+                const double pr = a * xv;
+                const double pe = fma(a, xv, -pr);
+                double t, e;
+                two_sum(s[q], pr, t, e);
+                s[q] = t;
+                c[q] += e + pe;
+                as[q] = fma(fabs(a), fabs(xv), as[q]);
+              }
+            }
+            ra += fabs(a);
+          }
+#pragma unroll
+          for (int q = 0; q < kResLanes; ++q) xc[q] = xn[q];
+        }
       }
     }
     for (int o = kResLanes / 2; o > 0; o >>= 1) {  // within the row's lanes
@@ -2364,15 +2401,13 @@ __global__ void k_residual_rhs(DevPlan P, const double *__restrict__ vals, const
       }
     }
     if (sub < nr && i < n) {
-      const int64_t o = (int64_t)sub * n + P.perm[i];
-      const double bi = b[o];
       double t, e;
       two_sum(bi, -S, t, e);
       const double res = t + (e - C);
-      r[o] = res;
+      r[ob] = res;
       m_r = fmax(m_r, fabs(res));
       m_a = fmax(m_a, ra);
-      m_x = fmax(m_x, fabs(xi[(int64_t)i * nr + sub]));
+      m_x = fmax(m_x, fabs(xs));
       m_b = fmax(m_b, fabs(bi));
       const double den = AS + fabs(bi);
       const double om = den > 0.0 ? fabs(res) / den : (res == 0.0 ? 0.0 : INFINITY);
