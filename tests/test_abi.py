@@ -78,9 +78,7 @@ def test_bad_arguments_are_rejected_before_the_device():
     assert L.smfg_last_times(None, None, None, None) == bad
     assert L.smfg_set_panel_teams(None, None) == bad
     assert L.smfg_set_front_precision(None, None) == bad
-    # a plan that exists is not needed to reject a bad refinement method
-    # or right-hand-side count
-    assert L.smfg_refine_method(None, x, x, 0, 0, 5, 0, 1e-12, None, None, None) == bad
+    assert L.smfg_tc_update(None, 1, 1, None, 1, None, 1, 1, 0) == bad
     L.smfg_plan_destroy(None)  # a null handle is ignored
     null = C.c_void_p()
     L.smfg_plan_destroy(C.byref(null))
@@ -171,3 +169,34 @@ def test_engine_analysis_rejects_a_bad_ordering():
     with pytest.raises(S.SmfgError) as e:
         S.analyse(n, cp, ri, perm=perm)
     assert e.value.code == _macro("SMFG_ERR_INVALID_ARG")
+
+
+_C_CALLER = r"""
+#include "smfg.h"
+int main(void) {
+  smfg_control_t c;
+  smfg_default_control(&c);
+  return (smfg_abi_version() == SMFG_ABI_VERSION && c.abi_version == SMFG_ABI_VERSION && c.nb == 16) ? 0 : 1;
+}
+"""
+
+
+@pytest.mark.parametrize("compiler,flags", [("gcc", ["-std=c99", "-pedantic"]),
+                                            ("g++", ["-std=c++17", "-x", "c++"])])
+def test_header_is_plain_c_and_cpp(compiler, flags, tmp_path):
+    """A C or C++ caller (smf's own code, or a plugin in C) includes the
+    header warning-free and links against the library; the two calls that
+    need no device run."""
+    import shutil
+    import subprocess
+    if shutil.which(compiler) is None:
+        pytest.skip(f"{compiler} not installed")
+    S.lib()
+    src = tmp_path / "caller.c"
+    src.write_text(_C_CALLER)
+    exe = tmp_path / f"caller_{compiler}"
+    libdir = os.path.dirname(S.library_path())
+    subprocess.run([compiler, *flags, "-Wall", "-Wextra", "-Werror", "-I", os.path.dirname(HEADER),
+                    str(src), "-L", libdir, "-lsmfg", f"-Wl,-rpath,{libdir}", "-o", str(exe)],
+                   check=True, capture_output=True)
+    assert subprocess.run([str(exe)]).returncode == 0
