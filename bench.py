@@ -282,6 +282,11 @@ def dgemm_peak_tflops():
 
 
 OMEGA_GATE = 1e-12  # the metric's scaled backward error bar
+# DRAM bytes k_large_defer moves per updated entry, from one ncu capture of
+# the kernel on an 8,000-row front (192.8 MB read + 134.8 MB written for
+# 23.9 M entries, profiles/k_large_defer_front8000.md); the bench's traffic
+# per launch is this times the entries its launches update
+DEFER_DRAM_BYTES_PER_ENTRY = (192.8e6 + 134.8e6) / 23.9e6
 GRAPH_REPLAY = {"kkt": False, "kkt3": False}  # configurations whose steps replay a CUDA graph (default: yes)
 
 
@@ -642,7 +647,10 @@ def main():
         roof = {
             "kernel": "k_large_defer (streamed FP64 deferred updates of the large fronts, rank <= 16)",
             "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-            "traffic": None, "peak_source": hbm_src,
+            "traffic": DEFER_DRAM_BYTES_PER_ENTRY * (prof["defer_bytes"] / 16.0) / max(prof["gemm_launches"], 1),
+            "traffic_source": "per launch, scaled by updated entries from the ncu capture of one "
+                              "8,000-row front (profiles/k_large_defer_front8000.md)",
+            "peak_source": hbm_src,
             "launches": prof["gemm_launches"], "front_updates": prof.get("defer_updates"),
             "front_updates_of_at_most_2_pivots": prof.get("defer_small"),
             "avg_launch_ms": defer_ms / max(prof["gemm_launches"], 1),
