@@ -128,6 +128,7 @@ class Reference:
             lib.refshim_solve.restype = C.c_int
             lib.refshim_refine.argtypes = [C.c_void_p, _f64p, _f64p, C.c_int, _f64p, _i32p]
             lib.refshim_refine.restype = C.c_int
+            lib.refshim_front_work.argtypes = [C.c_void_p, _f64p]
             cls._lib = lib
         return cls._lib
 
@@ -215,6 +216,13 @@ class Reference:
                             delayed=int(st[4]), two_by_two=int(st[5]), max_front=int(st[6]),
                             flops=float(fm[0]), factor_ms=float(fm[1]), f=f, p=p, blk_off=bo,
                             blocks=blocks, row_off=ro, rows=rows, tags=tags, scale=scale)
+
+    def front_work(self):
+        """(the last factorization's Info::front_work, the analysis'
+        delay_free_front_work)."""
+        out = np.zeros(2, dtype=np.float64)
+        self.L.refshim_front_work(self.h, out)
+        return float(out[0]), float(out[1])
 
     def solve(self, b, job: int = 0):
         """Full solve; b of shape (n,) or (nrhs, n). Returns (x, ms)."""

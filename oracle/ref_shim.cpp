@@ -13,6 +13,7 @@
 // Nothing here is linked into or loaded by the product library.
 #include "smf/analysis.hpp"
 #include "smf/control.hpp"
+#include "smf/factor_indef.hpp"
 #include "smf/factor_posdef.hpp"
 #include "smf/info.hpp"
 #include "smf/refinement.hpp"
@@ -196,6 +197,16 @@ int refshim_factor(void *hp, const double *values, int64_t *stats, double *flops
   flops_ms[0] = info.actual_flops;
   flops_ms[1] = h->factor_ms;
   return static_cast<int>(st);
+}
+
+// out[0]: the last factorization's front work (Info::front_work: fully
+// summed columns x rows^2 summed over the fronts,
+// solver/src/multifrontal_serial.cpp:875); out[1]: the analysis' delay-free
+// front work (delay_free_front_work, solver/src/factor_indef.cpp:896-903).
+void refshim_front_work(void *hp, double *out) {
+  auto *h = static_cast<RefHandle *>(hp);
+  out[0] = h->info.front_work;
+  out[1] = h->ak ? smf::delay_free_front_work(*h->ak) : 0.0;
 }
 
 // out: number of solve steps, extent of factor_values, total rows of the
