@@ -20,8 +20,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <functional>
 #include <limits>
-#include <queue>
 #include <stdexcept>
 #include <vector>
 
@@ -100,22 +100,32 @@ int matching_scale_impl(int n, const int *cp, const int *ri, const double *val, 
   std::vector<int> pred(n, -1);     // row -> column it was reached from
   std::vector<char> done(n, 0);
   std::vector<int> touched, popped;
+  std::vector<HeapItem> heap;  // a binary min-heap on (distance, row), kept across searches
+  const auto later = std::greater<HeapItem>();
   int unmatched = 0;
   for (int j0 = 0; j0 < n; ++j0) {
     if (col_mate[j0] >= 0) continue;
-    std::priority_queue<HeapItem, std::vector<HeapItem>, std::greater<HeapItem>> heap;
+    heap.clear();
     touched.clear();
     popped.clear();
+    // The search ends when the first free row leaves the heap, so no row
+    // farther than the nearest free row found so far (lsp) can leave it
+    // before that: such rows are not queued. The rows that leave the heap,
+    // their order and the augmenting path are those of the unbounded search.
+    double lsp = inf;
     auto relax = [&](int j, double dj) {
       for (int64_t k = cnt[j]; k < cnt[j + 1]; ++k) {
         const int i = row[k];
         if (done[i]) continue;
         const double nd = dj + std::max(0.0, cost[k] - u[i] - v[j]);
+        if (nd > lsp) continue;
+        if (row_mate[i] < 0) lsp = nd;
         if (nd < dist[i]) {
           if (dist[i] == inf) touched.push_back(i);
           dist[i] = nd;
           pred[i] = j;
-          heap.push({nd, i});
+          heap.push_back({nd, i});
+          std::push_heap(heap.begin(), heap.end(), later);
         }
       }
     };
@@ -123,8 +133,9 @@ int matching_scale_impl(int n, const int *cp, const int *ri, const double *val, 
     int free_row = -1;
     double D = inf;
     while (!heap.empty()) {
-      const HeapItem it = heap.top();
-      heap.pop();
+      std::pop_heap(heap.begin(), heap.end(), later);
+      const HeapItem it = heap.back();
+      heap.pop_back();
       const int i = it.row;
       if (done[i] || it.d > dist[i]) continue;
       done[i] = 1;

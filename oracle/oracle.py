@@ -129,6 +129,8 @@ class Reference:
             lib.refshim_refine.argtypes = [C.c_void_p, _f64p, _f64p, C.c_int, _f64p, _i32p]
             lib.refshim_refine.restype = C.c_int
             lib.refshim_front_work.argtypes = [C.c_void_p, _f64p]
+            lib.refshim_matching_scale.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p]
+            lib.refshim_matching_scale.restype = C.c_int
             cls._lib = lib
         return cls._lib
 
@@ -378,6 +380,16 @@ def restated_solve(a: Analysis, fx: FactorExport, posdef: bool, b, scale=None):
     x = np.empty(a.n)
     x[a.perm] = w * s[a.perm]
     return x
+
+
+def reference_matching_scale(n, col_ptr, row_idx, values):
+    """The reference's matching scaling (compute_matching_scale) of a lower
+    CSC matrix: (scale, ErrorCode)."""
+    s = np.zeros(n, dtype=np.float64)
+    rc = Reference.lib().refshim_matching_scale(
+        int(n), np.ascontiguousarray(col_ptr, dtype=np.int32), np.ascontiguousarray(row_idx, dtype=np.int32),
+        np.ascontiguousarray(values, dtype=np.float64), s)
+    return s, int(rc)
 
 
 def residual(n, col_ptr, row_idx, values, b, x):

@@ -17,6 +17,7 @@
 #include "smf/factor_posdef.hpp"
 #include "smf/info.hpp"
 #include "smf/refinement.hpp"
+#include "smf/scaling_matching.hpp"
 #include "smf/solver.hpp"
 #include "smf/workspace.hpp"
 
@@ -207,6 +208,23 @@ void refshim_front_work(void *hp, double *out) {
   auto *h = static_cast<RefHandle *>(hp);
   out[0] = h->info.front_work;
   out[1] = h->ak ? smf::delay_free_front_work(*h->ak) : 0.0;
+}
+
+// The reference's symmetric matching scaling of a lower CSC matrix
+// (compute_matching_scale, solver/src/scaling_matching.cpp:1109-1118),
+// n doubles into scale. Returns its ErrorCode (0: success).
+int refshim_matching_scale(int n, const int *col_ptr, const int *row_idx, const double *values,
+                           double *scale) {
+  smf::CscLower A;
+  A.n = n;
+  A.col_ptr.assign(col_ptr, col_ptr + n + 1);
+  A.row_idx.assign(row_idx, row_idx + col_ptr[n]);
+  A.values.assign(values, values + col_ptr[n]);
+  std::vector<double> s;
+  const smf::ErrorCode rc = smf::compute_matching_scale(A, s, 0);
+  if (rc == smf::ErrorCode::Success && s.size() == static_cast<size_t>(n))
+    std::copy(s.begin(), s.end(), scale);
+  return static_cast<int>(rc);
 }
 
 // out: number of solve steps, extent of factor_values, total rows of the
