@@ -8,9 +8,10 @@
 //   - a minimum-cost perfect matching (MC64 job 5, Duff & Koster, "On
 //     algorithms for permuting large entries to the diagonal of a sparse
 //     matrix", SIAM J. Matrix Anal. Appl. 22, 2001): row reduction, a greedy
-//     pass on zero-reduced-cost edges, then one Dijkstra shortest augmenting
-//     path per free column on the reduced costs c - u - v >= 0, the dual
-//     potentials u (rows) and v (columns) updated after each augmentation;
+//     pass on zero-reduced-cost edges and a second one with a one-step
+//     lookahead, then one Dijkstra shortest augmenting path per free column
+//     on the reduced costs c - u - v >= 0, the dual potentials u (rows) and
+//     v (columns) updated after each augmentation;
 //   - scale[i] = exp((u_i + v_i - log colmax_i) / 2), v re-derived on the
 //     matched edge, log-scale clamped to [-340, 340] (:1015-1016): then
 //     |s_i a_ij s_j| <= 1 with equality on the matched entries.
@@ -95,6 +96,35 @@ int matching_scale_impl(int n, const int *cp, const int *ri, const double *val, 
         break;
       }
     }
+  // second greedy pass (the one-step lookahead of MC64's initial matching):
+  // a free column takes a tight row whose column can move to another tight,
+  // free row; the duals stay as they are
+  for (int j = 0; j < n; ++j) {
+    if (col_mate[j] >= 0) continue;
+    bool found = false;
+    for (int64_t k = cnt[j]; k < cnt[j + 1] && !found; ++k) {
+      const int i = row[k];
+      if (cost[k] - u[i] - v[j] > 0.0) continue;
+      const int jj = row_mate[i];
+      if (jj < 0) {
+        row_mate[i] = j;
+        col_mate[j] = i;
+        found = true;
+        break;
+      }
+      for (int64_t q = cnt[jj]; q < cnt[jj + 1]; ++q) {
+        const int i2 = row[q];
+        if (row_mate[i2] < 0 && cost[q] - u[i2] - v[jj] <= 0.0) {
+          row_mate[i2] = jj;
+          col_mate[jj] = i2;
+          row_mate[i] = j;
+          col_mate[j] = i;
+          found = true;
+          break;
+        }
+      }
+    }
+  }
   // shortest augmenting paths from the free columns
   std::vector<double> dist(n, inf);
   std::vector<int> pred(n, -1);     // row -> column it was reached from
