@@ -42,9 +42,10 @@ def _columns_and_rows(a):
 
 
 def delay_free_front_work(a) -> float:
-    """Sum over fronts of columns x rows^2 as analysed (no delays)."""
+    """Sum over fronts of columns x rows^2 as analysed (no delays; int64
+    products and sum, exact below 9.2e18)."""
     ncol, fsym = _columns_and_rows(a)
-    return float(sum(int(c) * int(f) * int(f) for c, f in zip(ncol, fsym)))
+    return float(np.sum(ncol * fsym * fsym))
 
 
 def realized_front_sizes(a, delayed_out) -> np.ndarray:
@@ -64,7 +65,7 @@ def front_work(a, f) -> float:
     ncol, fsym = _columns_and_rows(a)
     f = np.asarray(f, dtype=np.int64)
     elig = ncol + f - fsym
-    return float(sum(int(e) * int(r) * int(r) for e, r in zip(elig, f)))
+    return float(np.sum(elig * f * f))
 
 
 def engine_front_work(solver, a) -> float:
@@ -79,9 +80,8 @@ def cleaned_values(a, values) -> np.ndarray:
     v = np.asarray(values, dtype=np.float64)
     o2c = np.asarray(a.orig_to_clean, dtype=np.int64)
     out = np.zeros(int(np.asarray(a.clean_col_ptr)[-1]), dtype=np.float64)
-    for k in range(v.size):
-        if o2c[k] >= 0:
-            out[o2c[k]] += v[k]
+    kept = o2c >= 0
+    np.add.at(out, o2c[kept], v[kept])  # unbuffered: in input order
     return out
 
 
@@ -112,6 +112,7 @@ def factor_scale_on_delay(solver, a, values, ratio: float = SCALE_ON_DELAY_RATIO
     if limit < 0 or work <= limit:
         return info, out
     out["tripped"] = True
+    out["first_status"] = FACTOR_MAX_PIVOT_DELAYS  # the try given up, as smf reports it
     s = rescue(a, values)
     if s is None:  # no matching scaling: the first factorization stands
         return info, out

@@ -74,7 +74,7 @@ def test_rescue_trips_and_rescales(ref_lib, oracle_lib):
     sv = _OracleSolver(O, a)
     fx, out = D.factor_scale_on_delay(sv, a, v, ratio=ratio)
     assert out["first_work"] == work_ref and out["limit"] == np.floor(ratio * free_ref)
-    assert out["tripped"] and out["rescued"]
+    assert out["tripped"] and out["rescued"] and out["first_status"] == D.FACTOR_MAX_PIVOT_DELAYS
     assert len(sv.scales) == 2 and sv.scales[0] is None and sv.scales[1] is not None
     # the matching scaling cuts the delays' inflation; the inertia stands
     assert out["work"] < out["first_work"]
