@@ -21,14 +21,13 @@ from . import smfg
 
 def merge_analyses(analyses):
     """One smfg.Analysis for the block-diagonal union of `analyses`."""
-    n_off = s_off = e_off = c_off = k_off = 0
+    n_off = s_off = e_off = c_off = k_off = r_off = 0
     parts = {k: [] for k in smfg._ANALYSIS_FIELDS}
     offsets = []
     for a in analyses:
         n, ns = int(a.n), int(a.nsn)
         nnz_perm = int(a.perm_col_ptr[-1])
         nnz_clean = int(a.clean_col_ptr[-1])
-        nin = int(np.asarray(a.orig_to_clean).size)
         offsets.append((n_off, s_off, k_off, c_off, e_off))
         parts["perm"].append(np.asarray(a.perm) + n_off)
         parts["sn_start"].append(np.asarray(a.sn_start) + n_off)
@@ -37,10 +36,10 @@ def merge_analyses(analyses):
         par[par >= 0] += s_off
         parts["sn_parent"].append(par)
         cp = np.asarray(a.child_ptr)
-        parts["child_ptr"].append((cp[:-1] if True else cp) + k_off)
+        parts["child_ptr"].append(cp[:-1] + k_off)
         parts["child_idx"].append(np.asarray(a.child_idx) + s_off)
         frp = np.asarray(a.front_row_ptr)
-        parts["front_row_ptr"].append(frp[:-1] + sum(len(x) for x in parts["front_row_idx"]))
+        parts["front_row_ptr"].append(frp[:-1] + r_off)
         parts["front_row_idx"].append(np.asarray(a.front_row_idx) + n_off)
         parts["postorder"].append(np.asarray(a.postorder) + s_off)
         pcp = np.asarray(a.perm_col_ptr)
@@ -58,7 +57,7 @@ def merge_analyses(analyses):
         k_off += int(cp[-1])
         c_off += nnz_perm
         e_off += nnz_clean
-        del nin
+        r_off += int(frp[-1])
     arrays = {}
     for k, v in parts.items():
         arr = np.concatenate(v).astype(np.int32) if v else np.zeros(0, np.int32)
