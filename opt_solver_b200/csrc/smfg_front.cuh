@@ -871,7 +871,7 @@ __device__ void select_pivot_blk(const FrontRef &v, int k, int limit, const Pivo
                                  FrontShared &sh) {
   const size_t sf = (size_t)v.ld;
   const double *F = v.F;
-  const int f = v.f, ne = v.ne;
+  const int f = v.f;
   int kind = 0, pa = -1, pb = -1;
   if (prm.posdef) {
     const double d = F[(size_t)k * sf + k];

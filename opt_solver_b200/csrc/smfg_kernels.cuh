@@ -1617,7 +1617,7 @@ __global__ void __launch_bounds__(kSolveNT, 4) k_fwd_front(DevPlan P, DevFactor 
   const size_t sf = (size_t)f;
   const bool large = P.sn_fsym[s] >= kLargeMin;
   __shared__ double Ls[32][33];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int warp = threadIdx.x >> 5;
   // every right-hand side at once: gather, children's update vectors in
   // child order, then per 32-column strip the triangle (a warp per
   // right-hand side) and the rows below (each L entry loaded once for all)
@@ -2494,8 +2494,8 @@ __global__ void k_axpy_coef(double *__restrict__ y, const double *__restrict__ x
     y[t] = fma(-c, x[t], y[t]);
 }
 
-// y = x * alpha
-__global__ void k_scale(double *__restrict__ y, const double *__restrict__ x, double alpha, int64_t n) {
+// y = x * alpha; y may be x (in place), so neither pointer is restrict
+__global__ void k_scale(double *y, const double *x, double alpha, int64_t n) {
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
     y[t] = x[t] * alpha;
 }
