@@ -281,6 +281,81 @@ def dgemm_peak_tflops():
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def dominant_roofline(prof: dict, head: str, A: dict, peaks: dict, dgemm_peak=None) -> dict:
+    """The roofline object of the JSON line for the step's dominant kernel,
+    from the profiled factorization's counters (``prof``), the timed arm
+    (``A``: its factor_ms) and the measured peaks."""
+    dgemm_peak = dgemm_peak or dgemm_peak_tflops
+    # the dominant large-front update kernel by device time: the streamed
+    # deferred updates (HBM-bound), the FP64 Schur updates, or the tensor-core
+    # passes of the mixed fronts
+    defer_ms = max(prof.get("gemm_ms", 0.0) - prof.get("schur_ms", 0.0), 0.0)
+    cands = {"defer": defer_ms, "tc": prof.get("tc_ms", 0.0) if head == "mixed" else 0.0,
+             "fp64": prof.get("gemm_ms", 0.0) if defer_ms <= 0.0 else prof.get("schur_ms", 0.0)}
+    dom = max(cands, key=cands.get) if max(cands.values()) > 0 else None
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    hbm_src = "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks.get("hbm_gbs") else "fallback 6650 GB/s"
+    if dom == "defer" and prof.get("defer_bytes", 0) > 0:
+        # bytes: every entry of each deferred update's trapezoid read and
+        # written once (16 bytes), summed on the device
+        achieved = prof["defer_bytes"] / (defer_ms * 1e-3) / 1e9
+        nupd = max(prof.get("defer_updates", 0), 1)
+        roof = {
+            "kernel": "k_large_defer (streamed FP64 deferred updates of the large fronts, rank <= 16)",
+            "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            "traffic": DEFER_DRAM_BYTES_PER_ENTRY * (prof["defer_bytes"] / 16.0) / max(prof["gemm_launches"], 1),
+            "traffic_source": "per launch, scaled by updated entries from the ncu capture of one "
+                              "8,000-row front (profiles/k_large_defer_front8000.md)",
+            "peak_source": hbm_src,
+            "launches": prof["gemm_launches"], "front_updates": prof.get("defer_updates"),
+            "front_updates_of_at_most_2_pivots": prof.get("defer_small"),
+            "avg_launch_ms": defer_ms / max(prof["gemm_launches"], 1),
+            "algorithmic_bytes_per_launch": prof["defer_bytes"] / max(prof["gemm_launches"], 1),
+            "algorithmic_bytes_per_front_update": prof["defer_bytes"] / nupd,
+            "kernel_ms": {"defer": defer_ms, "schur_fp64": prof.get("schur_ms"), "tc": prof.get("tc_ms"),
+                          "pivoting_panels": prof.get("panel_ms")},
+        }
+    elif dom == "tc":
+        # the tensor-core trailing updates (split + product kernels) against
+        # the tensor pipe's rate for TF32 (half the measured BF16 dense
+        # rate) divided by the 3 split products each algorithmic product costs
+        bf = peaks.get("bf16_tflops") or 1590.0
+        peak = bf / 2.0 / 3.0
+        achieved = prof["tc_flops"] / (prof["tc_ms"] * 1e-3) / 1e12
+        roof = {
+            "kernel": "k_tc_split + k_tc_syrk (tcgen05 TF32x3 trailing updates of the mixed fronts)",
+            "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "traffic": None,
+            "peak_source": ("MEASURED_PEAKS.json bf16_tflops" if peaks.get("bf16_tflops") else "fallback 1590")
+            + " / 2 (TF32 rate) / 3 (split products per algorithmic product)",
+            "launches": prof["tc_passes"], "avg_launch_ms": prof["tc_ms"] / max(prof["tc_passes"], 1),
+            "algorithmic_flops_per_launch": prof["tc_flops"] / max(prof["tc_passes"], 1),
+        }
+    elif dom == "fp64":
+        dpeak = dgemm_peak()
+        achieved = prof["gemm_flops"] / (prof["gemm_ms"] * 1e-3) / 1e12
+        roof = {
+            "kernel": "k_large_defer + k_large_schur (FP64 FMA updates of the large fronts)",
+            "bound": "tensor", "achieved": achieved, "peak": dpeak, "unit": "TFLOP/s",
+            "frac": achieved / dpeak if dpeak else None, "traffic": None,
+            "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (FP64 is not in MEASURED_PEAKS.json)",
+            "launches": prof["gemm_launches"], "avg_launch_ms": prof["gemm_ms"] / max(prof["gemm_launches"], 1),
+            "algorithmic_flops_per_launch": prof["gemm_flops"] / max(prof["gemm_launches"], 1),
+        }
+    else:
+        # no large fronts (the batch of small systems): the factor as a
+        # whole against HBM, its algorithmic bytes the front arena written by
+        # assembly and read + written by the front kernels (3 passes)
+        achieved = 3.0 * prof.get("arena_bytes", 0.0) / (A["factor_ms"] * 1e-3) / 1e9 if A["factor_ms"] else 0.0
+        roof = {
+            "kernel": "whole factorization (level kernels of small fronts)", "bound": "hbm",
+            "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+            "peak_source": hbm_src,
+            "algorithmic_bytes_per_factor": 3.0 * prof.get("arena_bytes", 0.0),
+        }
+    return roof
+
+
 OMEGA_GATE = 1e-12  # the metric's scaled backward error bar
 # DRAM bytes k_large_defer moves per updated entry, from one ncu capture of
 # the kernel on an 8,000-row front (192.8 MB read + 134.8 MB written for
@@ -630,73 +705,7 @@ def main():
     info = A["info"]
     peaks = measured_peaks()
     prof = r["profile"]
-    # the dominant large-front update kernel by device time: the streamed
-    # deferred updates (HBM-bound), the FP64 Schur updates, or the tensor-core
-    # passes of the mixed fronts
-    defer_ms = max(prof.get("gemm_ms", 0.0) - prof.get("schur_ms", 0.0), 0.0)
-    cands = {"defer": defer_ms, "tc": prof.get("tc_ms", 0.0) if head == "mixed" else 0.0,
-             "fp64": prof.get("gemm_ms", 0.0) if defer_ms <= 0.0 else prof.get("schur_ms", 0.0)}
-    dom = max(cands, key=cands.get) if max(cands.values()) > 0 else None
-    hbm = peaks.get("hbm_gbs") or 6650.0
-    hbm_src = "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks.get("hbm_gbs") else "fallback 6650 GB/s"
-    if dom == "defer" and prof.get("defer_bytes", 0) > 0:
-        # bytes: every entry of each deferred update's trapezoid read and
-        # written once (16 bytes), summed on the device
-        achieved = prof["defer_bytes"] / (defer_ms * 1e-3) / 1e9
-        nupd = max(prof.get("defer_updates", 0), 1)
-        roof = {
-            "kernel": "k_large_defer (streamed FP64 deferred updates of the large fronts, rank <= 16)",
-            "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-            "traffic": DEFER_DRAM_BYTES_PER_ENTRY * (prof["defer_bytes"] / 16.0) / max(prof["gemm_launches"], 1),
-            "traffic_source": "per launch, scaled by updated entries from the ncu capture of one "
-                              "8,000-row front (profiles/k_large_defer_front8000.md)",
-            "peak_source": hbm_src,
-            "launches": prof["gemm_launches"], "front_updates": prof.get("defer_updates"),
-            "front_updates_of_at_most_2_pivots": prof.get("defer_small"),
-            "avg_launch_ms": defer_ms / max(prof["gemm_launches"], 1),
-            "algorithmic_bytes_per_launch": prof["defer_bytes"] / max(prof["gemm_launches"], 1),
-            "algorithmic_bytes_per_front_update": prof["defer_bytes"] / nupd,
-            "kernel_ms": {"defer": defer_ms, "schur_fp64": prof.get("schur_ms"), "tc": prof.get("tc_ms"),
-                          "pivoting_panels": prof.get("panel_ms")},
-        }
-    elif dom == "tc":
-        # the tensor-core trailing updates (split + product kernels) against
-        # the tensor pipe's rate for TF32 (half the measured BF16 dense
-        # rate) divided by the 3 split products each algorithmic product costs
-        bf = peaks.get("bf16_tflops") or 1590.0
-        peak = bf / 2.0 / 3.0
-        achieved = prof["tc_flops"] / (prof["tc_ms"] * 1e-3) / 1e12
-        roof = {
-            "kernel": "k_tc_split + k_tc_syrk (tcgen05 TF32x3 trailing updates of the mixed fronts)",
-            "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": achieved / peak, "traffic": None,
-            "peak_source": ("MEASURED_PEAKS.json bf16_tflops" if peaks.get("bf16_tflops") else "fallback 1590")
-            + " / 2 (TF32 rate) / 3 (split products per algorithmic product)",
-            "launches": prof["tc_passes"], "avg_launch_ms": prof["tc_ms"] / max(prof["tc_passes"], 1),
-            "algorithmic_flops_per_launch": prof["tc_flops"] / max(prof["tc_passes"], 1),
-        }
-    elif dom == "fp64":
-        dpeak = dgemm_peak_tflops()
-        achieved = prof["gemm_flops"] / (prof["gemm_ms"] * 1e-3) / 1e12
-        roof = {
-            "kernel": "k_large_defer + k_large_schur (FP64 FMA updates of the large fronts)",
-            "bound": "tensor", "achieved": achieved, "peak": dpeak, "unit": "TFLOP/s",
-            "frac": achieved / dpeak if dpeak else None, "traffic": None,
-            "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (FP64 is not in MEASURED_PEAKS.json)",
-            "launches": prof["gemm_launches"], "avg_launch_ms": prof["gemm_ms"] / max(prof["gemm_launches"], 1),
-            "algorithmic_flops_per_launch": prof["gemm_flops"] / max(prof["gemm_launches"], 1),
-        }
-    else:
-        # no large fronts (the batch of small systems): the factor as a
-        # whole against HBM, its algorithmic bytes the front arena written by
-        # assembly and read + written by the front kernels (3 passes)
-        achieved = 3.0 * prof.get("arena_bytes", 0.0) / (A["factor_ms"] * 1e-3) / 1e9 if A["factor_ms"] else 0.0
-        roof = {
-            "kernel": "whole factorization (level kernels of small fronts)", "bound": "hbm",
-            "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
-            "peak_source": hbm_src,
-            "algorithmic_bytes_per_factor": 3.0 * prof.get("arena_bytes", 0.0),
-        }
+    roof = dominant_roofline(prof, head, A, peaks)
     cpu = None
     if not args.no_cpu_baseline:
         try:
