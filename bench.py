@@ -702,7 +702,6 @@ def main():
         return
     head = r["head"]
     A = r["arms"][head]
-    info = A["info"]
     peaks = measured_peaks()
     prof = r["profile"]
     roof = dominant_roofline(prof, head, A, peaks)
