@@ -221,20 +221,29 @@ SMFG_API int smfg_residual(smfg_plan_t plan, const double *b, const double *x, i
                            double *eta_inf, double *omega);
 
 /* smfg_residual for callers that cannot allocate memory. Not a counterpart
- * of any reference interface: smf has no such entry point. Some callers may
- * not allocate device memory while they run, such as an interior-point
- * iteration captured into a CUDA graph (an allocation there breaks the
- * capture) or a real-time controller that does all its allocation up front.
- * smfg_residual allocates its scratch per call; this variant takes device
- * buffers (b, x and r: n x nrhs, leading dimension n; r may be NULL) and
- * works in a fixed scratch array compiled into the library, sized for
- * n <= SMFG_NOALLOC_MAX_N (262,144: 6 MB that every GPU loading the library
- * keeps until the process exits). A larger plan is rejected with
- * SMFG_ERR_INVALID_ARG. The first call on a device looks up the array's
- * device address, so make it before any stream capture. All calls share the
- * one array: calls that overlap on the GPU (other threads or streams) race,
- * so serialize them. Synchronizes the plan's stream. */
+ * of any reference interface: smf has no such entry point. Some callers
+ * must not allocate device memory once they are running: a real-time
+ * controller that reserves everything at start-up (cudaMalloc can block for
+ * an unbounded time and may synchronize the device), or a host program whose
+ * memory is owned by its own pool allocator and already committed to it, so
+ * that an extra cudaMalloc fails for want of memory. smfg_residual allocates
+ * its scratch on every call; this variant takes device buffers (b, x and r:
+ * n x nrhs, leading dimension n; r may be NULL) and works in a fixed scratch
+ * array compiled into the library, sized for n <= SMFG_NOALLOC_MAX_N
+ * (262,144: about 6 MB that every GPU which loads the library holds until
+ * the process exits, whether or not this entry point is ever called). A
+ * larger plan is rejected with SMFG_ERR_INVALID_ARG, a plan that has not been
+ * factored with SMFG_ERR_SINGULAR. The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture. Every call shares the one array and the maxima
+ * in it are cleared at the start of each column, but calls that overlap on
+ * the GPU (from other threads or streams) race on it: serialize them. The
+ * call waits for its kernels (it synchronizes the plan's stream) and copies
+ * the error maxima back to the host to return them. */
 #define SMFG_NOALLOC_MAX_N 262144
+SMFG_API int smfg_residual_noalloc(smfg_plan_t plan, const double *d_b, const double *d_x, double *d_r,
+                                   int nrhs, double *eta_inf, double *omega);
+
 /* Kernel self-benchmark (no reference counterpart): the streamed deferred
  * update on one synthetic front of f rows, ne eligible columns, a pending
  * panel of k <= 16 pivots; best device time of reps launches (ms), the
@@ -242,9 +251,6 @@ SMFG_API int smfg_residual(smfg_plan_t plan, const double *b, const double *x, i
  * tiled kernel's result (0 expected). Allocates 3 (f^2 + 16 f) doubles. */
 SMFG_API int smfg_kernel_bench_defer(int f, int ne, int k, int reps, double *ms, double *bytes,
                                      long long *mismatches);
-
-SMFG_API int smfg_residual_noalloc(smfg_plan_t plan, const double *d_b, const double *d_x, double *d_r,
-                                   int nrhs, double *eta_inf, double *omega);
 
 /* Iterative refinement (classical, refinement.cpp:316-413) of x for b, host
  * arrays (n x nrhs, leading dimension n): at most max_steps solves, stopping

@@ -1404,6 +1404,10 @@ SMFG_API int smfg_residual_noalloc(smfg_plan_t plan, const double *d_b, const do
     set_last_error("smfg_residual_noalloc: matrix order exceeds SMFG_NOALLOC_MAX_N");
     return SMFG_ERR_INVALID_ARG;
   }
+  if (!pl.factored) {
+    set_last_error("smfg_residual_noalloc: the plan holds no factored values");
+    return SMFG_ERR_SINGULAR;
+  }
   try {
     SMFG_CUDA(cudaSetDevice(pl.device));
     clear_stale_error();
@@ -1447,6 +1451,10 @@ SMFG_API int smfg_residual(smfg_plan_t plan, const double *b, const double *x, i
                            double *eta_inf, double *omega) {
   if (!plan || !b || !x || nrhs < 1) return SMFG_ERR_INVALID_ARG;
   Plan &pl = plan->pl;
+  if (!pl.factored) {
+    set_last_error("smfg_residual: the plan holds no factored values");
+    return SMFG_ERR_SINGULAR;
+  }
   try {
     SMFG_CUDA(cudaSetDevice(pl.device));
     clear_stale_error();

@@ -354,6 +354,10 @@ class Solver:
         if rc != SMFG_OK:
             raise SmfgError(rc, "smfg_plan_create")
         self._h = h
+        if device < 0:  # the plan took the current device
+            import torch
+            device = torch.cuda.current_device()
+        self.device = int(device)
         self.posdef = False
         self.info = Info()
         self._scale = None
@@ -531,13 +535,36 @@ class Solver:
         return r, eta.value, om.value
 
     def residual_noalloc(self, d_b, d_x, d_r=None):
-        """smfg_residual_noalloc: the residual of device buffers (CUDA
-        tensors, shape (n,) or (nrhs, n)) computed without allocating
-        anything, for callers that may not allocate (a loop captured into a
-        CUDA graph, a real-time controller). Returns (eta_inf, omega); r is
-        written to d_r when given. The plan's order must not exceed
-        NOALLOC_MAX_N."""
-        nrhs = 1 if d_b.dim() == 1 else int(d_b.shape[0])
+        """smfg_residual_noalloc: the residual of device buffers (float64
+        CUDA tensors on the plan's device, contiguous, shape (n,) or (nrhs,
+        n)) computed in the library's fixed scratch array, allocating
+        nothing. For callers that must not allocate device memory while
+        they run, such as a real-time controller that reserves everything up
+        front, or a program whose device memory is all committed to its own
+        pool. Returns (eta_inf, omega); r is written to d_r when given. The
+        plan's order must not exceed NOALLOC_MAX_N, and calls that overlap
+        on the GPU race on the shared scratch. The buffers are checked here
+        before the library is called: a wrong dtype, layout, size or device
+        would make the kernels read or write past them."""
+        tensors = [("d_b", d_b), ("d_x", d_x)] + ([("d_r", d_r)] if d_r is not None else [])
+        shape = tuple(d_b.shape)
+        if len(shape) not in (1, 2) or shape[-1] != self.n:
+            raise ValueError(f"d_b must have shape (n,) or (nrhs, n) with n = {self.n}, got {shape}")
+        for name, t in tensors:
+            if str(t.dtype) != "torch.float64":
+                raise ValueError(f"{name} must be float64, got {t.dtype}")
+        for name, t in tensors:
+            if tuple(t.shape) != shape:
+                raise ValueError(f"{name} has shape {tuple(t.shape)}, d_b has {shape}")
+        for name, t in tensors:
+            if not t.is_contiguous():
+                raise ValueError(f"{name} must be contiguous")
+        for name, t in tensors:
+            if t.device.type != "cuda" or t.device.index != self.device:
+                raise ValueError(f"{name} must be on cuda:{self.device}, got {t.device}")
+        nrhs = 1 if len(shape) == 1 else shape[0]
+        if nrhs < 1:
+            raise ValueError("no right-hand side given")
         eta, om = C.c_double(), C.c_double()
         rc = lib().smfg_residual_noalloc(self._h, C.c_void_p(d_b.data_ptr()), C.c_void_p(d_x.data_ptr()),
                                          None if d_r is None else C.c_void_p(d_r.data_ptr()), nrhs,

@@ -200,3 +200,35 @@ def test_header_is_plain_c_and_cpp(compiler, flags, tmp_path):
                     str(src), "-L", libdir, "-lsmfg", f"-Wl,-rpath,{libdir}", "-o", str(exe)],
                    check=True, capture_output=True)
     assert subprocess.run([str(exe)]).returncode == 0
+
+
+def _planless_solver(n=8, device=0):
+    """A Solver object without a device plan: enough to exercise the
+    argument checks that run before the library is called."""
+    sv = S.Solver.__new__(S.Solver)
+    sv.n, sv.device, sv._h = n, device, None
+    return sv
+
+
+def test_residual_noalloc_checks_buffers_before_the_library():
+    """residual_noalloc passes raw device pointers to kernels that read and
+    write n * nrhs doubles: every buffer must be float64, contiguous, of
+    d_b's shape and on the plan's device, else ValueError before any call."""
+    import torch
+    sv = _planless_solver(n=8)
+    good = torch.zeros(8, dtype=torch.float64)
+    cases = [
+        (torch.zeros(8, dtype=torch.float32), good, None, "float64"),
+        (good, torch.zeros(8, dtype=torch.float32), None, "float64"),
+        (torch.zeros(2, 16, dtype=torch.float64)[:, ::2], torch.zeros(2, 8, dtype=torch.float64), None,
+         "contiguous"),
+        (torch.zeros(16, 2, dtype=torch.float64).t()[:, :8], torch.zeros(2, 8, dtype=torch.float64),
+         None, "contiguous"),
+        (good, torch.zeros(7, dtype=torch.float64), None, "shape"),
+        (torch.zeros(7, dtype=torch.float64), good, None, "shape"),
+        (good, good, torch.zeros(2, 8, dtype=torch.float64), "shape"),
+        (good, good, None, "cuda:0"),
+    ]
+    for d_b, d_x, d_r, what in cases:
+        with pytest.raises(ValueError, match=what):
+            sv.residual_noalloc(d_b, d_x, d_r)

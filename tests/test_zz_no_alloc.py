@@ -1,14 +1,16 @@
 """The residual entry point that allocates nothing (smfg_residual_noalloc).
 
-It exists for callers that may not allocate device memory while they run:
-an interior-point iteration captured into a CUDA graph, where an allocation
-would break the capture, or a real-time controller that allocates everything
-up front. Its scratch is a fixed array inside the library (orders up to
+It exists for callers that must not allocate device memory once they are
+running: a real-time controller that reserves all of its memory at start-up
+(cudaMalloc can block and may synchronize the device), or a program whose
+device memory is all committed to its own pool, where one more cudaMalloc
+fails. Its scratch is a fixed array inside the library (orders up to
 NOALLOC_MAX_N). These tests check it through the C ABI against the allocating
 smfg_residual on two calls in a row (the shared scratch must not carry
-anything from one call into the next), and that a plan above the size limit
-is refused. This file is collected last: it must pass on its own in a fresh
-process and after the other tests.
+anything from one call into the next), that a plan above the size limit is
+refused, and that a plan which was never factored is refused rather than
+read. This file is collected last: it must pass on its own in a fresh process
+and after the other tests.
 """
 import numpy as np
 import pytest
@@ -64,4 +66,23 @@ def test_noalloc_rejects_orders_above_the_limit():
         sv.residual_noalloc(d, d)
     assert exc.value.code == 1
     assert "SMFG_NOALLOC_MAX_N" in str(exc.value)
+    sv.close()
+
+
+def test_residuals_refuse_a_plan_never_factored():
+    import torch
+    from opt_solver_b200 import smfg
+    from opt_solver_b200 import workloads as W
+    n, cp, ri, v = W.laplacian_2d(12)
+    sv = smfg.Solver(smfg.analyse(n, cp, ri), device=0)
+    d = torch.zeros(n, dtype=torch.float64, device="cuda")
+    for call in (lambda: sv.residual_noalloc(d, d), lambda: sv.residual(np.ones(n), np.ones(n))):
+        with pytest.raises(smfg.SmfgError) as exc:
+            call()
+        assert exc.value.code == smfg.SMFG_ERR_SINGULAR
+    sv.factor(v, posdef=True)
+    b = np.ones(n)
+    x = sv.solve(b)
+    eta, om = sv.residual_noalloc(torch.from_numpy(b).cuda(), torch.from_numpy(np.ascontiguousarray(x)).cuda())
+    assert eta < 1e-14 and om < 1e-14
     sv.close()
