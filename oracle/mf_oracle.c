@@ -21,9 +21,10 @@
  *   fill_ld_column / schur   solver/src/ldlt_kernel.cpp:764-933
  *   portable GEMM loops      solver/src/dense_kernel_lapack.cpp:182-234
  *   add_inertia_2x2          solver/src/dense_indef.cpp:52-83
- * Not restated: static pivoting, delay budgets, the APTP/tile kernel used by
- * deterministic mode on indefinite fronts of >= 512 rows, and the banded SPD
- * path (tests use configurations that do not reach them).
+ *   ldlt_aptp_front          solver/src/ldlt_aptp.cpp:1-751 (deterministic
+ *                            mode's kernel on indefinite fronts of >= 512 rows)
+ * Not restated: static pivoting, delay budgets and the banded SPD path (tests
+ * use configurations that do not reach them).
  */
 #include "mf_oracle.h"
 
@@ -378,14 +379,555 @@ static void schur_update(double *F, int f, int p0, int p, int e, const int8_t *t
   }
 }
 
-/* ldlt_factor_front with first = 0, no static pivoting. Returns the number
- * of accepted pivots. */
-static int ldlt_factor_front(double *F, int f, int num_elig, int *rows, const mfo_params *prm,
-                             int8_t *tags, double *work, mfo_factor *o) {
+/* ------------------------------------------------------------------------
+ * A posteriori threshold pivoting (APTP), the dense kernel deterministic mode
+ * runs on every indefinite front of at least 512 rows
+ * (solver/src/ldlt_aptp.cpp:1-751; dispatch multifrontal_serial.cpp:796-821,
+ * parallel/thread_plan.hpp:43-47; outer block top_tile_nb = 256,
+ * control.hpp:638; inner block aptp_ib = 32, control.hpp:415). The tiled
+ * variant (parallel/tile_tasks.cpp:256-351) splits the same steps into row
+ * and column tiles; every entry takes the same operations in the same order,
+ * so the untiled sweep is restated. ldlt_aptp.cpp is compiled with GCC's
+ * default contraction: each a*b + c*d becomes fma(a, b, c*d), a*b - c*d
+ * becomes fma(a, b, -(c*d)), and c -= a*b a single fma.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+  double inv_u, small;
+  int nb, ib;
+  double *bk[2];    /* block-column backups, per level */
+  double *lt;       /* unit lower L of the tile (ld = block size) */
+  double *ga, *gb, *gc;
+  double *dinv;     /* 2 per pivot: inverse D, diagonal and off-diagonal */
+  double *colbuf;
+  int *top_lp, *q[2], *lpc[2], *cp_lp, *itmp;
+} aptp_ctx;
+
+typedef struct {
+  double *A;
+  int ld, m, ne, level, bs;
+  int8_t *tags;
+  int *rows, *lp, *Q;
+  int nq, num_elim;
+} aptp_sweep;
+
+static size_t ix(int j, int ld) { return (size_t)j * (size_t)ld; }
+
+/* symmetric transposition of view positions p and q (ldlt_aptp.cpp:67-80) */
+static void ap_swap(double *A, int ld, int m, int p, int q, int8_t *tags, int *rows, int *lp) {
+  if (p == q) return;
+  if (p > q) { const int t = p; p = q; q = t; }
+  double t;
+#define SW(x, y) (t = (x), (x) = (y), (y) = t)
+  SW(A[ix(p, ld) + p], A[ix(q, ld) + q]);
+  for (int c = 0; c < p; ++c) SW(A[ix(c, ld) + p], A[ix(c, ld) + q]);
+  for (int c = p + 1; c < q; ++c) SW(A[ix(p, ld) + c], A[ix(c, ld) + q]);
+  for (int r = q + 1; r < m; ++r) SW(A[ix(p, ld) + r], A[ix(q, ld) + r]);
+#undef SW
+  { const int8_t u = tags[p]; tags[p] = tags[q]; tags[q] = u; }
+  { const int u = rows[p]; rows[p] = rows[q]; rows[q] = u; }
+  { const int u = lp[p]; lp[p] = lp[q]; lp[q] = u; }
+}
+
+/* inverse of the 2x2 pivot, scaled by its largest entry (ldlt_aptp.cpp:83-93) */
+static void ap_inv2(double d00, double d10, double d11, double *i00, double *i10, double *i11) {
+  const double s = max3(fabs(d00), fabs(d10), fabs(d11));
+  const double a = d00 / s, b = d10 / s, c = d11 / s;
+  const double inv = 1.0 / (fma(a, c, -(b * b)) * s);
+  *i00 = c * inv;
+  *i10 = -b * inv;
+  *i11 = a * inv;
+}
+
+static double ap_sym(const double *A, int ld, int i, int j) {
+  return (i >= j) ? A[ix(j, ld) + i] : A[ix(i, ld) + j];
+}
+
+static int ap_lok(double l, double inv_u) { return fabs(l) <= inv_u; }
+
+/* complete pivoting on an n x n view (ldlt_aptp.cpp:101-210): returns the
+ * pivots taken; stops at a remaining block below `small` or at a pivot that
+ * would put an |l| > 1/u into the view */
+static int ap_complete(double *A, int ld, int n, int8_t *tags, int *rows, int *lp,
+                       const aptp_ctx *cx) {
+  for (int t = 0; t < n; ++t) { lp[t] = t; tags[t] = 0; }
   int k = 0;
+  while (k < n) {
+    double amax = -1.0;
+    int bi = -1, bj = -1;
+    for (int j = k; j < n; ++j)
+      for (int i = j; i < n; ++i) {
+        const double v = fabs(A[ix(j, ld) + i]);
+        if (v > amax) { amax = v; bi = i; bj = j; }
+      }
+    if (!(amax >= cx->small) || !is_fin(amax)) break;
+    int kind = 1, a = bj, b = -1;
+    if (bi != bj) {
+      const double amm = A[ix(bj, ld) + bj], att = A[ix(bi, ld) + bi], amt = A[ix(bj, ld) + bi];
+      const double delta = fma(amm, att, -(amt * amt));
+      if (fabs(delta) >= 0.5 * amt * amt) { kind = 2; b = bi; }
+      else a = (fabs(att) > fabs(amm)) ? bi : bj;
+    }
+    int ok = 1;
+    if (kind == 1) {
+      const double lim = cx->inv_u * fabs(A[ix(a, ld) + a]);
+      for (int r = k; r < n && ok; ++r)
+        if (r != a && !(fabs(ap_sym(A, ld, r, a)) <= lim)) ok = 0;
+    } else {
+      double i00, i10, i11;
+      ap_inv2(A[ix(a, ld) + a], A[ix(a, ld) + b], A[ix(b, ld) + b], &i00, &i10, &i11);
+      for (int r = k; r < n && ok; ++r) {
+        if (r == a || r == b) continue;
+        const double x0 = ap_sym(A, ld, r, a), x1 = ap_sym(A, ld, r, b);
+        if (!ap_lok(fma(i00, x0, i10 * x1), cx->inv_u) || !ap_lok(fma(i10, x0, i11 * x1), cx->inv_u)) ok = 0;
+      }
+    }
+    if (!ok) break;
+    if (kind == 1) {
+      ap_swap(A, ld, n, k, a, tags, rows, lp);
+      double *ck = A + ix(k, ld);
+      const double inv_d = 1.0 / ck[k];
+      for (int j = k + 1; j < n; ++j) {
+        const double lj = ck[j] * inv_d;
+        if (lj == 0.0) continue;
+        double *cj = A + ix(j, ld);
+        for (int i = j; i < n; ++i) cj[i] = fma(-ck[i], lj, cj[i]);
+      }
+      for (int i = k + 1; i < n; ++i) ck[i] *= inv_d;
+      tags[k] = 1;
+      k += 1;
+    } else {
+      int partner = b;
+      if (a != k) {
+        ap_swap(A, ld, n, k, a, tags, rows, lp);
+        if (partner == k) partner = a;
+      }
+      if (partner != k + 1) ap_swap(A, ld, n, k + 1, partner, tags, rows, lp);
+      double *c0 = A + ix(k, ld), *c1 = A + ix(k + 1, ld);
+      double i00, i10, i11;
+      ap_inv2(c0[k], c0[k + 1], c1[k + 1], &i00, &i10, &i11);
+      for (int j = k + 2; j < n; ++j) {
+        const double a0 = c0[j], a1 = c1[j];
+        const double l0 = fma(i00, a0, i10 * a1), l1 = fma(i10, a0, i11 * a1);
+        if (l0 == 0.0 && l1 == 0.0) continue;
+        double *cj = A + ix(j, ld);
+        for (int i = j; i < n; ++i) cj[i] = cj[i] - fma(c0[i], l0, c1[i] * l1);
+      }
+      for (int i = k + 2; i < n; ++i) {
+        const double a0 = c0[i], a1 = c1[i];
+        c0[i] = fma(i00, a0, i10 * a1);
+        c1[i] = fma(i10, a0, i11 * a1);
+      }
+      tags[k] = 2;
+      tags[k + 1] = -1;
+      k += 2;
+    }
+  }
+  return k;
+}
+
+/* rows [r0, r0 + w) of columns [0, ncols): new row r0 + t takes old row
+ * r0 + perm[t] (ldlt_aptp.cpp:214-221) */
+static void ap_permute_rows(double *A, int ld, int ncols, int r0, int w, const int *perm, double *buf) {
+  for (int c = 0; c < ncols; ++c) {
+    double *col = A + ix(c, ld) + r0;
+    for (int t = 0; t < w; ++t) buf[t] = col[perm[t]];
+    memcpy(col, buf, sizeof(double) * (size_t)w);
+  }
+}
+
+static int ap_identity(const int *perm, int w) {
+  for (int t = 0; t < w; ++t)
+    if (perm[t] != t) return 0;
+  return 1;
+}
+
+/* L = X D^-1 in place, pivot by pivot; the start of the first pivot with an
+ * |l| > 1/u in these rows, or k (ldlt_aptp.cpp:232-265) */
+static int ap_scale_check(double *X, int nrows, int ldx, int k, const int8_t *tags, const double *dinv,
+                          double inv_u) {
+  for (int t = 0; t < k; ++t) {
+    double *x0 = X + ix(t, ldx);
+    if (tags[t] == 2) {
+      double *x1 = x0 + ldx;
+      const double i00 = dinv[2 * t], i10 = dinv[2 * t + 1], i11 = dinv[2 * (t + 1)];
+      int ok = 1;
+      for (int r = 0; r < nrows; ++r) {
+        const double a0 = x0[r], a1 = x1[r];
+        const double l0 = fma(i00, a0, i10 * a1), l1 = fma(i10, a0, i11 * a1);
+        x0[r] = l0;
+        x1[r] = l1;
+        ok = ok && ap_lok(l0, inv_u) && ap_lok(l1, inv_u);
+      }
+      if (!ok) return t;
+      ++t;
+    } else {
+      const double id = dinv[2 * t];
+      int ok = 1;
+      for (int r = 0; r < nrows; ++r) {
+        const double l = x0[r] * id;
+        x0[r] = l;
+        ok = ok && ap_lok(l, inv_u);
+      }
+      if (!ok) return t;
+    }
+  }
+  return k;
+}
+
+/* out[t] = (L D)(row, t) for the pivots [0, k) of the tile (D inline in the
+ * tile) (ldlt_aptp.cpp:270-287) */
+static void ap_row_times_d(const double *lrow, size_t stride, int k, const double *T, int ld,
+                           const int8_t *tags, double *out, size_t ostride) {
+  for (int t = 0; t < k; ++t) {
+    const double d00 = T[ix(t, ld) + t];
+    if (tags[t] == 2) {
+      const double d10 = T[ix(t, ld) + t + 1], d11 = T[ix(t + 1, ld) + t + 1];
+      const double l0 = lrow[t * stride], l1 = lrow[(t + 1) * stride];
+      /* the fused forms GCC gives this function where it is inlined (found
+       * by comparing against the reference bit for bit): the first output
+       * fuses its second product, the second its first */
+      out[t * ostride] = fma(l1, d10, l0 * d00);
+      out[(t + 1) * ostride] = fma(l0, d10, l1 * d11);
+      ++t;
+    } else {
+      out[t * ostride] = lrow[t * stride] * d00;
+    }
+  }
+}
+
+/* X := X L^-T for the k x k unit lower L: column by column, each entry one
+ * fused chain over the earlier columns in order, a zero L entry skipped (the
+ * blocked TRSM + GEMM of ldlt_aptp.cpp:292-304 over the portable loops,
+ * dense_kernel_lapack.cpp:68-84 and :182-203, reduces to this chain). */
+static void ap_trsm(double *X, int nrows, int k, const double *L, int ldl, int ldx) {
+  for (int j = 0; j < k; ++j) {
+    double *xj = X + ix(j, ldx);
+    for (int p = 0; p < j; ++p) {
+      const double l = L[ix(p, ldl) + j];
+      if (l == 0.0) continue;
+      const double *xp = X + ix(p, ldx);
+      for (int i = 0; i < nrows; ++i) xj[i] = fma(-xp[i], l, xj[i]);
+    }
+  }
+}
+
+/* C[m x n] (ld ldc) -= A[m x k] B^T-ish product where the multiplier of
+ * column p for output column j is b(j, p): the portable dgemm / dgemmt loops
+ * with alpha = -1, beta = 1 (dense_kernel_lapack.cpp:159-234). lower: only
+ * rows i >= j of each column. */
+static void ap_gemm_sub(double *C, int m, int n, int k, const double *A, int lda, const double *B,
+                        size_t bj_stride, size_t bp_stride, int ldc, int lower) {
+  for (int j = 0; j < n; ++j) {
+    double *cj = C + ix(j, ldc);
+    for (int p = 0; p < k; ++p) {
+      const double b = B[j * bj_stride + p * bp_stride];
+      if (b == 0.0) continue;
+      const double *ap = A + ix(p, lda);
+      for (int i = lower ? j : 0; i < m; ++i) cj[i] = fma(-ap[i], b, cj[i]);
+    }
+  }
+}
+
+/* C = A B^T (beta 0, alpha 1): each entry a fused chain from zero over p,
+ * a zero B entry skipped (smf_dgemm_nt, dense_kernel_lapack.cpp:182-203) */
+static void ap_gemm_nt(double *C, int m, int n, int k, const double *A, int lda, const double *B, int ldb,
+                       int ldc) {
+  for (int j = 0; j < n; ++j) {
+    double *cj = C + ix(j, ldc);
+    for (int i = 0; i < m; ++i) cj[i] = 0.0;
+    for (int p = 0; p < k; ++p) {
+      const double b = B[ix(p, ldb) + j];
+      if (b == 0.0) continue;
+      const double *ap = A + ix(p, lda);
+      for (int i = 0; i < m; ++i) cj[i] = fma(ap[i], b, cj[i]);
+    }
+  }
+}
+
+static int ap_factor_tile(double *A, int ld, int w, int8_t *tags, int *rows, int *lp, aptp_ctx *cx);
+
+/* steps 1-4 of a block column (ldlt_aptp.cpp:390-449): backup, factor the
+ * diagonal tile, apply its permutation, L_t and D^-1; returns the tile's
+ * pivots */
+static int ap_block_factor(aptp_sweep *sw, int c0, int w, aptp_ctx *cx) {
+  double *A = sw->A;
+  const int ld = sw->ld, m = sw->m, bs = sw->bs;
+  int8_t *tags = sw->tags;
+  int *lp = sw->lp;
+  double *bk = cx->bk[sw->level];
+  int *lpc = cx->lpc[sw->level];
+  const int ldb = m - c0, rb = m - c0 - w;
+  for (int t = 0; t < w; ++t)
+    memcpy(bk + ix(t, ldb) + t, A + ix(c0 + t, ld) + c0 + t, sizeof(double) * (size_t)(m - c0 - t));
+  double *T = A + ix(c0, ld) + c0;
+  const int ne_t = sw->level == 0 ? ap_factor_tile(T, ld, w, tags + c0, sw->rows + c0, lpc, cx)
+                                  : ap_complete(T, ld, w, tags + c0, sw->rows + c0, lpc, cx);
+  if (!ap_identity(lpc, w)) {
+    ap_permute_rows(A, ld, c0, c0, w, lpc, cx->colbuf);
+    for (int t = 0; t < w; ++t)
+      memcpy(A + ix(c0 + t, ld) + c0 + w, bk + ix(lpc[t], ldb) + w, sizeof(double) * (size_t)rb);
+    for (int t = 0; t < w; ++t) cx->itmp[t] = lp[c0 + lpc[t]];
+    memcpy(lp + c0, cx->itmp, sizeof(int) * (size_t)w);
+  }
+  if (ne_t > 0) {
+    double *lt = cx->lt;
+    for (int j = 0; j < ne_t; ++j) {
+      double *lj = lt + ix(j, bs);
+      lj[j] = 1.0;
+      const double *tj = T + ix(j, ld);
+      for (int i = j + 1; i < ne_t; ++i) lj[i] = tj[i];
+    }
+    for (int j = 0; j < ne_t; ++j) {
+      const double *tj = T + ix(j, ld);
+      if (tags[c0 + j] == 2) {
+        lt[ix(j, bs) + j + 1] = 0.0;
+        double i00, i10, i11;
+        ap_inv2(tj[j], tj[j + 1], T[ix(j + 1, ld) + j + 1], &i00, &i10, &i11);
+        cx->dinv[2 * j] = i00;
+        cx->dinv[2 * j + 1] = i10;
+        cx->dinv[2 * (j + 1)] = i11;
+        cx->dinv[2 * (j + 1) + 1] = 0.0;
+        ++j;
+      } else {
+        cx->dinv[2 * j] = 1.0 / tj[j];
+        cx->dinv[2 * j + 1] = 0.0;
+      }
+    }
+  }
+  return ne_t;
+}
+
+/* ApplyN on rows [r0, r1) (ldlt_aptp.cpp:451-456) */
+static int ap_apply_n(const aptp_sweep *sw, int c0, int ne_t, int r0, int r1, const aptp_ctx *cx) {
+  if (ne_t <= 0 || r1 <= r0) return ne_t;
+  double *X = sw->A + ix(c0, sw->ld) + r0;
+  ap_trsm(X, r1 - r0, ne_t, cx->lt, sw->bs, sw->ld);
+  return ap_scale_check(X, r1 - r0, sw->ld, ne_t, sw->tags + c0, cx->dinv, cx->inv_u);
+}
+
+/* ApplyT, restore, UpdateNN (all eligible columns), UpdateNT / TN
+ * (ldlt_aptp.cpp:458-588) */
+static int ap_block_finish(aptp_sweep *sw, int c0, int w, int ne_t, int nelim, aptp_ctx *cx) {
+  double *A = sw->A;
+  const int ld = sw->ld, m = sw->m, ne = sw->ne, bs = sw->bs;
+  int8_t *tags = sw->tags;
+  const int *Q = sw->Q;
+  const int nq = sw->nq;
+  double *bk = cx->bk[sw->level];
+  const int *lpc = cx->lpc[sw->level];
+  const int ldb = m - c0, rb = m - c0 - w;
+  double *T = A + ix(c0, ld) + c0;
+  if (ne_t > 0) {
+    for (int i0 = 0; i0 < nq && nelim > 0; i0 += bs) {
+      const int nc = (bs < nq - i0) ? bs : nq - i0;
+      for (int t = 0; t < nelim; ++t)
+        for (int ii = 0; ii < nc; ++ii) cx->ga[ix(t, bs) + ii] = A[ix(Q[i0 + ii], ld) + c0 + t];
+      ap_trsm(cx->ga, nc, nelim, cx->lt, bs, bs);
+      nelim = ap_scale_check(cx->ga, nc, bs, nelim, tags + c0, cx->dinv, cx->inv_u);
+    }
+    if (nelim > 0 && tags[c0 + nelim - 1] == 2) --nelim;
+  }
+  if (nelim < w) {
+    for (int s2 = nelim; s2 < w; ++s2) {
+      double *col = T + ix(s2, ld);
+      for (int s1 = s2; s1 < w; ++s1) {
+        const int a = lpc[s1], b = lpc[s2];
+        col[s1] = (a >= b) ? bk[ix(b, ldb) + a] : bk[ix(a, ldb) + b];
+      }
+      memcpy(col + w, bk + ix(lpc[s2], ldb) + w, sizeof(double) * (size_t)rb);
+      tags[c0 + s2] = 0;
+    }
+  }
+  if (nelim > 0) {
+    for (int i0 = 0; i0 < nq; i0 += bs) {
+      const int nc = (bs < nq - i0) ? bs : nq - i0;
+      if (nq > bs) {
+        for (int t = 0; t < nelim; ++t)
+          for (int ii = 0; ii < nc; ++ii) cx->ga[ix(t, bs) + ii] = A[ix(Q[i0 + ii], ld) + c0 + t];
+        ap_trsm(cx->ga, nc, nelim, cx->lt, bs, bs);
+        ap_scale_check(cx->ga, nc, bs, nelim, tags + c0, cx->dinv, cx->inv_u);
+      }
+      for (int t = 0; t < nelim; ++t)
+        for (int ii = 0; ii < nc; ++ii) A[ix(Q[i0 + ii], ld) + c0 + t] = cx->ga[ix(t, bs) + ii];
+    }
+    /* UpdateNN: W = (L D)^T of the eligible columns [e0, ne) goes into the
+     * strict upper triangle rows [c0, c0 + nelim) of those columns */
+    const int e0 = c0 + nelim, msz = ne - e0;
+    if (msz > 0) {
+      for (int col = e0; col < ne; ++col)
+        ap_row_times_d(A + ix(c0, ld) + col, (size_t)ld, nelim, T, ld, tags + c0, A + ix(col, ld) + c0, 1);
+      const double *Wt = A + ix(e0, ld) + c0;
+      ap_gemm_sub(A + ix(e0, ld) + e0, msz, msz, nelim, A + ix(c0, ld) + e0, ld, Wt, (size_t)ld, 1, ld, 1);
+      if (m > ne)
+        ap_gemm_sub(A + ix(e0, ld) + ne, m - ne, msz, nelim, A + ix(c0, ld) + ne, ld, Wt, (size_t)ld, 1, ld, 0);
+    }
+    /* UpdateNT / TN: the earlier failed columns, rows [e0, m) and their
+     * block among themselves */
+    const int mr = m - e0;
+    for (int j0 = 0; j0 < nq; j0 += bs) {
+      const int nj = (bs < nq - j0) ? bs : nq - j0;
+      for (int jj = 0; jj < nj; ++jj)
+        ap_row_times_d(A + ix(Q[j0 + jj], ld) + c0, 1, nelim, T, ld, tags + c0, cx->gb + jj, (size_t)bs);
+      if (mr > 0) {
+        double *Tm = bk;
+        ap_gemm_nt(Tm, mr, nj, nelim, A + ix(c0, ld) + e0, ld, cx->gb, bs, mr);
+        for (int jj = 0; jj < nj; ++jj) {
+          double *dst = A + ix(Q[j0 + jj], ld) + e0;
+          const double *src = Tm + ix(jj, mr);
+          for (int r = 0; r < mr; ++r) dst[r] -= src[r];
+        }
+      }
+      for (int i0 = j0; i0 < nq; i0 += bs) {
+        const int ni = (bs < nq - i0) ? bs : nq - i0;
+        for (int t = 0; t < nelim; ++t)
+          for (int ii = 0; ii < ni; ++ii) cx->ga[ix(t, bs) + ii] = A[ix(Q[i0 + ii], ld) + c0 + t];
+        ap_gemm_nt(cx->gc, ni, nj, nelim, cx->ga, bs, cx->gb, bs, bs);
+        for (int jj = 0; jj < nj; ++jj) {
+          const int qj = Q[j0 + jj];
+          double *colq = A + ix(qj, ld);
+          for (int ii = 0; ii < ni; ++ii) {
+            const int qi = Q[i0 + ii];
+            if (qi >= qj) colq[qi] -= cx->gc[ix(jj, bs) + ii];
+          }
+        }
+      }
+    }
+  }
+  sw->num_elim += nelim;
+  for (int s = nelim; s < w; ++s) sw->Q[sw->nq++] = c0 + s;
+  return nelim;
+}
+
+/* one sweep over the leading ne columns of the m x m view; level 0 the
+ * front (block nb), level 1 a diagonal tile (block ib); then the failed
+ * columns behind the pivots and, at the front level, the deferred update of
+ * the non-eligible triangle (ldlt_aptp.cpp:317-330, :603-659) */
+static int ap_sweep(double *A, int ld, int m, int ne, int level, int8_t *tags, int *rows, int *lp,
+                    aptp_ctx *cx) {
+  aptp_sweep sw;
+  sw.A = A; sw.ld = ld; sw.m = m; sw.ne = ne; sw.level = level;
+  sw.bs = level == 0 ? cx->nb : cx->ib;
+  sw.tags = tags; sw.rows = rows; sw.lp = lp; sw.Q = cx->q[level];
+  sw.nq = 0; sw.num_elim = 0;
+  for (int t = 0; t < ne; ++t) { lp[t] = t; tags[t] = 0; }
+  for (int c0 = 0; c0 < ne; c0 += sw.bs) {
+    const int w = (sw.bs < ne - c0) ? sw.bs : ne - c0;
+    const int ne_t = ap_block_factor(&sw, c0, w, cx);
+    int nelim = ne_t;
+    if (ne_t > 0 && m - c0 - w > 0) nelim = ap_apply_n(&sw, c0, ne_t, c0 + w, m, cx);
+    ap_block_finish(&sw, c0, w, ne_t, nelim, cx);
+  }
+  if (sw.num_elim < sw.ne) {
+    int dst = 0;
+    for (int src = 0; src < sw.ne; ++src) {
+      if (sw.tags[src] == 0) continue;
+      if (src != dst) ap_swap(sw.A, sw.ld, sw.m, dst, src, sw.tags, sw.rows, sw.lp);
+      ++dst;
+    }
+  }
+  const int qn = sw.m - sw.ne, p = sw.num_elim;
+  if (qn > 0 && p > 0) {
+    for (int c = 0; c < p; ++c) {
+      const double *Lc = A + ix(c, ld);
+      if (tags[c] == 2) {
+        const double *Lc1 = Lc + ld;
+        const double d00 = Lc[c], d10 = Lc[c + 1], d11 = Lc1[c + 1];
+        for (int i = ne; i < m; ++i) {
+          A[ix(i, ld) + c] = fma(Lc[i], d00, Lc1[i] * d10);
+          A[ix(i, ld) + c + 1] = fma(Lc[i], d10, Lc1[i] * d11);
+        }
+        ++c;
+      } else {
+        const double d = Lc[c];
+        for (int i = ne; i < m; ++i) A[ix(i, ld) + c] = Lc[i] * d;
+      }
+    }
+    ap_gemm_sub(A + ix(ne, ld) + ne, qn, qn, p, A + ne, ld, A + ix(ne, ld), (size_t)ld, 1, ld, 1);
+  }
+  return sw.num_elim;
+}
+
+/* diagonal tile of the outer sweep: the inner sweep (block ib), then
+ * complete pivoting on what failed inside the tile (ldlt_aptp.cpp:335-350) */
+static int ap_factor_tile(double *A, int ld, int w, int8_t *tags, int *rows, int *lp, aptp_ctx *cx) {
+  if (w <= cx->ib) return ap_complete(A, ld, w, tags, rows, lp, cx);
+  int ne1 = ap_sweep(A, ld, w, w, 1, tags, rows, lp, cx);
+  if (ne1 < w) {
+    const int n2 = w - ne1;
+    int *lp2 = cx->cp_lp;
+    const int ne2 = ap_complete(A + ix(ne1, ld) + ne1, ld, n2, tags + ne1, rows + ne1, lp2, cx);
+    if (!ap_identity(lp2, n2)) {
+      ap_permute_rows(A, ld, ne1, ne1, n2, lp2, cx->colbuf);
+      for (int t = 0; t < n2; ++t) cx->itmp[t] = lp[ne1 + lp2[t]];
+      memcpy(lp + ne1, cx->itmp, sizeof(int) * (size_t)n2);
+    }
+    ne1 += ne2;
+  }
+  return ne1;
+}
+
+/* ldlt_aptp_front (ldlt_aptp.cpp:728-749): returns the pivots eliminated;
+ * inertia and flops added to o (front_result, :704-724: every pivot's
+ * inertia against the effective small value) */
+static int ldlt_aptp_front(double *F, int f, int num_elig, int *rows, const mfo_params *prm, int8_t *tags,
+                           mfo_factor *o) {
+  if (f <= 0 || num_elig <= 0) return 0;
+  const int ne1 = num_elig > 1 ? num_elig : 1;
+  int nb = prm->aptp_nb > 1 ? prm->aptp_nb : 1;
+  if (nb > ne1) nb = ne1;
+  int ib = prm->aptp_ib > 1 ? prm->aptp_ib : 1;
+  if (ib > nb) ib = nb;
+  aptp_ctx cx;
+  cx.inv_u = 1.0 / prm->u;
+  cx.small = prm->eff_small;
+  cx.nb = nb;
+  cx.ib = ib;
+  const size_t sf = (size_t)f, snb = (size_t)nb, sib = (size_t)ib;
+  double *mem = (double *)malloc(sizeof(double) * (sf * snb + snb * sib + 4 * snb * snb + 2 * snb + sf));
+  int *imem = (int *)malloc(sizeof(int) * (2 * (size_t)ne1 + 4 * snb + sib));
+  double *p = mem;
+  cx.bk[0] = p; p += sf * snb;
+  cx.bk[1] = p; p += snb * sib;
+  cx.lt = p; p += snb * snb;
+  cx.ga = p; p += snb * snb;
+  cx.gb = p; p += snb * snb;
+  cx.gc = p; p += snb * snb;
+  cx.dinv = p; p += 2 * snb;
+  cx.colbuf = p;
+  int *ip = imem;
+  cx.top_lp = ip; ip += ne1;
+  cx.q[0] = ip; ip += ne1;
+  cx.lpc[0] = ip; ip += nb;
+  cx.q[1] = ip; ip += nb;
+  cx.lpc[1] = ip; ip += ib;
+  cx.cp_lp = ip; ip += nb;
+  cx.itmp = ip;
+  const int pe = ap_sweep(F, f, f, num_elig, 0, tags, rows, cx.top_lp, &cx);
+  free(mem);
+  free(imem);
+  for (int k = 0; k < pe; ++k) {
+    if (tags[k] == 2) {
+      inertia_2x2(F[k * sf + k], F[k * sf + k + 1], F[(k + 1) * sf + k + 1], prm->eff_small, o);
+      const double rem = (double)(f - (k + 2));
+      o->flops += 6.0 * rem + 2.0 * rem * (rem + 1.0);
+      ++k;
+    } else {
+      inertia_1x1(F[k * sf + k], prm->eff_small, o);
+      const double rem = (double)(f - (k + 1));
+      o->flops += rem + rem * (rem + 1.0);
+    }
+  }
+  return pe;
+}
+
+/* ldlt_factor_front from column `first` (0, or the pivots an APTP sweep
+ * took before it), no static pivoting. Returns the number of accepted pivots. */
+static int ldlt_factor_front(double *F, int f, int num_elig, int *rows, const mfo_params *prm,
+                             int8_t *tags, double *work, int first, mfo_factor *o) {
+  int k = first;
   g_mixed_bits = (prm->mixed_bits > 0 && prm->mixed_min_front > 0 && f >= prm->mixed_min_front)
                      ? prm->mixed_bits : 0;
-  if (f < prm->blocked_min_front || prm->nb <= 1) {
+  if (f - first < prm->blocked_min_front || prm->nb <= 1) {
     while (k < num_elig) {
       pchoice pc = select_pivot(F, f, f, k, num_elig, num_elig, prm);
       if (pc.kind == 0) break;
@@ -466,7 +1008,7 @@ static int ldlt_factor_front(double *F, int f, int num_elig, int *rows, const mf
       deferred_update(F, f, ss, k, k, num_elig, W);
     }
   }
-  schur_update(F, f, 0, k, num_elig, tags, work);
+  schur_update(F, f, first, k, num_elig, tags, work);
   return k;
 }
 
@@ -475,7 +1017,7 @@ void mfo_factor_front(double *F, int f, int ne, int *rows, const mfo_params *prm
   mfo_factor o;
   memset(&o, 0, sizeof(o));
   double *work = (double *)malloc(sizeof(double) * ((size_t)f * (prm->nb + 2) + (size_t)f * f + 1));
-  const int k = ldlt_factor_front(F, f, ne, rows, prm, tags, work, &o);
+  const int k = ldlt_factor_front(F, f, ne, rows, prm, tags, work, 0, &o);
   free(work);
   out[0] = o.pos;
   out[1] = o.neg;
@@ -483,9 +1025,51 @@ void mfo_factor_front(double *F, int f, int ne, int *rows, const mfo_params *prm
   out[3] = k;
 }
 
+/* Test hook: the assembled front of one supernode, captured by the next
+ * mfo_factorize before its kernel runs (for dense-kernel parity on real
+ * fronts). */
+static int g_cap_s = -1;
+static double *g_cap_F = NULL;
+static int64_t g_cap_cap = 0;
+static int *g_cap_rows = NULL;
+static int g_cap_info[2];
+
+void mfo_capture_front(int s, double *F, int64_t cap, int *rows) {
+  g_cap_s = s;
+  g_cap_F = F;
+  g_cap_cap = cap;
+  g_cap_rows = rows;
+  g_cap_info[0] = g_cap_info[1] = -1;
+}
+
+void mfo_captured_size(int *f, int *num_elig) {
+  *f = g_cap_info[0];
+  *num_elig = g_cap_info[1];
+}
+
+/* The APTP kernel alone on a dense front (tests): out[0..4] = eliminated,
+ * failed, positive, negative, zero pivots. */
+void mfo_aptp_front(double *F, int f, int ne, int *rows, const mfo_params *prm, int8_t *tags, int64_t *out) {
+  mfo_factor o;
+  memset(&o, 0, sizeof(o));
+  const int pe = ldlt_aptp_front(F, f, ne, rows, prm, tags, &o);
+  out[0] = pe;
+  out[1] = ne - pe;
+  out[2] = o.pos;
+  out[3] = o.neg;
+  out[4] = o.zero;
+}
+
+/* Deterministic mode's choice of the APTP kernel: plain threshold pivoting
+ * on an indefinite front of at least aptp_min_rows realized rows, with
+ * u >= kWeakPivotRatio (thread_plan.cpp:264-268, thread_plan.hpp:43-52) */
+static int aptp_front(const mfo_params *prm, int f) {
+  return prm->aptp_min_rows > 0 && !prm->posdef && f >= prm->aptp_min_rows && prm->u >= WEAK_PIVOT_RATIO;
+}
+
 int mfo_factorize(const mfo_analysis *a, const double *pv, const mfo_params *prm, mfo_factor *o) {
   const int n = a->n, ns = a->nsn;
-  o->pos = o->neg = o->zero = o->delayed = o->two_by_two = o->max_front = 0;
+  o->pos = o->neg = o->zero = o->delayed = o->two_by_two = o->max_front = o->aptp_failed = 0;
   o->flops = 0.0;
   o->status = 0;
   double **front = (double **)calloc((size_t)ns, sizeof(double *));
@@ -544,9 +1128,26 @@ int mfo_factorize(const mfo_analysis *a, const double *pv, const mfo_params *prm
         }
       }
     }
+    if (s == g_cap_s) {
+      g_cap_info[0] = f;
+      g_cap_info[1] = num_elig;
+      if ((int64_t)f * f <= g_cap_cap) {
+        memcpy(g_cap_F, F, sizeof(double) * (size_t)f * f);
+        memcpy(g_cap_rows, rows, sizeof(int) * (size_t)f);
+      }
+    }
     int8_t *tags = (int8_t *)calloc((size_t)(f > 0 ? f : 1), 1);
     double *work = (double *)malloc(sizeof(double) * ((size_t)f * (prm->nb + 2) + (size_t)f * f + 1));
-    const int p = ldlt_factor_front(F, f, num_elig, rows, prm, tags, work, o);
+    int p;
+    if (aptp_front(prm, f)) {
+      /* APTP, then the threshold kernel on the columns it failed (their
+       * Schur state is current) (multifrontal_serial.cpp:796-821) */
+      p = ldlt_aptp_front(F, f, num_elig, rows, prm, tags, o);
+      o->aptp_failed += num_elig - p;
+      if (p < num_elig) p = ldlt_factor_front(F, f, num_elig, rows, prm, tags, work, p, o);
+    } else {
+      p = ldlt_factor_front(F, f, num_elig, rows, prm, tags, work, 0, o);
+    }
     free(work);
     if (f > o->max_front) o->max_front = f;
     const int is_root = a->sn_parent[s] < 0;

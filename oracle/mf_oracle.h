@@ -32,6 +32,10 @@ typedef struct {
    * mixed_bits significant bits: 8 for BF16x3, 11 for TF32x3; the three
    * products hi*hi, hi*lo, lo*hi summed in FP32) subtracted from FP64. */
   int mixed_min_front, mixed_bits;
+  /* Deterministic mode's APTP kernel (ldlt_aptp.cpp) on indefinite fronts of
+   * at least aptp_min_rows realized rows (0: never; the reference uses 512),
+   * outer block aptp_nb (256), inner block aptp_ib (32). */
+  int aptp_min_rows, aptp_nb, aptp_ib;
 } mfo_params;
 
 typedef struct {
@@ -47,6 +51,7 @@ typedef struct {
   int8_t *tags;
   /* counts */
   int64_t pos, neg, zero, delayed, two_by_two, max_front;
+  int64_t aptp_failed; /* columns the APTP kernel failed (Info::aptp_failed_columns) */
   double flops;
   int status; /* 0 ok, 1 not positive definite, 2 singular (zero pivots), 3 capacity, 4 non-finite D */
 } mfo_factor;
@@ -60,6 +65,17 @@ int mfo_factorize(const mfo_analysis *a, const double *pvals, const mfo_params *
  * the known-answer tests of the dense kernel. */
 void mfo_factor_front(double *F, int f, int ne, int *rows, const mfo_params *prm, int8_t *tags,
                       int64_t *out);
+
+/* Tests: capture supernode s's assembled front (f x f column-major, before
+ * its kernel) and realized rows during the next mfo_factorize, when f * f <=
+ * cap; mfo_captured_size gives its f and eligible columns (-1: not reached). */
+void mfo_capture_front(int s, double *F, int64_t cap, int *rows);
+void mfo_captured_size(int *f, int *num_elig);
+
+/* The APTP kernel alone on a dense front (ldlt_aptp_front,
+ * solver/src/ldlt_aptp.cpp:739): F, rows, tags (f) in place; out[0..4] =
+ * eliminated, failed, positive, negative, zero pivots. */
+void mfo_aptp_front(double *F, int f, int ne, int *rows, const mfo_params *prm, int8_t *tags, int64_t *out);
 
 /* In-place full solve of A x = b on the permuted, scaled system:
  * x (n, new numbering) overwritten. */

@@ -85,6 +85,7 @@ class FactorExport:
     rows: np.ndarray
     tags: np.ndarray | None
     scale: np.ndarray
+    aptp_failed: int = 0  # columns the APTP kernel failed (Info::aptp_failed_columns)
 
     def block(self, s: int) -> np.ndarray:
         f, p = int(self.f[s]), int(self.p[s])
@@ -129,6 +130,8 @@ class Reference:
             lib.refshim_refine.argtypes = [C.c_void_p, _f64p, _f64p, C.c_int, _f64p, _i32p]
             lib.refshim_refine.restype = C.c_int
             lib.refshim_front_work.argtypes = [C.c_void_p, _f64p]
+            lib.refshim_aptp_failed.argtypes = [C.c_void_p]
+            lib.refshim_aptp_failed.restype = C.c_int64
             lib.refshim_matching_scale.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p]
             lib.refshim_matching_scale.restype = C.c_int
             cls._lib = lib
@@ -217,7 +220,8 @@ class Reference:
         return FactorExport(status=int(st[0]), inertia=(int(st[1]), int(st[2]), int(st[3])),
                             delayed=int(st[4]), two_by_two=int(st[5]), max_front=int(st[6]),
                             flops=float(fm[0]), factor_ms=float(fm[1]), f=f, p=p, blk_off=bo,
-                            blocks=blocks, row_off=ro, rows=rows, tags=tags, scale=scale)
+                            blocks=blocks, row_off=ro, rows=rows, tags=tags, scale=scale,
+                            aptp_failed=int(self.L.refshim_aptp_failed(self.h)))
 
     def front_work(self):
         """(the last factorization's Info::front_work, the analysis'
@@ -258,7 +262,8 @@ class _MfoAnalysis(C.Structure):
 class _MfoParams(C.Structure):
     _fields_ = [("u", C.c_double), ("eff_small", C.c_double), ("small_pivot", C.c_double),
                 ("nb", C.c_int), ("blocked_min_front", C.c_int), ("posdef", C.c_int),
-                ("mixed_min_front", C.c_int), ("mixed_bits", C.c_int)]
+                ("mixed_min_front", C.c_int), ("mixed_bits", C.c_int),
+                ("aptp_min_rows", C.c_int), ("aptp_nb", C.c_int), ("aptp_ib", C.c_int)]
 
 
 class _MfoFactor(C.Structure):
@@ -267,7 +272,7 @@ class _MfoFactor(C.Structure):
                 ("rows", C.c_void_p), ("row_cap", C.c_int64), ("tags", C.c_void_p),
                 ("pos", C.c_int64), ("neg", C.c_int64), ("zero", C.c_int64),
                 ("delayed", C.c_int64), ("two_by_two", C.c_int64), ("max_front", C.c_int64),
-                ("flops", C.c_double), ("status", C.c_int)]
+                ("aptp_failed", C.c_int64), ("flops", C.c_double), ("status", C.c_int)]
 
 
 _olib = None
@@ -289,6 +294,12 @@ def _oracle_lib():
     return _olib
 
 
+# Deterministic mode's APTP kernel: indefinite fronts of at least 512 rows
+# (kTopTileMinFront, parallel/thread_plan.hpp:43), outer block 256
+# (Control::top_tile_nb, control.hpp:638), inner block 32 (Control::aptp_ib).
+APTP_MIN_ROWS, APTP_NB, APTP_IB = 512, 256, 32
+
+
 def factor_front(A, ne: int, u: float = 0.01, small: float = 1e-20, nb: int = 16,
                  blocked_min_front: int = 96, posdef: bool = False):
     """One dense front (f x f symmetric, lower triangle used, first ne columns
@@ -302,7 +313,7 @@ def factor_front(A, ne: int, u: float = 0.01, small: float = 1e-20, nb: int = 16
     out = np.zeros(4, dtype=np.int64)
     m = float(np.max(np.abs(F))) if F.size else 0.0
     eff = small * m if 0.0 < m < small else small
-    prm = _MfoParams(u, eff, small, nb, blocked_min_front, int(posdef), 0, 0)
+    prm = _MfoParams(u, eff, small, nb, blocked_min_front, int(posdef), 0, 0, 0, APTP_NB, APTP_IB)
     _oracle_lib().mfo_factor_front(flat, f, ne, rows, C.byref(prm), tags, out)
     return flat.reshape(f, f).T, rows, tags, tuple(int(x) for x in out)
 
@@ -334,17 +345,20 @@ def eff_small_of(pv, small=1e-20):
 
 def restated_factorize(a: Analysis, pv, posdef: bool, u: float = 0.01, small: float = 1e-20,
                        nb: int = 16, blocked_min_front: int = 96, mixed_min_front: int = 0,
-                       mixed_bits: int = 0):
-    """Run mf_oracle.c on analysis `a` and permuted values `pv`. mixed_*:
-    emulate the engine's split-product updates on fronts of at least
-    mixed_min_front rows (mixed_bits 8: BF16x3, 11: TF32x3)."""
+                       mixed_bits: int = 0, aptp_min_rows: int = APTP_MIN_ROWS):
+    """Run mf_oracle.c on analysis `a` and permuted values `pv`: the
+    reference's deterministic mode (APTP on indefinite fronts of at least
+    aptp_min_rows rows; 0 = threshold pivoting everywhere, the reference's
+    one-thread default mode). mixed_*: emulate the engine's split-product
+    updates on fronts of at least mixed_min_front rows (mixed_bits 8: BF16x3,
+    11: TF32x3)."""
     lib = _oracle_lib()
     keep = [np.ascontiguousarray(x, dtype=np.int32) for x in (
         a.sn_start, a.sn_end, a.sn_parent, a.child_ptr, a.child_idx, a.front_row_ptr,
         a.front_row_idx, a.postorder, a.perm_col_ptr, a.perm_row_idx)]
     ca = _MfoAnalysis(a.n, a.nsn, *[x.ctypes.data for x in keep])
     prm = _MfoParams(u, eff_small_of(pv, small), small, nb, blocked_min_front, int(posdef),
-                     int(mixed_min_front), int(mixed_bits))
+                     int(mixed_min_front), int(mixed_bits), int(aptp_min_rows), APTP_NB, APTP_IB)
     ns = a.nsn
     fsz = np.diff(a.front_row_ptr).astype(np.int64)
     # capacity: front rows grow with delays; allow generous room
@@ -364,7 +378,7 @@ def restated_factorize(a: Analysis, pv, posdef: bool, u: float = 0.01, small: fl
     fx = FactorExport(status=out.status, inertia=(out.pos, out.neg, out.zero), delayed=out.delayed,
                       two_by_two=out.two_by_two, max_front=out.max_front, flops=out.flops,
                       factor_ms=0.0, f=f, p=p, blk_off=bo, blocks=blocks, row_off=ro, rows=rows,
-                      tags=None if posdef else tags, scale=np.zeros(0))
+                      tags=None if posdef else tags, scale=np.zeros(0), aptp_failed=out.aptp_failed)
     fx._c = (ca, keep, out)  # keep alive for solves
     return fx
 

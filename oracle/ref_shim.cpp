@@ -16,6 +16,8 @@
 #include "smf/factor_indef.hpp"
 #include "smf/factor_posdef.hpp"
 #include "smf/info.hpp"
+#include "smf/ldlt_aptp.hpp"
+#include "parallel/tile_tasks.hpp"
 #include "smf/refinement.hpp"
 #include "smf/scaling_matching.hpp"
 #include "smf/solver.hpp"
@@ -198,6 +200,36 @@ int refshim_factor(void *hp, const double *values, int64_t *stats, double *flops
   flops_ms[0] = info.actual_flops;
   flops_ms[1] = h->factor_ms;
   return static_cast<int>(st);
+}
+
+// The reference's dense APTP front kernel alone (ldlt_aptp.cpp:739, or the
+// tile-task form deterministic mode runs, parallel/tile_tasks.cpp:256, on one
+// thread): F f x f column-major (lower), the first ne columns eligible; rows
+// and tags (f) updated in place. out[0..4] = eliminated, failed, positive,
+// negative, zero pivots.
+void refshim_aptp_front(double *F, int f, int ne, int *rows, double u, double small, int nb, int ib,
+                        int tiled, int8_t *tags, int64_t *out) {
+  smf::AptpParams prm;
+  prm.u = u;
+  prm.small = small;
+  prm.nb = nb;
+  prm.ib = ib;
+  std::vector<double> work(smf::aptp_work_size(f, ne, prm) + 1);
+  smf::TileWorkspace tws;
+  const smf::AptpResult r =
+      tiled ? smf::ldlt_aptp_front_tiled(F, f, ne, rows, prm, tags, work.data(), tws, 1, nullptr)
+            : smf::ldlt_aptp_front(F, f, ne, rows, prm, tags, work.data());
+  out[0] = r.num_eliminated;
+  out[1] = r.num_failed;
+  out[2] = r.inertia.positive;
+  out[3] = r.inertia.negative;
+  out[4] = r.inertia.zero;
+}
+
+// Info::aptp_failed_columns of the last factorization: the columns the APTP
+// kernel failed (then tried by the threshold kernel).
+int64_t refshim_aptp_failed(void *hp) {
+  return static_cast<RefHandle *>(hp)->info.aptp_failed_columns;
 }
 
 // out[0]: the last factorization's front work (Info::front_work: fully
