@@ -249,6 +249,17 @@ SMFG_API int smfg_residual_noalloc(smfg_plan_t plan, const double *d_b, const do
  * panel of k <= 16 pivots; best device time of reps launches (ms), the
  * update's algorithmic bytes, and the entries whose bits differ from the
  * tiled kernel's result (0 expected). Allocates 3 (f^2 + 16 f) doubles. */
+/* Kernel self-test (no reference counterpart as an entry point): the APTP
+ * front kernel that factors every indefinite front of at least 512 rows
+ * (deterministic mode's kernel, solver/src/ldlt_aptp.cpp:739) on one dense
+ * front in device memory: d_F f x f column-major (lower triangle), its first
+ * ne columns eligible, d_rows / d_tags (f) permuted and tagged in place,
+ * threshold u, zero-pivot value small. out[0..4] = pivots eliminated,
+ * columns failed, positive, negative, zero pivots. The failed columns are
+ * left behind the pivots with their Schur complement current (the caller's
+ * threshold kernel takes them next). Allocates its scratch. */
+SMFG_API int smfg_aptp_front_dense(double *d_F, int f, int ne, int *d_rows, int8_t *d_tags, double u, double small,
+                                   int64_t *out);
 SMFG_API int smfg_kernel_bench_defer(int f, int ne, int k, int reps, double *ms, double *bytes,
                                      long long *mismatches);
 

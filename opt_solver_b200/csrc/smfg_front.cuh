@@ -327,7 +327,7 @@ __device__ __forceinline__ double fat(const FrontRef &v, int i, int j) {  // ele
 
 // Returns whether it swapped (and so ended with a team barrier).
 template <int NT, int C = 1>
-__device__ bool sym_swap_blk(const FrontRef &v, int p, int q, int w_cols, bool synced = false) {
+static __device__ bool sym_swap_blk(const FrontRef &v, int p, int q, int w_cols, bool synced = false) {
   if (p == q) return false;
   if (p > q) {
     const int t = p;
@@ -456,7 +456,7 @@ constexpr int kElimCols = 16;
 constexpr int kElimGroup = 8;  // loads in flight per thread
 
 template <int NT, int C = 1>
-__device__ void eliminate_1x1_blk(const FrontRef &v, int k, int ucol_end, bool useW, int w_col,
+static __device__ void eliminate_1x1_blk(const FrontRef &v, int k, int ucol_end, bool useW, int w_col,
                                   bool synced = false) {
   using LY = Lay<NT>;
   const int rk = team_rank<C>();
@@ -515,7 +515,7 @@ __device__ void eliminate_1x1_blk(const FrontRef &v, int k, int ucol_end, bool u
 }
 
 template <int NT, int C = 1>
-__device__ void eliminate_2x2_blk(const FrontRef &v, int k, int ucol_end, bool useW, int w_col,
+static __device__ void eliminate_2x2_blk(const FrontRef &v, int k, int ucol_end, bool useW, int w_col,
                                   bool synced = false) {
   using LY = Lay<NT>;
   const int rk = team_rank<C>();
@@ -670,7 +670,7 @@ __device__ __forceinline__ void scanv(const double *__restrict__ col, int lo, in
 // one-CTA result). Two buffers alternate: a buffer is rewritten only after
 // the barrier of the next reduction, which every CTA reaches after reading.
 template <int NT, int C>
-__device__ void team_bundle(const FrontRef &v, FrontShared &sh, Top2 &t, double &x1, double &x2) {
+static __device__ void team_bundle(const FrontRef &v, FrontShared &sh, Top2 &t, double &x1, double &x2) {
   Block<NT>::bundle(t, x1, x2, sh);
   if constexpr (C > 1) {
     const int buf = sh.tr_seq & 1;
@@ -706,7 +706,7 @@ __device__ void team_bundle(const FrontRef &v, FrontShared &sh, Top2 &t, double 
 // One candidate's test (as cand_eval_warp) by the whole team: its scans
 // split by rows over every thread of every CTA, two team reductions.
 template <int NT, int C>
-__device__ int cand_eval_team(const FrontRef &v, int k, int limit, int cand, const PivotParams &prm,
+static __device__ int cand_eval_team(const FrontRef &v, int k, int limit, int cand, const PivotParams &prm,
                               FrontShared &sh, int &pa, int &pb) {
   const int tid = team_rank<C>() * NT + (int)threadIdx.x;
   constexpr int NTT = C * NT;
@@ -788,7 +788,7 @@ __device__ int cand_eval_team(const FrontRef &v, int k, int limit, int cand, con
 // independent and the search takes the first candidate that gives one, so
 // warps may test consecutive candidates at once; maxima are exact in any
 // order, ties go to the lowest row as in the reference's scan.
-__device__ int cand_eval_warp(const FrontRef &v, int k, int limit, int cand, const PivotParams &prm, int &pa,
+static __device__ int cand_eval_warp(const FrontRef &v, int k, int limit, int cand, const PivotParams &prm, int &pa,
                               int &pb) {
   const int lane = threadIdx.x & 31;
   const size_t sf = (size_t)v.ld;
@@ -867,7 +867,7 @@ __device__ int cand_eval_warp(const FrontRef &v, int k, int limit, int cand, con
 }
 
 template <int NT, int C = 1>
-__device__ void select_pivot_blk(const FrontRef &v, int k, int limit, const PivotParams &prm,
+static __device__ void select_pivot_blk(const FrontRef &v, int k, int limit, const PivotParams &prm,
                                  FrontShared &sh) {
   const size_t sf = (size_t)v.ld;
   const double *F = v.F;
@@ -997,7 +997,7 @@ __device__ void select_pivot_blk(const FrontRef &v, int k, int limit, const Pivo
 
 // apply_pivot (ldlt_kernel.cpp:666-698). The pivot choice is in sh.
 template <int NT, int C = 1>
-__device__ void apply_pivot_blk(const FrontRef &v, int &k, bool useW, int w_cols, int ucol_end,
+static __device__ void apply_pivot_blk(const FrontRef &v, int &k, bool useW, int w_cols, int ucol_end,
                                 const PivotParams &prm, FrontShared &sh) {
   const size_t sf = (size_t)v.ld;
   const int f = v.f;
@@ -1064,7 +1064,7 @@ __device__ __forceinline__ double ld_entry(const FrontRef &v, int c, int j) {
 // Every entry keeps its chain c = fma(-l, b, c) over the pivots in order
 // (b = 0 skipped): the loops it replaces give the same bits.
 template <bool SCHUR>
-__device__ void front_update_tiles(const FrontRef &v, int c0, int cend, int p0, int kk) {
+static __device__ void front_update_tiles(const FrontRef &v, int c0, int cend, int p0, int kk) {
   constexpr int T = 64, KC = 16;
   __shared__ double As[KC][T], Bs[KC][T];
   const int f = v.f;
@@ -1125,7 +1125,7 @@ __device__ void front_update_tiles(const FrontRef &v, int c0, int cend, int p0, 
 }
 
 template <int NT>
-__device__ void deferred_update_blk(const FrontRef &v, int p0, int p1, int c0, int e) {
+static __device__ void deferred_update_blk(const FrontRef &v, int p0, int p1, int c0, int e) {
   using LY = Lay<NT>;
   const int jb = p1 - p0;
   if (jb <= 0 || e - c0 <= 0) return;
@@ -1154,7 +1154,7 @@ __device__ void deferred_update_blk(const FrontRef &v, int p0, int p1, int c0, i
 // schur_update (ldlt_kernel.cpp:820-933): F[e:f, e:f] -= L LD^T over the
 // pivots [p0, p) in order.
 template <int NT>
-__device__ void schur_update_blk(const FrontRef &v, int p0, int p, int e) {
+static __device__ void schur_update_blk(const FrontRef &v, int p0, int p, int e) {
   using LY = Lay<NT>;
   const int f = v.f;
   if (p <= p0 || f - e <= 0) return;
@@ -1273,7 +1273,7 @@ __device__ __forceinline__ void pairing_targets(const FrontRef &v, int k, int f,
 // the pivots [0, S.k) remains). The caller applies F[c0:f, c0:e] -=
 // L[c0:f, p0:p1] W[c0:e, :]^T between two calls.
 template <int NT, int C = 1>
-__device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontShared &sh, TppState &S) {
+static __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontShared &sh, TppState &S) {
   const int f = v.f, ne = v.ne;
   const size_t sf = (size_t)v.ld;
   // stale eligible columns past the outer block exist (mixed fronts)
@@ -1452,7 +1452,7 @@ __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontSha
 // ldlt_factor_front (first = 0, no static pivoting). Returns the accepted
 // pivot count (uniform across the block); statistics in sh.st.
 template <int NT>
-__device__ int ldlt_factor_front_blk(const FrontRef &v, const PivotParams &prm, FrontShared &sh,
+static __device__ int ldlt_factor_front_blk(const FrontRef &v, const PivotParams &prm, FrontShared &sh,
                                      bool do_schur = true) {
   const int f = v.f, ne = v.ne;
   int k = 0;

@@ -301,6 +301,35 @@ TC_TF32X3, TC_BF16X3 = 0, 1
 REFINE_CLASSICAL, REFINE_FGMRES, REFINE_AUTO = 0, 1, 2
 
 
+def aptp_front_dense(A, ne: int, u: float = 0.01, small: float = 1e-20, device: int = 0):
+    """smfg_aptp_front_dense: the APTP front kernel on one dense symmetric
+    front A (f x f, lower triangle used, first ne columns eligible) on the
+    GPU. Returns (F (f x f, lower part meaningful), rows, tags, (eliminated,
+    failed, positive, negative, zero))."""
+    import torch
+    A = np.asarray(A, dtype=np.float64)
+    f = A.shape[0]
+    if A.shape != (f, f) or not 0 < ne <= f:
+        raise ValueError("A must be square with 0 < ne <= f")
+    dev = torch.device("cuda", device)
+    # column-major storage: the transpose's rows are A's columns
+    dF = torch.from_numpy(np.ascontiguousarray(np.tril(A).T)).to(dev)
+    drows = torch.arange(f, dtype=torch.int32, device=dev)
+    dtags = torch.zeros(f, dtype=torch.int8, device=dev)
+    out = np.zeros(5, dtype=np.int64)
+    L = lib()
+    L.smfg_aptp_front_dense.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_double,
+                                        C.c_double, C.c_void_p]
+    torch.cuda.synchronize(dev)
+    with torch.cuda.device(dev):
+        rc = L.smfg_aptp_front_dense(C.c_void_p(dF.data_ptr()), f, int(ne), C.c_void_p(drows.data_ptr()),
+                                     C.c_void_p(dtags.data_ptr()), float(u), float(small), out.ctypes.data)
+    if rc != SMFG_OK:
+        raise SmfgError(rc, "smfg_aptp_front_dense")
+    F = dF.cpu().numpy().T
+    return F, drows.cpu().numpy(), dtags.cpu().numpy(), tuple(int(x) for x in out)
+
+
 def kernel_bench_defer(f: int = 8000, ne: int = 4000, k: int = 16, reps: int = 5) -> dict:
     """smfg_kernel_bench_defer: the streamed deferred-update kernel on one
     synthetic front (f rows, ne eligible columns, k pending pivots): best
