@@ -124,7 +124,16 @@ typedef struct {
    * A replay that finds a front needing more pivoting steps than captured,
    * or an arena too small, falls back to the normal path. */
   int graph;
-  int reserved_i[2];
+  /* Dense kernel of the indefinite fronts: fronts of at least aptp_min_rows
+   * realized rows take a posteriori threshold pivoting in 256-column tiles,
+   * then the threshold kernel on the columns it failed -- smf's
+   * deterministic mode (multifrontal_serial.cpp:796-821, kTopTileMinFront =
+   * 512, parallel/thread_plan.hpp:43), the default (512). 0: the threshold
+   * kernel on every front (smf's one-thread default mode). Plans whose
+   * indefinite factorizations reach such fronts are not captured as a graph
+   * (graph = 1 then factors without capture). */
+  int aptp_min_rows;
+  int reserved_i[1];
   double reserved_d[8];
 } smfg_control_t;
 
@@ -144,7 +153,9 @@ typedef struct {
   int kernel_launches;    /* kernels launched by the last call */
   int mixed_fronts;       /* fronts whose trailing updates ran on the tensor cores */
   int reserved_i[7];      /* [0] profiled FP64 update launches, [1] tensor-core update passes,
-                             [2] deferred front updates, [3] those of at most 2 pivots */
+                             [2] deferred front updates, [3] those of at most 2 pivots,
+                             [4] columns the APTP sweeps failed (Info::aptp_failed_columns),
+                             [5] fronts swept by APTP */
   double reserved_d[8];   /* [0] profiled FP64 update ms (deferred + Schur), [1] FP64 update
                              flops, [2] arena bytes, [3] tensor-core update flops (2 per
                              multiply-add), [4] profiled tensor-core update ms (split + product

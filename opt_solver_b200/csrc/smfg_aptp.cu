@@ -722,7 +722,7 @@ void set_attrs() {
   done = true;
 }
 
-int sweep(const Front *d_fr, State *d_st, int nf, int kmax, const SweepHost &h, cudaStream_t st) {
+int sweep_blocks(const Front *d_fr, State *d_st, int nf, int kmax, const SweepHost &h, cudaStream_t st) {
   set_attrs();
   const int sms = h.sms;
   int launches = 0;
@@ -740,14 +740,24 @@ int sweep(const Front *d_fr, State *d_st, int nf, int kmax, const SweepHost &h, 
     k_update<<<2 * sms, 256, sizeof(GemmSmem), st>>>(d_fr, d_st, nf, k, 0);
     launches += 7;
   }
-  k_compact_perm<<<(nf + 31) / 32, 32, 0, st>>>(d_fr, d_st, nf);
-  launches += 1;
-  for (int q = 0; q < nf; ++q) {
-    if (!h.scratch) break;
-    k_compact_gather<<<2 * sms, 256, 0, st>>>(d_fr, d_st, q, h.scratch, 0);
-    k_compact_gather<<<2 * sms, 256, 0, st>>>(d_fr, d_st, q, h.scratch, 1);
-    launches += 2;
+  check(cudaGetLastError());
+  return launches;
+}
+
+int sweep_finish(const Front *d_fr, State *d_st, int nf, const int *compact, int ncompact, const SweepHost &h,
+                 cudaStream_t st) {
+  const int sms = h.sms;
+  int launches = 0;
+  if (ncompact > 0) {
+    k_compact_perm<<<(nf + 31) / 32, 32, 0, st>>>(d_fr, d_st, nf);
+    ++launches;
+    for (int u = 0; u < ncompact; ++u) {
+      k_compact_gather<<<2 * sms, 256, 0, st>>>(d_fr, d_st, compact[u], h.scratch, 0);
+      k_compact_gather<<<2 * sms, 256, 0, st>>>(d_fr, d_st, compact[u], h.scratch, 1);
+      launches += 2;
+    }
   }
+  const dim3 g2(std::max(1, 2 * sms / std::max(1, nf)), nf);
   k_trailing_w<<<g2, 256, 0, st>>>(d_fr, d_st);
   k_update<<<2 * sms, 256, sizeof(GemmSmem), st>>>(d_fr, d_st, nf, 0, 1);
   k_stats<<<nf, 256, 0, st>>>(d_fr, d_st, h.small_bits);
@@ -805,9 +815,11 @@ extern "C" SMFG_API int smfg_aptp_front_dense(double *d_F, int f, int ne, int *d
     check(cudaMemcpy(d_small, &sb, sizeof(sb), cudaMemcpyHostToDevice));
     check(cudaMemcpy(d_fr, &F, sizeof(Front), cudaMemcpyHostToDevice));
     SweepHost h{sms, 1.0 / u, d_small, gather};
-    sweep(d_fr, d_st, 1, (ne + F.nb - 1) / F.nb, h, 0);
-    check(cudaDeviceSynchronize());
+    sweep_blocks(d_fr, d_st, 1, (ne + F.nb - 1) / F.nb, h, 0);
     State S;
+    check(cudaMemcpy(&S, d_st, sizeof(State), cudaMemcpyDeviceToHost));
+    const int only = 0;
+    sweep_finish(d_fr, d_st, 1, &only, S.num_elim < ne ? 1 : 0, h, 0);
     check(cudaMemcpy(&S, d_st, sizeof(State), cudaMemcpyDeviceToHost));
     out[0] = S.num_elim;
     out[1] = ne - S.num_elim;

@@ -54,10 +54,15 @@ struct SweepHost {
   double *scratch;                        // device: max over the fronts of f * ne doubles
 };
 
-// The APTP sweep of nf fronts (d_fr, d_st device arrays), kmax block
-// columns (at least the most any front needs), on stream st. Returns the
-// kernels launched.
-int sweep(const Front *d_fr, State *d_st, int nf, int kmax, const SweepHost &h, cudaStream_t st);
+// The APTP sweep of nf fronts (d_fr, d_st device arrays) on stream st, in
+// two parts: the block columns (kmax: at least the most any front needs),
+// then, once the caller has read the states, the compaction of the fronts
+// with failed columns (compact[0 .. ncompact), their indices; h.scratch
+// holds f * ne doubles of the largest), the trailing update and the counts.
+// Each returns the kernels it launched.
+int sweep_blocks(const Front *d_fr, State *d_st, int nf, int kmax, const SweepHost &h, cudaStream_t st);
+int sweep_finish(const Front *d_fr, State *d_st, int nf, const int *compact, int ncompact, const SweepHost &h,
+                 cudaStream_t st);
 
 }  // namespace aptp
 }  // namespace smfg

@@ -87,6 +87,66 @@ size_t front_smem_bytes(int fmax, int nb, int blocked_min_front = 0) {
 // ---------------------------------------------------------------------------
 // Plan creation (per analysis).
 
+// The large-front lists by level from pl.h_large (in each level's order),
+// with each level's widest and largest symbolic front.
+static void large_lists(Plan &pl) {
+  const int nl = pl.nlevels;
+  pl.lvl_large_ptr.assign(nl + 1, 0);
+  pl.lvl_large_maxw.assign(nl, 0);
+  pl.lvl_large_maxf.assign(nl, 0);
+  pl.h_lvl_large.clear();
+  pl.max_large = 0;
+  for (int l = 0; l < nl; ++l) {
+    for (int i = pl.lvl_ptr[l]; i < pl.lvl_ptr[l + 1]; ++i) {
+      const int s = pl.h_lvl_sn[i];
+      if (pl.h_large[s]) {
+        pl.h_lvl_large.push_back(s);
+        pl.lvl_large_maxw[l] = std::max(pl.lvl_large_maxw[l], pl.h_width[s]);
+        pl.lvl_large_maxf[l] = std::max(pl.lvl_large_maxf[l], pl.h_fsym[s]);
+      }
+    }
+    pl.lvl_large_ptr[l + 1] = (int)pl.h_lvl_large.size();
+    pl.max_large = std::max(pl.max_large, pl.lvl_large_ptr[l + 1] - pl.lvl_large_ptr[l]);
+  }
+}
+
+// Device state sized by the most large fronts of a level.
+static void large_state(Plan &pl) {
+  DevFactor &x = pl.x;
+  for (void *p : {(void *)x.tpp, (void *)x.team_bar, (void *)x.team_red, (void *)x.tc_jobs, (void *)x.tc_ipref,
+                  (void *)x.tc_tpref, (void *)pl.aptp_sizes, (void *)pl.aptp_q})
+    dfree(pl, p);
+  const size_t ml = (size_t)std::max(1, pl.max_large);
+  x.tpp = dalloc<TppState>(pl, 2 * ml);  // two buffers (SPD panels)
+  x.team_bar = dalloc<unsigned>(pl, 2 * ml);
+  SMFG_CUDA(cudaMemsetAsync(x.team_bar, 0, sizeof(unsigned) * 2 * ml, pl.stream));
+  x.team_red = dalloc<double>(pl, (size_t)kTeamRedDoubles * ml);
+  x.tc_jobs = dalloc<tc::Job>(pl, ml);
+  x.tc_ipref = dalloc<int64_t>(pl, ml + 1);
+  x.tc_tpref = dalloc<int>(pl, ml + 1);
+  pl.aptp_sizes = dalloc<int64_t>(pl, 4 * ml);
+  pl.aptp_q = dalloc<int>(pl, ml);
+}
+
+// Fronts that delays took to the APTP size outside the large-front path
+// join it (the caller redoes the factorization).
+static void add_large(Plan &pl, const std::vector<int> &sn) {
+  // a captured graph holds the old lists' and states' addresses
+  if (pl.graph_exec) {
+    cudaGraphExecDestroy(pl.graph_exec);
+    pl.graph_exec = nullptr;
+    pl.graph_key.clear();
+  }
+  for (int s : sn) pl.h_large[s] = 1;
+  large_lists(pl);
+  dfree(pl, pl.d.lvl_large);
+  dfree(pl, pl.d.sn_large);
+  pl.d.lvl_large = dupload(pl, pl.h_lvl_large);
+  pl.d.sn_large = dupload(pl, pl.h_large);
+  large_state(pl);
+  SMFG_CUDA(cudaStreamSynchronize(pl.stream));
+}
+
 static void build_plan(Plan &pl, const smfg_analysis_t &a) {
   const int n = a.n, ns = a.nsn;
   pl.n = n;
@@ -117,23 +177,14 @@ static void build_plan(Plan &pl, const smfg_analysis_t &a) {
     const int s = a.postorder[i];
     lvl_sn[fill[level[s]]++] = s;
   }
-  // large fronts (multi-block path), by level, in the level's order
-  pl.lvl_large_ptr.assign(nl + 1, 0);
-  pl.lvl_large_maxw.assign(nl, 0);
-  pl.lvl_large_maxf.assign(nl, 0);
-  std::vector<int> lvl_large;
-  for (int l = 0; l < nl; ++l) {
-    for (int i = pl.lvl_ptr[l]; i < pl.lvl_ptr[l + 1]; ++i) {
-      const int s = lvl_sn[i];
-      if (fsym[s] >= kLargeMin) {
-        lvl_large.push_back(s);
-        pl.lvl_large_maxw[l] = std::max(pl.lvl_large_maxw[l], width[s]);
-        pl.lvl_large_maxf[l] = std::max(pl.lvl_large_maxf[l], fsym[s]);
-      }
-    }
-    pl.lvl_large_ptr[l + 1] = (int)lvl_large.size();
-    pl.max_large = std::max(pl.max_large, pl.lvl_large_ptr[l + 1] - pl.lvl_large_ptr[l]);
-  }
+  // large fronts (multi-block path): by symbolic rows; fronts that delays
+  // take to the APTP size join later (large_lists)
+  pl.h_large.assign(ns, 0);
+  for (int s = 0; s < ns; ++s) pl.h_large[s] = fsym[s] >= kLargeMin ? 1 : 0;
+  pl.h_lvl_sn = lvl_sn;
+  pl.h_width = width;
+  pl.h_fsym = fsym;
+  large_lists(pl);
   pl.lvl_maxf.assign(nl, 0);
   pl.lvl_maxkids.assign(nl, 0);
   for (int s = 0; s < ns; ++s) {
@@ -250,8 +301,8 @@ static void build_plan(Plan &pl, const smfg_analysis_t &a) {
   d.cpr_off = dupload(pl, cpr_off);
   d.cpr_idx = dupload(pl, cpr_idx);
   d.lvl_sn = dupload(pl, lvl_sn);
-  d.lvl_large = dupload(pl, lvl_large);
-  pl.h_lvl_large = lvl_large;
+  d.lvl_large = dupload(pl, pl.h_lvl_large);
+  d.sn_large = dupload(pl, pl.h_large);
   d.sn_level = dupload(pl, level);
   d.pcp = dupload(pl, std::vector<int>(a.perm_col_ptr, a.perm_col_ptr + n + 1));
   d.pri = dupload(pl, std::vector<int>(a.perm_row_idx, a.perm_row_idx + pl.nnz));
@@ -282,17 +333,11 @@ static void build_plan(Plan &pl, const smfg_analysis_t &a) {
   x.sn_flops = dalloc<double>(pl, ns);
   x.lvl_blk = dalloc<int>(pl, (size_t)ns + nl + 1);
   x.counters = dalloc<unsigned long long>(pl, kCCount + 8);
-  x.tpp = dalloc<TppState>(pl, 2 * (size_t)std::max(1, pl.max_large));  // two buffers (SPD panels)
-  x.team_bar = dalloc<unsigned>(pl, 2 * (size_t)std::max(1, pl.max_large));
-  SMFG_CUDA(cudaMemsetAsync(x.team_bar, 0, sizeof(unsigned) * 2 * std::max(1, pl.max_large), pl.stream));
-  x.team_red = dalloc<double>(pl, (size_t)kTeamRedDoubles * std::max(1, pl.max_large));
   x.sn_mixed = dalloc<int8_t>(pl, ns);
   SMFG_CUDA(cudaMemsetAsync(x.sn_mixed, 0, ns, pl.stream));
-  x.tc_jobs = dalloc<tc::Job>(pl, std::max(1, pl.max_large));
-  x.tc_ipref = dalloc<int64_t>(pl, (size_t)std::max(1, pl.max_large) + 1);
-  x.tc_tpref = dalloc<int>(pl, (size_t)std::max(1, pl.max_large) + 1);
   x.tc_njobs = dalloc<int>(pl, 1);
-  pl.h_fsym = fsym;
+  x.aptp_miss = dalloc<int>(pl, kAptpMissCap);
+  large_state(pl);
   x.arena = nullptr;
   x.arena_cap = 0;
   x.rows = nullptr;
@@ -509,6 +554,116 @@ static void enqueue_tc(Plan &pl, const MixedCfg &mc, const int *lg, int nL, TppS
   lc.n += 3;
 }
 
+// APTP (smf's deterministic mode) applies to this factorization's
+// indefinite fronts of at least aptp_min_rows rows.
+static bool aptp_active(const smfg_control_t &c) {
+  return !c.posdef && c.aptp_min_rows > 0 && c.u >= kWeakPivotRatio;
+}
+
+// The level's large fronts of at least aptp_min_rows realized rows (list
+// positions into aq), with every large front's realized rows, eligible
+// columns, arena and row offsets (asz, 4 per front). One synchronization.
+static void aptp_select(Plan &pl, const smfg_control_t &c, const int *lg, int nL, std::vector<int64_t> &asz,
+                        std::vector<int> &aq, LaunchCount &lc) {
+  asz.assign(4 * (size_t)nL, 0);
+  k_large_sizes<<<(nL + 127) / 128, 128, 0, pl.stream>>>(pl.x, lg, nL, pl.aptp_sizes);
+  SMFG_CUDA(cudaMemcpyAsync(asz.data(), pl.aptp_sizes, sizeof(int64_t) * 4 * nL, cudaMemcpyDeviceToHost, pl.stream));
+  unsigned long long flags = 0;
+  SMFG_CUDA(cudaMemcpyAsync(&flags, pl.x.counters + kCFlags, sizeof(flags), cudaMemcpyDeviceToHost, pl.stream));
+  SMFG_CUDA(cudaStreamSynchronize(pl.stream));
+  lc.n += 1;
+  aq.clear();
+  // an aborted factorization (arena or rows too small: offsets past the
+  // arena) is redone; nothing is swept
+  if ((unsigned)flags & kFAbort) return;
+  for (int q = 0; q < nL; ++q)
+    if (asz[4 * q] >= c.aptp_min_rows) aq.push_back(q);
+}
+
+template <class T>
+static T *grow_buf(Plan &pl, T *p, int64_t &cap, int64_t need) {
+  if (need <= cap && p) return p;
+  dfree(pl, p);
+  cap = std::max<int64_t>(need, cap + cap / 2);
+  return dalloc<T>(pl, (size_t)cap);
+}
+
+// The APTP sweep of the level's fronts aq (positions in its large list;
+// asz from aptp_select), then their threshold-kernel state: the fronts with
+// failed columns continue in the threshold kernel's steps. Returns whether
+// any large front of the level needs those steps.
+static bool aptp_sweep(Plan &pl, const smfg_control_t &c, const std::vector<int64_t> &asz,
+                       const std::vector<int> &aq, int nL, LaunchCount &lc) {
+  cudaStream_t st = pl.stream;
+  DevFactor &x = pl.x;
+  const int nf = (int)aq.size();
+  int64_t need = 0;
+  int kmax = 0;
+  for (int q : aq) {
+    const int f = (int)asz[4 * q], ne = (int)asz[4 * q + 1];
+    need += aptp::scratch_doubles(f, ne) + ne;  // + Q and pi (2 ne ints)
+    const int nb = std::min(aptp::kNb, std::max(1, ne));
+    kmax = std::max(kmax, (ne + nb - 1) / nb);
+  }
+  pl.aptp_buf = grow_buf(pl, pl.aptp_buf, pl.aptp_buf_cap, need);
+  if (nf > pl.aptp_cap) {
+    dfree(pl, pl.aptp_fr);
+    dfree(pl, pl.aptp_st);
+    pl.aptp_cap = std::max(nf, 2 * pl.aptp_cap);
+    pl.aptp_fr = dalloc<aptp::Front>(pl, pl.aptp_cap);
+    pl.aptp_st = dalloc<aptp::State>(pl, pl.aptp_cap);
+  }
+  std::vector<aptp::Front> hf(nf);
+  int64_t o = 0;
+  for (int i = 0; i < nf; ++i) {
+    const int q = aq[i];
+    const int f = (int)asz[4 * q], ne = (int)asz[4 * q + 1];
+    aptp::Front &F = hf[i];
+    F.A = x.arena + asz[4 * q + 2];
+    F.rows = x.rows + asz[4 * q + 3];
+    F.tags = x.tags + asz[4 * q + 3];
+    F.loc = x.ploc + asz[4 * q + 3];
+    F.f = f;
+    F.ne = ne;
+    F.nb = std::min(aptp::kNb, std::max(1, ne));
+    F.ib = std::min(aptp::kIb, F.nb);
+    F.bk = pl.aptp_buf + o;
+    o += (int64_t)f * aptp::kNb;
+    F.ga = pl.aptp_buf + o;
+    o += (int64_t)ne * aptp::kNb;
+    F.gb = pl.aptp_buf + o;
+    o += (int64_t)ne * aptp::kNb;
+    F.Q = reinterpret_cast<int *>(pl.aptp_buf + o);
+    F.pi = F.Q + ne;
+    o += ne;
+  }
+  auto *d_fr = static_cast<aptp::Front *>(pl.aptp_fr);
+  auto *d_st = static_cast<aptp::State *>(pl.aptp_st);
+  SMFG_CUDA(cudaMemcpyAsync(d_fr, hf.data(), sizeof(aptp::Front) * nf, cudaMemcpyHostToDevice, st));
+  SMFG_CUDA(cudaMemcpyAsync(pl.aptp_q, aq.data(), sizeof(int) * nf, cudaMemcpyHostToDevice, st));
+  aptp::SweepHost h{sm_count(pl.device), 1.0 / c.u, x.counters + kCEffSmall, nullptr};
+  lc.n += aptp::sweep_blocks(d_fr, d_st, nf, kmax, h, st);
+  std::vector<aptp::State> hs(nf);
+  SMFG_CUDA(cudaMemcpyAsync(hs.data(), d_st, sizeof(aptp::State) * nf, cudaMemcpyDeviceToHost, st));
+  SMFG_CUDA(cudaStreamSynchronize(st));
+  std::vector<int> compact;
+  int64_t gneed = 0;
+  for (int i = 0; i < nf; ++i)
+    if (hs[i].num_elim < hf[i].ne) {
+      compact.push_back(i);
+      gneed = std::max(gneed, (int64_t)hf[i].f * hf[i].ne);
+      pl.aptp_failed += hf[i].ne - hs[i].num_elim;
+    }
+  pl.aptp_fronts += nf;
+  if (gneed > 0) pl.aptp_gather = grow_buf(pl, pl.aptp_gather, pl.aptp_gather_cap, gneed);
+  h.scratch = pl.aptp_gather;
+  lc.n += aptp::sweep_finish(d_fr, d_st, nf, compact.data(), (int)compact.size(), h, st);
+  k_aptp_to_tpp<<<nf, 256, 0, st>>>(d_fr, d_st, pl.aptp_q, x.rows_cap, x.tpp, c.blocked_min_front);
+  lc.n += 1;
+  // the host vectors above are read by copies already waited for
+  return nf < nL || !compact.empty();
+}
+
 static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_t &c, LaunchCount &lc,
                            GemmProfile &gp, bool fixed = false) {
   DevPlan &d = pl.d;
@@ -530,7 +685,9 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
       x.counters);
   k_eff_small<<<1, 1, 0, st>>>(x.counters, c.small_pivot);
   lc.n += 2;
-  PivotParams prm{c.u, c.small_pivot, c.small_pivot, c.nb, c.blocked_min_front, c.posdef};
+  const bool aptp_on = aptp_active(c);
+  PivotParams prm{c.u, c.small_pivot, c.small_pivot, c.nb, c.blocked_min_front, c.posdef,
+                  aptp_on ? c.aptp_min_rows : 0};
   const MixedCfg mc = mixed_cfg(c);
   const int wcols = w_rows(pl, c, gp.on);
   // the shared-memory front kernels by size bucket: each launch's shared
@@ -556,11 +713,30 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
     const int nL = pl.lvl_large_ptr[l + 1] - pl.lvl_large_ptr[l];
     if (nL > 0) {
       const int *lg = d.lvl_large + pl.lvl_large_ptr[l];
+      // the fronts of at least aptp_min_rows realized rows take the APTP
+      // sweep first (in FP64: they leave the mixed set)
+      std::vector<int64_t> asz;
+      std::vector<int> aq;
+      if (aptp_on && !fixed) {
+        aptp_select(pl, c, lg, nL, asz, aq, lc);
+        for (int q : aq) {
+          const int s = pl.h_lvl_large[pl.lvl_large_ptr[l] + q];
+          if (pl.h_mixed[s]) {
+            pl.h_mixed[s] = 0;
+            --pl.mixed_count;
+            SMFG_CUDA(cudaMemsetAsync(x.sn_mixed + s, 0, 1, st));
+          }
+        }
+      }
       bool lvl_mixed = false;
       if (mc.on)
         for (int i = pl.lvl_large_ptr[l]; i < pl.lvl_large_ptr[l + 1] && !lvl_mixed; ++i)
           lvl_mixed = pl.h_mixed[pl.h_lvl_large[i]] != 0;
       k_large_init<<<nL, 256, 0, st>>>(d, x, lg, nL, c.posdef, lvl_mixed ? mc.nbo : 0);
+      // the threshold kernel's steps are needed unless every large front of
+      // the level was swept without a failed column
+      bool tpp_work = true;
+      if (!aq.empty()) tpp_work = aptp_sweep(pl, c, asz, aq, nL, lc);
       const int team = level_team(pl, c, pl.lvl_large_maxf[l]);
       SMFG_CUDA(cudaMemsetAsync(x.counters + kCActive, 0, sizeof(unsigned long long), st));
       const int ggrid = 2 * sms;
@@ -604,6 +780,8 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
         if (ahead) SMFG_CUDA(cudaStreamWaitEvent(st, pl.ev_rest, 0));  // join before the Schur update
         fin = x.tpp + (size_t)(steps & 1) * pl.max_large;
         lc.n += 2 * steps;
+      } else if (!tpp_work) {
+        // every front of the level swept by APTP without a failed column
       } else if (c.posdef) {
         const int steps = (pl.lvl_large_maxw[l] + c.nb - 1) / c.nb + 1;
         for (; it < steps; ++it) {
@@ -739,7 +917,8 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
     key.insert(key.end(), b, b + n);
   };
   bool replayed = false;
-  const bool use_graph = c.graph != 0 && !gp.on;
+  // the APTP sweeps read sizes back between levels: no capture then
+  bool use_graph = c.graph != 0 && !gp.on && !(aptp_active(c) && pl.max_large > 0);
   if (use_graph) {
     smfg_control_t kc = c;
     kc.scale = c.scale ? reinterpret_cast<const double *>(1) : nullptr;  // the scale's values are copied per call
@@ -761,10 +940,11 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
       SMFG_CUDA(cudaStreamSynchronize(pl.stream));
       SMFG_CUDA(cudaEventElapsedTime(&ms, pl.ev0, pl.ev1));
       const unsigned fl = (unsigned)h_cnt[kCFlags];
-      replayed = !(fl & (kFArena | kFRows | kFTcCap | kFSteps));
+      replayed = !(fl & (kFArena | kFRows | kFTcCap | kFSteps | kFAptpMiss));
       lc.n = pl.graph_launches;
     }
   }
+  int attempt_extra = 0;
   for (int attempt = 0; attempt < 4 && !replayed; ++attempt) {
     ensure_arena(pl, std::max(need_a, pl.x.arena_cap), std::max(need_r, pl.x.rows_cap));
     if (pl.x.tc_img_cap < tc_need) {
@@ -774,6 +954,8 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
     }
     lc = LaunchCount{};
     gp.used = 0;
+    pl.aptp_failed = 0;
+    pl.aptp_fronts = 0;
     SMFG_CUDA(cudaEventRecord(pl.ev0, pl.stream));
     enqueue_factor(pl, d_values, c, lc, gp);
     static_assert(sizeof(FactorTotals) <= 8 * sizeof(unsigned long long), "totals slot");
@@ -794,9 +976,20 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
       tc_need = std::max<int64_t>(tc_need * 2, 1 << 24);
       continue;
     }
+    if (flags & kFAptpMiss) {
+      // fronts that delays took to the APTP size join the large-front path
+      const int nm = (int)std::min<unsigned long long>(h_cnt[kCAptpMiss], (unsigned long long)kAptpMissCap);
+      std::vector<int> miss(nm);
+      SMFG_CUDA(cudaMemcpy(miss.data(), pl.x.aptp_miss, sizeof(int) * nm, cudaMemcpyDeviceToHost));
+      add_large(pl, miss);
+      use_graph = use_graph && !(aptp_active(c) && pl.max_large > 0);
+      ++attempt_extra;
+      if (attempt_extra < 8) --attempt;
+      continue;
+    }
     break;
   }
-  if (use_graph && !replayed && !((unsigned)h_cnt[kCFlags] & (kFArena | kFRows | kFTcCap))) {
+  if (use_graph && !replayed && !((unsigned)h_cnt[kCFlags] & (kFArena | kFRows | kFTcCap | kFAptpMiss))) {
     // capture the sequence for the next call with this configuration
     key.clear();
     smfg_control_t kc = c;
@@ -872,7 +1065,9 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
   inf.mixed_fronts = pl.mixed_count;
   int rc = SMFG_OK;
   pl.factor_status = SMFG_FACTOR_SUCCESS;
-  if (flags & (kFArena | kFRows | kFTcCap)) rc = SMFG_ERR_ARENA;
+  inf.reserved_i[4] = (int)pl.aptp_failed;
+  inf.reserved_i[5] = pl.aptp_fronts;
+  if (flags & (kFArena | kFRows | kFTcCap | kFAptpMiss)) rc = SMFG_ERR_ARENA;
   else if (flags & kFTcWait) rc = SMFG_ERR_TIMEOUT;
   else if (flags & kFNonfinite) rc = SMFG_ERR_NONFINITE;
   else if (flags & (kFMap | kFInternal)) rc = SMFG_ERR_INTERNAL;
@@ -1013,6 +1208,7 @@ SMFG_API void smfg_default_control(smfg_control_t *c) {
   c->precision = SMFG_PREC_FP64;
   c->max_negative_pivots = -1;
   c->scale = nullptr;
+  c->aptp_min_rows = aptp::kMinRows;  // deterministic mode
 }
 
 SMFG_API const char *smfg_last_error(void) { return g_last_error.c_str(); }

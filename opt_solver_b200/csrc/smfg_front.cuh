@@ -28,6 +28,7 @@ constexpr double kWeakPivotRatio = 1e-6;  // ldlt_kernel.hpp:100
 struct PivotParams {
   double u, eff_small, small_pivot;
   int nb, blocked_min_front, posdef;
+  int aptp_min;  // indefinite fronts of at least this many rows take the APTP kernel (0: none)
 };
 
 struct FrontStats {
@@ -1179,7 +1180,8 @@ static __device__ void schur_update_blk(const FrontRef &v, int p0, int p, int e)
 
 // State of the blocked path of ldlt_factor_front between its panel steps
 // (ldlt_kernel.cpp:1010-1131): the first pass over the columns (phase 0,
-// indefinite only), the main panel loop (phase 1), done (phase 2); `post`
+// indefinite only), the main panel loop (phase 1), done (phase 2), or the
+// unblocked loop after an APTP sweep (phase 3); `post`
 // says what follows the deferred update the last step asked for. Every
 // thread of the block holds the same copy (all decisions are uniform).
 struct TppState {
@@ -1276,6 +1278,19 @@ template <int NT, int C = 1>
 static __device__ bool tpp_step_blk(const FrontRef &v, const PivotParams &prm, FrontShared &sh, TppState &S) {
   const int f = v.f, ne = v.ne;
   const size_t sf = (size_t)v.ld;
+  if (S.phase == 3) {
+    // unblocked, from the pivots an APTP sweep took (fewer than
+    // blocked_min_front rows remain, ldlt_kernel.cpp:977-992): every pivot
+    // updates the whole trailing triangle, no deferred or Schur update
+    while (S.k < ne) {
+      select_pivot_blk<NT, C>(v, S.k, ne, prm, sh);
+      if (sh.kind == 0) break;
+      apply_pivot_blk<NT, C>(v, S.k, false, 0, f, prm, sh);
+    }
+    S.pad[3] = S.k;
+    S.phase = 2;
+    return false;
+  }
   // stale eligible columns past the outer block exist (mixed fronts)
   auto stale = [&]() { return S.mixed && S.tc_done < S.k && min(S.se, ne) < ne; };
   for (int guard = 0; guard < 4 * (ne + 8); ++guard) {

@@ -36,6 +36,7 @@ struct DevPlan {
   int64_t *sidx = nullptr;                     // its entry -> permuted slot
   int *sn_level = nullptr;
   int *lvl_large = nullptr;                    // large fronts by level
+  int8_t *sn_large = nullptr;                  // 1: the front takes the large-front path
 };
 
 // Device state of one factorization (sized per plan, grown on demand).
@@ -61,6 +62,7 @@ struct DevFactor {
   TppState *tpp = nullptr;    // per large front of a level: blocked-pivoting state
   unsigned *team_bar = nullptr;  // per large front of a level: its CTA team's barrier words
   double *team_red = nullptr;    // per large front of a level: its team's reduction scratch
+  int *aptp_miss = nullptr;   // fronts that reached the APTP size outside the large-front path
   double *work = nullptr;     // solve / refinement scratch
   int64_t work_cap = 0;
   // mixed precision: fronts whose trailing updates run on the tensor cores
@@ -85,6 +87,8 @@ struct Plan {
   std::vector<int> lvl_large_maxf; // largest symbolic front among them
   std::vector<int> lvl_large_pmax; // most stored pivots among them (last factorization)
   std::vector<int> h_lvl_large;    // host copy of the large-front lists
+  std::vector<int8_t> h_large;     // per supernode: the large-front path (symbolic rows, or grown by delays)
+  std::vector<int> h_lvl_sn, h_width;  // supernodes by level; pivot columns
   int max_large = 0;
   int64_t sum_f2 = 0, sum_f = 0; // symbolic
   int max_fsym = 0;
@@ -120,6 +124,17 @@ struct Plan {
   std::vector<unsigned char> graph_key;
   int graph_launches = 0;
   std::vector<void *> allocs;
+  // APTP fronts of a level: descriptors, states, scratch, staging
+  void *aptp_fr = nullptr, *aptp_st = nullptr;
+  int aptp_cap = 0;
+  double *aptp_buf = nullptr;
+  int64_t aptp_buf_cap = 0;
+  double *aptp_gather = nullptr;
+  int64_t aptp_gather_cap = 0;
+  int64_t *aptp_sizes = nullptr;  // device: f, ne, arena offset, row offset per large front
+  int *aptp_q = nullptr;          // device: list positions of the APTP fronts
+  int64_t aptp_failed = 0;        // last factorization: columns the APTP sweeps failed
+  int aptp_fronts = 0;            // last factorization: fronts swept
 };
 
 }  // namespace smfg

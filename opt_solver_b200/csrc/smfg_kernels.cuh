@@ -2,6 +2,7 @@
 // set-up, assembly / extend-add, front factorization by size class, the
 // supernodal solves and the residual.
 #pragma once
+#include "smfg_aptp_host.h"
 #include "smfg_internal.cuh"
 #include "smfg_tc.cuh"
 
@@ -10,15 +11,19 @@ namespace smfg {
 // counters[] slots
 enum : int { kCArena = 0, kCRows = 1, kCFlags = 2, kCMaxAbs = 3, kCAux = 4, kCEffSmall = 5,
              kCActive = 6, kCGemmFlops = 7, kCTcFlops = 8, kCDeferBytes = 9, kCDeferUpd = 10,
-             kCDeferSmall = 11, kCCount = 12 };
+             kCDeferSmall = 11, kCAptpMiss = 12, kCCount = 13 };
 // error flag bits (counters[kCFlags])
 enum : unsigned { kFArena = 1u, kFRows = 2u, kFNonfinite = 4u, kFNotPosdef = 8u, kFNonfiniteD = 16u,
-                  kFMap = 32u, kFInternal = 64u, kFTcWait = 128u, kFTcCap = 256u, kFSteps = 512u };
+                  kFMap = 32u, kFInternal = 64u, kFTcWait = 128u, kFTcCap = 256u, kFSteps = 512u,
+                  kFAptpMiss = 1024u };
 // team reduction scratch per large front (2 buffers x 16 CTAs x 6 doubles)
 constexpr int kTeamRedDoubles = 256;
 // flags after which the rest of a factorization is skipped (retried with
 // more room, or reported)
-constexpr unsigned kFAbort = kFArena | kFRows | kFTcWait | kFTcCap;
+constexpr unsigned kFAbort = kFArena | kFRows | kFTcWait | kFTcCap | kFAptpMiss;
+// fronts recorded per factorization that grew past the APTP size outside the
+// large-front path (they join it, and the factorization is redone)
+constexpr int kAptpMissCap = 1024;
 
 __device__ __forceinline__ void set_flag(unsigned long long *cnt, unsigned bit) {
   atomicOr(cnt + kCFlags, (unsigned long long)bit);
@@ -477,7 +482,17 @@ __global__ void __launch_bounds__(NT) k_factor(DevPlan P, DevFactor X, int lo, i
   if (X.counters[kCFlags] & kFAbort) return;
   const int s = P.lvl_sn[lo + blockIdx.x];
   const int f = X.sn_f[s];
-  if (f < FMIN || f > FMAX || P.sn_fsym[s] >= kLargeMin) return;
+  if (f < FMIN || f > FMAX || P.sn_large[s]) return;
+  if (!SMEM && prm.aptp_min > 0 && !prm.posdef && f >= prm.aptp_min && prm.u >= kWeakPivotRatio) {
+    // delays took the front to the APTP size: it must take the large-front
+    // path; recorded, and the factorization is redone
+    if (threadIdx.x == 0) {
+      const unsigned long long i = atomicAdd(X.counters + kCAptpMiss, 1ull);
+      if (i < (unsigned long long)kAptpMissCap) X.aptp_miss[i] = s;
+      set_flag(X.counters, kFAptpMiss);
+    }
+    return;
+  }
   factor_one_front<NT, SMEM>(P, X, s, prm, smem);
 }
 
@@ -524,6 +539,45 @@ __global__ void k_large_init(DevPlan P, DevFactor X, const int *__restrict__ lar
     S.pad[0] = 0;  // deferred update pending
     X.tpp[blockIdx.x] = S;
   }
+}
+
+// Realized rows, eligible columns, arena and row offsets of a level's large
+// fronts (read by the host to set up their APTP sweep).
+__global__ void k_large_sizes(DevFactor X, const int *__restrict__ large, int nlarge, int64_t *__restrict__ out) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nlarge) return;
+  const int s = large[q];
+  out[4 * q] = X.sn_f[s];
+  out[4 * q + 1] = X.sn_ne[s];
+  out[4 * q + 2] = X.sn_off[s];
+  out[4 * q + 3] = X.sn_roff[s];
+}
+
+// The threshold kernel's state of the APTP fronts after their sweep: it
+// continues from the APTP pivots on the columns the sweep failed (blocked,
+// or unblocked when fewer than blocked_min_front rows remain:
+// multifrontal_serial.cpp:810-814, ldlt_kernel.cpp:977), its Schur update
+// from those pivots on; the sweep's counts carried, and the position map
+// (inv, the inverse of loc, which the sweep permuted) rebuilt. One block per
+// front.
+__global__ void k_aptp_to_tpp(const aptp::Front *__restrict__ fr, const aptp::State *__restrict__ st,
+                              const int *__restrict__ qpos, int64_t rows_cap, TppState *__restrict__ tpp, int bmf) {
+  const int i = blockIdx.x;
+  const aptp::Front F = fr[i];
+  int *inv = F.loc + rows_cap;
+  for (int t = threadIdx.x; t < F.f; t += blockDim.x) inv[F.loc[t]] = t;
+  if (threadIdx.x != 0) return;
+  const aptp::State &A = st[i];
+  TppState &T = tpp[qpos[i]];
+  T.k = A.num_elim;
+  T.live = F.ne;
+  T.k_paired = -1;
+  T.post = 0;
+  T.st = A.st;
+  T.pad[3] = A.num_elim;
+  T.mixed = 0;
+  T.se = 1 << 30;
+  T.phase = (A.num_elim >= F.ne) ? 2 : (F.f - A.num_elim < bmf ? 3 : 0);
 }
 
 // One blocked-TPP step (tpp_step_blk) of each large front of a level; a
@@ -964,10 +1018,11 @@ __global__ void __launch_bounds__(256) k_large_schur(DevPlan P, DevFactor X, con
       pref[0] = 0;
       for (int q = 0; q < cnt; ++q) {
         const int s = large[chunk + q];
-        const int e = X.sn_ne[s], f = X.sn_f[s], k = tpp[chunk + q].k;
+        // pivots [pad[3], k): an APTP front's trailing update covered its own
+        const int e = X.sn_ne[s], f = X.sn_f[s], k = tpp[chunk + q].k, k0 = tpp[chunk + q].pad[3];
         // mixed fronts: the tensor-core updates covered the contribution block
         const bool fp64 = !tpp[chunk + q].mixed;
-        pref[q + 1] = pref[q] + ((f > e && k > 0 && fp64) ? trap_tiles2(f - e, f - e) : 0);
+        pref[q + 1] = pref[q] + ((f > e && k > k0 && fp64) ? trap_tiles2(f - e, f - e) : 0);
       }
     }
     __syncthreads();
@@ -981,12 +1036,12 @@ __global__ void __launch_bounds__(256) k_large_schur(DevPlan P, DevFactor X, con
       }
       const int q = chunk + a;
       const int s = large[q];
-      const int f = X.sn_f[s], e = X.sn_ne[s], kk = tpp[q].k;
+      const int f = X.sn_f[s], e = X.sn_ne[s], k0 = tpp[q].pad[3], kk = tpp[q].k - k0;
       const size_t sf = (size_t)f;
       double *F = X.arena + X.sn_off[s];
       int ti, tj;
       trap_tile2(w - pref[a], f - e, f - e, ti, tj);
-      tile_update<true>(F, sf, nullptr, 0, X.tags + X.sn_roff[s], e + ti * kTM, e + tj * kTN, f, f, 0, kk, sm);
+      tile_update<true>(F, sf, nullptr, 0, X.tags + X.sn_roff[s], e + ti * kTM, e + tj * kTN, f, f, k0, kk, sm);
     }
   }
 }
@@ -1006,8 +1061,8 @@ __global__ void __launch_bounds__(NT) k_large_finish(DevPlan P, DevFactor X, con
   const size_t sf = (size_t)f;
   if (threadIdx.x == 0 && !S.mixed) {
     const double q = (double)(f - ne);
-    if (q > 0 && p > 0)
-      atomicAdd(reinterpret_cast<double *>(X.counters + kCGemmFlops), 2.0 * p * (q * (q + 1) / 2));
+    if (q > 0 && p > S.pad[3])
+      atomicAdd(reinterpret_cast<double *>(X.counters + kCGemmFlops), 2.0 * (p - S.pad[3]) * (q * (q + 1) / 2));
   }
   const bool is_root = P.sn_parent[s] < 0;
   int pstore = p;
@@ -1615,7 +1670,7 @@ __global__ void __launch_bounds__(kSolveNT, 4) k_fwd_front(DevPlan P, DevFactor 
   const int *rows = X.rows + roff;
   const double *L = X.arena + X.sn_off[s];
   const size_t sf = (size_t)f;
-  const bool large = P.sn_fsym[s] >= kLargeMin;
+  const bool large = P.sn_large[s] != 0;
   __shared__ double Ls[32][33];
   const int warp = threadIdx.x >> 5;
   // every right-hand side at once: gather, children's update vectors in
@@ -1789,7 +1844,7 @@ __global__ void __launch_bounds__(kSolveNT) k_bwd_front(DevPlan P, DevFactor X, 
   const int *rows = X.rows + roff;
   const double *L = X.arena + X.sn_off[s];
   const size_t sf = (size_t)f;
-  const bool large = P.sn_fsym[s] >= kLargeMin;
+  const bool large = P.sn_large[s] != 0;
   __shared__ double Ls[32][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // every right-hand side at once. D^-1 of each pivot block; 2x2 blocks

@@ -22,6 +22,9 @@ SMFG_OK = 0
 SMFG_ERR_SINGULAR = 2
 SOLVE_FULL, SOLVE_FORWARD, SOLVE_DIAGONAL, SOLVE_BACKWARD = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
+# indefinite fronts of at least this many rows take the APTP kernel (smf's
+# deterministic mode, kTopTileMinFront)
+APTP_MIN_ROWS = 512
 NOALLOC_MAX_N = 262144  # SMFG_NOALLOC_MAX_N
 
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -58,7 +61,7 @@ class Control(C.Structure):
                 ("precision", C.c_int), ("max_negative_pivots", C.c_int),
                 ("scale", C.c_void_p), ("profile", C.c_int), ("mixed_block", C.c_int),
                 ("mixed_kind", C.c_int), ("mixed_min_front", C.c_int), ("panel_team", C.c_int),
-                ("graph", C.c_int), ("reserved_i", C.c_int * 2),
+                ("graph", C.c_int), ("aptp_min_rows", C.c_int), ("reserved_i", C.c_int * 1),
                 ("reserved_d", C.c_double * 8)]
 
 
@@ -75,6 +78,15 @@ class Info(C.Structure):
     @property
     def inertia(self):
         return (self.num_pos, self.num_neg, self.num_zero)
+
+    @property
+    def aptp_failed(self):
+        """Columns the APTP sweeps failed (smf's Info::aptp_failed_columns)."""
+        return self.reserved_i[4]
+
+    @property
+    def aptp_fronts(self):
+        return self.reserved_i[5]
 
 
 _lib = None
@@ -432,14 +444,19 @@ class Solver:
     def factor(self, values, posdef: bool = False, u: float = 0.01, small: float = 1e-20,
                scale=None, precision: int = PREC_FP64, max_negative_pivots: int = -1,
                raise_on_singular: bool = False, mixed_block: int = 0, mixed_kind: int = 0,
-               mixed_min_front: int = 0, panel_team: int = 0, graph: bool = False) -> Info:
+               mixed_min_front: int = 0, panel_team: int = 0, graph: bool = False,
+               aptp_min_rows: int = APTP_MIN_ROWS) -> Info:
         """Factor new values (the caller's entry order). ``values`` is a
         numpy array, or any object with ``data_ptr()`` (a CUDA tensor) for
         values already in device memory. precision=PREC_MIXED: tensor-core
         trailing updates on large fronts (mixed_block pivots per update,
         mixed_kind TC_TF32X3 / TC_BF16X3, fronts of mixed_min_front rows or
-        more; 0 = the library's defaults)."""
+        more; 0 = the library's defaults). aptp_min_rows: indefinite fronts of
+        at least this many rows take the APTP kernel (smf's deterministic
+        mode, the default 512); 0 = the threshold kernel everywhere (smf's
+        one-thread default mode)."""
         c = default_control(posdef, u, small, precision, max_negative_pivots)
+        c.aptp_min_rows = int(aptp_min_rows)
         c.mixed_block = mixed_block
         c.mixed_kind = mixed_kind
         c.mixed_min_front = mixed_min_front

@@ -39,9 +39,10 @@ def cases(size: str = "small"):
         out += [
             # fronts above 384 rows: the multi-block large-front path
             ("var3d_24", lambda: W.varcoef_3d(24, seed=4), True, "metis", "none", (24 ** 3, 0, 0)),
-            # large indefinite fronts with delays (reference in its one-thread
-            # threshold mode: no APTP tiles, see reference_for)
-            ("kkt_10_700", lambda: W.kkt_ipm(10, 700, seed=6), False, "auto1t", "auto", (1000, 700, 0)),
+            # large indefinite fronts with delays: a front of 977 rows takes
+            # deterministic mode's APTP kernel, then the threshold kernel on
+            # the 739 columns it fails
+            ("kkt_10_700", lambda: W.kkt_ipm(10, 700, seed=6), False, "auto", "auto", (1000, 700, 0)),
         ]
     if size == "full":
         out += [
@@ -56,10 +57,11 @@ def cases(size: str = "small"):
 
 def reference_for(O, posdef, ordering, scaling, deterministic=True):
     """The reference configured as the parity oracle: deterministic mode, one
-    thread. Ordering "auto1t": AutoParallel in the one-thread default mode
-    instead, whose indefinite fronts of >= 512 rows keep the threshold
-    pivoting kernel (deterministic mode tiles them with its APTP kernel,
-    which this engine does not restate)."""
+    thread (its indefinite fronts of >= 512 rows take the APTP kernel, as
+    the engine's and the oracle's do by default). Ordering "auto1t":
+    AutoParallel in the one-thread default mode instead, whose fronts keep
+    the threshold kernel everywhere (the engine's and the oracle's
+    aptp_min_rows = 0)."""
     if ordering == "auto1t":
         ordering, deterministic = "auto", False
     order = {"amd": O.ORDER_AMD, "metis": O.ORDER_METIS, "auto": O.ORDER_AUTO_PARALLEL}[ordering]

@@ -1,13 +1,17 @@
-"""The CUDA APTP front kernel against the oracle, bit for bit.
+"""The CUDA APTP front kernel against the oracle and the reference, bit for
+bit.
 
 The kernel factors every indefinite front of at least 512 rows in the
-reference's deterministic mode (solver/src/ldlt_aptp.cpp:739). Here it runs
-alone on dense fronts through the C ABI (smfg_aptp_front_dense) and must
+reference's deterministic mode (solver/src/ldlt_aptp.cpp:739), the threshold
+kernel then taking the columns it fails (multifrontal_serial.cpp:796-821).
+Alone on dense fronts through the C ABI (smfg_aptp_front_dense) it must
 reproduce the oracle's restatement, itself pinned to the reference
 (tests/test_oracle_aptp.py): the lower triangle of the factored front (L, D
 and the failed columns' Schur complement), the row order, the pivot tags and
 the counts, on fronts with many 2x2 pivots, failed columns inside and
-outside the tiles, tall trailing blocks and more than one block column.
+outside the tiles, tall trailing blocks and more than one block column. In
+whole factorizations (KKT systems whose top fronts take APTP) the engine must
+reproduce the reference's deterministic-mode factor front by front.
 """
 import numpy as np
 import pytest
@@ -57,3 +61,72 @@ def test_aptp_dense_matches_golden():
         assert np.array_equal(np.asarray(res), z[f"{name}_result"]), name
         assert np.array_equal(rows, z[f"{name}_rows"]) and np.array_equal(tags, z[f"{name}_tags"]), name
         assert block_digest(np.tril(F)) == str(z[f"{name}_sha256"]), name
+
+
+@pytest.mark.parametrize("grid,m,seed", [(10, 700, 6), (12, 1200, 1), (14, 2000, 2)])
+def test_aptp_factor_bitwise_vs_deterministic_reference(grid, m, seed, ref_lib):
+    """Whole KKT factorizations on the reference's own analysis and scaling:
+    every front's realized size, rows, tags and L / D block, the inertia,
+    delays, 2x2 pivots, flops and the APTP failed-column count."""
+    from opt_solver_b200 import smfg
+    from opt_solver_b200 import workloads as W
+    from tests.cases import reference_for
+    from tests.test_gpu_parity import _compare_factor
+    O = ref_lib
+    n, cp, ri, v = W.kkt_ipm(grid, m, seed=seed)
+    ref = reference_for(O, False, "auto", "auto", deterministic=True)
+    a = ref.analyse(n, cp, ri, v)
+    fx = ref.factor(v)
+    assert fx.aptp_failed > 0
+    sv = smfg.Solver(a, device=0)
+    gi = sv.factor(v, posdef=False, scale=fx.scale)
+    assert gi.aptp_fronts == int(np.sum(fx.f >= 512))
+    assert gi.aptp_failed == fx.aptp_failed
+    _compare_factor(a, fx, sv.export(), gi)
+    assert gi.inertia == (grid ** 3, m, 0)
+    b = W.rhs(n, 1, seed=3)
+    x = sv.solve(b)
+    xr, _ = ref.solve(b)
+    assert np.max(np.abs(x - xr)) <= 1e-9 * max(1.0, np.max(np.abs(xr)))
+    sv.close()
+
+
+def test_aptp_factor_matches_golden():
+    """The reference's digests of its deterministic-mode factor (no reference
+    library needed)."""
+    import os
+    from oracle import oracle as O
+    from opt_solver_b200 import smfg
+    from tests.test_golden import FIELDS
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "kkt_10_700_digest.npz"))
+    a = O.Analysis(n=int(z["n"]), matching_scale=np.zeros(0), **{k: z["an_" + k] for k in FIELDS})
+    sv = smfg.Solver(a, device=0)
+    gi = sv.factor(z["values"], posdef=False, scale=z["scale"])
+    gx = sv.export()
+    assert gi.inertia == tuple(int(x) for x in z["inertia"])
+    assert (gi.delayed_pivots, gi.two_by_two_pivots, gi.flops) == (int(z["delayed"]), int(z["two_by_two"]),
+                                                                    float(z["flops"]))
+    assert gi.aptp_failed == int(z["aptp_failed"])
+    for s in range(a.nsn):
+        assert block_digest(gx.block(s)) == str(z["block_sha256"][s]), s
+    sv.close()
+
+
+def test_threshold_kernel_everywhere_is_the_default_mode(ref_lib):
+    """aptp_min_rows = 0: the threshold kernel on every front, bit for bit the
+    reference's one-thread default mode."""
+    from opt_solver_b200 import smfg
+    from opt_solver_b200 import workloads as W
+    from tests.cases import reference_for
+    from tests.test_gpu_parity import _compare_factor
+    O = ref_lib
+    n, cp, ri, v = W.kkt_ipm(10, 700, seed=6)
+    ref = reference_for(O, False, "auto1t", "auto")
+    a = ref.analyse(n, cp, ri, v)
+    fx = ref.factor(v)
+    assert fx.aptp_failed == 0
+    sv = smfg.Solver(a, device=0)
+    gi = sv.factor(v, posdef=False, scale=fx.scale, aptp_min_rows=0)
+    assert gi.aptp_fronts == 0
+    _compare_factor(a, fx, sv.export(), gi)
+    sv.close()

@@ -174,11 +174,13 @@ def test_panel_teams_bitwise(team, oracle_lib):
     from opt_solver_b200 import workloads as W
     n, cp, ri, v = W.kkt_ipm(12, 800, seed=11)
     a = smfg.analyse(n, cp, ri)
-    ox = O.restated_factorize(a, O.permuted_values(a, v), False)
+    # the threshold kernel on every front (the one-thread default mode), so
+    # that the team kernels take the fronts of 512 rows and more as well
+    ox = O.restated_factorize(a, O.permuted_values(a, v), False, aptp_min_rows=0)
     sv = smfg.Solver(a, device=0)
-    g1 = sv.factor(v, posdef=False, panel_team=1)
+    g1 = sv.factor(v, posdef=False, panel_team=1, aptp_min_rows=0)
     e1 = sv.export()
-    gt = sv.factor(v, posdef=False, panel_team=team)
+    gt = sv.factor(v, posdef=False, panel_team=team, aptp_min_rows=0)
     et = sv.export()
     assert gt.inertia == g1.inertia == ox.inertia == (12 ** 3, 800, 0)
     assert gt.delayed_pivots == g1.delayed_pivots == ox.delayed > 0

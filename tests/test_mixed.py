@@ -82,15 +82,17 @@ def test_mixed_mask_zero_is_plain():
 
 
 @pytest.mark.parametrize("m,ncon,block", [(12, 800, 256), (14, 1500, 64), (16, 2000, 256)])
-def test_mixed_kkt(m, ncon, block):
+def test_mixed_kkt_threshold_kernel(m, ncon, block):
+    """The threshold kernel's mixed path (aptp_min_rows = 0): FP64 pivoting,
+    tensor-core contribution-block updates every `block` pivots."""
     from opt_solver_b200 import smfg
     n, cp, ri, v = W.kkt_ipm(m, ncon, seed=7)
     a = smfg.analyse(n, cp, ri)
     b = W.rhs(n, 1, seed=8, kind="normal")
     sv = smfg.Solver(a, device=0)
-    ip = sv.factor(v, posdef=False)
+    ip = sv.factor(v, posdef=False, aptp_min_rows=0)
     assert ip.inertia == (m ** 3, ncon, 0)
-    im = sv.factor(v, posdef=False, precision=smfg.PREC_MIXED, mixed_block=block)
+    im = sv.factor(v, posdef=False, precision=smfg.PREC_MIXED, mixed_block=block, aptp_min_rows=0)
     assert im.status == 0 and im.mixed_fronts > 0
     assert im.inertia == ip.inertia
     x, om, it = _solve_refine(sv, b)
