@@ -3,9 +3,10 @@
 
 Default workload (the headline metric's configuration): the SPD
 variable-coefficient 7-point operator on a 64^3 grid (n = 262,144; edge
-conductivities log-uniform in [1e-3, 1e3], seed 0), nested-dissection
-analysis, one right-hand side uniform in [-1, 1]. One step = numeric
-factorization of the values + one solve.
+conductivities log-uniform in [1e-3, 1e3], seed 0) on smf's own METIS
+analysis (rebuilt from the record tests/golden/spd3d64_smf_partition.npz),
+one right-hand side uniform in [-1, 1]. One step = numeric factorization of
+the values + one solve + refinement to the metric's backward-error bar.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--config spd3d|spd3d40|lap2d|traj|kkt|kkt3|batch] [--precision fp64|mixed|both]
@@ -38,8 +39,7 @@ CONFIGS = {
     "traj": ("trajectory KKT T=200 (n=5,612), 8 RHS", "traj200", False, 8),
     "kkt": ("IPM KKT 20^3 + 4,000 constraints (n=12,000), smf's METIS ordering, 1 RHS N(0,1)",
             "kkt_ipm(20, 4000)", False, 1),
-    # configuration 3 at full size: the analysis on smf's own METIS ordering
-    # (tests/golden/kkt40_32000_metis_perm.npz, made by the reference)
+    # configuration 3 at full size on smf's own METIS analysis
     "kkt3": ("IPM KKT 40^3 + 32,000 constraints (n=96,000), Sigma 10^U[-8,8], delta 1e-8, smf's METIS "
              "ordering, u=0.01, 1 RHS N(0,1)", "kkt_ipm(40, 32000)", False, 1),
     # the same generator as spd3d at 40^3: the small case of the ncu captures
@@ -96,10 +96,15 @@ class _Workload:
             self.expected = [(16 * ((m[0] - 12) // 28) + 12, 12 * ((m[0] - 12) // 28), 0) for m in mats]
         else:
             n, cp, ri, v = build_matrix(cfg)
-            perm = given_ordering(cfg)
-            a = smfg.analyse(n, cp, ri, perm=perm)
-            self.ordering = "smf's METIS ordering (committed fixture)" if perm is not None else \
-                "engine nested dissection (smfg_analyse)"
+            rec = smf_record(cfg)
+            if rec is not None:
+                from opt_solver_b200 import smf_analysis
+                a = smf_analysis.load(rec, n, cp, ri)
+                self.ordering = "smf's own analysis (%s), rebuilt from its record %s" % (
+                    SMF_RECORDS[cfg][1], os.path.relpath(rec, ROOT))
+            else:
+                a = smfg.analyse(n, cp, ri)
+                self.ordering = "engine nested dissection (smfg_analyse)"
             self.analyse_s = time.time() - t0
             self.sv = smfg.Solver(a, device=device)
             self.solver = self.sv
@@ -113,20 +118,32 @@ class _Workload:
             self.systems = 1
             self.expected = None
 
-    def inertia_ok(self):
+    def inertia_ok(self, rank=0, world=1):
+        """Every system's inertia exact: on N ranks each rank's slice of the
+        batch is gathered in system order first."""
         if self.expected is None:
             return True
-        return [s[:3] for s in self.solver.system_stats()] == self.expected
+        if world == 1:
+            return [s[:3] for s in self.solver.system_stats()] == self.expected
+        from opt_solver_b200.batch import gather_system_stats, shard
+        lo, _ = shard(BATCH_COUNT, rank, world)
+        allst = gather_system_stats(self.solver.system_stats(), lo, BATCH_COUNT, world)
+        want = [(16 * ((m[0] - 12) // 28) + 12, 12 * ((m[0] - 12) // 28), 0) for m in batch_systems()]
+        return [tuple(int(x) for x in r[:3]) for r in allst] == want
 
 
-def given_ordering(cfg: str):
-    """smf's own fill-reducing ordering of the KKT workloads (perm[new] =
-    old), committed under tests/golden/ by make_kkt_orderings.py; None: the
-    engine's analysis orders the matrix itself."""
-    name = {"kkt": "kkt20_4000", "kkt3": "kkt40_32000"}.get(cfg)
-    if name is None:
+# smf's analysis of each workload, recorded by the reference itself
+# (tests/golden/make_smf_partitions.py): (record, ordering smf used)
+SMF_RECORDS = {"spd3d": ("spd3d64", "METIS"), "lap2d": ("lap2d150", "its minimum degree (AMD)"),
+               "kkt": ("kkt20_4000", "METIS"), "kkt3": ("kkt40_32000", "METIS")}
+
+
+def smf_record(cfg: str):
+    """The record of smf's analysis of a workload (perm and supernode
+    partition), or None: the engine's own analysis orders the matrix."""
+    if cfg not in SMF_RECORDS:
         return None
-    return np.load(os.path.join(ROOT, "tests", "golden", f"{name}_metis_perm.npz"))["perm"]
+    return os.path.join(ROOT, "tests", "golden", f"{SMF_RECORDS[cfg][0]}_smf_partition.npz")
 
 
 def build_matrix(cfg: str):
@@ -144,22 +161,6 @@ def build_matrix(cfg: str):
     if cfg == "spd3d40":
         return W.varcoef_3d(40, seed=0)
     raise ValueError(cfg)
-
-
-def sample_matrix(cfg: str):
-    """The bounded CPU sample of each workload (reference on the host cores):
-    (list of matrices, description, factor to scale the time to the full
-    workload or None to scale by the reference's delay-free flop counts)."""
-    from opt_solver_b200 import workloads as W
-    if cfg == "spd3d":
-        return [W.varcoef_3d(32, seed=0)], "varcoef_3d(32) (n=32,768), same generator", None
-    if cfg == "batch":
-        mats = batch_systems()[:64]
-        return mats, "the first 64 of the 1,024 systems, one smf analyse/factor/solve each", BATCH_COUNT / 64
-    if cfg == "kkt3":
-        # smf refuses the full size (its largest front exceeds its storage cap)
-        return [W.kkt_ipm(20, 4000, seed=0)], "kkt_ipm(20, 4000) (n=12,000), same generator", None
-    return [build_matrix(cfg)], "the full workload", 1.0
 
 
 def dist_init():
@@ -281,21 +282,36 @@ def dgemm_peak_tflops():
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def dominant_roofline(prof: dict, head: str, A: dict, peaks: dict, dgemm_peak=None) -> dict:
-    """The roofline object of the JSON line for the step's dominant kernel,
-    from the profiled factorization's counters (``prof``), the timed arm
-    (``A``: its factor_ms) and the measured peaks."""
+def dominant_roofline(prof: dict, head: str, A: dict, peaks: dict, dgemm_peak=None, solve=None) -> dict:
+    """The roofline object of the JSON line for the step's dominant kernel by
+    device time, from the profiled factorization's counters (``prof``), the
+    timed arm (``A``: its factor_ms) and the measured peaks. Candidates: the
+    streamed FP64 deferred updates (HBM-bound), the FP64 Schur updates, the
+    tensor-core passes of the mixed fronts, the pivoting panels, and the
+    solves of the step (``solve``: ms per solve, solves per step including
+    the refinement's, algorithmic bytes per solve)."""
     dgemm_peak = dgemm_peak or dgemm_peak_tflops
-    # the dominant large-front update kernel by device time: the streamed
-    # deferred updates (HBM-bound), the FP64 Schur updates, or the tensor-core
-    # passes of the mixed fronts
     defer_ms = max(prof.get("gemm_ms", 0.0) - prof.get("schur_ms", 0.0), 0.0)
     cands = {"defer": defer_ms, "tc": prof.get("tc_ms", 0.0) if head == "mixed" else 0.0,
-             "fp64": prof.get("gemm_ms", 0.0) if defer_ms <= 0.0 else prof.get("schur_ms", 0.0)}
+             "fp64": prof.get("gemm_ms", 0.0) if defer_ms <= 0.0 else prof.get("schur_ms", 0.0),
+             "solve": solve["ms"] * solve["count"] if solve and solve.get("bytes") else 0.0}
+    kernel_ms = {"defer": defer_ms, "schur_fp64": prof.get("schur_ms"), "tc": prof.get("tc_ms"),
+                 "pivoting_panels": prof.get("panel_ms"), "solves": cands["solve"]}
     dom = max(cands, key=cands.get) if max(cands.values()) > 0 else None
     hbm = peaks.get("hbm_gbs") or 6650.0
     hbm_src = "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks.get("hbm_gbs") else "fallback 6650 GB/s"
-    if dom == "defer" and prof.get("defer_bytes", 0) > 0:
+    if dom == "solve":
+        achieved = solve["bytes"] / (solve["ms"] * 1e-3) / 1e9
+        roof = {
+            "kernel": "supernodal forward + backward sweeps (k_fwd_* / k_bwd_*, gather and scatter), one solve",
+            "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            "traffic": solve.get("traffic"), "traffic_source": solve.get("traffic_source"),
+            "peak_source": hbm_src, "solves_per_step": solve["count"], "avg_solve_ms": solve["ms"],
+            "algorithmic_bytes_per_solve": solve["bytes"],
+            "algorithmic_bytes_source": "2 sweeps x (8 |L| + 4 sum f + 16 n nrhs)",
+            "kernel_ms": kernel_ms,
+        }
+    elif dom == "defer" and prof.get("defer_bytes", 0) > 0:
         # bytes: every entry of each deferred update's trapezoid read and
         # written once (16 bytes), summed on the device
         achieved = prof["defer_bytes"] / (defer_ms * 1e-3) / 1e9
@@ -305,15 +321,14 @@ def dominant_roofline(prof: dict, head: str, A: dict, peaks: dict, dgemm_peak=No
             "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
             "traffic": DEFER_DRAM_BYTES_PER_ENTRY * (prof["defer_bytes"] / 16.0) / max(prof["gemm_launches"], 1),
             "traffic_source": "per launch, scaled by updated entries from the ncu capture of one "
-                              "8,000-row front (profiles/k_large_defer_front8000.md)",
+                              "8,000-row front of the kernel",
             "peak_source": hbm_src,
             "launches": prof["gemm_launches"], "front_updates": prof.get("defer_updates"),
             "front_updates_of_at_most_2_pivots": prof.get("defer_small"),
             "avg_launch_ms": defer_ms / max(prof["gemm_launches"], 1),
             "algorithmic_bytes_per_launch": prof["defer_bytes"] / max(prof["gemm_launches"], 1),
             "algorithmic_bytes_per_front_update": prof["defer_bytes"] / nupd,
-            "kernel_ms": {"defer": defer_ms, "schur_fp64": prof.get("schur_ms"), "tc": prof.get("tc_ms"),
-                          "pivoting_panels": prof.get("panel_ms")},
+            "kernel_ms": kernel_ms,
         }
     elif dom == "tc":
         # the tensor-core trailing updates (split + product kernels) against
@@ -359,10 +374,12 @@ def dominant_roofline(prof: dict, head: str, A: dict, peaks: dict, dgemm_peak=No
 OMEGA_GATE = 1e-12  # the metric's scaled backward error bar
 # DRAM bytes k_large_defer moves per updated entry, from one ncu capture of
 # the kernel on an 8,000-row front (192.8 MB read + 134.8 MB written for
-# 23.9 M entries, profiles/k_large_defer_front8000.md); the bench's traffic
+# 23.9 M entries); the bench's traffic
 # per launch is this times the entries its launches update
 DEFER_DRAM_BYTES_PER_ENTRY = (192.8e6 + 134.8e6) / 23.9e6
 GRAPH_REPLAY = {"kkt": False, "kkt3": False}  # configurations whose steps replay a CUDA graph (default: yes)
+# repeats of the full workload in the CPU-baseline leg (about 10-30 s of host work)
+CPU_REPS = {"spd3d": 3, "lap2d": 30, "kkt": 5, "traj": 30, "batch": 1}
 
 
 def run_ours(args, rank, world, local):
@@ -387,6 +404,7 @@ def run_ours(args, rank, world, local):
     use_graph = GRAPH_REPLAY.get(args.config, True)
     head = "mixed" if "mixed" in arms else "fp64"
     res = {}
+    xs = {}
     clocks = None
     for arm in arms:
         prec = smfg.PREC_MIXED if arm == "mixed" else smfg.PREC_FP64
@@ -413,6 +431,7 @@ def run_ours(args, rank, world, local):
                 parts.append(pr)
         torch.cuda.synchronize()
         barrier(world)
+        xs[arm] = d_x.cpu().numpy().copy()
         if arm == head:
             clocks = clk.summary()
         ms_step = allmax(sum(dev) / len(dev), world)
@@ -422,14 +441,16 @@ def run_ours(args, rank, world, local):
         res[arm] = {
             "ms": ms_step, "factor_ms": sum(fm) / len(fm), "solve_ms": sum(sm_) / len(sm_),
             "refine_ms": sum(rm) / len(rm), "eta_inf": acc[0], "omega": acc[1], "refine_solves": acc[2],
-            "inertia": list(info.inertia), "inertia_exact_per_system": wl.inertia_ok(),
+            "inertia": list(info.inertia), "inertia_exact_per_system": wl.inertia_ok(rank, world),
             "mixed_fronts": int(info.mixed_fronts), "kernel_launches": int(info.kernel_launches),
             "flops": info.flops, "delayed": int(info.delayed_pivots),
             "info": info,
         }
-    # the arms agree on the inertia
+    # the arms agree on the inertia; the mixed arm's forward error against
+    # the plain FP64 arm's solution
     if len(arms) == 2:
         res["inertia_same"] = res["fp64"]["inertia"] == res["mixed"]["inertia"]
+        res["mixed"]["forward_error_vs_fp64"] = forward_error(xs["mixed"], xs["fp64"])
     # e2e: host buffers through the C ABI (copies inside the timed region)
     prec = smfg.PREC_MIXED if head == "mixed" else smfg.PREC_FP64
     e2e = []
@@ -447,6 +468,8 @@ def run_ours(args, rank, world, local):
     e2e_ms = allmax(sum(e2e) / len(e2e), world)
     _, eta, om = sv.residual(wl.b, x)
     prof = sv.profile_factor(d_vals, posdef=posdef, precision=prec, scale=wl.scale)
+    A_info = res[head]["info"]
+    front_rows = int(sv.factor_sizes()[1])
     return {
         "arms": res, "head": head, "e2e_ms": e2e_ms, "e2e_eta": eta, "e2e_omega": om,
         "analyse_s": wl.analyse_s, "n": wl.n, "nnz": wl.nnz, "nrhs": wl.nrhs, "desc": wl.desc,
@@ -454,6 +477,8 @@ def run_ours(args, rank, world, local):
         "ordering": getattr(wl, "ordering", "engine nested dissection (smfg_analyse)"),
         "clocks": clocks, "nsn": wl.nsn, "systems": wl.systems,
         "h2d": wl.nnz * 8 + wl.n * wl.nrhs * 8, "d2h": wl.n * wl.nrhs * 8, "profile": prof,
+        "x_fp64": xs.get("fp64"), "b": wl.b, "values": wl.values,
+        "factor_entries": int(A_info.factor_entries), "front_rows": front_rows,
     }
 
 
@@ -476,7 +501,12 @@ def run_stream(args, rank, world, local):
     desc, base, posdef = STREAMS[args.config]
     n, cp, ri, v = build_matrix(base)
     t0 = time.time()
-    a = smfg.analyse(n, cp, ri, perm=given_ordering(base))
+    rec = smf_record(base)
+    if rec is not None:
+        from opt_solver_b200 import smf_analysis
+        a = smf_analysis.load(rec, n, cp, ri)
+    else:
+        a = smfg.analyse(n, cp, ri)
     analyse_s = time.time() - t0
     dslot = W.diagonal_slots(n, cp, ri)
     base_vals = np.array(v, dtype=np.float64)
@@ -565,50 +595,58 @@ def run_stream(args, rank, world, local):
     }
 
 
-def cpu_reference_ms(cfg, threads):
+def forward_error(x, x_ref):
+    """max |x - x_ref| / max |x_ref| (both n x nrhs)."""
+    den = float(np.max(np.abs(x_ref))) if np.size(x_ref) else 0.0
+    return float(np.max(np.abs(np.asarray(x) - np.asarray(x_ref)))) / den if den > 0 else None
+
+
+# Configuration 3 at full size is beyond the reference: its root front of
+# 32,150 rows exceeds smf's factor storage cap (kMaxFactorStorageEntries =
+# 2^29 entries, solver/include/smf/types.hpp:13, checked in
+# solver/src/factor_indef.cpp:33-54)
+REF_REFUSES = {"kkt3": "smf refuses it: its 32,150-row root front exceeds kMaxFactorStorageEntries = 2^29 "
+                       "(types.hpp:13, factor_indef.cpp:33-54)"}
+REF_BLAS = "smf's own portable BLAS loops (SMF_BLAS_REFERENCE; the image has no BLAS library)"
+
+
+def reference_step(cfg, threads, reps):
     """The reference smf solver (oracle/_ref, compiled from its sources) on
-    the host cores, fastest host mode (non-deterministic, `threads` threads,
-    its own analysis: METIS on the 3D grid, its automatic choice otherwise;
-    LAPACK-style SPD fronts): factor + solve ms of a bounded sample, scaled to
-    the full workload. Returns (ms, sample description)."""
+    the host cores in its fastest host mode (non-deterministic, `threads`
+    threads, LAPACK-style SPD front kernel, its own analysis with the
+    ordering the GPU arm's record holds): factor + solve ms of the full
+    workload, median of `reps` runs, the analysis outside the timed region
+    as in the GPU arm (a refactor). Configuration 4 times its first 64
+    systems and scales by the system count. Returns (ms, sample, x of the
+    first right-hand side or None)."""
     from oracle import oracle as O
     from opt_solver_b200 import workloads as W
-    mats, sample, scale = sample_matrix(cfg)
-    posdef = CONFIGS[cfg][2]
-    nrhs = CONFIGS[cfg][3]
-    ordering = O.ORDER_METIS if (cfg.startswith("spd3d") or cfg.startswith("kkt")) else O.ORDER_AUTO_PARALLEL
-    total = 0.0
-    analyses = []
+    posdef, nrhs = CONFIGS[cfg][2], CONFIGS[cfg][3]
+    if cfg == "batch":
+        mats, scale = batch_systems()[:64], BATCH_COUNT / 64
+        sample = "the first 64 of the 1,024 systems (one smf analyse, then factor + solve each); time x16"
+    else:
+        mats, scale = [build_matrix(cfg)], 1.0
+        sample = "the full workload"
+    order = {"spd3d": O.ORDER_METIS, "kkt": O.ORDER_METIS, "lap2d": O.ORDER_AMD}.get(cfg, O.ORDER_AUTO_PARALLEL)
+    refs = []
     for i, (n, cp, ri, v) in enumerate(mats):
-        ref = O.Reference(posdef=posdef, ordering=ordering, deterministic=False, num_threads=threads,
+        ref = O.Reference(posdef=posdef, ordering=order, deterministic=False, num_threads=threads,
                           scaling=O.SCALE_AUTO, posdef_kernel=O.POSDEF_KERNEL_LAPACK)
-        a = ref.analyse(n, cp, ri, v)
-        analyses.append(a)
-        b = W.rhs(n, nrhs, seed=i, kind="normal")
+        ref.analyse(n, cp, ri, v)
+        refs.append((ref, v, W.rhs(n, nrhs, seed=i if cfg == "batch" else 1,
+                                   kind="normal" if cfg != "spd3d" and cfg != "lap2d" else "uniform")))
+    times, x0 = [], None
+    for _ in range(max(1, reps)):
         t = time.perf_counter()
-        ref.factor(v, export=False)
-        ref.solve(b)
-        total += (time.perf_counter() - t) * 1e3
-    if scale is None:
-        n, cp, ri, v = build_matrix(cfg)
-        ref = O.Reference(posdef=posdef, ordering=ordering, deterministic=False, num_threads=threads)
-        a_full = ref.analyse(n, cp, ri, v)
-        scale = delay_free_flops(a_full) / max(delay_free_flops(analyses[0]), 1.0)
-        sample += f"; time x{scale:.2f} (the reference's delay-free flops, full / sample)"
-    elif scale != 1.0:
-        sample += f"; time x{scale:.0f}"
-    return total * scale, sample
-
-
-def delay_free_flops(a):
-    f = np.diff(a.front_row_ptr).astype(np.float64)
-    p = (np.asarray(a.sn_end) - np.asarray(a.sn_start)).astype(np.float64)
-    # sum over k < p of r + r (r + 1), r = f - k - 1
-    tot = 0.0
-    for fi, pi in zip(f, p):
-        r = fi - 1 - np.arange(pi)
-        tot += float(np.sum(r + r * (r + 1.0)))
-    return tot
+        for ref, v, b in refs:
+            ref.factor(v, export=False)
+            x, _ = ref.solve(b)
+            if x0 is None:
+                x0 = x
+        times.append((time.perf_counter() - t) * 1e3)
+    sample += f"; {REF_BLAS}; median of {len(times)} run(s)"
+    return statistics.median(times) * scale, sample, (x0 if cfg != "batch" else None)
 
 
 def run_reference_arm(args, rank, world):
@@ -617,12 +655,14 @@ def run_reference_arm(args, rank, world):
     from oracle import oracle as O
     if not O.ref_available():
         return {"impl": "reference", "unavailable": "oracle/_ref not built (the reference sources were absent at build time)"}
+    cfg = STREAMS[args.config][1] if args.config in STREAMS else args.config
+    if cfg in REF_REFUSES:
+        return {"impl": "reference", "unavailable": REF_REFUSES[cfg]}
     threads = os.cpu_count() or 1
     times = []
     sample = ""
-    cfg = STREAMS[args.config][1] if args.config in STREAMS else args.config
     for i in range(args.warmup + args.steps):
-        ms, sample = cpu_reference_ms(cfg, threads)
+        ms, sample, _ = reference_step(cfg, threads, 1)
         if i >= args.warmup:
             times.append(ms)
     ms_step = statistics.median(times)
@@ -704,18 +744,31 @@ def main():
     A = r["arms"][head]
     peaks = measured_peaks()
     prof = r["profile"]
-    roof = dominant_roofline(prof, head, A, peaks)
+    # the solves of the step: one, plus the refinement's
+    sol = {"ms": A["solve_ms"], "count": 1 + int(A["refine_solves"] or 0),
+           "bytes": 2.0 * (8.0 * r["factor_entries"] + 4.0 * r["front_rows"] + 16.0 * r["n"] * r["nrhs"])}
+    roof = dominant_roofline(prof, head, A, peaks, solve=sol)
     cpu = None
+    x_ref = None
     if not args.no_cpu_baseline:
         try:
             from oracle import oracle as O
-            if O.ref_available():
+            if args.config in REF_REFUSES:
+                cpu = {"value": None, "unit": "ms", "cores": 0, "kind": "reference",
+                       "sample": REF_REFUSES[args.config]}
+            elif O.ref_available():
                 threads = os.cpu_count() or 1
-                ms, sample = cpu_reference_ms(args.config, threads)
+                # about 10-30 s of host work: repeats of the full workload
+                ms, sample, x_ref = reference_step(args.config, threads, CPU_REPS.get(args.config, 3))
                 cpu = {"value": ms, "unit": "ms", "cores": threads, "kind": "reference",
                        "sample": sample}
         except Exception as exc:  # noqa: BLE001
             cpu = {"value": None, "unit": "ms", "cores": 0, "kind": "reference", "sample": f"failed: {exc}"}
+    if x_ref is not None and r.get("x_fp64") is not None and "fp64" in r["arms"]:
+        # the plain arm's solution against the reference's own (its FP64
+        # factor on the host, unrefined)
+        r["arms"]["fp64"]["forward_error_vs_reference"] = forward_error(
+            r["x_fp64"].reshape(np.shape(x_ref)), x_ref)
     batch = args.config == "batch"
     arms = {}
     for k, v in r["arms"].items():

@@ -551,6 +551,15 @@ class Solver:
             raise SmfgError(rc, "smfg_front_stats")
         return st.reshape(self.nsn, 5)
 
+    def factor_sizes(self):
+        """(stored factor entries sum f * p, realized front rows sum f) of
+        the last factorization (smfg_factor_sizes)."""
+        be, re_ = C.c_int64(), C.c_int64()
+        rc = lib().smfg_factor_sizes(self._h, C.byref(be), C.byref(re_))
+        if rc != SMFG_OK:
+            raise SmfgError(rc, "smfg_factor_sizes")
+        return int(be.value), int(re_.value)
+
     def export(self) -> FrontFactor:
         be, re_ = C.c_int64(), C.c_int64()
         lib().smfg_factor_sizes(self._h, C.byref(be), C.byref(re_))

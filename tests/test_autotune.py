@@ -10,15 +10,16 @@ from opt_solver_b200 import workloads as W
 
 
 def _kkt():
+    """The 20^3 + 4,000 KKT on smf's own METIS analysis (its record)."""
+    from opt_solver_b200 import smf_analysis as SA
     n, cp, ri, v = W.kkt_ipm(20, 4000, seed=0)
-    perm = np.load(os.path.join(os.path.dirname(__file__), "golden", "kkt20_4000_metis_perm.npz"))["perm"]
-    return n, cp, ri, v, perm
+    a = SA.load(os.path.join(os.path.dirname(__file__), "golden", "kkt20_4000_smf_partition.npz"), n, cp, ri)
+    return n, cp, ri, v, a
 
 
 def test_buckets_present():
-    from opt_solver_b200 import autotune, smfg
-    n, cp, ri, v, perm = _kkt()
-    a = smfg.analyse(n, cp, ri, perm=perm)
+    from opt_solver_b200 import autotune
+    n, cp, ri, v, a = _kkt()
     b = autotune._buckets_present(a)
     assert b == sorted(b, reverse=True) and set(b) <= {0, 1, 2, 3} and 3 in b
 
@@ -26,8 +27,7 @@ def test_buckets_present():
 @pytest.mark.gpu
 def test_autotune_teams():
     from opt_solver_b200 import autotune, smfg
-    n, cp, ri, v, perm = _kkt()
-    a = smfg.analyse(n, cp, ri, perm=perm)
+    n, cp, ri, v, a = _kkt()
     scale = smfg.matching_scale(n, cp, ri, v)[0]
     sv = smfg.Solver(a, device=0)
     sv.factor(v, posdef=False, scale=scale)

@@ -51,3 +51,15 @@ def test_small_fronts_only(peaks):
     _check(roof, "hbm", "GB/s")
     assert roof["traffic"] is None
     assert roof["peak"] == (6555.2 if peaks else 6650.0)
+
+
+def test_solves_dominant():
+    """Four solves a step (one, three refinement) outweigh the factor's
+    kernels: the solves are the named kernel, against HBM."""
+    prof = {"gemm_ms": 6.0, "schur_ms": 0.3, "defer_bytes": 1e9, "gemm_launches": 40, "tc_ms": 3.8,
+            "tc_flops": 1e12, "tc_passes": 5, "panel_ms": 19.0}
+    solve = {"ms": 9.3, "count": 4, "bytes": 1.51e9}
+    roof = bench.dominant_roofline(prof, "mixed", ARM, PEAKS, solve=solve)
+    _check(roof, "hbm", "GB/s")
+    assert math.isclose(roof["achieved"], 1.51e9 / 9.3e-3 / 1e9)
+    assert roof["kernel_ms"]["solves"] == 4 * 9.3

@@ -12,7 +12,7 @@ import pytest
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 FILES = sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
-FILES = [f for f in FILES if not os.path.basename(f).endswith(("_metis_perm.npz", "_digest.npz"))]
+FILES = [f for f in FILES if not os.path.basename(f).endswith(("_smf_partition.npz", "_digest.npz"))]
 FIELDS = ["perm", "sn_start", "sn_end", "sn_parent", "child_ptr", "child_idx", "front_row_ptr",
           "front_row_idx", "postorder", "perm_col_ptr", "perm_row_idx", "clean_to_perm",
           "orig_to_clean", "clean_col_ptr", "clean_row_idx"]
