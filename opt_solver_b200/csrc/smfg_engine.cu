@@ -1114,7 +1114,24 @@ static int large_pmax(const Plan &pl, int l) {
   return l < (int)pl.lvl_large_pmax.size() ? pl.lvl_large_pmax[l] : pl.lvl_large_maxf[l];
 }
 
+static void enqueue_solve_chunk(Plan &pl, double *d_b, int nrhs, int ldb, int job, bool scaled, LaunchCount &lc);
+
+// Up to kSolveRhs right-hand sides per sweep (the large fronts' block
+// kernels keep that many columns of the block's values in shared memory).
+constexpr int kSolveRhs = 8;
+
 static void enqueue_solve(Plan &pl, double *d_b, int nrhs, int ldb, int job, bool scaled, LaunchCount &lc) {
+  static bool attrs = false;
+  if (!attrs) {
+    SMFG_CUDA(cudaFuncSetAttribute(k_fwd_tri, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TriSmem)));
+    SMFG_CUDA(cudaFuncSetAttribute(k_bwd_tri, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TriSmem)));
+    attrs = true;
+  }
+  for (int r0 = 0; r0 < nrhs; r0 += kSolveRhs)
+    enqueue_solve_chunk(pl, d_b + (size_t)r0 * ldb, std::min(kSolveRhs, nrhs - r0), ldb, job, scaled, lc);
+}
+
+static void enqueue_solve_chunk(Plan &pl, double *d_b, int nrhs, int ldb, int job, bool scaled, LaunchCount &lc) {
   DevPlan &d = pl.d;
   DevFactor &x = pl.x;
   cudaStream_t st = pl.stream;
@@ -1139,14 +1156,15 @@ static void enqueue_solve(Plan &pl, double *d_b, int nrhs, int ldb, int job, boo
   if (fwd) {
     for (int l = 0; l < pl.nlevels; ++l) {
       const int lo = pl.lvl_ptr[l], m = pl.lvl_ptr[l + 1] - lo;
+      k_fwd_small<<<(m + 7) / 8, 256, 0, st>>>(d, x, lo, m, pl.posdef, xv, wk, rows_total, nrhs);
       k_fwd_front<<<m, kSolveNT, 0, st>>>(d, x, lo, pl.posdef, xv, wk, rows_total, nrhs);
-      lc.n++;
+      lc.n += 2;
       const int nL = pl.lvl_large_ptr[l + 1] - pl.lvl_large_ptr[l];
       if (nL > 0) {
         const int *lg = d.lvl_large + pl.lvl_large_ptr[l];
         const int nb = (large_pmax(pl, l) + kSB - 1) / kSB;
         for (int b = 0; b < nb; ++b) {
-          k_fwd_tri<<<nL, kTriNT, 0, st>>>(d, x, lg, b, pl.posdef, xv, wk, rows_total, nrhs);
+          k_fwd_tri<<<nL, kTriNT, sizeof(TriSmem), st>>>(d, x, lg, b, pl.posdef, xv, wk, rows_total, nrhs);
           k_fwd_gemv<<<lgrid, 256, 0, st>>>(d, x, lg, nL, b, wk, rows_total, nrhs);
         }
         lc.n += 2 * nb;
@@ -1161,15 +1179,16 @@ static void enqueue_solve(Plan &pl, double *d_b, int nrhs, int ldb, int job, boo
         k_bwd_l21<<<lgrid, 256, 0, st>>>(d, x, d.lvl_large + pl.lvl_large_ptr[l], nL, xv, wk, rows_total, nrhs);
         lc.n++;
       }
+      k_bwd_small<<<(m + 7) / 8, 256, 0, st>>>(d, x, lo, m, pl.posdef, xv, nrhs, use_d ? 1 : 0, use_lt ? 1 : 0);
       k_bwd_front<<<m, kSolveNT, 0, st>>>(d, x, lo, pl.posdef, xv, wk, rows_total, nrhs,
                                           use_d ? 1 : 0, use_lt ? 1 : 0);
-      lc.n++;
+      lc.n += 2;
       if (nL > 0 && use_lt) {
         const int *lg = d.lvl_large + pl.lvl_large_ptr[l];
         const int nb = (large_pmax(pl, l) + kSB - 1) / kSB;
         for (int b = nb - 1; b >= 0; --b) {
           k_bwd_dots<<<lgrid, 256, 0, st>>>(d, x, lg, nL, b, wk, rows_total, nrhs);
-          k_bwd_tri<<<nL, kTriNT, 0, st>>>(d, x, lg, b, pl.posdef, xv, wk, rows_total, nrhs);
+          k_bwd_tri<<<nL, kTriNT, sizeof(TriSmem), st>>>(d, x, lg, b, pl.posdef, xv, wk, rows_total, nrhs);
         }
         lc.n += 2 * nb;
       }

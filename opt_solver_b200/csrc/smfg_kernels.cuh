@@ -1633,14 +1633,22 @@ __device__ __forceinline__ void load_tri32_async(const double *L, size_t sf, int
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // w[jb:jb+nb) <- L11^-1 w (unit, or non-unit for SPD): lane = row.
+// (the lane's row of the triangle in registers and the SPD diagonal's
+// reciprocal taken ahead: a step of the chain is a shuffle and an fma)
 __device__ __forceinline__ void tri_fwd_warp(double *w, int jb, int nb, int posdef, const double (*Ls)[33]) {
   const int lane = threadIdx.x & 31;
+  double lrow[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) lrow[j] = (j < lane && lane < nb) ? Ls[lane][j] : 0.0;
+  const double rdiag = (posdef && lane < nb) ? 1.0 / Ls[lane][lane] : 1.0;
   double wi = (lane < nb) ? w[jb + lane] : 0.0;
-  for (int j = 0; j < nb; ++j) {
-    double wj = __shfl_sync(0xffffffffu, wi, j);
-    if (posdef) wj = wj / Ls[j][j];
-    if (lane == j) wi = wj;
-    if (lane > j && lane < nb) wi = fma(-Ls[lane][j], wj, wi);
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    if (j < nb) {
+      if (lane == j) wi = wi * rdiag;
+      const double wj = __shfl_sync(0xffffffffu, wi, j);
+      if (lrow[j] != 0.0) wi = fma(-lrow[j], wj, wi);
+    }
   }
   if (lane < nb) w[jb + lane] = wi;
 }
@@ -1648,19 +1656,196 @@ __device__ __forceinline__ void tri_fwd_warp(double *w, int jb, int nb, int posd
 // v[jb:jb+nb) <- L11^-T v: lane = row.
 __device__ __forceinline__ void tri_bwd_warp(double *v, int jb, int nb, int posdef, const double (*Ls)[33]) {
   const int lane = threadIdx.x & 31;
+  double lcol[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) lcol[j] = (j > lane && j < nb) ? Ls[j][lane] : 0.0;
+  const double rdiag = (posdef && lane < nb) ? 1.0 / Ls[lane][lane] : 1.0;
   double vi = (lane < nb) ? v[jb + lane] : 0.0;
-  for (int j = nb - 1; j >= 0; --j) {
-    double xj = __shfl_sync(0xffffffffu, vi, j);
-    if (posdef) xj = xj / Ls[j][j];
-    if (lane == j) vi = xj;
-    if (lane < j) vi = fma(-Ls[j][lane], xj, vi);
+#pragma unroll
+  for (int j = 31; j >= 0; --j) {
+    if (j < nb) {
+      if (lane == j) vi = vi * rdiag;
+      const double xj = __shfl_sync(0xffffffffu, vi, j);
+      if (lcol[j] != 0.0) vi = fma(-lcol[j], xj, vi);
+    }
   }
   if (lane < nb) v[jb + lane] = vi;
 }
 
+// Fronts of at most this many rows take the warp-per-front solve kernels.
+constexpr int kSolveSmall = 64;
+
+// D^-1 of the 2x2 pivot [d00 d10; d10 d11] applied to (r0, r1) by the scaled
+// Cramer rule (solve_diag.cpp:49-123); zero for a singular block.
+__device__ __forceinline__ void dinv2_apply(double d00, double d10, double d11, double r0, double r1, double &z0,
+                                            double &z1) {
+  const double s2 = max3_ref(fabs(d00), fabs(d10), fabs(d11));
+  z0 = 0.0;
+  z1 = 0.0;
+  if (isfinite(s2) && s2 != 0.0) {
+    const double a = d00 / s2, bb = d10 / s2, cc = d11 / s2;
+    const double det = __dsub_rn(__dmul_rn(a, cc), __dmul_rn(bb, bb));
+    if (isfinite(det) && det != 0.0) {
+      if (!isfinite(r0) || !isfinite(r1)) {
+        z0 = r0;
+        z1 = r1;
+      } else {
+        const double rs = fmax(fabs(r0), fabs(r1));
+        if (rs != 0.0) {
+          const double q0 = r0 / rs, q1 = r1 / rs;
+          const double u0 = __dsub_rn(__dmul_rn(cc, q0), __dmul_rn(bb, q1)) / det;
+          const double u1 = __dadd_rn(__dmul_rn(-bb, q0), __dmul_rn(a, q1)) / det;
+          const double ratio = rs / s2;
+          z0 = __dmul_rn(u0, ratio);
+          z1 = __dmul_rn(u1, ratio);
+        }
+      }
+    }
+  }
+}
+
+// Forward sweep of the level's fronts of at most kSolveSmall rows, a warp
+// per front (no block barriers; eight fronts a block): gather, the
+// children's update vectors in child order, then column by column over the
+// whole front (the unit, or SPD non-unit, L11 solve and w[p:f) -= L21
+// w[0:p) in one pass), the front's L columns loaded eight at a time ahead
+// of their use.
+__global__ void __launch_bounds__(256, 4) k_fwd_small(DevPlan P, DevFactor X, int lo, int m, int posdef, double *x,
+                                                   double *wk, int64_t rows_total, int nrhs) {
+  __shared__ double sw_all[8][kSolveSmall];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int item = blockIdx.x * 8 + wid;
+  if (item >= m) return;
+  const int s = P.lvl_sn[lo + item];
+  const int f = X.sn_f[s];
+  if (f > kSolveSmall || P.sn_large[s]) return;
+  const int p = X.sn_pstore[s];
+  const int64_t roff = X.sn_roff[s];
+  const int *rows = X.rows + roff;
+  const double *L = X.arena + X.sn_off[s];
+  double *sw = sw_all[wid];
+  for (int r = 0; r < nrhs; ++r) {
+    double *w = wk + (int64_t)r * rows_total + roff;
+    double *xr = x + (int64_t)r * P.n;
+    for (int i = lane; i < f; i += 32) sw[i] = (i < p) ? xr[rows[i]] : 0.0;
+    __syncwarp();
+    for (int t = P.child_ptr[s]; t < P.child_ptr[s + 1]; ++t) {
+      const int c = P.child_idx[t];
+      const int pc = X.sn_pstore[c], q = X.sn_f[c] - pc;
+      const int *cmap = X.cbmap + X.sn_roff[c] + pc;
+      const double *wc = wk + (int64_t)r * rows_total + X.sn_roff[c] + pc;
+      for (int i = lane; i < q; i += 32) sw[cmap[i]] += wc[i];
+      __syncwarp();
+    }
+    // rows lane and lane + 32
+    double w0 = (lane < f) ? sw[lane] : 0.0, w1 = (lane + 32 < f) ? sw[lane + 32] : 0.0;
+    for (int j0 = 0; j0 < p; j0 += 8) {
+      double l0[8], l1[8], dj[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int j = j0 + u;
+        const bool in = j < p;
+        l0[u] = (in && lane > j && lane < f) ? __ldg(L + (size_t)j * f + lane) : 0.0;
+        l1[u] = (in && lane + 32 < f) ? __ldg(L + (size_t)j * f + lane + 32) : 0.0;
+        dj[u] = (in && posdef) ? __ldg(L + (size_t)j * f + j) : 1.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int j = j0 + u;
+        if (j >= p) break;
+        // w_j of the row's owner lane
+        double wj = __shfl_sync(0xffffffffu, j < 32 ? w0 : w1, j & 31);
+        if (posdef) wj = wj / dj[u];
+        if (lane == j) w0 = wj;
+        if (lane + 32 == j) w1 = wj;
+        if (l0[u] != 0.0) w0 = fma(-l0[u], wj, w0);
+        if (l1[u] != 0.0 && lane + 32 > j) w1 = fma(-l1[u], wj, w1);
+      }
+    }
+    if (lane < f) w[lane] = w0;
+    if (lane + 32 < f) w[lane + 32] = w1;
+    if (lane < p) xr[rows[lane]] = w0;
+    if (lane + 32 < p) xr[rows[lane + 32]] = w1;
+    __syncwarp();
+  }
+}
+
+// Backward sweep of the level's fronts of at most kSolveSmall rows, a warp
+// per front: D^-1 of every pivot block (2x2 blocks where the upper slot (c,
+// c+1) is nonzero), v -= L21^T x_ext, then L11^-T from the last column on
+// (each column's dot with the solved part a warp reduction).
+__global__ void __launch_bounds__(256, 4) k_bwd_small(DevPlan P, DevFactor X, int lo, int m, int posdef, double *x,
+                                                   int nrhs, int apply_d, int apply_lt) {
+  __shared__ double sv_all[8][kSolveSmall];
+  __shared__ double sx_all[8][kSolveSmall];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int item = blockIdx.x * 8 + wid;
+  if (item >= m) return;
+  const int s = P.lvl_sn[lo + item];
+  const int f = X.sn_f[s];
+  if (f > kSolveSmall || P.sn_large[s]) return;
+  const int p = X.sn_pstore[s];
+  const int *rows = X.rows + X.sn_roff[s];
+  const double *L = X.arena + X.sn_off[s];
+  const size_t sf = (size_t)f;
+  double *sv = sv_all[wid], *sx = sx_all[wid];
+  for (int r = 0; r < nrhs; ++r) {
+    double *xr = x + (int64_t)r * P.n;
+    for (int i = lane; i < f; i += 32) sx[i] = (i >= p) ? xr[rows[i]] : 0.0;
+    for (int c = lane; c < p; c += 32) {
+      const bool second = apply_d && !posdef && c > 0 && L[(size_t)c * sf + c - 1] != 0.0;
+      if (second) continue;
+      double y0 = xr[rows[c]];
+      if (!posdef && apply_d) {
+        const double d00 = L[(size_t)c * sf + c];
+        const double d10 = (c + 1 < p) ? L[(size_t)(c + 1) * sf + c] : 0.0;
+        if (d10 != 0.0) {
+          double z0, z1;
+          dinv2_apply(d00, d10, L[(size_t)(c + 1) * sf + c + 1], y0, xr[rows[c + 1]], z0, z1);
+          sv[c] = z0;
+          sv[c + 1] = z1;
+          continue;
+        }
+        y0 = (d00 == 0.0 || !isfinite(d00)) ? 0.0 : y0 / d00;
+      }
+      sv[c] = y0;
+    }
+    __syncwarp();
+    if (apply_lt) {
+      // v[c] -= L(p:f, c)^T x_ext: a lane per column
+      for (int c = lane; c < p; c += 32) {
+        const double *Lc = L + (size_t)c * sf;
+        double acc = 0.0;
+        for (int i = p; i < f; ++i) acc = fma(Lc[i], sx[i], acc);
+        sv[c] -= acc;
+      }
+      __syncwarp();
+      // L11^-T, last column first: x_j = (v_j - L(j+1:p, j)^T x) / L_jj
+      for (int j = p - 1; j >= 0; --j) {
+        const double *Lj = L + (size_t)j * sf;
+        double acc = 0.0;
+        for (int i = j + 1 + lane; i < p; i += 32) acc = fma(Lj[i], sx[i], acc);
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) {
+          double xj = sv[j] - acc;
+          if (posdef) xj = xj / Lj[j];
+          sx[j] = xj;
+        }
+        __syncwarp();
+      }
+    } else {
+      for (int c = lane; c < p; c += 32) sx[c] = sv[c];
+      __syncwarp();
+    }
+    for (int c = lane; c < p; c += 32) xr[rows[c]] = sx[c];
+    __syncwarp();
+  }
+}
+
 // Forward sweep of one level: gather, children's update vectors in child
 // order, blocked unit (indefinite) or non-unit (SPD) L11 solve, then
-// w[p:f) -= L21 w[0:p) unless the front is large.
+// w[p:f) -= L21 w[0:p) unless the front is large. Fronts of at most
+// kSolveSmall rows are k_fwd_small's.
 __global__ void __launch_bounds__(kSolveNT, 4) k_fwd_front(DevPlan P, DevFactor X, int lo, int posdef,
                                                         double *x, double *wk, int64_t rows_total,
                                                         int nrhs) {
@@ -1671,6 +1856,7 @@ __global__ void __launch_bounds__(kSolveNT, 4) k_fwd_front(DevPlan P, DevFactor 
   const double *L = X.arena + X.sn_off[s];
   const size_t sf = (size_t)f;
   const bool large = P.sn_large[s] != 0;
+  if (!large && f <= kSolveSmall) return;  // k_fwd_small's
   __shared__ double Ls[32][33];
   const int warp = threadIdx.x >> 5;
   // every right-hand side at once: gather, children's update vectors in
@@ -1845,6 +2031,7 @@ __global__ void __launch_bounds__(kSolveNT) k_bwd_front(DevPlan P, DevFactor X, 
   const double *L = X.arena + X.sn_off[s];
   const size_t sf = (size_t)f;
   const bool large = P.sn_large[s] != 0;
+  if (!large && f <= kSolveSmall) return;  // k_bwd_small's
   __shared__ double Ls[32][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // every right-hand side at once. D^-1 of each pivot block; 2x2 blocks
@@ -2002,9 +2189,37 @@ __device__ __forceinline__ double strip_dot32(const double *L, size_t sf, int i,
   return acc;
 }
 
+// The 256-column blocks' strips of L staged in shared memory: strip k (32
+// columns jb.., rows [jb, j1) of the block) at buf[k & 1][u][row - j0],
+// copied with cp.async two strips ahead of their use.
+struct TriSmem {
+  double buf[2][32][kSB];
+  double w[8][kSB];  // the block's values, per right-hand side (at most 8)
+};
+
+__device__ __forceinline__ void tri_strip_async(const double *L, size_t sf, int j0, int j1, int jb, int nb,
+                                                double (*dst)[kSB]) {
+  const int rows = j1 - jb;
+  for (int t = threadIdx.x; t < nb * rows; t += kTriNT) {
+    const int u = t / rows, rr = t % rows;
+    const double *src = L + (size_t)(jb + u) * sf + jb + rr;
+    const unsigned d = (unsigned)__cvta_generic_to_shared(&dst[u][jb - j0 + rr]);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Forward block b of each large front: w[j0:j1) <- L_bb^-1 w[j0:j1), strip
+// by strip (a warp per right-hand side solves the 32 x 32 triangle, then
+// every thread a row of the block below it), the strips' L streaming into
+// shared memory two ahead.
 __global__ void __launch_bounds__(kTriNT) k_fwd_tri(DevPlan P, DevFactor X, const int *__restrict__ large,
                                                     int b, int posdef, double *x, double *wk,
                                                     int64_t rows_total, int nrhs) {
+  extern __shared__ __align__(16) unsigned char tri_smem[];
+  TriSmem &sm = *reinterpret_cast<TriSmem *>(tri_smem);
   const int s = large[blockIdx.x];
   const int f = X.sn_f[s], p = X.sn_pstore[s];
   const int j0 = b * kSB;
@@ -2015,64 +2230,56 @@ __global__ void __launch_bounds__(kTriNT) k_fwd_tri(DevPlan P, DevFactor X, cons
   const double *L = X.arena + X.sn_off[s];
   const size_t sf = (size_t)f;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  __shared__ double Ls[32][33];
-  __shared__ double ws[kSB];
-  for (int r = 0; r < nrhs; ++r) {
-    double *w = wk + (int64_t)r * rows_total + roff;
-    for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) ws[t] = w[j0 + t];
-    for (int jb = j0; jb < j1; jb += 32) {
-      const int nb = min(32, j1 - jb);
-      // every load of the strip first (its triangle, and this thread's row
-      // below it: at most 224 rows, one a thread), so that they are in
-      // flight across the barriers and the triangle solve
-      double tv[1024 / kTriNT];
+  const int nstrip = (j1 - j0 + 31) / 32;
+  tri_strip_async(L, sf, j0, j1, j0, min(32, j1 - j0), sm.buf[0]);
+  if (nstrip > 1) tri_strip_async(L, sf, j0, j1, j0 + 32, min(32, j1 - j0 - 32), sm.buf[1]);
+  for (int r = 0; r < nrhs; ++r)
+    for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) sm.w[r][t] = wk[(int64_t)r * rows_total + roff + j0 + t];
+  for (int k = 0; k < nstrip; ++k) {
+    const int jb = j0 + 32 * k, nb = min(32, j1 - jb);
+    const double(*Lb)[kSB] = sm.buf[k & 1];
+    if (k + 1 < nstrip) cp_async_wait_one();
+    else cp_async_wait_all();
+    __syncthreads();
+    if (warp < nrhs) {
+      // lane = row jb + lane: its row of the triangle in registers, the
+      // SPD diagonal's reciprocal taken ahead, so that a step of the chain
+      // is one shuffle and one fused multiply-add
+      double *w = sm.w[warp];
+      double lrow[32];
 #pragma unroll
-      for (int u = 0; u < 1024 / kTriNT; ++u) {
-        const int t = (int)threadIdx.x + kTriNT * u, r = t & 31, c = t >> 5;
-        tv[u] = (r < nb && c < nb && c <= r) ? __ldg(L + (size_t)(jb + c) * sf + jb + r) : 0.0;
-      }
-      const int i = jb + nb + warp * 32 + lane;
-      double l[32];
-      if (nb == 32 && i < j1) {
+      for (int j = 0; j < 32; ++j) lrow[j] = (j < lane && lane < nb) ? Lb[j][jb - j0 + lane] : 0.0;
+      const double rdiag = (posdef && lane < nb) ? 1.0 / Lb[lane][jb - j0 + lane] : 1.0;
+      double wi = (lane < nb) ? w[jb - j0 + lane] : 0.0;
 #pragma unroll
-        for (int u = 0; u < 32; ++u) l[u] = __ldg(L + (size_t)(jb + u) * sf + i);
-      }
-      __syncthreads();  // the previous strip's readers of Ls and ws are done
-#pragma unroll
-      for (int u = 0; u < 1024 / kTriNT; ++u) {
-        const int t = (int)threadIdx.x + kTriNT * u;
-        Ls[t & 31][t >> 5] = tv[u];
-      }
-      __syncthreads();
-      if (warp == 0) {
-        // the 32 x 32 triangle on the block's values in shared memory
-        double wi = (lane < nb) ? ws[jb - j0 + lane] : 0.0;
-        for (int j = 0; j < nb; ++j) {
-          double wj = __shfl_sync(0xffffffffu, wi, j);
-          if (posdef) wj = wj / Ls[j][j];
-          if (lane == j) wi = wj;
-          if (lane > j && lane < nb) wi = fma(-Ls[lane][j], wj, wi);
+      for (int j = 0; j < 32; ++j) {
+        if (j < nb) {
+          if (lane == j) wi = wi * rdiag;
+          const double wj = __shfl_sync(0xffffffffu, wi, j);
+          if (lrow[j] != 0.0) wi = fma(-lrow[j], wj, wi);
         }
-        if (lane < nb) ws[jb - j0 + lane] = wi;
       }
-      __syncthreads();
-      // the block's rows below this strip: a warp per 32 rows
-      if (i < j1) {
-        double acc = 0.0;
-        if (nb == 32) {
-#pragma unroll
-          for (int u = 0; u < 32; ++u) acc = fma(l[u], ws[jb + u - j0], acc);
-        } else {
-          acc = strip_dot32(L, sf, i, jb, nb, ws, j0);
-        }
-        ws[i - j0] -= acc;
-      }
+      if (lane < nb) w[jb - j0 + lane] = wi;
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) w[j0 + t] = ws[t];
+    const int i = jb + nb + (int)threadIdx.x;
+    if (i < j1) {
+      for (int r = 0; r < nrhs; ++r) {
+        double acc = 0.0;
+        for (int u = 0; u < nb; ++u) acc = fma(Lb[u][i - j0], sm.w[r][jb - j0 + u], acc);
+        sm.w[r][i - j0] -= acc;
+      }
+    }
+    __syncthreads();  // this strip's buffer is free
+    if (k + 2 < nstrip) tri_strip_async(L, sf, j0, j1, jb + 64, min(32, j1 - jb - 64), sm.buf[k & 1]);
+  }
+  for (int r = 0; r < nrhs; ++r) {
+    double *w = wk + (int64_t)r * rows_total + roff;
     double *xr = x + (int64_t)r * P.n;
-    for (int j = j0 + threadIdx.x; j < j1; j += kTriNT) xr[rows[j]] = ws[j - j0];
-    __syncthreads();
+    for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) {
+      w[j0 + t] = sm.w[r][t];
+      xr[rows[j0 + t]] = sm.w[r][t];
+    }
   }
 }
 
@@ -2197,9 +2404,16 @@ __global__ void __launch_bounds__(256) k_bwd_dots(DevPlan P, DevFactor X, const 
   }
 }
 
+// Backward block b of each large front (its rows past the block already
+// taken by k_bwd_dots): strips from the last, each with its dots against
+// the block's solved rows below it (a warp per column) and then the 32 x 32
+// transposed triangle (a warp per right-hand side), the strips' L streaming
+// into shared memory two ahead.
 __global__ void __launch_bounds__(kTriNT) k_bwd_tri(DevPlan P, DevFactor X, const int *__restrict__ large,
                                                     int b, int posdef, double *x, double *wk,
                                                     int64_t rows_total, int nrhs) {
+  extern __shared__ __align__(16) unsigned char tri_smem[];
+  TriSmem &sm = *reinterpret_cast<TriSmem *>(tri_smem);
   const int s = large[blockIdx.x];
   const int f = X.sn_f[s], p = X.sn_pstore[s];
   const int j0 = b * kSB;
@@ -2210,61 +2424,71 @@ __global__ void __launch_bounds__(kTriNT) k_bwd_tri(DevPlan P, DevFactor X, cons
   const double *L = X.arena + X.sn_off[s];
   const size_t sf = (size_t)f;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  __shared__ double Ls[32][33];
-  __shared__ double vs[kSB];
-  for (int r = 0; r < nrhs; ++r) {
-    double *v = wk + (int64_t)r * rows_total + roff;
-    for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) vs[t] = v[j0 + t];
+  const int nstrip = (j1 - j0 + 31) / 32;
+  // strips numbered from the last: strip k covers [jb_k, jb_k + nb_k)
+  auto strip = [&](int k, int &jb, int &nb) {
+    const int idx = nstrip - 1 - k;
+    jb = j0 + 32 * idx;
+    nb = min(32, j1 - jb);
+  };
+  int jb, nb;
+  strip(0, jb, nb);
+  tri_strip_async(L, sf, j0, j1, jb, nb, sm.buf[0]);
+  if (nstrip > 1) {
+    strip(1, jb, nb);
+    tri_strip_async(L, sf, j0, j1, jb, nb, sm.buf[1]);
+  }
+  for (int r = 0; r < nrhs; ++r)
+    for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) sm.w[r][t] = wk[(int64_t)r * rows_total + roff + j0 + t];
+  for (int k = 0; k < nstrip; ++k) {
+    strip(k, jb, nb);
+    const int je = jb + nb;
+    const double(*Lb)[kSB] = sm.buf[k & 1];
+    if (k + 1 < nstrip) cp_async_wait_one();
+    else cp_async_wait_all();
     __syncthreads();
-    for (int je = j1; je > j0; je -= 32) {
-      const int jb = max(j0, je - 32), nb = je - jb;
-      // the strip's triangle loaded first, in flight during the dots
-      double tv[1024 / kTriNT];
-#pragma unroll
-      for (int u = 0; u < 1024 / kTriNT; ++u) {
-        const int t = (int)threadIdx.x + kTriNT * u, r = t & 31, c = t >> 5;
-        tv[u] = (r < nb && c < nb && c <= r) ? __ldg(L + (size_t)(jb + c) * sf + jb + r) : 0.0;
-      }
-      // v[j] -= sum over the block's solved rows [je, j1) of L(i, j) v[i]:
-      // a warp per column, its lanes' rows (at most 7 a lane) loaded at once
-      for (int j = jb + warp; j < je; j += kTriNT / 32) {
-        const double *Lj = L + (size_t)j * sf;
-        double l[7], y[7];
-#pragma unroll
-        for (int u = 0; u < 7; ++u) {
-          const int i = je + lane + 32 * u;
-          l[u] = (i < j1) ? Lj[i] : 0.0;
-          y[u] = (i < j1) ? vs[i - j0] : 0.0;
-        }
+    // v[j] -= sum over the block's solved rows [je, j1) of L(i, j) v[i]
+    for (int u = warp; u < nb; u += kTriNT / 32) {
+      for (int r = 0; r < nrhs; ++r) {
         double acc = 0.0;
-#pragma unroll
-        for (int u = 0; u < 7; ++u) acc = fma(l[u], y[u], acc);
+        for (int i = je + lane; i < j1; i += 32) acc = fma(Lb[u][i - j0], sm.w[r][i - j0], acc);
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) vs[j - j0] -= acc;
+        if (lane == 0) sm.w[r][jb - j0 + u] -= acc;
       }
-      // (the previous strip's solve, the last reader of Ls, ended at a barrier)
-#pragma unroll
-      for (int u = 0; u < 1024 / kTriNT; ++u) {
-        const int t = (int)threadIdx.x + kTriNT * u;
-        Ls[t & 31][t >> 5] = tv[u];
-      }
-      __syncthreads();
-      if (warp == 0) {
-        double vi = (lane < nb) ? vs[jb - j0 + lane] : 0.0;
-        for (int j = nb - 1; j >= 0; --j) {
-          double xj = __shfl_sync(0xffffffffu, vi, j);
-          if (posdef) xj = xj / Ls[j][j];
-          if (lane == j) vi = xj;
-          if (lane < j) vi = fma(-Ls[j][lane], xj, vi);
-        }
-        if (lane < nb) vs[jb - j0 + lane] = vi;
-      }
-      __syncthreads();
     }
-    for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) v[j0 + t] = vs[t];
-    double *xr = x + (int64_t)r * P.n;
-    for (int j = j0 + threadIdx.x; j < j1; j += kTriNT) xr[rows[j]] = vs[j - j0];
     __syncthreads();
+    if (warp < nrhs) {
+      // lane = column jb + lane: its column of the triangle in registers
+      double *w = sm.w[warp];
+      double lcol[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) lcol[j] = (j > lane && j < nb) ? Lb[lane][jb - j0 + j] : 0.0;
+      const double rdiag = (posdef && lane < nb) ? 1.0 / Lb[lane][jb - j0 + lane] : 1.0;
+      double vi = (lane < nb) ? w[jb - j0 + lane] : 0.0;
+#pragma unroll
+      for (int j = 31; j >= 0; --j) {
+        if (j < nb) {
+          if (lane == j) vi = vi * rdiag;
+          const double xj = __shfl_sync(0xffffffffu, vi, j);
+          if (lcol[j] != 0.0) vi = fma(-lcol[j], xj, vi);
+        }
+      }
+      if (lane < nb) w[jb - j0 + lane] = vi;
+    }
+    __syncthreads();  // this strip's buffer is free
+    if (k + 2 < nstrip) {
+      int jb2, nb2;
+      strip(k + 2, jb2, nb2);
+      tri_strip_async(L, sf, j0, j1, jb2, nb2, sm.buf[k & 1]);
+    }
+  }
+  for (int r = 0; r < nrhs; ++r) {
+    double *w = wk + (int64_t)r * rows_total + roff;
+    double *xr = x + (int64_t)r * P.n;
+    for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) {
+      w[j0 + t] = sm.w[r][t];
+      xr[rows[j0 + t]] = sm.w[r][t];
+    }
   }
 }
 
