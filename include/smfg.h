@@ -51,7 +51,8 @@ extern "C" {
 #define SMFG_FACTOR_SUCCESS 0
 #define SMFG_FACTOR_NOT_POSDEF 1
 #define SMFG_FACTOR_SINGULAR 2
-#define SMFG_FACTOR_INERTIA_EXCEEDED 4
+#define SMFG_FACTOR_MAX_PIVOT_DELAYS 3  /* stopped at the work limit (smfg_control_t.work_limit) */
+#define SMFG_FACTOR_INERTIA_EXCEEDED 4  /* stopped once the negative pivots passed max_negative_pivots */
 
 /* Solve jobs (smf::SolveJob / SMF_SOLVE_*). */
 #define SMFG_SOLVE_FULL 0
@@ -105,7 +106,11 @@ typedef struct {
   int nb;                 /* panel width (Control::indef_panel_size, 16) */
   int blocked_min_front;  /* blocked kernel from this many rows (96) */
   int precision;          /* SMFG_PREC_* */
-  int max_negative_pivots;/* < 0: off (Control::max_negative_pivots) */
+  int max_negative_pivots;/* < 0: off (Control::max_negative_pivots). Indefinite: the
+                             factorization stops after the tree level at which the negative
+                             pivots so far pass it (the rest skipped, SMFG_ERR_WRONG_INERTIA,
+                             SMFG_FACTOR_INERTIA_EXCEEDED, partial counts; the factor is
+                             unusable), multifrontal_serial.cpp:1619-1628 */
   const double *scale;    /* optional S (length n, original numbering), NULL = none */
   int profile;            /* 1: time the large-front update kernels (info.reserved_d[0..1]) */
   /* SMFG_PREC_MIXED: large fronts of at least mixed_min_front rows (0: 384)
@@ -134,7 +139,13 @@ typedef struct {
    * (graph = 1 then factors without capture). */
   int aptp_min_rows;
   int reserved_i[1];
-  double reserved_d[8];
+  /* Indefinite: >= 0 stops the factorization after the tree level at which
+   * the front work so far (sum over fronts of fully summed columns x
+   * rows^2) passes floor(work_limit) -- the scale-on-delay rescue's limit
+   * (multifrontal_serial.cpp:660-671): status SMFG_OK, factor_status
+   * SMFG_FACTOR_MAX_PIVOT_DELAYS, no usable factor. < 0: off. */
+  double work_limit;
+  double reserved_d[7];
 } smfg_control_t;
 
 typedef struct {

@@ -672,6 +672,11 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
   const int sms = sm_count(pl.device);
   SMFG_CUDA(cudaMemsetAsync(x.counters, 0, sizeof(unsigned long long) * kCCount, st));
   SMFG_CUDA(cudaMemsetAsync(x.sn_dout, 0, sizeof(int) * pl.nsn, st));
+  // per-front counts start at zero: a stopped factorization's totals are
+  // those of the fronts it factored
+  SMFG_CUDA(cudaMemsetAsync(x.sn_stat, 0, sizeof(int) * 4 * pl.nsn, st));
+  SMFG_CUDA(cudaMemsetAsync(x.sn_flops, 0, sizeof(double) * pl.nsn, st));
+  SMFG_CUDA(cudaMemsetAsync(x.sn_pstore, 0, sizeof(int) * pl.nsn, st));
   const double *scale = nullptr;
   if (c.scale) {
     // a graph reads the scale the host put in x.scale before the replay
@@ -686,6 +691,12 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
   k_eff_small<<<1, 1, 0, st>>>(x.counters, c.small_pivot);
   lc.n += 2;
   const bool aptp_on = aptp_active(c);
+  // early stops (indefinite): max_negative_pivots, the work limit
+  const long long neg_limit = c.posdef ? -1 : (long long)c.max_negative_pivots;
+  const long long work_cap =
+      (c.posdef || !(c.work_limit >= 0.0)) ? -1
+      : (c.work_limit >= 9.0e18 ? (long long)9e18 : (long long)std::floor(c.work_limit));
+  const bool limits = neg_limit >= 0 || work_cap >= 0;
   PivotParams prm{c.u, c.small_pivot, c.small_pivot, c.nb, c.blocked_min_front, c.posdef,
                   aptp_on ? c.aptp_min_rows : 0};
   const MixedCfg mc = mixed_cfg(c);
@@ -836,6 +847,10 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
       k_large_finish<512><<<nL, 512, 0, st>>>(d, x, lg, fin, prm);
       k_large_store<<<ggrid, 256, 0, st>>>(d, x, lg, nL, c.posdef);
       lc.n += 4;
+    }
+    if (limits) {
+      k_level_limits<<<1, 256, 0, st>>>(d, x, lo, hi, neg_limit, work_cap);
+      lc.n += 1;
     }
   }
   SMFG_CUDA(cudaGetLastError());
@@ -1069,6 +1084,14 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
   inf.reserved_i[5] = pl.aptp_fronts;
   if (flags & (kFArena | kFRows | kFTcCap | kFAptpMiss)) rc = SMFG_ERR_ARENA;
   else if (flags & kFTcWait) rc = SMFG_ERR_TIMEOUT;
+  else if (flags & kFInertia) {
+    // stopped early: the negative pivots passed max_negative_pivots
+    rc = SMFG_ERR_WRONG_INERTIA;
+    pl.factor_status = SMFG_FACTOR_INERTIA_EXCEEDED;
+  } else if (flags & kFWork) {
+    // stopped at the work limit (the scale-on-delay rescue's trigger)
+    pl.factor_status = SMFG_FACTOR_MAX_PIVOT_DELAYS;
+  }
   else if (flags & kFNonfinite) rc = SMFG_ERR_NONFINITE;
   else if (flags & (kFMap | kFInternal)) rc = SMFG_ERR_INTERNAL;
   else if (flags & kFNotPosdef) {
@@ -1091,7 +1114,8 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
   inf.status = rc;
   inf.factor_status = pl.factor_status;
   pl.posdef = c.posdef;
-  pl.factored = (rc == SMFG_OK || rc == SMFG_ERR_SINGULAR) && pl.factor_status != SMFG_FACTOR_NOT_POSDEF;
+  pl.factored = (rc == SMFG_OK || rc == SMFG_ERR_SINGULAR) && pl.factor_status != SMFG_FACTOR_NOT_POSDEF &&
+                pl.factor_status != SMFG_FACTOR_MAX_PIVOT_DELAYS;
   pl.info = inf;
   if (info) *info = inf;
   return rc;
@@ -1228,6 +1252,7 @@ SMFG_API void smfg_default_control(smfg_control_t *c) {
   c->max_negative_pivots = -1;
   c->scale = nullptr;
   c->aptp_min_rows = aptp::kMinRows;  // deterministic mode
+  c->work_limit = -1.0;               // no work limit
 }
 
 SMFG_API const char *smfg_last_error(void) { return g_last_error.c_str(); }

@@ -11,16 +11,16 @@ namespace smfg {
 // counters[] slots
 enum : int { kCArena = 0, kCRows = 1, kCFlags = 2, kCMaxAbs = 3, kCAux = 4, kCEffSmall = 5,
              kCActive = 6, kCGemmFlops = 7, kCTcFlops = 8, kCDeferBytes = 9, kCDeferUpd = 10,
-             kCDeferSmall = 11, kCAptpMiss = 12, kCCount = 13 };
+             kCDeferSmall = 11, kCAptpMiss = 12, kCNegSoFar = 13, kCWorkSoFar = 14, kCCount = 15 };
 // error flag bits (counters[kCFlags])
 enum : unsigned { kFArena = 1u, kFRows = 2u, kFNonfinite = 4u, kFNotPosdef = 8u, kFNonfiniteD = 16u,
                   kFMap = 32u, kFInternal = 64u, kFTcWait = 128u, kFTcCap = 256u, kFSteps = 512u,
-                  kFAptpMiss = 1024u };
+                  kFAptpMiss = 1024u, kFInertia = 2048u, kFWork = 4096u };
 // team reduction scratch per large front (2 buffers x 16 CTAs x 6 doubles)
 constexpr int kTeamRedDoubles = 256;
 // flags after which the rest of a factorization is skipped (retried with
 // more room, or reported)
-constexpr unsigned kFAbort = kFArena | kFRows | kFTcWait | kFTcCap | kFAptpMiss;
+constexpr unsigned kFAbort = kFArena | kFRows | kFTcWait | kFTcCap | kFAptpMiss | kFInertia | kFWork;
 // fronts recorded per factorization that grew past the APTP size outside the
 // large-front path (they join it, and the factorization is redone)
 constexpr int kAptpMissCap = 1024;
@@ -538,6 +538,45 @@ __global__ void k_large_init(DevPlan P, DevFactor X, const int *__restrict__ lar
     tpp_init(S, X.sn_ne[s], posdef != 0, mixed, nbo);
     S.pad[0] = 0;  // deferred update pending
     X.tpp[blockIdx.x] = S;
+  }
+}
+
+// The early stops of an indefinite factorization, after each level
+// (multifrontal_serial.cpp:1619-1628, :660-671): the negative pivots and the
+// front work (fully summed columns x rows^2, exact integers) of the fronts
+// factored so far; past max_negative_pivots (neg_limit >= 0) or past the
+// work cap (work_cap >= 0) the rest of the factorization is skipped. Both
+// counts only grow, so a run that stops is exactly one whose finished count
+// would have passed the limit.
+__global__ void k_level_limits(DevPlan P, DevFactor X, int lo, int hi, long long neg_limit, long long work_cap) {
+  __shared__ long long red[2][32];
+  if (X.counters[kCFlags] & kFAbort) return;
+  long long neg = 0, work = 0;
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const int s = P.lvl_sn[i];
+    const long long f = X.sn_f[s];
+    neg += X.sn_stat[4 * s + 1];
+    work += (long long)X.sn_ne[s] * f * f;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    neg += __shfl_xor_sync(0xffffffffu, neg, o);
+    work += __shfl_xor_sync(0xffffffffu, work, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = neg;
+    red[1][threadIdx.x >> 5] = work;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    neg = work = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      neg += red[0][w];
+      work += red[1][w];
+    }
+    const long long tn = (long long)atomicAdd(X.counters + kCNegSoFar, (unsigned long long)neg) + neg;
+    const long long tw = (long long)atomicAdd(X.counters + kCWorkSoFar, (unsigned long long)work) + work;
+    if (neg_limit >= 0 && tn > neg_limit) set_flag(X.counters, kFInertia);
+    if (work_cap >= 0 && tw > work_cap) set_flag(X.counters, kFWork);
   }
 }
 

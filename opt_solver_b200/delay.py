@@ -15,16 +15,22 @@ The scale-on-delay rescue (Control::scale_on_delay_ratio, default 16,
 solver/src/solve.cpp:289-560): an indefinite factorization whose front work
 passes floor(ratio x delay-free work) is given up (MaxPivotDelays) and redone
 with the maximum-product matching scaling of its own values; without such
-a scaling (structurally singular values) the first factorization stands.
-This engine factors level by level and has no early stop, so, as the
-reference's task-parallel engine does (factor_indef.cpp:834-851), the limit
-is checked on the finished factor: the decision is the same, the work of
-the first try is not saved. The reference's refinements of that policy (a
-kept scale reused across refactors, the tighter next limit, the early stop
-on projected inflation, the static-pivoting fallback) are not restated.
+a scaling (structurally singular values) the factorization runs as Auto
+resolves it, to the end (solve.cpp:304-306).
+The engine stops a try on the device (smfg_control_t.work_limit): after each
+tree level it adds the level's front work to the count so far and skips the
+rest once the count passes the limit (the reference stops after the front,
+multifrontal_serial.cpp:660-671; the count only grows, so both stop exactly
+when the finished count would pass). A back end without that stop is
+checked on its finished factor, as the reference's task-parallel engine
+does (factor_indef.cpp:834-851): the same decision, no work saved. The
+reference's refinements of that policy (a kept scale reused across
+refactors, the tighter next limit, the early stop on projected inflation,
+the static-pivoting fallback) are not restated.
 """
 from __future__ import annotations
 
+import inspect
 import math
 
 import numpy as np
@@ -95,26 +101,46 @@ def rescue_scale(a, values):
     return s
 
 
+def _has_early_stop(solver) -> bool:
+    try:
+        return "work_limit" in inspect.signature(solver.factor).parameters
+    except (TypeError, ValueError):
+        return False
+
+
 def factor_scale_on_delay(solver, a, values, ratio: float = SCALE_ON_DELAY_RATIO, scale=None,
-                          rescue=rescue_scale, **factor_kw):
+                          rescue=rescue_scale, early_stop=None, **factor_kw):
     """Indefinite factor with the scale-on-delay rescue. ``solver`` has
     ``factor(values, posdef=False, scale=..., **kw)`` and ``front_stats()``
     (smfg.Solver); ``scale`` is the first try's scaling, as the caller's
-    Auto resolved it. Returns (info of the kept factor, outcome) where
-    outcome holds the delay-free work, the limit, each try's front work and
-    whether the rescue ran."""
+    Auto resolved it. ``early_stop`` (default: when solver.factor takes
+    ``work_limit``) stops the first try on the device at the limit. Returns
+    (info of the kept factor, outcome) where outcome holds the delay-free
+    work, the limit, each try's front work (None for a try stopped early),
+    whether the limit tripped, whether the try stopped early and whether the
+    rescue ran."""
     free = delay_free_front_work(a)
     limit = math.floor(ratio * free) if ratio >= 0 else -1
-    info = solver.factor(values, posdef=False, scale=scale, **factor_kw)
-    work = engine_front_work(solver, a)
-    out = {"free_work": free, "limit": limit, "first_work": work, "tripped": False,
-           "rescued": False, "work": work, "scale": scale}
-    if limit < 0 or work <= limit:
+    if early_stop is None:
+        early_stop = _has_early_stop(solver)
+    stop = early_stop and limit >= 0
+    kw = dict(factor_kw, work_limit=float(limit)) if stop else factor_kw
+    info = solver.factor(values, posdef=False, scale=scale, **kw)
+    stopped = stop and getattr(info, "factor_status", 0) == FACTOR_MAX_PIVOT_DELAYS
+    work = None if stopped else engine_front_work(solver, a)
+    out = {"free_work": free, "limit": limit, "first_work": work, "tripped": stopped,
+           "stopped_early": stopped, "rescued": False, "work": work, "scale": scale}
+    if not stopped and (limit < 0 or work <= limit):
         return info, out
     out["tripped"] = True
     out["first_status"] = FACTOR_MAX_PIVOT_DELAYS  # the try given up, as smf reports it
     s = rescue(a, values)
-    if s is None:  # no matching scaling: the first factorization stands
+    if s is None:
+        # no matching scaling: the factorization as Auto resolves it stands,
+        # run to the end when the try stopped early
+        if stopped:
+            info = solver.factor(values, posdef=False, scale=scale, **factor_kw)
+            out["work"] = engine_front_work(solver, a)
         return info, out
     info = solver.factor(values, posdef=False, scale=s, **factor_kw)
     out.update(rescued=True, work=engine_front_work(solver, a), scale=s)

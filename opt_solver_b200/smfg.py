@@ -20,6 +20,10 @@ from . import build as _build
 
 SMFG_OK = 0
 SMFG_ERR_SINGULAR = 2
+SMFG_ERR_WRONG_INERTIA = 4
+# smfg_info_t.factor_status
+SMFG_FACTOR_SUCCESS, SMFG_FACTOR_NOT_POSDEF, SMFG_FACTOR_SINGULAR = 0, 1, 2
+SMFG_FACTOR_MAX_PIVOT_DELAYS, SMFG_FACTOR_INERTIA_EXCEEDED = 3, 4
 SOLVE_FULL, SOLVE_FORWARD, SOLVE_DIAGONAL, SOLVE_BACKWARD = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 # indefinite fronts of at least this many rows take the APTP kernel (smf's
@@ -62,7 +66,7 @@ class Control(C.Structure):
                 ("scale", C.c_void_p), ("profile", C.c_int), ("mixed_block", C.c_int),
                 ("mixed_kind", C.c_int), ("mixed_min_front", C.c_int), ("panel_team", C.c_int),
                 ("graph", C.c_int), ("aptp_min_rows", C.c_int), ("reserved_i", C.c_int * 1),
-                ("reserved_d", C.c_double * 8)]
+                ("work_limit", C.c_double), ("reserved_d", C.c_double * 7)]
 
 
 class Info(C.Structure):
@@ -445,7 +449,7 @@ class Solver:
                scale=None, precision: int = PREC_FP64, max_negative_pivots: int = -1,
                raise_on_singular: bool = False, mixed_block: int = 0, mixed_kind: int = 0,
                mixed_min_front: int = 0, panel_team: int = 0, graph: bool = False,
-               aptp_min_rows: int = APTP_MIN_ROWS) -> Info:
+               aptp_min_rows: int = APTP_MIN_ROWS, work_limit: float = -1.0) -> Info:
         """Factor new values (the caller's entry order). ``values`` is a
         numpy array, or any object with ``data_ptr()`` (a CUDA tensor) for
         values already in device memory. precision=PREC_MIXED: tensor-core
@@ -454,9 +458,15 @@ class Solver:
         more; 0 = the library's defaults). aptp_min_rows: indefinite fronts of
         at least this many rows take the APTP kernel (smf's deterministic
         mode, the default 512); 0 = the threshold kernel everywhere (smf's
-        one-thread default mode)."""
+        one-thread default mode). max_negative_pivots >= 0 on an indefinite
+        matrix: the factorization stops after the tree level where the
+        negative pivots pass it (factor_status SMFG_FACTOR_INERTIA_EXCEEDED,
+        partial counts, returned rather than raised). work_limit >= 0: it
+        stops once the realized work (sum over factored fronts of pivots x
+        rows^2) passes it (factor_status SMFG_FACTOR_MAX_PIVOT_DELAYS)."""
         c = default_control(posdef, u, small, precision, max_negative_pivots)
         c.aptp_min_rows = int(aptp_min_rows)
+        c.work_limit = float(work_limit)
         c.mixed_block = mixed_block
         c.mixed_kind = mixed_kind
         c.mixed_min_front = mixed_min_front
@@ -478,6 +488,8 @@ class Solver:
             rc = lib().smfg_factor(self._h, v.ctypes.data, C.byref(c), C.byref(info))
         self.posdef = posdef
         self.info = info
+        if rc == SMFG_ERR_WRONG_INERTIA and max_negative_pivots >= 0:
+            return info
         if rc not in (SMFG_OK, SMFG_ERR_SINGULAR) or (rc == SMFG_ERR_SINGULAR and raise_on_singular):
             raise SmfgError(rc, "smfg_factor")
         return info

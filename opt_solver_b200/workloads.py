@@ -89,6 +89,42 @@ def kkt_ipm(m: int, n_con: int, seed: int = 0, delta: float = 1e-8,
     return (n,) + _csc_from_coo(n, np.concatenate(rows), np.concatenate(cols), np.concatenate(vals))
 
 
+def kkt_ipm_stream(m: int, n_con: int, steps: int = 8, seed: int = 0, wrong=(3, 6),
+                   n_neg: int = 12, shift: float = 60.0, reg: float = 100.0):
+    """An interior-point method's value stream on one kkt_ipm pattern: step 0
+    the base values; every later step a barrier update (each Sigma entry
+    times 10^U(-0.5, 0.5)); at the steps in ``wrong`` the Hessian block made
+    indefinite (``n_neg`` diagonal entries set to -``shift``: more
+    negative pivots than the n_con constraints give), and the step after each
+    the method's inertia correction (the same values plus ``reg`` on the
+    Hessian diagonal). Returns (n, col_ptr, row_idx, [values per step],
+    [kind per step]) with kind "base", "barrier", "wrong" or "corrected"."""
+    n, cp, ri, v0 = kkt_ipm(m, n_con, seed=seed)
+    nh = m ** 3
+    rng = np.random.default_rng(seed + 1000)
+    hdiag = cp[:nh].astype(np.int64)       # rows sorted: a column's diagonal comes first
+    sigma = v0[hdiag] - 6.0
+    neg_rows = rng.choice(nh, size=min(n_neg, nh), replace=False)
+    vals, kinds = [v0.copy()], ["base"]
+    prev = v0
+    for k in range(1, steps):
+        if kinds[-1] == "wrong":
+            v = prev.copy()
+            v[hdiag] += reg
+            kinds.append("corrected")
+        else:
+            v = v0.copy()
+            v[hdiag] = 6.0 + sigma * 10.0 ** rng.uniform(-0.5, 0.5, size=nh)
+            if k in wrong:
+                v[hdiag[neg_rows]] = -shift
+                kinds.append("wrong")
+            else:
+                kinds.append("barrier")
+        vals.append(v)
+        prev = v
+    return n, cp, ri, vals, kinds
+
+
 def trajectory_kkt(T: int, rng: np.random.Generator, nx: int = 12, nu: int = 4, eq_reg: float = 1e-9):
     """One trajectory-optimisation KKT system (configuration 4): stages
     [x_k, u_k, lambda_{k+1}] for k < T, then x_T; stage Hessians Q = G G^T +

@@ -134,6 +134,13 @@ class Reference:
             lib.refshim_aptp_failed.restype = C.c_int64
             lib.refshim_matching_scale.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p]
             lib.refshim_matching_scale.restype = C.c_int
+            lib.refshim_ipm_create.restype = C.c_void_p
+            lib.refshim_ipm_free.argtypes = [C.c_void_p]
+            lib.refshim_ipm_analyse.argtypes = [C.c_void_p, C.c_int, _i32p, _i32p, _f64p, C.c_int]
+            lib.refshim_ipm_analyse.restype = C.c_int
+            lib.refshim_ipm_factor.argtypes = [C.c_void_p, _f64p, C.c_int64, C.c_int, _i64p]
+            lib.refshim_ipm_solve.argtypes = [C.c_void_p, _f64p, C.c_int, _i64p]
+            lib.refshim_ipm_solve.restype = C.c_int
             cls._lib = lib
         return cls._lib
 
@@ -248,6 +255,46 @@ class Reference:
         it = np.zeros(2, dtype=np.int32)
         self.L.refshim_refine(self.h, b.reshape(-1), x.reshape(-1), nrhs, res, it)
         return x, float(res[0]), float(res[1]), int(it[0])
+
+
+class ReferenceIpmSession:
+    """The reference's smf::IpmSession (solver/src/ipm_session.cpp) in its
+    default Control (AutoSerial ordering, Auto scaling), deterministic mode,
+    one thread, indefinite: analyse once, then factor / solve a stream of
+    values. factor() returns (IpmFactorStatus 0 Ok / 1 WrongInertia /
+    2 Singular / 3 Error, inertia, delayed pivots); solve() returns (x, rc,
+    inertia afterwards, learned expectation or None)."""
+
+    def __init__(self):
+        self.L = Reference.lib()
+        self.h = self.L.refshim_ipm_create()
+        self.n = 0
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.refshim_ipm_free(self.h)
+            self.h = None
+
+    def analyse(self, n, col_ptr, row_idx, values, abort_on_wrong_inertia: bool = True) -> int:
+        self.n = int(n)
+        self.nnz = int(col_ptr[-1])
+        return self.L.refshim_ipm_analyse(self.h, self.n, np.ascontiguousarray(col_ptr, dtype=np.int32),
+                                          np.ascontiguousarray(row_idx, dtype=np.int32),
+                                          np.ascontiguousarray(values, dtype=np.float64),
+                                          int(abort_on_wrong_inertia))
+
+    def factor(self, values, expected_negatives=None):
+        out = np.zeros(5, dtype=np.int64)
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        self.L.refshim_ipm_factor(self.h, v, v.size, -1 if expected_negatives is None else int(expected_negatives),
+                                  out)
+        return int(out[0]), (int(out[1]), int(out[2]), int(out[3])), int(out[4])
+
+    def solve(self, b):
+        x = np.array(b, dtype=np.float64, copy=True)
+        out = np.zeros(4, dtype=np.int64)
+        rc = self.L.refshim_ipm_solve(self.h, x, self.n, out)
+        return x, rc, (int(out[0]), int(out[1]), int(out[2])), (None if out[3] < 0 else int(out[3]))
 
 
 # --------------------------------------------------------------------------

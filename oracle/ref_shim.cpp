@@ -16,6 +16,7 @@
 #include "smf/factor_indef.hpp"
 #include "smf/factor_posdef.hpp"
 #include "smf/info.hpp"
+#include "smf/ipm_session.hpp"
 #include "smf/ldlt_aptp.hpp"
 #include "parallel/tile_tasks.hpp"
 #include "smf/refinement.hpp"
@@ -224,6 +225,59 @@ void refshim_aptp_front(double *F, int f, int ne, int *rows, double u, double sm
   out[2] = r.inertia.positive;
   out[3] = r.inertia.negative;
   out[4] = r.inertia.zero;
+}
+
+// The reference's IpmSession (ipm_session.hpp:120-273), Feature 1 (inertia
+// learning and the early abort on wrong inertia), for comparing the
+// engine's session decisions step by step. Deterministic mode, one thread,
+// AutoParallel ordering, automatic scaling, indefinite.
+void *refshim_ipm_create(void) { return new smf::IpmSession(); }
+void refshim_ipm_free(void *h) { delete static_cast<smf::IpmSession *>(h); }
+
+int refshim_ipm_analyse(void *hp, int n, const int *col_ptr, const int *row_idx, const double *values,
+                        int abort_on_wrong_inertia) {
+  auto *s = static_cast<smf::IpmSession *>(hp);
+  smf::CscLower A;
+  A.n = n;
+  A.col_ptr.assign(col_ptr, col_ptr + n + 1);
+  A.row_idx.assign(row_idx, row_idx + col_ptr[n]);
+  smf::Control ctrl{};
+  ctrl.deterministic = true;
+  ctrl.num_threads = 1;
+  ctrl.matrix_type = smf::MatrixType::RealSymmetricIndefinite;
+  smf::IpmControl ipm{};
+  ipm.abort_on_wrong_inertia = abort_on_wrong_inertia != 0;
+  const std::size_t nnz = static_cast<std::size_t>(col_ptr[n]);
+  return static_cast<int>(s->analyse(A, std::span<const double>(values, nnz), ctrl, ipm));
+}
+
+// out[0..4]: IpmFactorStatus (0 Ok, 1 WrongInertia, 2 Singular, 3 Error),
+// positive, negative, zero pivots, delayed pivots. expected < 0: none given.
+void refshim_ipm_factor(void *hp, const double *values, int64_t nnz, int expected, int64_t *out) {
+  auto *s = static_cast<smf::IpmSession *>(hp);
+  std::optional<int> e;
+  if (expected >= 0) e = expected;
+  const smf::IpmFactorStatus st = s->factor(std::span<const double>(values, static_cast<std::size_t>(nnz)), e);
+  const smf::InertiaCounts in = s->inertia();
+  out[0] = static_cast<int64_t>(st);
+  out[1] = in.positive;
+  out[2] = in.negative;
+  out[3] = in.zero;
+  out[4] = s->info().delayed_pivots;
+}
+
+// Solve in place (one right-hand side); out[0..2]: the inertia afterwards
+// (an aborted factor is completed first), out[3]: the learned expectation
+// (-1: none).
+int refshim_ipm_solve(void *hp, double *b, int n, int64_t *out) {
+  auto *s = static_cast<smf::IpmSession *>(hp);
+  const int rc = s->solve(b, n, 1);
+  const smf::InertiaCounts in = s->inertia();
+  out[0] = in.positive;
+  out[1] = in.negative;
+  out[2] = in.zero;
+  out[3] = s->expected_negatives() ? *s->expected_negatives() : -1;
+  return rc;
 }
 
 // Info::aptp_failed_columns of the last factorization: the columns the APTP
