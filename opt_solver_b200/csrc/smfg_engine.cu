@@ -1155,6 +1155,24 @@ static void enqueue_solve(Plan &pl, double *d_b, int nrhs, int ldb, int job, boo
     enqueue_solve_chunk(pl, d_b + (size_t)r0 * ldb, std::min(kSolveRhs, nrhs - r0), ldb, job, scaled, lc);
 }
 
+// A launch with programmatic stream serialization: the kernel may start
+// while the one before it on the stream still runs, and waits for it in
+// pdl_wait() (the solve kernels).
+template <typename... KArgs, typename... Args>
+static void launch_pdl(void (*kern)(KArgs...), int grid, int block, size_t smem, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  SMFG_CUDA(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
+}
+
 static void enqueue_solve_chunk(Plan &pl, double *d_b, int nrhs, int ldb, int job, bool scaled, LaunchCount &lc) {
   DevPlan &d = pl.d;
   DevFactor &x = pl.x;
@@ -1180,16 +1198,16 @@ static void enqueue_solve_chunk(Plan &pl, double *d_b, int nrhs, int ldb, int jo
   if (fwd) {
     for (int l = 0; l < pl.nlevels; ++l) {
       const int lo = pl.lvl_ptr[l], m = pl.lvl_ptr[l + 1] - lo;
-      k_fwd_small<<<(m + 7) / 8, 256, 0, st>>>(d, x, lo, m, pl.posdef, xv, wk, rows_total, nrhs);
-      k_fwd_front<<<m, kSolveNT, 0, st>>>(d, x, lo, pl.posdef, xv, wk, rows_total, nrhs);
+      launch_pdl(k_fwd_small, (m + 7) / 8, 256, 0, st, d, x, lo, m, pl.posdef, xv, wk, rows_total, nrhs);
+      launch_pdl(k_fwd_front, m, kSolveNT, 0, st, d, x, lo, pl.posdef, xv, wk, rows_total, nrhs);
       lc.n += 2;
       const int nL = pl.lvl_large_ptr[l + 1] - pl.lvl_large_ptr[l];
       if (nL > 0) {
         const int *lg = d.lvl_large + pl.lvl_large_ptr[l];
         const int nb = (large_pmax(pl, l) + kSB - 1) / kSB;
         for (int b = 0; b < nb; ++b) {
-          k_fwd_tri<<<nL, kTriNT, sizeof(TriSmem), st>>>(d, x, lg, b, pl.posdef, xv, wk, rows_total, nrhs);
-          k_fwd_gemv<<<lgrid, 256, 0, st>>>(d, x, lg, nL, b, wk, rows_total, nrhs);
+          launch_pdl(k_fwd_tri, nL, kTriNT, sizeof(TriSmem), st, d, x, lg, b, pl.posdef, xv, wk, rows_total, nrhs);
+          launch_pdl(k_fwd_gemv, lgrid, 256, 0, st, d, x, lg, nL, b, wk, rows_total, nrhs);
         }
         lc.n += 2 * nb;
       }
@@ -1200,25 +1218,25 @@ static void enqueue_solve_chunk(Plan &pl, double *d_b, int nrhs, int ldb, int jo
       const int lo = pl.lvl_ptr[l], m = pl.lvl_ptr[l + 1] - lo;
       const int nL = pl.lvl_large_ptr[l + 1] - pl.lvl_large_ptr[l];
       if (nL > 0 && use_lt) {
-        k_bwd_l21<<<lgrid, 256, 0, st>>>(d, x, d.lvl_large + pl.lvl_large_ptr[l], nL, xv, wk, rows_total, nrhs);
+        launch_pdl(k_bwd_l21, lgrid, 256, 0, st, d, x, d.lvl_large + pl.lvl_large_ptr[l], nL, xv, wk, rows_total, nrhs);
         lc.n++;
       }
-      k_bwd_small<<<(m + 7) / 8, 256, 0, st>>>(d, x, lo, m, pl.posdef, xv, nrhs, use_d ? 1 : 0, use_lt ? 1 : 0);
-      k_bwd_front<<<m, kSolveNT, 0, st>>>(d, x, lo, pl.posdef, xv, wk, rows_total, nrhs,
-                                          use_d ? 1 : 0, use_lt ? 1 : 0);
+      launch_pdl(k_bwd_small, (m + 7) / 8, 256, 0, st, d, x, lo, m, pl.posdef, xv, nrhs, use_d ? 1 : 0, use_lt ? 1 : 0);
+      launch_pdl(k_bwd_front, m, kSolveNT, 0, st, d, x, lo, pl.posdef, xv, wk, rows_total, nrhs, use_d ? 1 : 0,
+                 use_lt ? 1 : 0);
       lc.n += 2;
       if (nL > 0 && use_lt) {
         const int *lg = d.lvl_large + pl.lvl_large_ptr[l];
         const int nb = (large_pmax(pl, l) + kSB - 1) / kSB;
         for (int b = nb - 1; b >= 0; --b) {
-          k_bwd_dots<<<lgrid, 256, 0, st>>>(d, x, lg, nL, b, wk, rows_total, nrhs);
-          k_bwd_tri<<<nL, kTriNT, sizeof(TriSmem), st>>>(d, x, lg, b, pl.posdef, xv, wk, rows_total, nrhs);
+          launch_pdl(k_bwd_dots, lgrid, 256, 0, st, d, x, lg, nL, b, wk, rows_total, nrhs);
+          launch_pdl(k_bwd_tri, nL, kTriNT, sizeof(TriSmem), st, d, x, lg, b, pl.posdef, xv, wk, rows_total, nrhs);
         }
         lc.n += 2 * nb;
       }
     }
   }
-  k_solve_scatter<<<g, 256, 0, st>>>(d_b, ldb, nrhs, pl.n, d.perm, sc_out, xv);
+  launch_pdl(k_solve_scatter, g, 256, 0, st, d_b, ldb, nrhs, pl.n, d.perm, sc_out, xv);
   lc.n++;
   SMFG_CUDA(cudaGetLastError());
 }

@@ -1605,9 +1605,22 @@ __global__ void k_finish(DevPlan P, DevFactor X, FactorTotals *out) {
 // ---------------------------------------------------------------------------
 // Solves. x (new numbering, n x nrhs) and per-front work vectors w at the
 // fronts' row offsets (rows_total x nrhs).
+//
+// The solve kernels are launched with programmatic stream serialization: a
+// kernel may start while the one before it on the stream still runs. Before
+// pdl_wait() it reads only what no solve kernel writes (the factor, its row
+// maps and sizes), so that its loads of L overlap the kernel before it;
+// pdl_wait() returns once that kernel has completed and its writes are
+// visible (at once when the launch had no such dependency), and
+// pdl_trigger() lets the next kernel start its own prologue.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __global__ void k_solve_gather(const double *__restrict__ b, int ldb, int nrhs, int n,
                                const int *__restrict__ perm, const double *__restrict__ scale,
                                double *__restrict__ x) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t tot = (int64_t)n * nrhs;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot;
        t += (int64_t)gridDim.x * blockDim.x) {
@@ -1622,6 +1635,8 @@ __global__ void k_solve_gather(const double *__restrict__ b, int ldb, int nrhs, 
 __global__ void k_solve_scatter(double *__restrict__ b, int ldb, int nrhs, int n,
                                 const int *__restrict__ perm, const double *__restrict__ scale,
                                 const double *__restrict__ x) {
+  pdl_wait();
+  pdl_trigger();
   const int64_t tot = (int64_t)n * nrhs;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot;
        t += (int64_t)gridDim.x * blockDim.x) {
@@ -1758,6 +1773,8 @@ __global__ void __launch_bounds__(256, 4) k_fwd_small(DevPlan P, DevFactor X, in
   const int s = P.lvl_sn[lo + item];
   const int f = X.sn_f[s];
   if (f > kSolveSmall || P.sn_large[s]) return;
+  pdl_wait();
+  pdl_trigger();
   const int p = X.sn_pstore[s];
   const int64_t roff = X.sn_roff[s];
   const int *rows = X.rows + roff;
@@ -1823,6 +1840,8 @@ __global__ void __launch_bounds__(256, 4) k_bwd_small(DevPlan P, DevFactor X, in
   const int s = P.lvl_sn[lo + item];
   const int f = X.sn_f[s];
   if (f > kSolveSmall || P.sn_large[s]) return;
+  pdl_wait();
+  pdl_trigger();
   const int p = X.sn_pstore[s];
   const int *rows = X.rows + X.sn_roff[s];
   const double *L = X.arena + X.sn_off[s];
@@ -1896,6 +1915,8 @@ __global__ void __launch_bounds__(kSolveNT, 4) k_fwd_front(DevPlan P, DevFactor 
   const size_t sf = (size_t)f;
   const bool large = P.sn_large[s] != 0;
   if (!large && f <= kSolveSmall) return;  // k_fwd_small's
+  pdl_wait();
+  pdl_trigger();
   __shared__ double Ls[32][33];
   const int warp = threadIdx.x >> 5;
   // every right-hand side at once: gather, children's update vectors in
@@ -2018,6 +2039,8 @@ __global__ void __launch_bounds__(256) k_bwd_l21(DevPlan P, DevFactor X, const i
                                                  int64_t rows_total, int nrhs) {
   __shared__ int pref[65];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  pdl_wait();
+  pdl_trigger();
   for (int chunk = 0; chunk < nlarge; chunk += 64) {
     const int cnt = min(64, nlarge - chunk);
     if (threadIdx.x == 0) {
@@ -2071,6 +2094,8 @@ __global__ void __launch_bounds__(kSolveNT) k_bwd_front(DevPlan P, DevFactor X, 
   const size_t sf = (size_t)f;
   const bool large = P.sn_large[s] != 0;
   if (!large && f <= kSolveSmall) return;  // k_bwd_small's
+  pdl_wait();
+  pdl_trigger();
   __shared__ double Ls[32][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // every right-hand side at once. D^-1 of each pivot block; 2x2 blocks
@@ -2209,25 +2234,6 @@ __global__ void __launch_bounds__(kSolveNT) k_bwd_front(DevPlan P, DevFactor X, 
 constexpr int kSB = 256;
 constexpr int kTriNT = 256;  // threads of the triangle kernels
 
-// acc over the 32 columns [jb, jb + nb) of row i: sum of L(i, j) w[j]
-// (w in shared memory, indexed from wb), all loads issued first.
-__device__ __forceinline__ double strip_dot32(const double *L, size_t sf, int i, int jb, int nb,
-                                              const double *w, int wb) {
-  // (L is only read while the solves run: the read-only path)
-  const double *li = L + (size_t)jb * sf + i;
-  double acc = 0.0;
-  if (nb == 32) {
-    double l[32];
-#pragma unroll
-    for (int u = 0; u < 32; ++u) l[u] = __ldg(li + (size_t)u * sf);
-#pragma unroll
-    for (int u = 0; u < 32; ++u) acc = fma(l[u], w[jb + u - wb], acc);
-  } else {
-    for (int u = 0; u < nb; ++u) acc = fma(__ldg(li + (size_t)u * sf), w[jb + u - wb], acc);
-  }
-  return acc;
-}
-
 // The 256-column blocks' strips of L staged in shared memory: strip k (32
 // columns jb.., rows [jb, j1) of the block) at buf[k & 1][u][row - j0],
 // copied with cp.async two strips ahead of their use.
@@ -2238,12 +2244,15 @@ struct TriSmem {
 
 __device__ __forceinline__ void tri_strip_async(const double *L, size_t sf, int j0, int j1, int jb, int nb,
                                                 double (*dst)[kSB]) {
+  // a warp per column (coalesced rows), no index division in the issue loop
   const int rows = j1 - jb;
-  for (int t = threadIdx.x; t < nb * rows; t += kTriNT) {
-    const int u = t / rows, rr = t % rows;
-    const double *src = L + (size_t)(jb + u) * sf + jb + rr;
-    const unsigned d = (unsigned)__cvta_generic_to_shared(&dst[u][jb - j0 + rr]);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+  const int lane = threadIdx.x & 31;
+  for (int u = threadIdx.x >> 5; u < nb; u += kTriNT / 32) {
+    const double *src = L + (size_t)(jb + u) * sf + jb;
+    const unsigned d = (unsigned)__cvta_generic_to_shared(&dst[u][jb - j0]);
+    for (int rr = lane; rr < rows; rr += 32)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d + 8u * (unsigned)rr), "l"(src + rr)
+                   : "memory");
   }
   asm volatile("cp.async.commit_group;" ::: "memory");
 }
@@ -2272,6 +2281,8 @@ __global__ void __launch_bounds__(kTriNT) k_fwd_tri(DevPlan P, DevFactor X, cons
   const int nstrip = (j1 - j0 + 31) / 32;
   tri_strip_async(L, sf, j0, j1, j0, min(32, j1 - j0), sm.buf[0]);
   if (nstrip > 1) tri_strip_async(L, sf, j0, j1, j0 + 32, min(32, j1 - j0 - 32), sm.buf[1]);
+  pdl_wait();  // the strips of L in flight meanwhile
+  pdl_trigger();
   for (int r = 0; r < nrhs; ++r)
     for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) sm.w[r][t] = wk[(int64_t)r * rows_total + roff + j0 + t];
   for (int k = 0; k < nstrip; ++k) {
@@ -2332,6 +2343,7 @@ __global__ void __launch_bounds__(256) k_fwd_gemv(DevPlan P, DevFactor X, const 
   __shared__ double part[8][33];
   __shared__ int pref[65];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  bool waited = false;
   for (int chunk = 0; chunk < nlarge; chunk += 64) {
     const int cnt = min(64, nlarge - chunk);
     __syncthreads();
@@ -2361,13 +2373,27 @@ __global__ void __launch_bounds__(256) k_fwd_gemv(DevPlan P, DevFactor X, const 
       double *w = wk + (int64_t)r * rows_total + X.sn_roff[s];
       const double *L = X.arena + X.sn_off[s];
       const size_t sf = (size_t)f;
+      const int i = j1 + rc * 32 + lane;
+      const int jb = j0 + warp * 32;
+      const int nbw = (i < f && jb < j1) ? min(32, j1 - jb) : 0;
+      // this lane's 32 entries of L in flight before the wait (the first
+      // item: while the triangle kernel before this one still runs)
+      double l[32];
+      const double *li = L + (size_t)jb * sf + i;
+#pragma unroll
+      for (int u = 0; u < 32; ++u) l[u] = (u < nbw) ? __ldg(li + (size_t)u * sf) : 0.0;
+      if (!waited) {
+        pdl_wait();
+        pdl_trigger();
+        waited = true;
+      }
       __syncthreads();
       for (int t = threadIdx.x; t < j1 - j0; t += 256) ws[t] = w[j0 + t];
       __syncthreads();
-      const int i = j1 + rc * 32 + lane;
-      const int jb = j0 + warp * 32;
       double acc = 0.0;
-      if (i < f && jb < j1) acc = strip_dot32(L, sf, i, jb, min(32, j1 - jb), ws, j0);
+#pragma unroll
+      for (int u = 0; u < 32; ++u)
+        if (u < nbw) acc = fma(l[u], ws[jb + u - j0], acc);
       part[warp][lane] = acc;
       __syncthreads();
       if (warp == 0 && i < f) {
@@ -2390,6 +2416,8 @@ __global__ void __launch_bounds__(256) k_bwd_dots(DevPlan P, DevFactor X, const 
   __shared__ int pref[65];
   __shared__ double red[8];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  pdl_wait();
+  pdl_trigger();
   for (int chunk = 0; chunk < nlarge; chunk += 64) {
     const int cnt = min(64, nlarge - chunk);
     __syncthreads();
@@ -2477,6 +2505,8 @@ __global__ void __launch_bounds__(kTriNT) k_bwd_tri(DevPlan P, DevFactor X, cons
     strip(1, jb, nb);
     tri_strip_async(L, sf, j0, j1, jb, nb, sm.buf[1]);
   }
+  pdl_wait();  // the strips of L in flight meanwhile
+  pdl_trigger();
   for (int r = 0; r < nrhs; ++r)
     for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) sm.w[r][t] = wk[(int64_t)r * rows_total + roff + j0 + t];
   for (int k = 0; k < nstrip; ++k) {
