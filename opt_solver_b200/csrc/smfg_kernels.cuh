@@ -2032,22 +2032,31 @@ __global__ void __launch_bounds__(256) k_fwd_l21(DevPlan P, DevFactor X, const i
   }
 }
 
-// t[0:p) = L21^T x_ext of the level's large fronts (warp per column),
-// stored at the front's work vector positions [0, p).
+// t[0:p) = L21^T x_ext of the level's large fronts, stored at the front's
+// work vector positions [0, p): a work item is kL21Cols columns of one
+// front for one right-hand side. x_ext is gathered into shared memory a
+// tile of rows at a time, once for all the item's columns; a warp takes
+// kL21Cols / 8 columns, lane = row. Each column's sum runs over its rows as
+// a warp per column would take them (lane l: rows p + l + 32m in turn),
+// then a shuffle tree.
+constexpr int kL21Cols = 16, kL21Tile = 1024;
 __global__ void __launch_bounds__(256) k_bwd_l21(DevPlan P, DevFactor X, const int *__restrict__ large,
                                                  int nlarge, const double *x, double *wk,
                                                  int64_t rows_total, int nrhs) {
+  constexpr int CW = kL21Cols / 8;  // columns a warp
   __shared__ int pref[65];
+  __shared__ double xs[kL21Tile];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   pdl_wait();
   pdl_trigger();
   for (int chunk = 0; chunk < nlarge; chunk += 64) {
     const int cnt = min(64, nlarge - chunk);
+    __syncthreads();
     if (threadIdx.x == 0) {
       pref[0] = 0;
       for (int q = 0; q < cnt; ++q) {
         const int s = large[chunk + q];
-        pref[q + 1] = pref[q] + (X.sn_pstore[s] + 7) / 8 * nrhs;
+        pref[q + 1] = pref[q] + (X.sn_pstore[s] + kL21Cols - 1) / kL21Cols * nrhs;
       }
     }
     __syncthreads();
@@ -2061,21 +2070,35 @@ __global__ void __launch_bounds__(256) k_bwd_l21(DevPlan P, DevFactor X, const i
       }
       const int s = large[chunk + a];
       const int f = X.sn_f[s], p = X.sn_pstore[s];
-      const int ncc = (p + 7) / 8;
+      const int ncc = (p + kL21Cols - 1) / kL21Cols;
       const int item = wi - pref[a];
       const int r = item / ncc, cc = item % ncc;
-      const int j = cc * 8 + warp;
-      if (j < p) {
-        const int *rows = X.rows + X.sn_roff[s];
-        const double *Lj = X.arena + X.sn_off[s] + (size_t)j * f;
-        const double *xr = x + (int64_t)r * P.n;
-        double acc = 0.0;
-        for (int i = p + lane; i < f; i += 32) acc = fma(Lj[i], xr[rows[i]], acc);
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) wk[(int64_t)r * rows_total + X.sn_roff[s] + j] = acc;
+      const int jw = cc * kL21Cols + warp * CW;
+      const int *rows = X.rows + X.sn_roff[s] + p;
+      const double *L = X.arena + X.sn_off[s] + p;
+      const double *xr = x + (int64_t)r * P.n;
+      double acc[CW];
+#pragma unroll
+      for (int c = 0; c < CW; ++c) acc[c] = 0.0;
+      for (int t0 = 0; t0 < f - p; t0 += kL21Tile) {
+        const int tn = min(kL21Tile, f - p - t0);
+        __syncthreads();  // the tile before read
+        for (int i = threadIdx.x; i < tn; i += 256) xs[i] = xr[rows[t0 + i]];
+        __syncthreads();
+        for (int i = lane; i < tn; i += 32) {
+          const double xv = xs[i];
+#pragma unroll
+          for (int c = 0; c < CW; ++c)
+            if (jw + c < p) acc[c] = fma(L[(size_t)(jw + c) * f + t0 + i], xv, acc[c]);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < CW; ++c) {
+        double v = acc[c];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0 && jw + c < p) wk[(int64_t)r * rows_total + X.sn_roff[s] + jw + c] = v;
       }
     }
-    __syncthreads();
   }
 }
 
@@ -2235,19 +2258,25 @@ constexpr int kSB = 256;
 constexpr int kTriNT = 256;  // threads of the triangle kernels
 
 // The 256-column blocks' strips of L staged in shared memory: strip k (32
-// columns jb.., rows [jb, j1) of the block) at buf[k & 1][u][row - j0],
-// copied with cp.async two strips ahead of their use.
+// columns, the block's rows from the strip's first on) at
+// buf[k % kRing][column][row - j0], copied with cp.async ahead of its use.
+// Rows are padded to kSBP doubles, so that lanes reading one row across a
+// strip's 32 columns hit distinct banks.
+constexpr int kSBP = kSB + 1;
+constexpr int kRing = 3;
 struct TriSmem {
-  double buf[2][32][kSB];
+  double buf[kRing][32][kSBP];
   double w[8][kSB];  // the block's values, per right-hand side (at most 8)
 };
 
+// Strip [jb, jb + nb) of the block [j0, j1) (its rows [jb, j1)) into dst by
+// threads [t0, t0 + nt): a warp per column (coalesced rows), one cp.async
+// group.
 __device__ __forceinline__ void tri_strip_async(const double *L, size_t sf, int j0, int j1, int jb, int nb,
-                                                double (*dst)[kSB]) {
-  // a warp per column (coalesced rows), no index division in the issue loop
+                                                double (*dst)[kSBP], int t0 = 0, int nt = kTriNT) {
   const int rows = j1 - jb;
   const int lane = threadIdx.x & 31;
-  for (int u = threadIdx.x >> 5; u < nb; u += kTriNT / 32) {
+  for (int u = ((int)threadIdx.x - t0) >> 5; u < nb; u += nt / 32) {
     const double *src = L + (size_t)(jb + u) * sf + jb;
     const unsigned d = (unsigned)__cvta_generic_to_shared(&dst[u][jb - j0]);
     for (int rr = lane; rr < rows; rr += 32)
@@ -2257,12 +2286,234 @@ __device__ __forceinline__ void tri_strip_async(const double *L, size_t sf, int 
   asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
-__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+// wait until at most `pending` (0..2) of this thread's cp.async groups are in flight
+__device__ __forceinline__ void cp_async_wait_pending(int pending) {
+  if (pending >= 2) asm volatile("cp.async.wait_group 2;" ::: "memory");
+  else if (pending == 1) asm volatile("cp.async.wait_group 1;" ::: "memory");
+  else asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
 
-// Forward block b of each large front: w[j0:j1) <- L_bb^-1 w[j0:j1), strip
-// by strip (a warp per right-hand side solves the 32 x 32 triangle, then
-// every thread a row of the block below it), the strips' L streaming into
-// shared memory two ahead.
+// All threads of a subset of whole warps (n of them, from warp-aligned
+// threads) meet at barrier `id` (1..15; 0 is __syncthreads).
+__device__ __forceinline__ void warps_sync(int id, int n) {
+  __syncwarp();
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+// Strips of a forward block: strip k covers [j0 + 32k, ...).
+__device__ __forceinline__ void fwd_strip(int j0, int j1, int k, int &jb, int &nb) {
+  jb = j0 + 32 * k;
+  nb = min(32, j1 - jb);
+}
+// Strips of a backward block, numbered from the last.
+__device__ __forceinline__ void bwd_strip(int j0, int j1, int k, int &jb, int &nb) {
+  const int nstrip = (j1 - j0 + 31) / 32;
+  jb = j0 + 32 * (nstrip - 1 - k);
+  nb = min(32, j1 - jb);
+}
+
+// Block [j0, j1) of a large front: its first kRing strips of L issued to
+// shared memory (all threads; one cp.async group each).
+__device__ __forceinline__ void fwd_block_issue(const double *L, size_t sf, int j0, int j1, TriSmem &sm) {
+  const int nstrip = (j1 - j0 + 31) / 32;
+  for (int k = 0; k < min(kRing, nstrip); ++k) {
+    int jb, nb;
+    fwd_strip(j0, j1, k, jb, nb);
+    tri_strip_async(L, sf, j0, j1, jb, nb, sm.buf[k]);
+  }
+}
+__device__ __forceinline__ void bwd_block_issue(const double *L, size_t sf, int j0, int j1, TriSmem &sm) {
+  const int nstrip = (j1 - j0 + 31) / 32;
+  for (int k = 0; k < min(kRing, nstrip); ++k) {
+    int jb, nb;
+    bwd_strip(j0, j1, k, jb, nb);
+    tri_strip_async(L, sf, j0, j1, jb, nb, sm.buf[k]);
+  }
+}
+
+// The forward 32 x 32 triangle of strip [jb, jb + nb) for one right-hand
+// side (a warp; lane = row jb + lane), `pre` (the product of the strip
+// before, from the look-ahead) subtracted first: w[jb + lane] <- its solved
+// value, also returned. The row of the triangle is in registers and the SPD
+// diagonal's reciprocal taken ahead, so a step of the chain is one shuffle
+// and one fused multiply-add.
+__device__ __forceinline__ double fwd_chain32(const double (*Lb)[kSBP], int j0, int jb, int nb, int posdef,
+                                              double *w, double pre) {
+  const int lane = threadIdx.x & 31;
+  double lrow[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) lrow[j] = (j < lane && lane < nb) ? Lb[j][jb - j0 + lane] : 0.0;
+  const double rdiag = (posdef && lane < nb) ? 1.0 / Lb[lane][jb - j0 + lane] : 1.0;
+  double wi = (lane < nb) ? w[jb - j0 + lane] - pre : 0.0;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    if (j < nb) {
+      if (lane == j) wi = wi * rdiag;
+      const double wj = __shfl_sync(0xffffffffu, wi, j);
+      if (lrow[j] != 0.0) wi = fma(-lrow[j], wj, wi);
+    }
+  }
+  if (lane < nb) w[jb - j0 + lane] = wi;
+  return wi;
+}
+
+// The backward (transposed) 32 x 32 triangle of strip [jb, jb + nb) for one
+// right-hand side (lane = column jb + lane), `pre` subtracted first.
+__device__ __forceinline__ double bwd_chain32(const double (*Lb)[kSBP], int j0, int jb, int nb, int posdef,
+                                              double *w, double pre) {
+  const int lane = threadIdx.x & 31;
+  double lcol[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) lcol[j] = (j > lane && j < nb) ? Lb[lane][jb - j0 + j] : 0.0;
+  const double rdiag = (posdef && lane < nb) ? 1.0 / Lb[lane][jb - j0 + lane] : 1.0;
+  double vi = (lane < nb) ? w[jb - j0 + lane] - pre : 0.0;
+#pragma unroll
+  for (int j = 31; j >= 0; --j) {
+    if (j < nb) {
+      if (lane == j) vi = vi * rdiag;
+      const double xj = __shfl_sync(0xffffffffu, vi, j);
+      if (lcol[j] != 0.0) vi = fma(-lcol[j], xj, vi);
+    }
+  }
+  if (lane < nb) w[jb - j0 + lane] = vi;
+  return vi;
+}
+
+// Look-ahead products of a solved strip (values x in the lanes of the
+// warp) with the next strip, summed in strip order by one fused
+// multiply-add chain. Forward: rows jn + lane of the next strip over the
+// columns of this one (Lb: this strip's buffer). Backward: columns jn +
+// lane of the next strip over the rows jb.. of this one (Ln: the next
+// strip's buffer).
+__device__ __forceinline__ double fwd_ahead32(const double (*Lb)[kSBP], int j0, int j1, int jb, double x) {
+  const int i = jb + 32 + (int)(threadIdx.x & 31);
+  double la = 0.0;
+#pragma unroll
+  for (int u = 0; u < 32; ++u) {
+    const double xu = __shfl_sync(0xffffffffu, x, u);
+    if (i < j1) la = fma(Lb[u][i - j0], xu, la);
+  }
+  return la;
+}
+__device__ __forceinline__ double bwd_ahead32(const double (*Ln)[kSBP], int j0, int jb, int nb, double x) {
+  const int lane = threadIdx.x & 31;
+  double la = 0.0;
+#pragma unroll
+  for (int t = 0; t < 32; ++t) {
+    const double xt = __shfl_sync(0xffffffffu, x, t);
+    if (t < nb) la = fma(Ln[lane][jb + t - j0], xt, la);
+  }
+  return la;
+}
+
+// The block's rows [r0, j1) minus a strip's products (each row its own fused
+// multiply-add chain over the strip's columns, then one subtraction), for
+// rhs 0..nrhs-1; threads [t0, t0 + nt) take rows in turn.
+__device__ __forceinline__ void fwd_rows_update(const double (*Lb)[kSBP], int j0, int j1, int jb, int nb, int r0,
+                                                int nrhs, TriSmem &sm, int t, int nt) {
+  for (int i = r0 + t; i < j1; i += nt) {
+    for (int r = 0; r < nrhs; ++r) {
+      double acc = 0.0;
+      for (int u = 0; u < nb; ++u) acc = fma(Lb[u][i - j0], sm.w[r][jb - j0 + u], acc);
+      sm.w[r][i - j0] -= acc;
+    }
+  }
+}
+
+// Columns of a backward strip (buffer L2, columns [j2, j2 + n2)) minus their
+// products with the solved rows [r0, j1): a warp per column (warps w0.. of
+// nw), lanes over the rows, a shuffle tree.
+__device__ __forceinline__ void bwd_cols_update(const double (*L2)[kSBP], int j0, int j1, int j2, int n2, int r0,
+                                                int nrhs, TriSmem &sm, int w0, int nw) {
+  const int lane = threadIdx.x & 31;
+  for (int u = w0; u < n2; u += nw) {
+    for (int r = 0; r < nrhs; ++r) {
+      double acc = 0.0;
+      for (int i = r0 + lane; i < j1; i += 32) acc = fma(L2[u][i - j0], sm.w[r][i - j0], acc);
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) sm.w[r][j2 - j0 + u] -= acc;
+    }
+  }
+}
+
+// At most this many right-hand sides take the pipelined block solves (the
+// first nrhs warps run the triangle chains, the others the rest of the
+// block a strip behind); more take the step-by-step form, which computes
+// the same sums.
+constexpr int kPipeRhs = 4;
+
+// sm.w[r][0, j1 - j0) <- L_bb^-1 sm.w[r] for each right-hand side, the
+// block's first kRing strips issued by fwd_block_issue. Row i of the block
+// takes each strip's product in strip order: the strips up to two before
+// its own from the rows update, the one just before from the chain warp's
+// look-ahead. Ends at a barrier.
+__device__ void fwd_block_solve(const double *L, size_t sf, int j0, int j1, int posdef, int nrhs, TriSmem &sm) {
+  const int warp = threadIdx.x >> 5;
+  const int nstrip = (j1 - j0 + 31) / 32;
+  if (nrhs > kPipeRhs) {
+    cp_async_wait_pending(0);
+    __syncthreads();
+    for (int k = 0; k < nstrip; ++k) {
+      int jb, nb;
+      fwd_strip(j0, j1, k, jb, nb);
+      const double(*Lb)[kSBP] = sm.buf[k % kRing];
+      if (k >= kRing) cp_async_wait_pending(min(kRing - 1, nstrip - 1 - k));
+      __syncthreads();
+      if (warp < nrhs) fwd_chain32(Lb, j0, jb, nb, posdef, sm.w[warp], 0.0);
+      __syncthreads();
+      fwd_rows_update(Lb, j0, j1, jb, nb, jb + nb, nrhs, sm, (int)threadIdx.x, kTriNT);
+      __syncthreads();  // this strip's buffer is free
+      if (k + kRing < nstrip) {
+        int jb3, nb3;
+        fwd_strip(j0, j1, k + kRing, jb3, nb3);
+        tri_strip_async(L, sf, j0, j1, jb3, nb3, sm.buf[k % kRing]);
+      }
+    }
+    __syncthreads();
+    return;
+  }
+  // Step k: the chain warps solve strip k and form its look-ahead product
+  // with strip k + 1's rows; the other warps apply strip k - 1 to the rows
+  // past strip k and then stream strip k + 2 into strip k - 1's buffer.
+  const int C = nrhs, nf = kTriNT - 32 * C, ft = (int)threadIdx.x - 32 * C;
+  cp_async_wait_pending(min(kRing - 1, nstrip - 1));  // strip 0 landed
+  __syncthreads();
+  double la = 0.0;
+  for (int k = 0; k <= nstrip; ++k) {
+    if (warp < C) {
+      if (k < nstrip) {
+        int jb, nb;
+        fwd_strip(j0, j1, k, jb, nb);
+        const double(*Lb)[kSBP] = sm.buf[k % kRing];
+        const double x = fwd_chain32(Lb, j0, jb, nb, posdef, sm.w[warp], la);
+        la = (k + 1 < nstrip) ? fwd_ahead32(Lb, j0, j1, jb, x) : 0.0;
+      }
+    } else {
+      bool issued = false;
+      if (k >= 1) {
+        int jm, nm;
+        fwd_strip(j0, j1, k - 1, jm, nm);
+        fwd_rows_update(sm.buf[(k - 1) % kRing], j0, j1, jm, nm, jm + 64, C, sm, ft, nf);
+        if (k - 1 + kRing < nstrip) {
+          warps_sync(1, nf);  // every reader of strip k - 1's buffer done
+          int jb3, nb3;
+          fwd_strip(j0, j1, k - 1 + kRing, jb3, nb3);
+          tri_strip_async(L, sf, j0, j1, jb3, nb3, sm.buf[(k - 1) % kRing], 32 * C, nf);
+          issued = true;
+        }
+      }
+      // strip k + 1 (issued a step ago) landed before the chains take it
+      if (k + 1 < nstrip && k + 1 >= kRing) cp_async_wait_pending(issued ? 1 : 0);
+    }
+    // strips 1 and 2, issued by every thread at the start
+    if (k == 0 && nstrip > 1) cp_async_wait_pending(nstrip > 2 ? 1 : 0);
+    if (k == 1 && nstrip > 2) cp_async_wait_pending(warp >= C && k - 1 + kRing < nstrip ? 1 : 0);
+    __syncthreads();
+  }
+}
+
+// Forward block b of each large front (a block of threads per front):
+// w[j0:j1) <- L_bb^-1 w[j0:j1).
 __global__ void __launch_bounds__(kTriNT) k_fwd_tri(DevPlan P, DevFactor X, const int *__restrict__ large,
                                                     int b, int posdef, double *x, double *wk,
                                                     int64_t rows_total, int nrhs) {
@@ -2277,52 +2528,12 @@ __global__ void __launch_bounds__(kTriNT) k_fwd_tri(DevPlan P, DevFactor X, cons
   const int *rows = X.rows + roff;
   const double *L = X.arena + X.sn_off[s];
   const size_t sf = (size_t)f;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nstrip = (j1 - j0 + 31) / 32;
-  tri_strip_async(L, sf, j0, j1, j0, min(32, j1 - j0), sm.buf[0]);
-  if (nstrip > 1) tri_strip_async(L, sf, j0, j1, j0 + 32, min(32, j1 - j0 - 32), sm.buf[1]);
+  fwd_block_issue(L, sf, j0, j1, sm);
   pdl_wait();  // the strips of L in flight meanwhile
   pdl_trigger();
   for (int r = 0; r < nrhs; ++r)
     for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) sm.w[r][t] = wk[(int64_t)r * rows_total + roff + j0 + t];
-  for (int k = 0; k < nstrip; ++k) {
-    const int jb = j0 + 32 * k, nb = min(32, j1 - jb);
-    const double(*Lb)[kSB] = sm.buf[k & 1];
-    if (k + 1 < nstrip) cp_async_wait_one();
-    else cp_async_wait_all();
-    __syncthreads();
-    if (warp < nrhs) {
-      // lane = row jb + lane: its row of the triangle in registers, the
-      // SPD diagonal's reciprocal taken ahead, so that a step of the chain
-      // is one shuffle and one fused multiply-add
-      double *w = sm.w[warp];
-      double lrow[32];
-#pragma unroll
-      for (int j = 0; j < 32; ++j) lrow[j] = (j < lane && lane < nb) ? Lb[j][jb - j0 + lane] : 0.0;
-      const double rdiag = (posdef && lane < nb) ? 1.0 / Lb[lane][jb - j0 + lane] : 1.0;
-      double wi = (lane < nb) ? w[jb - j0 + lane] : 0.0;
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        if (j < nb) {
-          if (lane == j) wi = wi * rdiag;
-          const double wj = __shfl_sync(0xffffffffu, wi, j);
-          if (lrow[j] != 0.0) wi = fma(-lrow[j], wj, wi);
-        }
-      }
-      if (lane < nb) w[jb - j0 + lane] = wi;
-    }
-    __syncthreads();
-    const int i = jb + nb + (int)threadIdx.x;
-    if (i < j1) {
-      for (int r = 0; r < nrhs; ++r) {
-        double acc = 0.0;
-        for (int u = 0; u < nb; ++u) acc = fma(Lb[u][i - j0], sm.w[r][jb - j0 + u], acc);
-        sm.w[r][i - j0] -= acc;
-      }
-    }
-    __syncthreads();  // this strip's buffer is free
-    if (k + 2 < nstrip) tri_strip_async(L, sf, j0, j1, jb + 64, min(32, j1 - jb - 64), sm.buf[k & 1]);
-  }
+  fwd_block_solve(L, sf, j0, j1, posdef, nrhs, sm);
   for (int r = 0; r < nrhs; ++r) {
     double *w = wk + (int64_t)r * rows_total + roff;
     double *xr = x + (int64_t)r * P.n;
@@ -2471,11 +2682,91 @@ __global__ void __launch_bounds__(256) k_bwd_dots(DevPlan P, DevFactor X, const 
   }
 }
 
-// Backward block b of each large front (its rows past the block already
-// taken by k_bwd_dots): strips from the last, each with its dots against
-// the block's solved rows below it (a warp per column) and then the 32 x 32
-// transposed triangle (a warp per right-hand side), the strips' L streaming
-// into shared memory two ahead.
+// sm.w[r][0, j1 - j0) <- L_bb^-T sm.w[r] (the rows past the block already
+// taken), the block's first kRing strips issued by bwd_block_issue: strips
+// from the last. A column of strip m takes, before its triangle, the
+// product with the solved rows of the strips up to m - 2 (one shuffle-tree
+// sum) and then that with strip m - 1's rows (the chain warp's look-ahead).
+// Ends at a barrier.
+__device__ void bwd_block_solve(const double *L, size_t sf, int j0, int j1, int posdef, int nrhs, TriSmem &sm) {
+  const int warp = threadIdx.x >> 5;
+  const int nstrip = (j1 - j0 + 31) / 32;
+  if (nrhs > kPipeRhs) {
+    cp_async_wait_pending(0);
+    __syncthreads();
+    for (int k = 0; k < nstrip; ++k) {
+      int jb, nb;
+      bwd_strip(j0, j1, k, jb, nb);
+      const double(*Lb)[kSBP] = sm.buf[k % kRing];
+      if (k >= kRing) cp_async_wait_pending(min(kRing - 1, nstrip - 1 - k));
+      __syncthreads();
+      if (k >= 2) {
+        int jm, nm;
+        bwd_strip(j0, j1, k - 2, jm, nm);
+        bwd_cols_update(Lb, j0, j1, jb, nb, jm, nrhs, sm, warp, kTriNT / 32);
+      }
+      __syncthreads();
+      if (warp < nrhs) {
+        double la = 0.0;
+        if (k >= 1) {
+          // strip k - 1's solved values in the lanes, as the chain left them
+          int jp, np;
+          bwd_strip(j0, j1, k - 1, jp, np);
+          const int lane = threadIdx.x & 31;
+          const double xp = (lane < np) ? sm.w[warp][jp - j0 + lane] : 0.0;
+          la = bwd_ahead32(Lb, j0, jp, np, xp);
+        }
+        bwd_chain32(Lb, j0, jb, nb, posdef, sm.w[warp], la);
+      }
+      __syncthreads();  // this strip's buffer is free
+      if (k + kRing < nstrip) {
+        int jb3, nb3;
+        bwd_strip(j0, j1, k + kRing, jb3, nb3);
+        tri_strip_async(L, sf, j0, j1, jb3, nb3, sm.buf[k % kRing]);
+      }
+    }
+    __syncthreads();
+    return;
+  }
+  // Step k: the chain warps solve strip k and form its look-ahead product
+  // with strip k + 1's columns; the other warps stream strip k + 2 into
+  // strip k - 1's buffer and apply the rows solved up to strip k - 1 to
+  // strip k + 1's columns.
+  const int C = nrhs, nf = kTriNT - 32 * C, fw = warp - C, nfw = nf / 32;
+  cp_async_wait_pending(nstrip > 2 ? 1 : 0);  // strips 0 and 1 landed
+  __syncthreads();
+  double la = 0.0;
+  for (int k = 0; k < nstrip; ++k) {
+    if (warp < C) {
+      int jb, nb;
+      bwd_strip(j0, j1, k, jb, nb);
+      const double x = bwd_chain32(sm.buf[k % kRing], j0, jb, nb, posdef, sm.w[warp], la);
+      la = 0.0;
+      if (k + 1 < nstrip) la = bwd_ahead32(sm.buf[(k + 1) % kRing], j0, jb, nb, x);
+    } else {
+      if (k >= 1 && k - 1 + kRing < nstrip) {
+        // strip k - 1's buffer: its last readers (chain k - 1, look-ahead
+        // k - 2, the columns update one step before) are done
+        int jb3, nb3;
+        bwd_strip(j0, j1, k - 1 + kRing, jb3, nb3);
+        tri_strip_async(L, sf, j0, j1, jb3, nb3, sm.buf[(k - 1) % kRing], 32 * C, nf);
+      }
+      if (k >= 1 && k + 1 < nstrip) {
+        int jm, nm, j2, n2;
+        bwd_strip(j0, j1, k - 1, jm, nm);
+        bwd_strip(j0, j1, k + 1, j2, n2);
+        bwd_cols_update(sm.buf[(k + 1) % kRing], j0, j1, j2, n2, jm, C, sm, fw, nfw);
+      }
+      // strip k + 2 landed before the next step's readers take it
+      if (k + 2 < nstrip && k + 2 >= kRing) cp_async_wait_pending(0);
+    }
+    if (k == 0 && nstrip > 2) cp_async_wait_pending(0);  // strip 2, issued by every thread at the start
+    __syncthreads();
+  }
+}
+
+// Backward block b of each large front (a block of threads per front; its
+// rows past the block already taken by k_bwd_dots).
 __global__ void __launch_bounds__(kTriNT) k_bwd_tri(DevPlan P, DevFactor X, const int *__restrict__ large,
                                                     int b, int posdef, double *x, double *wk,
                                                     int64_t rows_total, int nrhs) {
@@ -2490,67 +2781,12 @@ __global__ void __launch_bounds__(kTriNT) k_bwd_tri(DevPlan P, DevFactor X, cons
   const int *rows = X.rows + roff;
   const double *L = X.arena + X.sn_off[s];
   const size_t sf = (size_t)f;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nstrip = (j1 - j0 + 31) / 32;
-  // strips numbered from the last: strip k covers [jb_k, jb_k + nb_k)
-  auto strip = [&](int k, int &jb, int &nb) {
-    const int idx = nstrip - 1 - k;
-    jb = j0 + 32 * idx;
-    nb = min(32, j1 - jb);
-  };
-  int jb, nb;
-  strip(0, jb, nb);
-  tri_strip_async(L, sf, j0, j1, jb, nb, sm.buf[0]);
-  if (nstrip > 1) {
-    strip(1, jb, nb);
-    tri_strip_async(L, sf, j0, j1, jb, nb, sm.buf[1]);
-  }
+  bwd_block_issue(L, sf, j0, j1, sm);
   pdl_wait();  // the strips of L in flight meanwhile
   pdl_trigger();
   for (int r = 0; r < nrhs; ++r)
     for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) sm.w[r][t] = wk[(int64_t)r * rows_total + roff + j0 + t];
-  for (int k = 0; k < nstrip; ++k) {
-    strip(k, jb, nb);
-    const int je = jb + nb;
-    const double(*Lb)[kSB] = sm.buf[k & 1];
-    if (k + 1 < nstrip) cp_async_wait_one();
-    else cp_async_wait_all();
-    __syncthreads();
-    // v[j] -= sum over the block's solved rows [je, j1) of L(i, j) v[i]
-    for (int u = warp; u < nb; u += kTriNT / 32) {
-      for (int r = 0; r < nrhs; ++r) {
-        double acc = 0.0;
-        for (int i = je + lane; i < j1; i += 32) acc = fma(Lb[u][i - j0], sm.w[r][i - j0], acc);
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) sm.w[r][jb - j0 + u] -= acc;
-      }
-    }
-    __syncthreads();
-    if (warp < nrhs) {
-      // lane = column jb + lane: its column of the triangle in registers
-      double *w = sm.w[warp];
-      double lcol[32];
-#pragma unroll
-      for (int j = 0; j < 32; ++j) lcol[j] = (j > lane && j < nb) ? Lb[lane][jb - j0 + j] : 0.0;
-      const double rdiag = (posdef && lane < nb) ? 1.0 / Lb[lane][jb - j0 + lane] : 1.0;
-      double vi = (lane < nb) ? w[jb - j0 + lane] : 0.0;
-#pragma unroll
-      for (int j = 31; j >= 0; --j) {
-        if (j < nb) {
-          if (lane == j) vi = vi * rdiag;
-          const double xj = __shfl_sync(0xffffffffu, vi, j);
-          if (lcol[j] != 0.0) vi = fma(-lcol[j], xj, vi);
-        }
-      }
-      if (lane < nb) w[jb - j0 + lane] = vi;
-    }
-    __syncthreads();  // this strip's buffer is free
-    if (k + 2 < nstrip) {
-      int jb2, nb2;
-      strip(k + 2, jb2, nb2);
-      tri_strip_async(L, sf, j0, j1, jb2, nb2, sm.buf[k & 1]);
-    }
-  }
+  bwd_block_solve(L, sf, j0, j1, posdef, nrhs, sm);
   for (int r = 0; r < nrhs; ++r) {
     double *w = wk + (int64_t)r * rows_total + roff;
     double *xr = x + (int64_t)r * P.n;
