@@ -1223,6 +1223,38 @@ __global__ void __launch_bounds__(256) k_large_store(DevPlan P, DevFactor X, con
   }
 }
 
+// In-place unit-LDL^T of the nbp x nbp lower block T (the SPD panels'
+// diagonal blocks), all threads of the block: pivot k's reciprocal to
+// linv[k], its multipliers l_kj = t_jk / d_k to lm[k][j], then every entry
+// (i, j), k < j <= i, takes t_ij - t_ik l_kj (skipped for l_kj = 0), and
+// column k scales to t_ik / d_k -- per entry the one-warp loop's operations
+// in its order. Stops at the first pivot that is not positive and finite;
+// returns the pivots taken. Starts and ends at a barrier.
+template <int NB>
+__device__ __forceinline__ int spd_diag_factor(double (*T)[NB + 1], double (*lm)[NB], double *linv, int nbp) {
+  const int t = threadIdx.x;
+  const int ti = t / NB, tj = t % NB;  // threads [0, NB * NB): entry (ti, tj)
+  __syncthreads();
+  int np = 0;
+  for (int k = 0; k < nbp; ++k) {
+    const double d = T[k][k];
+    if (!(d > 0.0 && isfinite(d))) break;
+    const double inv = 1.0 / d;
+    if (t == 0) linv[k] = inv;
+    if (t > k && t < nbp) lm[k][t] = __dmul_rn(T[t][k], inv);
+    __syncthreads();
+    if (t < NB * NB && tj > k && tj <= ti && ti < nbp) {
+      const double l = lm[k][tj];
+      if (l != 0.0) T[ti][tj] = __dsub_rn(T[ti][tj], __dmul_rn(T[ti][k], l));
+    }
+    __syncthreads();
+    if (t > k && t < nbp) T[t][k] = __dmul_rn(T[t][k], inv);
+    __syncthreads();
+    ++np;
+  }
+  return np;
+}
+
 // Two SPD panels per launch (32 pivots, then one rank-32 deferred update:
 // half the launches and half the deferred traffic of one panel at a time).
 // Per entry the operations and their order are the one-panel path's: the
@@ -1243,7 +1275,7 @@ __global__ void __launch_bounds__(256) k_large_panel_spd2(DevPlan P, DevFactor X
   __shared__ double lm[NB][NB], lm2[NB][NB];
   __shared__ double linv[NB], linv2[NB];
   __shared__ double Wr[NB][NB], Lr[NB][NB];  // [row of panel 2][pivot of panel 1]
-  __shared__ int np_sh, np2_sh;
+  __shared__ int np2_sh;
   if (X.counters[kCFlags] & kFAbort) return;
   const int q = blockIdx.y;
   const int s = large[q];
@@ -1269,37 +1301,12 @@ __global__ void __launch_bounds__(256) k_large_panel_spd2(DevPlan P, DevFactor X
   const int wpar = w2 ? (iter & 1) : 0;
   double *W = F + sf * sf + (size_t)wpar * 2 * NB * sf;
   const double eff_small = __longlong_as_double((long long)X.counters[kCEffSmall]);
-  const int lane = threadIdx.x & 31;
   // panel 1's diagonal block
   for (int t = threadIdx.x; t < NB * NB; t += 256) {
     const int r = t / NB, c = t % NB;
     T[r][c] = (r < nbp && c <= r) ? F[(size_t)(ps + c) * sf + ps + r] : 0.0;
   }
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    int np = 0;
-    for (int k = 0; k < nbp; ++k) {
-      const double d = T[k][k];
-      if (!(d > 0.0 && isfinite(d))) break;
-      const double inv = 1.0 / d;
-      if (lane == 0) linv[k] = inv;
-      if (lane > k && lane < nbp) lm[k][lane] = __dmul_rn(T[lane][k], inv);
-      __syncwarp();
-      if (lane > k && lane < nbp) {
-        const double tik = T[lane][k];
-        for (int j = k + 1; j <= lane; ++j) {
-          const double l = lm[k][j];
-          if (l != 0.0) T[lane][j] = __dsub_rn(T[lane][j], __dmul_rn(tik, l));
-        }
-        T[lane][k] = __dmul_rn(tik, inv);
-      }
-      __syncwarp();
-      ++np;
-    }
-    if (lane == 0) np_sh = np;
-  }
-  __syncthreads();
-  const int np1 = np_sh;
+  const int np1 = spd_diag_factor<NB>(T, lm, linv, nbp);
   const bool two = np1 == NB && nbp == NB && nbp2 > 0;
   if (two) {
     // panel 1's pivots on panel 2's rows (threads 0..15: one row each)
@@ -1340,34 +1347,11 @@ __global__ void __launch_bounds__(256) k_large_panel_spd2(DevPlan P, DevFactor X
         T2[r][c] = v;
       }
     }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      int np = 0;
-      for (int k = 0; k < nbp2; ++k) {
-        const double d = T2[k][k];
-        if (!(d > 0.0 && isfinite(d))) break;
-        const double inv = 1.0 / d;
-        if (lane == 0) linv2[k] = inv;
-        if (lane > k && lane < nbp2) lm2[k][lane] = __dmul_rn(T2[lane][k], inv);
-        __syncwarp();
-        if (lane > k && lane < nbp2) {
-          const double tik = T2[lane][k];
-          for (int j = k + 1; j <= lane; ++j) {
-            const double l = lm2[k][j];
-            if (l != 0.0) T2[lane][j] = __dsub_rn(T2[lane][j], __dmul_rn(tik, l));
-          }
-          T2[lane][k] = __dmul_rn(tik, inv);
-        }
-        __syncwarp();
-        ++np;
-      }
-      if (lane == 0) np2_sh = np;
-    }
-  } else if (threadIdx.x == 0) {
-    np2_sh = 0;
+    const int n2 = spd_diag_factor<NB>(T2, lm2, linv2, nbp2);
+    if (threadIdx.x == 0) np2_sh = n2;
   }
   __syncthreads();
-  const int np2 = np2_sh;
+  const int np2 = two ? np2_sh : 0;
   const int i = r0 + threadIdx.x;
   if (i < f) {
     double a[NB];
