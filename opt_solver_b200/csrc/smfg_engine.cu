@@ -711,7 +711,8 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
     const int lo = pl.lvl_ptr[l], hi = pl.lvl_ptr[l + 1], m = hi - lo;
     k_level_setup<1024><<<1, 1024, 0, st>>>(d, x, lo, hi, l, wcols);
     k_level_rows<<<m, 128, 0, st>>>(d, x, lo, hi);
-    const int asm_grid = std::max(1, std::min(4 * sms, m * 64));
+    // 32-column work items: a level of a few large fronts has hundreds
+    const int asm_grid = 4 * sms;
     k_level_assemble<<<asm_grid, 256, 0, st>>>(d, x, lo, hi, l);
     k_factor<32, 1, 32, true><<<m, 32, smem_s32, st>>>(d, x, lo, hi, prm);
     k_factor<32, 33, 48, true><<<m, 32, smem_s48, st>>>(d, x, lo, hi, prm);

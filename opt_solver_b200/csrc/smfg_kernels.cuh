@@ -234,12 +234,11 @@ __global__ void k_level_assemble(DevPlan P, DevFactor X, int lo, int hi, int lvl
     const int j1 = min(j0 + kAsmCols, f);
     double *F = X.arena + X.sn_off[s];
     const size_t sf = (size_t)f;
-    // (the loops below run over (column, row) pairs of the item, so small
-    // fronts keep every thread busy)
-    // 1. zero the lower part of columns [j0, j1)
-    for (int t = threadIdx.x; t < (j1 - j0) * f; t += blockDim.x) {
-      const int jj = j0 + t / f, i = t % f;
-      if (i >= jj) F[jj * sf + i] = 0.0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    // 1. zero the lower part of columns [j0, j1): a warp per column
+    for (int jj = j0 + warp; jj < j1; jj += nwarp) {
+      double *Fj = F + jj * sf;
+      for (int i = jj + lane; i < f; i += 32) Fj[i] = 0.0;
     }
     __syncthreads();
     // 2. original entries of the pivot columns in [j0, j1): their slots are
@@ -282,37 +281,36 @@ __global__ void k_level_assemble(DevPlan P, DevFactor X, int lo, int hi, int lvl
       const int ja = rng[0], jb = rng[1];
       const double *Fc = X.arena + X.sn_off[c];
       const size_t sfc = (size_t)fc;
-      // (column, row) pairs of the child's block, four a thread in flight;
-      // its targets are distinct
-      const int np2 = (jb - ja) * q;
-      for (int t0 = threadIdx.x; t0 < np2; t0 += 4 * (int)blockDim.x) {
-        double sv[4], dv[4];
-        size_t di[4];
-        bool ok[4];
+      // the child's block columns [ja, jb): a warp per column, lanes over
+      // its rows (contiguous in the child, increasing in the parent), four a
+      // lane in flight; its targets are distinct
+      for (int jj = ja + warp; jj < jb; jj += nwarp) {
+        const int lj = cmap[jj];
+        const double *Fcj = Fc + (size_t)(pc + jj) * sfc + pc;
+        double *Fj = F + (size_t)lj * sf;
+        for (int i0 = jj + lane; i0 < q; i0 += 4 * 32) {
+          double sv[4], dv[4];
+          int li[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int t = t0 + u * (int)blockDim.x;
-          ok[u] = false;
-          di[u] = 0;
-          sv[u] = dv[u] = 0.0;
-          if (t < np2) {
-            const int jj = ja + t / q, ii = t % q;
-            if (ii >= jj) {
-              const int lj = cmap[jj], li = cmap[ii];
-              if (li < lj) {
+          for (int u = 0; u < 4; ++u) {
+            const int ii = i0 + 32 * u;
+            li[u] = -1;
+            sv[u] = dv[u] = 0.0;
+            if (ii < q) {
+              li[u] = cmap[ii];
+              if (li[u] < lj) {
                 set_flag(cnt, kFMap);
+                li[u] = -1;
               } else {
-                ok[u] = true;
-                di[u] = (size_t)lj * sf + li;
-                sv[u] = Fc[(size_t)(pc + jj) * sfc + pc + ii];
-                dv[u] = F[di[u]];
+                sv[u] = Fcj[ii];
+                dv[u] = Fj[li[u]];
               }
             }
           }
-        }
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
-          if (ok[u]) F[di[u]] = dv[u] + sv[u];
+          for (int u = 0; u < 4; ++u)
+            if (li[u] >= 0) Fj[li[u]] = dv[u] + sv[u];
+        }
       }
       __syncthreads();
     }
