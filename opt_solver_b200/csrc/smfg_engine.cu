@@ -718,8 +718,15 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
     k_factor<32, 33, 48, true><<<m, 32, smem_s48, st>>>(d, x, lo, hi, prm);
     k_factor<32, 49, 56, true><<<m, 32, smem_s56, st>>>(d, x, lo, hi, prm);
     k_factor<32, 57, kSmallMax, true><<<m, 32, smem_s64, st>>>(d, x, lo, hi, prm);
-    k_factor<128, kSmallMax + 1, 96, true><<<m, 128, smem_m96, st>>>(d, x, lo, hi, prm);
-    k_factor<128, 97, kMediumMax, true><<<m, 128, smem_m128, st>>>(d, x, lo, hi, prm);
+    // SPD fronts of 65..128 rows take their updates with four times the
+    // threads (per entry the same operations in the same order)
+    if (c.posdef) {
+      k_factor<512, kSmallMax + 1, 96, true><<<m, 512, smem_m96, st>>>(d, x, lo, hi, prm);
+      k_factor<512, 97, kMediumMax, true><<<m, 512, smem_m128, st>>>(d, x, lo, hi, prm);
+    } else {
+      k_factor<128, kSmallMax + 1, 96, true><<<m, 128, smem_m96, st>>>(d, x, lo, hi, prm);
+      k_factor<128, 97, kMediumMax, true><<<m, 128, smem_m128, st>>>(d, x, lo, hi, prm);
+    }
     k_factor<512, kMediumMax + 1, 1 << 30, false><<<m, 512, 0, st>>>(d, x, lo, hi, prm);
     lc.n += 10;
     const int nL = pl.lvl_large_ptr[l + 1] - pl.lvl_large_ptr[l];
@@ -873,6 +880,10 @@ static void set_kernel_attrs(int nb) {
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_smem_bytes(96, nb)));
   SMFG_CUDA(cudaFuncSetAttribute(k_factor<128, 97, kMediumMax, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)front_smem_bytes(kMediumMax, nb)));
+  SMFG_CUDA(cudaFuncSetAttribute(k_factor<512, 97, kMediumMax, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)front_smem_bytes(kMediumMax, nb)));
+  SMFG_CUDA(cudaFuncSetAttribute(k_factor<512, kSmallMax + 1, 96, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)front_smem_bytes(96, nb)));
   SMFG_CUDA(cudaFuncSetAttribute(k_large_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TileSmem)));
   SMFG_CUDA(cudaFuncSetAttribute(tc::k_tc_syrk<tc::kTF32x3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)sizeof(tc::Smem)));

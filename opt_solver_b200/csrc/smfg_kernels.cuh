@@ -326,6 +326,109 @@ __device__ void store_front(DevPlan &P, DevFactor &X, int s, const FrontRef &v, 
 // Fronts of at least this many symbolic rows take the multi-block path.
 constexpr int kLargeMin = 384;
 
+// In-place unit-LDL^T of the nbp x nbp lower block T (the SPD panels'
+// diagonal blocks), all threads of the block: pivot k's reciprocal to
+// linv[k], its multipliers l_kj = t_jk / d_k to lm[k][j], then every entry
+// (i, j), k < j <= i, takes t_ij - t_ik l_kj (skipped for l_kj = 0), and
+// column k scales to t_ik / d_k -- per entry the one-warp loop's operations
+// in its order. Stops at the first pivot that is not positive and finite;
+// returns the pivots taken. Starts and ends at a barrier.
+template <int NB, int NT = 256>
+__device__ __forceinline__ int spd_diag_factor(double (*T)[NB + 1], double (*lm)[NB], double *linv, int nbp) {
+  const int t = threadIdx.x;
+  __syncthreads();
+  int np = 0;
+  for (int k = 0; k < nbp; ++k) {
+    const double d = T[k][k];
+    if (!(d > 0.0 && isfinite(d))) break;
+    const double inv = 1.0 / d;
+    if (t == 0) linv[k] = inv;
+    if (t > k && t < nbp) lm[k][t] = __dmul_rn(T[t][k], inv);
+    __syncthreads();
+    for (int e = t; e < NB * NB; e += NT) {
+      const int ti = e / NB, tj = e % NB;
+      if (tj > k && tj <= ti && ti < nbp) {
+        const double l = lm[k][tj];
+        if (l != 0.0) T[ti][tj] = __dsub_rn(T[ti][tj], __dmul_rn(T[ti][k], l));
+      }
+    }
+    __syncthreads();
+    if (t > k && t < nbp) T[t][k] = __dmul_rn(T[t][k], inv);
+    __syncthreads();
+    ++np;
+  }
+  return np;
+}
+
+// SPD fronts of the blocked size classes (nb = 16, at least
+// blocked_min_front rows) in their one block of threads: the medium
+// kernel's pivoting steps (tpp_step_blk, one pivot at a time) replaced by
+// the large fronts' panel arithmetic. Panels of 16 pivots: the diagonal
+// block factored by all threads (spd_diag_factor), every row of the
+// panel's columns by one thread (the multiply-subtract chain of
+// k_large_panel_spd2's rows, w kept in W), then the medium kernel's own
+// deferred update of the eligible columns and, at the end, its Schur update
+// of the contribution block. A pivot that is not positive ends the
+// pivoting. Returns the pivots taken.
+template <int NT>
+__device__ int spd_front_panels(FrontRef &v, const PivotParams &prm, FrontShared &sh) {
+  constexpr int NB = 16;
+  __shared__ double T[NB][NB + 1], lm[NB][NB], linv[NB];
+  const int f = v.f, ne = v.ne;
+  const size_t sf = (size_t)v.ld;
+  double *F = v.F, *W = v.W;  // W row q (f doubles): w of the panel's pivot q
+  int p = 0;
+  for (int ps = 0; ps < ne; ps += NB) {
+    const int pe = min(ne, ps + NB), nbp = pe - ps;
+    for (int t = threadIdx.x; t < NB * NB; t += NT) {
+      const int r = t / NB, c = t % NB;
+      T[r][c] = (r < nbp && c <= r) ? F[(size_t)(ps + c) * sf + ps + r] : 0.0;
+    }
+    const int np = spd_diag_factor<NB, NT>(T, lm, linv, nbp);
+    for (int i = ps + threadIdx.x; i < f; i += NT) {
+      double a[NB];
+#pragma unroll
+      for (int c = 0; c < NB; ++c) a[c] = (c < nbp && ps + c <= i) ? F[(size_t)(ps + c) * sf + i] : 0.0;
+#pragma unroll
+      for (int k = 0; k < NB; ++k) {
+        if (k < np && i > ps + k) {
+          const double w = a[k];
+          W[(size_t)k * sf + i] = w;
+#pragma unroll
+          for (int j = k + 1; j < NB; ++j) {
+            if (j < nbp && ps + j <= i) {
+              const double l = lm[k][j];
+              if (l != 0.0) a[j] = __dsub_rn(a[j], __dmul_rn(w, l));
+            }
+          }
+          a[k] = __dmul_rn(w, linv[k]);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < NB; ++c)
+        if (c < nbp && ps + c <= i) F[(size_t)(ps + c) * sf + i] = a[c];
+    }
+    if (threadIdx.x == 0) {
+      for (int k = 0; k < np; ++k) {
+        v.tags[ps + k] = 1;
+        inertia_1x1(T[k][k], prm.eff_small, sh.st);
+        const double rem = (double)(f - (ps + k + 1));
+        sh.st.flops += rem + rem * (rem + 1.0);
+      }
+    }
+    p = ps + np;
+    __syncthreads();
+    if (np < nbp) break;
+    // the eligible columns past the panel, every row below: the medium
+    // kernel's deferred update
+    deferred_update_blk<NT>(v, ps, pe, pe, ne);
+  }
+  // the contribution block: its Schur update over every pivot, as the
+  // medium kernel takes it
+  schur_update_blk<NT>(v, 0, p, ne);
+  return p;
+}
+
 // Front factorization + store (process_front's kernel call and D handling,
 // multifrontal_serial.cpp:790-945): one block per front of the size class
 // [FMIN, FMAX]; SMEM: the front is copied into shared memory.
@@ -377,7 +480,8 @@ __device__ void factor_one_front(DevPlan &P, DevFactor &X, int s, const PivotPar
   }
   if (threadIdx.x == 0) sh.st = FrontStats{0, 0, 0, 0, 0.0};
   __syncthreads();
-  const int p = ldlt_factor_front_blk<NT>(v, prm, sh);
+  const bool spd_panels = prm.posdef && nb == 16 && f >= prm0.blocked_min_front && NT >= 128;
+  const int p = spd_panels ? spd_front_panels<NT>(v, prm, sh) : ldlt_factor_front_blk<NT>(v, prm, sh);
   store_front<NT, SMEM>(P, X, s, v, p, prm, sh, inv, Fg, rows_g, tags_g);
 }
 
@@ -1219,38 +1323,6 @@ __global__ void __launch_bounds__(256) k_large_store(DevPlan P, DevFactor X, con
     }
     __syncthreads();
   }
-}
-
-// In-place unit-LDL^T of the nbp x nbp lower block T (the SPD panels'
-// diagonal blocks), all threads of the block: pivot k's reciprocal to
-// linv[k], its multipliers l_kj = t_jk / d_k to lm[k][j], then every entry
-// (i, j), k < j <= i, takes t_ij - t_ik l_kj (skipped for l_kj = 0), and
-// column k scales to t_ik / d_k -- per entry the one-warp loop's operations
-// in its order. Stops at the first pivot that is not positive and finite;
-// returns the pivots taken. Starts and ends at a barrier.
-template <int NB>
-__device__ __forceinline__ int spd_diag_factor(double (*T)[NB + 1], double (*lm)[NB], double *linv, int nbp) {
-  const int t = threadIdx.x;
-  const int ti = t / NB, tj = t % NB;  // threads [0, NB * NB): entry (ti, tj)
-  __syncthreads();
-  int np = 0;
-  for (int k = 0; k < nbp; ++k) {
-    const double d = T[k][k];
-    if (!(d > 0.0 && isfinite(d))) break;
-    const double inv = 1.0 / d;
-    if (t == 0) linv[k] = inv;
-    if (t > k && t < nbp) lm[k][t] = __dmul_rn(T[t][k], inv);
-    __syncthreads();
-    if (t < NB * NB && tj > k && tj <= ti && ti < nbp) {
-      const double l = lm[k][tj];
-      if (l != 0.0) T[ti][tj] = __dsub_rn(T[ti][tj], __dmul_rn(T[ti][k], l));
-    }
-    __syncthreads();
-    if (t > k && t < nbp) T[t][k] = __dmul_rn(T[t][k], inv);
-    __syncthreads();
-    ++np;
-  }
-  return np;
 }
 
 // Two SPD panels per launch (32 pivots, then one rank-32 deferred update:
