@@ -113,7 +113,8 @@ typedef struct {
                              unusable), multifrontal_serial.cpp:1619-1628 */
   const double *scale;    /* optional S (length n, original numbering), NULL = none */
   int profile;            /* 1: time the large-front update kernels (info.reserved_d[0..1]) */
-  /* SMFG_PREC_MIXED: large fronts of at least mixed_min_front rows (0: 384)
+  /* SMFG_PREC_MIXED: large fronts of at least mixed_min_front rows (0: 1024
+   * for an SPD factorization, 384 for an indefinite one)
    * that smfg_set_front_precision allows are factored in outer blocks of
    * mixed_block pivots (0: 256; a multiple of 64): the threshold-pivoting
    * panels stay FP64 and the columns past each block get one tensor-core
@@ -295,7 +296,7 @@ SMFG_API int smfg_refine(smfg_plan_t plan, const double *b, double *x, int nrhs,
  * classical x += M^-1 r; right-preconditioned FGMRES(restart) with the
  * factor as preconditioner (refinement.cpp:451-643); auto = classical,
  * escalating to FGMRES when a step contracts the gate measure by less than
- * 0.5. Gate: eta_inf <= 1e-10 and omega <= omega_target; at most max_iters
+ * 0.5 (on a factor with mixed-precision fronts auto is FGMRES). Gate: eta_inf <= 1e-10 and omega <= omega_target; at most max_iters
  * solves in all; x is left at the best iterate. restart <= 0: 20. */
 #define SMFG_REFINE_CLASSICAL 0
 #define SMFG_REFINE_FGMRES 1

@@ -417,12 +417,21 @@ struct MixedCfg {
   int min_front = kLargeMin;
 };
 
+// Default smallest mixed front of an SPD factorization. SPD fronts below
+// about a thousand rows save little time on the tensor cores, but their
+// split-product error still enters the factor: on the 64^3 operator
+// (TF32x3, outer block 256) mixed fronts from 384 rows factor in 39.5 ms
+// and FGMRES needs three solves to omega <= 1e-12, from 1024 rows 39.8 ms
+// and two solves.
+constexpr int kMixedMinFrontSpd = 1024;
+
 static MixedCfg mixed_cfg(const smfg_control_t &c) {
   MixedCfg m;
   m.on = c.precision == SMFG_PREC_MIXED;
   if (c.mixed_block > 0) m.nbo = std::max(64, (c.mixed_block + 63) / 64 * 64);
   if (c.mixed_kind == SMFG_TC_BF16X3) m.kind = tc::kBF16x3;
   if (c.mixed_min_front > 0) m.min_front = std::max(kLargeMin, c.mixed_min_front);
+  else if (c.posdef) m.min_front = kMixedMinFrontSpd;
   return m;
 }
 
@@ -1958,6 +1967,11 @@ int refine_core(smfg_plan_s *plan, double *db, double *dx, int nrhs, int method,
   double be = 0, bo = 0;
   bool stalled = false;
   int used = 0;
+  // auto on a factor with mixed-precision fronts: FGMRES from the start
+  // (the split products' error makes classical steps contract slowly;
+  // GMRES-based refinement after Carson and Higham, SIAM J. Sci. Comput. 40
+  // (2018) A817-A847); an FP64 factor keeps smf's auto
+  if (method == SMFG_REFINE_AUTO && pl.mixed_count > 0) method = SMFG_REFINE_FGMRES;
   if (method == SMFG_REFINE_CLASSICAL || method == SMFG_REFINE_AUTO)
     used = classical_refine(plan, db, dx, r.p, best.p, nrhs, max_iters, tgt, method == SMFG_REFINE_AUTO,
                             be, bo, stalled);

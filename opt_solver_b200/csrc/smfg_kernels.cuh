@@ -329,12 +329,15 @@ constexpr int kLargeMin = 384;
 // In-place unit-LDL^T of the nbp x nbp lower block T (the SPD panels'
 // diagonal blocks), all threads of the block: pivot k's reciprocal to
 // linv[k], its multipliers l_kj = t_jk / d_k to lm[k][j], then every entry
-// (i, j), k < j <= i, takes t_ij - t_ik l_kj (skipped for l_kj = 0), and
-// column k scales to t_ik / d_k -- per entry the one-warp loop's operations
-// in its order. Stops at the first pivot that is not positive and finite;
-// returns the pivots taken. Starts and ends at a barrier.
+// (i, j), k < j <= i, takes t_ij - t_ik l_kj (skipped for l_kj = 0) -- per
+// entry the one-warp loop's operations in its order. The strictly lower
+// part keeps the unscaled values (its multipliers are lm; the callers read
+// only the diagonal of T afterwards). Stops at the first pivot that is not
+// positive and finite; returns the pivots taken. Starts and ends at a
+// barrier. `zero` (shared, optional) is set to 1 when a multiplier is zero.
 template <int NB, int NT = 256>
-__device__ __forceinline__ int spd_diag_factor(double (*T)[NB + 1], double (*lm)[NB], double *linv, int nbp) {
+__device__ __forceinline__ int spd_diag_factor(double (*T)[NB + 1], double (*lm)[NB], double *linv, int nbp,
+                                               int *zero = nullptr) {
   const int t = threadIdx.x;
   __syncthreads();
   int np = 0;
@@ -343,7 +346,11 @@ __device__ __forceinline__ int spd_diag_factor(double (*T)[NB + 1], double (*lm)
     if (!(d > 0.0 && isfinite(d))) break;
     const double inv = 1.0 / d;
     if (t == 0) linv[k] = inv;
-    if (t > k && t < nbp) lm[k][t] = __dmul_rn(T[t][k], inv);
+    if (t > k && t < nbp) {
+      const double l = __dmul_rn(T[t][k], inv);
+      lm[k][t] = l;
+      if (zero && l == 0.0) *zero = 1;
+    }
     __syncthreads();
     for (int e = t; e < NB * NB; e += NT) {
       const int ti = e / NB, tj = e % NB;
@@ -352,8 +359,6 @@ __device__ __forceinline__ int spd_diag_factor(double (*T)[NB + 1], double (*lm)
         if (l != 0.0) T[ti][tj] = __dsub_rn(T[ti][tj], __dmul_rn(T[ti][k], l));
       }
     }
-    __syncthreads();
-    if (t > k && t < nbp) T[t][k] = __dmul_rn(T[t][k], inv);
     __syncthreads();
     ++np;
   }
@@ -1345,7 +1350,7 @@ __global__ void __launch_bounds__(256) k_large_panel_spd2(DevPlan P, DevFactor X
   __shared__ double lm[NB][NB], lm2[NB][NB];
   __shared__ double linv[NB], linv2[NB];
   __shared__ double Wr[NB][NB], Lr[NB][NB];  // [row of panel 2][pivot of panel 1]
-  __shared__ int np2_sh;
+  __shared__ int np2_sh, zero_sh;
   if (X.counters[kCFlags] & kFAbort) return;
   const int q = blockIdx.y;
   const int s = large[q];
@@ -1371,76 +1376,148 @@ __global__ void __launch_bounds__(256) k_large_panel_spd2(DevPlan P, DevFactor X
   const int wpar = w2 ? (iter & 1) : 0;
   double *W = F + sf * sf + (size_t)wpar * 2 * NB * sf;
   const double eff_small = __longlong_as_double((long long)X.counters[kCEffSmall]);
-  // panel 1's diagonal block
-  for (int t = threadIdx.x; t < NB * NB; t += 256) {
-    const int r = t / NB, c = t % NB;
-    T[r][c] = (r < nbp && c <= r) ? F[(size_t)(ps + c) * sf + ps + r] : 0.0;
+  // Every load of F this thread needs is issued here, so that their
+  // latency overlaps the two diagonal factors: none of these entries is
+  // written in this launch before it is read (the panels' diagonal rows are
+  // staged in W, and each row below belongs to one thread, which writes
+  // panel 1's columns only after reading panel 2's).
+  const int i = r0 + threadIdx.x;
+  static_assert(NB * NB == 256, "one entry of T and T2 per thread");
+  const int tr = threadIdx.x / NB, tc = threadIdx.x % NB;
+  const double t1v = (tr < nbp && tc <= tr) ? F[(size_t)(ps + tc) * sf + ps + tr] : 0.0;
+  const double t2v = (tr < nbp2 && tc <= tr) ? F[(size_t)(ps2 + tc) * sf + ps2 + tr] : 0.0;
+  double ra[NB], rb[NB], wa[NB];
+#pragma unroll
+  for (int c = 0; c < NB; ++c) {
+    ra[c] = (i < f && c < nbp && ps + c <= i) ? F[(size_t)(ps + c) * sf + i] : 0.0;
+    rb[c] = (i < f && c < nbp2 && ps2 + c <= i) ? F[(size_t)(ps2 + c) * sf + i] : 0.0;
+    wa[c] = (threadIdx.x < nbp2 && nbp == NB) ? F[(size_t)(ps + c) * sf + ps2 + threadIdx.x] : 0.0;
   }
-  const int np1 = spd_diag_factor<NB>(T, lm, linv, nbp);
+  // panel 1's diagonal block
+  T[tr][tc] = t1v;
+  if (threadIdx.x == 0) zero_sh = 0;
+  const int np1 = spd_diag_factor<NB>(T, lm, linv, nbp, &zero_sh);
   const bool two = np1 == NB && nbp == NB && nbp2 > 0;
   if (two) {
     // panel 1's pivots on panel 2's rows (threads 0..15: one row each)
     if (threadIdx.x < nbp2) {
-      const int i = ps2 + threadIdx.x;
       double a[NB];
 #pragma unroll
-      for (int c = 0; c < NB; ++c) a[c] = F[(size_t)(ps + c) * sf + i];
+      for (int c = 0; c < NB; ++c) a[c] = wa[c];
+      bool zw = false;
 #pragma unroll
       for (int k = 0; k < NB; ++k) {
         const double w = a[k];
         Wr[threadIdx.x][k] = w;
+        zw = zw || w == 0.0;
 #pragma unroll
         for (int j = k + 1; j < NB; ++j) {
           const double l = lm[k][j];
-          if (l != 0.0) a[j] = __dsub_rn(a[j], __dmul_rn(w, l));
+          const double u = __dsub_rn(a[j], __dmul_rn(w, l));
+          a[j] = l != 0.0 ? u : a[j];
         }
         a[k] = __dmul_rn(w, linv[k]);
         Lr[threadIdx.x][k] = a[k];
       }
+      if (zw) zero_sh = 1;
     }
     // panel 2's diagonal block, panel 1's update applied as the deferred
     // update applies it
-    for (int t = threadIdx.x; t < NB * NB; t += 256) {
-      const int r = t / NB, c = t % NB;
-      T2[r][c] = (r < nbp2 && c <= r) ? F[(size_t)(ps2 + c) * sf + ps2 + r] : 0.0;
-    }
     __syncthreads();
-    for (int t = threadIdx.x; t < NB * NB; t += 256) {
-      const int r = t / NB, c = t % NB;
-      if (r < nbp2 && c <= r) {
-        double v = T2[r][c];
+    if (tr < nbp2 && tc <= tr) {
+      double v = t2v;
 #pragma unroll
-        for (int p = 0; p < NB; ++p) {
-          const double bw = Wr[c][p];
-          if (bw != 0.0) v = fma(-Lr[r][p], bw, v);
-        }
-        T2[r][c] = v;
+      for (int p = 0; p < NB; ++p) {
+        const double bw = Wr[tc][p];
+        const double u = fma(-Lr[tr][p], bw, v);
+        v = bw != 0.0 ? u : v;
       }
+      T2[tr][tc] = v;
+    } else {
+      T2[tr][tc] = 0.0;
     }
-    const int n2 = spd_diag_factor<NB>(T2, lm2, linv2, nbp2);
+    const int n2 = spd_diag_factor<NB>(T2, lm2, linv2, nbp2, &zero_sh);
     if (threadIdx.x == 0) np2_sh = n2;
   }
   __syncthreads();
   const int np2 = two ? np2_sh : 0;
-  const int i = r0 + threadIdx.x;
-  if (i < f) {
+  // warps whose rows all lie past the panels' diagonal blocks, with every
+  // pivot taken and no zero multiplier or w: each entry takes every update
+  // (no tests), the same operations in the same order
+  const bool fast = zero_sh == 0 && nbp == NB && np1 == NB && (!two || (nbp2 == NB && np2 == NB)) &&
+                    r0 + (int)(threadIdx.x & ~31u) >= (two ? pl2 : pl);
+  if (fast && i < f) {
     double a[NB];
 #pragma unroll
-    for (int c = 0; c < NB; ++c) a[c] = (c < nbp && ps + c <= i) ? F[(size_t)(ps + c) * sf + i] : 0.0;
+    for (int c = 0; c < NB; ++c) a[c] = ra[c];
 #pragma unroll
     for (int k = 0; k < NB; ++k) {
-      if (k < np1 && i > ps + k) {
-        const double w = a[k];
-        W[(size_t)k * f + i] = w;
+      const double w = a[k];
+      W[(size_t)k * f + i] = w;
 #pragma unroll
-        for (int j = k + 1; j < NB; ++j) {
-          if (j < nbp && ps + j <= i) {
-            const double l = lm[k][j];
-            if (l != 0.0) a[j] = __dsub_rn(a[j], __dmul_rn(w, l));
-          }
-        }
-        a[k] = __dmul_rn(w, linv[k]);
+      for (int j = k + 1; j < NB; ++j) a[j] = __dsub_rn(a[j], __dmul_rn(w, lm[k][j]));
+      a[k] = __dmul_rn(w, linv[k]);
+    }
+#pragma unroll
+    for (int c = 0; c < NB; ++c) F[(size_t)(ps + c) * sf + i] = a[c];
+    if (two) {
+      double b[NB];
+#pragma unroll
+      for (int c = 0; c < NB; ++c) {
+        double v = rb[c];
+#pragma unroll
+        for (int p = 0; p < NB; ++p) v = fma(-a[p], Wr[c][p], v);
+        b[c] = v;
       }
+#pragma unroll
+      for (int k = 0; k < NB; ++k) {
+        const double w = b[k];
+        W[(size_t)(NB + k) * f + i] = w;
+#pragma unroll
+        for (int j = k + 1; j < NB; ++j) b[j] = __dsub_rn(b[j], __dmul_rn(w, lm2[k][j]));
+        b[k] = __dmul_rn(w, linv2[k]);
+      }
+#pragma unroll
+      for (int c = 0; c < NB; ++c) F[(size_t)(ps2 + c) * sf + i] = b[c];
+    }
+  } else if (r0 == ps && i < (two ? pl2 : pl)) {
+    // the panels' diagonal rows (block 0's first rows): the diagonal
+    // factors computed their final values by the same operations -- the
+    // multipliers (lm, Lr, lm2) for the pivots taken, the rest of T and T2
+    // (unscaled, their pivots' updates applied) -- so they are staged from
+    // shared memory
+    const int r = i - ps;
+    if (r < NB) {
+#pragma unroll
+      for (int c = 0; c < NB; ++c)
+        if (c < nbp && c <= r) W[(size_t)c * f + i] = (c < r && c < np1) ? lm[c][r] : T[r][c];
+    } else {
+      const int r2 = r - NB;
+#pragma unroll
+      for (int c = 0; c < NB; ++c) W[(size_t)c * f + i] = Lr[r2][c];
+#pragma unroll
+      for (int c = 0; c < NB; ++c)
+        if (c < nbp2 && c <= r2) W[(size_t)(NB + c) * f + i] = (c < r2 && c < np2) ? lm2[c][r2] : T2[r2][c];
+    }
+  } else if (i < f) {
+    double a[NB];
+#pragma unroll
+    for (int c = 0; c < NB; ++c) a[c] = ra[c];
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+      // (selects, not branches: the multipliers' loads issue ahead of the
+      // chain; an entry skipped keeps its value exactly)
+      const bool take = k < np1 && i > ps + k;
+      const double w = a[k];
+      if (take) W[(size_t)k * f + i] = w;
+#pragma unroll
+      for (int j = k + 1; j < NB; ++j) {
+        const double l = lm[k][j];
+        const double u = __dsub_rn(a[j], __dmul_rn(w, l));
+        a[j] = (take && j < nbp && ps + j <= i && l != 0.0) ? u : a[j];
+      }
+      const double sk = __dmul_rn(w, linv[k]);
+      a[k] = take ? sk : a[k];
     }
     // rows of the panels' diagonal blocks go to W (columns [ps, pend) at
     // W rows c): other blocks read their original values in this launch;
@@ -1460,29 +1537,29 @@ __global__ void __launch_bounds__(256) k_large_panel_spd2(DevPlan P, DevFactor X
       for (int c = 0; c < NB; ++c) {
         b[c] = 0.0;
         if (c < nbp2 && ps2 + c <= i) {
-          double v = F[(size_t)(ps2 + c) * sf + i];
+          double v = rb[c];
 #pragma unroll
           for (int p = 0; p < NB; ++p) {
             const double bw = Wr[c][p];
-            if (bw != 0.0) v = fma(-a[p], bw, v);
+            const double u = fma(-a[p], bw, v);
+            v = bw != 0.0 ? u : v;
           }
           b[c] = v;
         }
       }
 #pragma unroll
       for (int k = 0; k < NB; ++k) {
-        if (k < np2 && i > ps2 + k) {
-          const double w = b[k];
-          W[(size_t)(NB + k) * f + i] = w;
+        const bool take = k < np2 && i > ps2 + k;
+        const double w = b[k];
+        if (take) W[(size_t)(NB + k) * f + i] = w;
 #pragma unroll
-          for (int j = k + 1; j < NB; ++j) {
-            if (j < nbp2 && ps2 + j <= i) {
-              const double l = lm2[k][j];
-              if (l != 0.0) b[j] = __dsub_rn(b[j], __dmul_rn(w, l));
-            }
-          }
-          b[k] = __dmul_rn(w, linv2[k]);
+        for (int j = k + 1; j < NB; ++j) {
+          const double l = lm2[k][j];
+          const double u = __dsub_rn(b[j], __dmul_rn(w, l));
+          b[j] = (take && j < nbp2 && ps2 + j <= i && l != 0.0) ? u : b[j];
         }
+        const double sk = __dmul_rn(w, linv2[k]);
+        b[k] = take ? sk : b[k];
       }
 #pragma unroll
       for (int c = 0; c < NB; ++c)
@@ -1492,21 +1569,34 @@ __global__ void __launch_bounds__(256) k_large_panel_spd2(DevPlan P, DevFactor X
         }
     }
   }
-  if (lead && threadIdx.x == 0) {
+  if (lead && threadIdx.x < 32) {
+    // the pivots' tags, inertia and flops, a lane each (lanes 0..15 panel
+    // 1, 16..31 panel 2): the counts by ballot, the flop terms (integers,
+    // exact in a double, as is every partial sum of a front's) summed by
+    // shuffles -- the same totals as a pivot-by-pivot loop
+    const int lane = threadIdx.x;
+    const bool p1 = lane < np1, p2 = lane >= NB && lane - NB < np2;
+    double dv = 0.0, term = 0.0;
+    if (p1 || p2) {
+      const int col = p1 ? ps + lane : ps2 + lane - NB;
+      X.tags[X.sn_roff[s] + col] = 1;
+      dv = p1 ? T[lane][lane] : T2[lane - NB][lane - NB];
+      const double rem = (double)(f - (col + 1));
+      term = rem + rem * (rem + 1.0);
+    }
+    const bool zr = (p1 || p2) && (!isfinite(dv) || fabs(dv) < eff_small);
+    const bool po = (p1 || p2) && !zr && dv > 0.0;
+    const bool ng = (p1 || p2) && !zr && !(dv > 0.0);
+    const int nzr = __popc(__ballot_sync(0xffffffffu, zr)), npo = __popc(__ballot_sync(0xffffffffu, po)),
+              nng = __popc(__ballot_sync(0xffffffffu, ng));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) term += __shfl_xor_sync(0xffffffffu, term, o);
+    if (lane != 0) return;
     TppState o = S;
-    int8_t *tags = X.tags + X.sn_roff[s];
-    for (int k = 0; k < np1; ++k) {
-      tags[ps + k] = 1;
-      inertia_1x1(T[k][k], eff_small, o.st);
-      const double rem = (double)(f - (ps + k + 1));
-      o.st.flops += rem + rem * (rem + 1.0);
-    }
-    for (int k = 0; k < np2; ++k) {
-      tags[ps2 + k] = 1;
-      inertia_1x1(T2[k][k], eff_small, o.st);
-      const double rem = (double)(f - (ps2 + k + 1));
-      o.st.flops += rem + rem * (rem + 1.0);
-    }
+    o.st.zero += nzr;
+    o.st.pos += npo;
+    o.st.neg += nng;
+    o.st.flops += term;
     const int np = np1 + np2;
     const int pend = two ? pl2 : pl;  // the deferred update starts past the panels done
     o.k = ps + np;

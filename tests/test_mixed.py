@@ -43,7 +43,8 @@ def test_mixed_spd(block, kind):
     sv.factor(v, posdef=True)
     plain = sv.export()
     xp = sv.solve(b)
-    im = sv.factor(v, posdef=True, precision=smfg.PREC_MIXED, mixed_block=block, mixed_kind=kind)
+    im = sv.factor(v, posdef=True, precision=smfg.PREC_MIXED, mixed_block=block, mixed_kind=kind,
+                   mixed_min_front=384)
     assert im.status == 0 and im.mixed_fronts > 0 and im.reserved_d[3] > 0
     assert im.inertia == (n, 0, 0)
     mixed = sv.export()
