@@ -673,6 +673,30 @@ static bool aptp_sweep(Plan &pl, const smfg_control_t &c, const std::vector<int6
   return nf < nL || !compact.empty();
 }
 
+// Room for the inverses of the large fronts' 32 x 32 diagonal blocks (SPD
+// factorizations; the fronts' widths, as SPD fronts take no delays) and
+// the list of blocks k_tri_invert forms, once per plan. Fronts outside the
+// list keep sn_ioff = -1 (their solves take the triangle chains).
+static void ensure_tri_inv(Plan &pl) {
+  if (pl.x.tri_inv || pl.h_lvl_large.empty()) return;
+  std::vector<int64_t> off(pl.nsn, -1);
+  std::vector<int> items;
+  int64_t tot = 0;
+  for (int s : pl.h_lvl_large) {
+    const int nblk = (pl.h_width[s] + 31) / 32;
+    off[s] = tot;
+    for (int b = 0; b < nblk; ++b) {
+      items.push_back(s);
+      items.push_back(b);
+    }
+    tot += (int64_t)nblk * 1024;
+  }
+  pl.x.sn_ioff = dupload(pl, off);
+  pl.x.inv_items = dupload(pl, items);
+  pl.x.inv_nitems = (int)(items.size() / 2);
+  pl.x.tri_inv = dalloc<double>(pl, (size_t)tot);
+}
+
 static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_t &c, LaunchCount &lc,
                            GemmProfile &gp, bool fixed = false) {
   DevPlan &d = pl.d;
@@ -870,12 +894,18 @@ static void enqueue_factor(Plan &pl, const double *d_values, const smfg_control_
       lc.n += 1;
     }
   }
+  // SPD: the large fronts' diagonal blocks inverted for the solves
+  if (c.posdef && x.inv_nitems > 0) {
+    k_tri_invert<<<(x.inv_nitems + kInvWarps - 1) / kInvWarps, 32 * kInvWarps, kInvSmem, st>>>(x);
+    lc.n += 1;
+  }
   SMFG_CUDA(cudaGetLastError());
 }
 
 static void set_kernel_attrs(int nb) {
   static int done_nb = -1;
   if (done_nb == nb) return;
+  SMFG_CUDA(cudaFuncSetAttribute(k_tri_invert, cudaFuncAttributeMaxDynamicSharedMemorySize, kInvSmem));
   // (the with-W sizes: launches ask for at most these)
   SMFG_CUDA(cudaFuncSetAttribute(k_factor<32, 1, 32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)front_smem_bytes(32, nb)));
@@ -939,6 +969,7 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
     }
   }
   SMFG_CUDA(cudaMemcpyAsync(pl.x.sn_mixed, pl.h_mixed.data(), pl.nsn, cudaMemcpyHostToDevice, pl.stream));
+  if (c.posdef) ensure_tri_inv(pl);
   FactorTotals *d_tot = reinterpret_cast<FactorTotals *>(pl.x.counters + kCCount);
   unsigned long long h_cnt[kCCount];
   FactorTotals tot{};
@@ -965,6 +996,7 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
     put(&pl.x.arena_cap, sizeof(int64_t));
     put(&pl.x.rows_cap, sizeof(int64_t));
     put(&pl.x.tc_img, sizeof(pl.x.tc_img));
+    put(&pl.x.tri_inv, sizeof(pl.x.tri_inv));
     if (pl.graph_exec && key == pl.graph_key) {
       if (c.scale)
         SMFG_CUDA(cudaMemcpyAsync(pl.x.scale, c.scale, sizeof(double) * pl.n, cudaMemcpyHostToDevice, pl.stream));
@@ -1037,6 +1069,7 @@ static int run_factor(Plan &pl, const double *d_values, const smfg_control_t &c,
     put(&pl.x.arena_cap, sizeof(int64_t));
     put(&pl.x.rows_cap, sizeof(int64_t));
     put(&pl.x.tc_img, sizeof(pl.x.tc_img));
+    put(&pl.x.tri_inv, sizeof(pl.x.tri_inv));
     if (pl.graph_exec) {
       cudaGraphExecDestroy(pl.graph_exec);
       pl.graph_exec = nullptr;

@@ -73,6 +73,12 @@ struct DevFactor {
   int *tc_njobs = nullptr;
   uint8_t *tc_img = nullptr;     // operand images
   int64_t tc_img_cap = 0;
+  // SPD factorizations: the inverses of the large fronts' 32 x 32 diagonal
+  // blocks of L (column-major, 1024 doubles a block), for the solves
+  double *tri_inv = nullptr;
+  int64_t *sn_ioff = nullptr;    // per supernode: its first block's offset in tri_inv, -1 none
+  int *inv_items = nullptr;      // (supernode, block) pairs, 2 ints each
+  int inv_nitems = 0;
 };
 
 struct Plan {

@@ -344,18 +344,18 @@ __device__ __forceinline__ int spd_diag_factor(double (*T)[NB + 1], double (*lm)
   for (int k = 0; k < nbp; ++k) {
     const double d = T[k][k];
     if (!(d > 0.0 && isfinite(d))) break;
-    const double inv = 1.0 / d;
+    const double inv = __drcp_rn(d);  // 1.0 / d, correctly rounded
     if (t == 0) linv[k] = inv;
-    if (t > k && t < nbp) {
-      const double l = __dmul_rn(T[t][k], inv);
-      lm[k][t] = l;
-      if (zero && l == 0.0) *zero = 1;
-    }
-    __syncthreads();
+    // each entry's thread forms the multiplier it needs itself (column k
+    // is read, not written, in this step): one barrier a pivot
     for (int e = t; e < NB * NB; e += NT) {
       const int ti = e / NB, tj = e % NB;
       if (tj > k && tj <= ti && ti < nbp) {
-        const double l = lm[k][tj];
+        const double l = __dmul_rn(T[tj][k], inv);
+        if (ti == tj) {
+          lm[k][tj] = l;
+          if (zero && l == 0.0) *zero = 1;
+        }
         if (l != 0.0) T[ti][tj] = __dsub_rn(T[ti][tj], __dmul_rn(T[ti][k], l));
       }
     }
@@ -2413,19 +2413,62 @@ struct TriSmem {
   double w[8][kSB];  // the block's values, per right-hand side (at most 8)
 };
 
+// Inverses of the SPD large fronts' 32 x 32 diagonal blocks of L (after
+// the store: L = L_unit sqrt(D)), for the triangle solves: a warp per
+// block, lane c forms column c of the inverse by forward substitution
+// (x_c = 1 / l_cc, x_i = -(sum_{c <= k < i} l_ik x_k) / l_ii, the sum in k
+// order), the result written column-major through shared memory.
+constexpr int kInvWarps = 8;
+constexpr int kInvSmem = kInvWarps * 32 * 33 * (int)sizeof(double);
+__global__ void __launch_bounds__(32 * kInvWarps) k_tri_invert(DevFactor X) {
+  extern __shared__ __align__(16) unsigned char inv_smem[];
+  double(*S)[33] = reinterpret_cast<double(*)[33]>(inv_smem) + (threadIdx.x >> 5) * 32;
+  if (X.counters[kCFlags] & kFAbort) return;
+  const int lane = threadIdx.x & 31;
+  const int item = blockIdx.x * kInvWarps + (threadIdx.x >> 5);
+  if (item >= X.inv_nitems) return;
+  const int s = X.inv_items[2 * item], blk = X.inv_items[2 * item + 1];
+  const int f = X.sn_f[s], p = X.sn_pstore[s];
+  const int jb = 32 * blk, nb = min(32, p - jb);
+  double *out = X.tri_inv + X.sn_ioff[s] + (int64_t)blk * 1024;
+  const double *L = X.arena + X.sn_off[s];
+  // S[i][k] = l_ik (rows of the block, lower part)
+  for (int k = 0; k < 32; ++k) S[lane][k] = (k < nb && lane < nb && lane >= k) ? L[(size_t)(jb + k) * f + jb + lane] : 0.0;
+  __syncwarp();
+  double x[32];
+  const int c = lane;
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < i; ++k) acc = fma(S[i][k], x[k], acc);
+    const double rd = (i < nb) ? 1.0 / S[i][i] : 0.0;
+    x[i] = (i < nb && c < nb && i >= c) ? ((i == c) ? rd : -acc * rd) : 0.0;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < 32; ++i) S[c][i] = x[i];  // S[c][i] = (L^-1)_ic
+  __syncwarp();
+  for (int k = 0; k < 32; ++k) out[k * 32 + lane] = S[k][lane];
+}
+
 // Strip [jb, jb + nb) of the block [j0, j1) (its rows [jb, j1)) into dst by
 // threads [t0, t0 + nt): a warp per column (coalesced rows), one cp.async
 // group.
 __device__ __forceinline__ void tri_strip_async(const double *L, size_t sf, int j0, int j1, int jb, int nb,
-                                                double (*dst)[kSBP], int t0 = 0, int nt = kTriNT) {
+                                                double (*dst)[kSBP], int t0 = 0, int nt = kTriNT,
+                                                const double *inv = nullptr) {
   const int rows = j1 - jb;
   const int lane = threadIdx.x & 31;
   for (int u = ((int)threadIdx.x - t0) >> 5; u < nb; u += nt / 32) {
     const double *src = L + (size_t)(jb + u) * sf + jb;
     const unsigned d = (unsigned)__cvta_generic_to_shared(&dst[u][jb - j0]);
-    for (int rr = lane; rr < rows; rr += 32)
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d + 8u * (unsigned)rr), "l"(src + rr)
-                   : "memory");
+    for (int rr = lane; rr < rows; rr += 32) {
+      // the diagonal block's rows from its inverse (inv: the front's
+      // blocks; jb is a multiple of 32), when there is one
+      const double *sp = (inv && rr < 32) ? inv + (size_t)(jb >> 5) * 1024 + (size_t)u * 32 + rr : src + rr;
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d + 8u * (unsigned)rr), "l"(sp) : "memory");
+    }
   }
   asm volatile("cp.async.commit_group;" ::: "memory");
 }
@@ -2458,20 +2501,22 @@ __device__ __forceinline__ void bwd_strip(int j0, int j1, int k, int &jb, int &n
 
 // Block [j0, j1) of a large front: its first kRing strips of L issued to
 // shared memory (all threads; one cp.async group each).
-__device__ __forceinline__ void fwd_block_issue(const double *L, size_t sf, int j0, int j1, TriSmem &sm) {
+__device__ __forceinline__ void fwd_block_issue(const double *L, size_t sf, int j0, int j1, TriSmem &sm,
+                                                const double *inv) {
   const int nstrip = (j1 - j0 + 31) / 32;
   for (int k = 0; k < min(kRing, nstrip); ++k) {
     int jb, nb;
     fwd_strip(j0, j1, k, jb, nb);
-    tri_strip_async(L, sf, j0, j1, jb, nb, sm.buf[k]);
+    tri_strip_async(L, sf, j0, j1, jb, nb, sm.buf[k], 0, kTriNT, inv);
   }
 }
-__device__ __forceinline__ void bwd_block_issue(const double *L, size_t sf, int j0, int j1, TriSmem &sm) {
+__device__ __forceinline__ void bwd_block_issue(const double *L, size_t sf, int j0, int j1, TriSmem &sm,
+                                                const double *inv) {
   const int nstrip = (j1 - j0 + 31) / 32;
   for (int k = 0; k < min(kRing, nstrip); ++k) {
     int jb, nb;
     bwd_strip(j0, j1, k, jb, nb);
-    tri_strip_async(L, sf, j0, j1, jb, nb, sm.buf[k]);
+    tri_strip_async(L, sf, j0, j1, jb, nb, sm.buf[k], 0, kTriNT, inv);
   }
 }
 
@@ -2482,8 +2527,23 @@ __device__ __forceinline__ void bwd_block_issue(const double *L, size_t sf, int 
 // diagonal's reciprocal taken ahead, so a step of the chain is one shuffle
 // and one fused multiply-add.
 __device__ __forceinline__ double fwd_chain32(const double (*Lb)[kSBP], int j0, int jb, int nb, int posdef,
-                                              double *w, double pre) {
+                                              double *w, double pre, bool use_inv) {
   const int lane = threadIdx.x & 31;
+  if (use_inv) {
+    // the strip's diagonal block holds its inverse: x = L_bb^-1 (w - pre),
+    // lane i's row of the inverse against the lanes' values (four partial
+    // sums, no dependent chain across the lanes)
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    const double r = (lane < nb) ? w[jb - j0 + lane] - pre : 0.0;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const double g = (j <= lane && lane < nb) ? Lb[j][jb - j0 + lane] : 0.0;
+      a[j & 3] = fma(g, __shfl_sync(0xffffffffu, r, j), a[j & 3]);
+    }
+    const double xi = (a[0] + a[1]) + (a[2] + a[3]);
+    if (lane < nb) w[jb - j0 + lane] = xi;
+    return xi;
+  }
   double lrow[32];
 #pragma unroll
   for (int j = 0; j < 32; ++j) lrow[j] = (j < lane && lane < nb) ? Lb[j][jb - j0 + lane] : 0.0;
@@ -2504,8 +2564,21 @@ __device__ __forceinline__ double fwd_chain32(const double (*Lb)[kSBP], int j0, 
 // The backward (transposed) 32 x 32 triangle of strip [jb, jb + nb) for one
 // right-hand side (lane = column jb + lane), `pre` subtracted first.
 __device__ __forceinline__ double bwd_chain32(const double (*Lb)[kSBP], int j0, int jb, int nb, int posdef,
-                                              double *w, double pre) {
+                                              double *w, double pre, bool use_inv) {
   const int lane = threadIdx.x & 31;
+  if (use_inv) {
+    // x = L_bb^-T (w - pre): lane i's column of the inverse
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    const double r = (lane < nb) ? w[jb - j0 + lane] - pre : 0.0;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const double g = (j >= lane && j < nb) ? Lb[lane][jb - j0 + j] : 0.0;
+      a[j & 3] = fma(g, __shfl_sync(0xffffffffu, r, j), a[j & 3]);
+    }
+    const double xi = (a[0] + a[1]) + (a[2] + a[3]);
+    if (lane < nb) w[jb - j0 + lane] = xi;
+    return xi;
+  }
   double lcol[32];
 #pragma unroll
   for (int j = 0; j < 32; ++j) lcol[j] = (j > lane && j < nb) ? Lb[lane][jb - j0 + j] : 0.0;
@@ -2591,7 +2664,8 @@ constexpr int kPipeRhs = 4;
 // takes each strip's product in strip order: the strips up to two before
 // its own from the rows update, the one just before from the chain warp's
 // look-ahead. Ends at a barrier.
-__device__ void fwd_block_solve(const double *L, size_t sf, int j0, int j1, int posdef, int nrhs, TriSmem &sm) {
+__device__ void fwd_block_solve(const double *L, size_t sf, int j0, int j1, int posdef, int nrhs, TriSmem &sm,
+                                const double *inv) {
   const int warp = threadIdx.x >> 5;
   const int nstrip = (j1 - j0 + 31) / 32;
   if (nrhs > kPipeRhs) {
@@ -2603,14 +2677,14 @@ __device__ void fwd_block_solve(const double *L, size_t sf, int j0, int j1, int 
       const double(*Lb)[kSBP] = sm.buf[k % kRing];
       if (k >= kRing) cp_async_wait_pending(min(kRing - 1, nstrip - 1 - k));
       __syncthreads();
-      if (warp < nrhs) fwd_chain32(Lb, j0, jb, nb, posdef, sm.w[warp], 0.0);
+      if (warp < nrhs) fwd_chain32(Lb, j0, jb, nb, posdef, sm.w[warp], 0.0, inv != nullptr);
       __syncthreads();
       fwd_rows_update(Lb, j0, j1, jb, nb, jb + nb, nrhs, sm, (int)threadIdx.x, kTriNT);
       __syncthreads();  // this strip's buffer is free
       if (k + kRing < nstrip) {
         int jb3, nb3;
         fwd_strip(j0, j1, k + kRing, jb3, nb3);
-        tri_strip_async(L, sf, j0, j1, jb3, nb3, sm.buf[k % kRing]);
+        tri_strip_async(L, sf, j0, j1, jb3, nb3, sm.buf[k % kRing], 0, kTriNT, inv);
       }
     }
     __syncthreads();
@@ -2629,7 +2703,7 @@ __device__ void fwd_block_solve(const double *L, size_t sf, int j0, int j1, int 
         int jb, nb;
         fwd_strip(j0, j1, k, jb, nb);
         const double(*Lb)[kSBP] = sm.buf[k % kRing];
-        const double x = fwd_chain32(Lb, j0, jb, nb, posdef, sm.w[warp], la);
+        const double x = fwd_chain32(Lb, j0, jb, nb, posdef, sm.w[warp], la, inv != nullptr);
         la = (k + 1 < nstrip) ? fwd_ahead32(Lb, j0, j1, jb, x) : 0.0;
       }
     } else {
@@ -2642,7 +2716,7 @@ __device__ void fwd_block_solve(const double *L, size_t sf, int j0, int j1, int 
           warps_sync(1, nf);  // every reader of strip k - 1's buffer done
           int jb3, nb3;
           fwd_strip(j0, j1, k - 1 + kRing, jb3, nb3);
-          tri_strip_async(L, sf, j0, j1, jb3, nb3, sm.buf[(k - 1) % kRing], 32 * C, nf);
+          tri_strip_async(L, sf, j0, j1, jb3, nb3, sm.buf[(k - 1) % kRing], 32 * C, nf, inv);
           issued = true;
         }
       }
@@ -2672,12 +2746,14 @@ __global__ void __launch_bounds__(kTriNT) k_fwd_tri(DevPlan P, DevFactor X, cons
   const int *rows = X.rows + roff;
   const double *L = X.arena + X.sn_off[s];
   const size_t sf = (size_t)f;
-  fwd_block_issue(L, sf, j0, j1, sm);
+  // SPD: the diagonal blocks' inverses, when the factorization formed them
+  const double *inv = (posdef && X.tri_inv && X.sn_ioff[s] >= 0) ? X.tri_inv + X.sn_ioff[s] : nullptr;
+  fwd_block_issue(L, sf, j0, j1, sm, inv);
   pdl_wait();  // the strips of L in flight meanwhile
   pdl_trigger();
   for (int r = 0; r < nrhs; ++r)
     for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) sm.w[r][t] = wk[(int64_t)r * rows_total + roff + j0 + t];
-  fwd_block_solve(L, sf, j0, j1, posdef, nrhs, sm);
+  fwd_block_solve(L, sf, j0, j1, posdef, nrhs, sm, inv);
   for (int r = 0; r < nrhs; ++r) {
     double *w = wk + (int64_t)r * rows_total + roff;
     double *xr = x + (int64_t)r * P.n;
@@ -2832,7 +2908,8 @@ __global__ void __launch_bounds__(256) k_bwd_dots(DevPlan P, DevFactor X, const 
 // product with the solved rows of the strips up to m - 2 (one shuffle-tree
 // sum) and then that with strip m - 1's rows (the chain warp's look-ahead).
 // Ends at a barrier.
-__device__ void bwd_block_solve(const double *L, size_t sf, int j0, int j1, int posdef, int nrhs, TriSmem &sm) {
+__device__ void bwd_block_solve(const double *L, size_t sf, int j0, int j1, int posdef, int nrhs, TriSmem &sm,
+                                const double *inv) {
   const int warp = threadIdx.x >> 5;
   const int nstrip = (j1 - j0 + 31) / 32;
   if (nrhs > kPipeRhs) {
@@ -2860,13 +2937,13 @@ __device__ void bwd_block_solve(const double *L, size_t sf, int j0, int j1, int 
           const double xp = (lane < np) ? sm.w[warp][jp - j0 + lane] : 0.0;
           la = bwd_ahead32(Lb, j0, jp, np, xp);
         }
-        bwd_chain32(Lb, j0, jb, nb, posdef, sm.w[warp], la);
+        bwd_chain32(Lb, j0, jb, nb, posdef, sm.w[warp], la, inv != nullptr);
       }
       __syncthreads();  // this strip's buffer is free
       if (k + kRing < nstrip) {
         int jb3, nb3;
         bwd_strip(j0, j1, k + kRing, jb3, nb3);
-        tri_strip_async(L, sf, j0, j1, jb3, nb3, sm.buf[k % kRing]);
+        tri_strip_async(L, sf, j0, j1, jb3, nb3, sm.buf[k % kRing], 0, kTriNT, inv);
       }
     }
     __syncthreads();
@@ -2884,7 +2961,7 @@ __device__ void bwd_block_solve(const double *L, size_t sf, int j0, int j1, int 
     if (warp < C) {
       int jb, nb;
       bwd_strip(j0, j1, k, jb, nb);
-      const double x = bwd_chain32(sm.buf[k % kRing], j0, jb, nb, posdef, sm.w[warp], la);
+      const double x = bwd_chain32(sm.buf[k % kRing], j0, jb, nb, posdef, sm.w[warp], la, inv != nullptr);
       la = 0.0;
       if (k + 1 < nstrip) la = bwd_ahead32(sm.buf[(k + 1) % kRing], j0, jb, nb, x);
     } else {
@@ -2893,7 +2970,7 @@ __device__ void bwd_block_solve(const double *L, size_t sf, int j0, int j1, int 
         // k - 2, the columns update one step before) are done
         int jb3, nb3;
         bwd_strip(j0, j1, k - 1 + kRing, jb3, nb3);
-        tri_strip_async(L, sf, j0, j1, jb3, nb3, sm.buf[(k - 1) % kRing], 32 * C, nf);
+        tri_strip_async(L, sf, j0, j1, jb3, nb3, sm.buf[(k - 1) % kRing], 32 * C, nf, inv);
       }
       if (k >= 1 && k + 1 < nstrip) {
         int jm, nm, j2, n2;
@@ -2925,12 +3002,13 @@ __global__ void __launch_bounds__(kTriNT) k_bwd_tri(DevPlan P, DevFactor X, cons
   const int *rows = X.rows + roff;
   const double *L = X.arena + X.sn_off[s];
   const size_t sf = (size_t)f;
-  bwd_block_issue(L, sf, j0, j1, sm);
+  const double *inv = (posdef && X.tri_inv && X.sn_ioff[s] >= 0) ? X.tri_inv + X.sn_ioff[s] : nullptr;
+  bwd_block_issue(L, sf, j0, j1, sm, inv);
   pdl_wait();  // the strips of L in flight meanwhile
   pdl_trigger();
   for (int r = 0; r < nrhs; ++r)
     for (int t = threadIdx.x; t < j1 - j0; t += kTriNT) sm.w[r][t] = wk[(int64_t)r * rows_total + roff + j0 + t];
-  bwd_block_solve(L, sf, j0, j1, posdef, nrhs, sm);
+  bwd_block_solve(L, sf, j0, j1, posdef, nrhs, sm, inv);
   for (int r = 0; r < nrhs; ++r) {
     double *w = wk + (int64_t)r * rows_total + roff;
     double *xr = x + (int64_t)r * P.n;
