@@ -1843,9 +1843,13 @@ __device__ __forceinline__ void tri_fwd_warp(double *w, int jb, int nb, int posd
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     if (j < nb) {
-      if (lane == j) wi = wi * rdiag;
+      // (selects: no divergent branch in the chain; the values as the
+      // branches would leave them)
+      const double sc = wi * rdiag;
+      wi = lane == j ? sc : wi;
       const double wj = __shfl_sync(0xffffffffu, wi, j);
-      if (lrow[j] != 0.0) wi = fma(-lrow[j], wj, wi);
+      const double u = fma(-lrow[j], wj, wi);
+      wi = lrow[j] != 0.0 ? u : wi;
     }
   }
   if (lane < nb) w[jb + lane] = wi;
@@ -1862,9 +1866,11 @@ __device__ __forceinline__ void tri_bwd_warp(double *v, int jb, int nb, int posd
 #pragma unroll
   for (int j = 31; j >= 0; --j) {
     if (j < nb) {
-      if (lane == j) vi = vi * rdiag;
+      const double sc = vi * rdiag;
+      vi = lane == j ? sc : vi;
       const double xj = __shfl_sync(0xffffffffu, vi, j);
-      if (lcol[j] != 0.0) vi = fma(-lcol[j], xj, vi);
+      const double u = fma(-lcol[j], xj, vi);
+      vi = lcol[j] != 0.0 ? u : vi;
     }
   }
   if (lane < nb) v[jb + lane] = vi;
@@ -2066,18 +2072,46 @@ __global__ void __launch_bounds__(kSolveNT, 4) k_fwd_front(DevPlan P, DevFactor 
   // every right-hand side at once: gather, children's update vectors in
   // child order, then per 32-column strip the triangle (a warp per
   // right-hand side) and the rows below (each L entry loaded once for all)
-  for (int64_t t = threadIdx.x; t < (int64_t)f * nrhs; t += kSolveNT) {
-    const int r = (int)(t / f), i = (int)(t % f);
-    wk[(int64_t)r * rows_total + roff + i] = (i < p) ? x[(int64_t)r * P.n + rows[i]] : 0.0;
+  // (four rows a thread in flight: a large front's gather and children's
+  // vectors are thousands of rows for one block)
+  for (int r = 0; r < nrhs; ++r) {
+    double *w = wk + (int64_t)r * rows_total + roff;
+    const double *xr = x + (int64_t)r * P.n;
+    for (int i0 = threadIdx.x; i0 < f; i0 += 4 * kSolveNT) {
+      double v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = i0 + u * kSolveNT;
+        v[u] = (i < p) ? xr[rows[i]] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (i0 + u * kSolveNT < f) w[i0 + u * kSolveNT] = v[u];
+    }
   }
   __syncthreads();
   for (int t = P.child_ptr[s]; t < P.child_ptr[s + 1]; ++t) {
     const int c = P.child_idx[t];
     const int pc = X.sn_pstore[c], q = X.sn_f[c] - pc;
     const int *cmap = X.cbmap + X.sn_roff[c] + pc;
-    for (int64_t u = threadIdx.x; u < (int64_t)q * nrhs; u += kSolveNT) {
-      const int r = (int)(u / q), i = (int)(u % q);
-      wk[(int64_t)r * rows_total + roff + cmap[i]] += wk[(int64_t)r * rows_total + X.sn_roff[c] + pc + i];
+    for (int r = 0; r < nrhs; ++r) {
+      double *w = wk + (int64_t)r * rows_total + roff;
+      const double *wc = wk + (int64_t)r * rows_total + X.sn_roff[c] + pc;
+      for (int i0 = threadIdx.x; i0 < q; i0 += 4 * kSolveNT) {
+        double v[4], o[4];
+        int m[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int i = i0 + u * kSolveNT;
+          m[u] = (i < q) ? cmap[i] : 0;
+          v[u] = (i < q) ? wc[i] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) o[u] = (i0 + u * kSolveNT < q) ? w[m[u]] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (i0 + u * kSolveNT < q) w[m[u]] = o[u] + v[u];
+      }
     }
     __syncthreads();
   }
@@ -2122,8 +2156,8 @@ __global__ void __launch_bounds__(kSolveNT, 4) k_fwd_front(DevPlan P, DevFactor 
     }
   }
   __syncthreads();
-  for (int64_t t = threadIdx.x; t < (int64_t)p * nrhs; t += kSolveNT) {
-    const int r = (int)(t / p), i = (int)(t % p);
+  for (int t = threadIdx.x; t < p * nrhs; t += kSolveNT) {
+    const int r = nrhs == 1 ? 0 : t / p, i = nrhs == 1 ? t : t - r * p;
     x[(int64_t)r * P.n + rows[i]] = wk[(int64_t)r * rows_total + roff + i];
   }
 }
@@ -2268,8 +2302,8 @@ __global__ void __launch_bounds__(kSolveNT) k_bwd_front(DevPlan P, DevFactor X, 
   // every right-hand side at once. D^-1 of each pivot block; 2x2 blocks
   // start where the upper slot (c, c+1) is nonzero. (large: v[0:p) holds
   // L21^T x_ext)
-  for (int64_t t = threadIdx.x; t < (int64_t)p * nrhs; t += kSolveNT) {
-    const int r = (int)(t / p), c = (int)(t % p);
+  for (int t = threadIdx.x; t < p * nrhs; t += kSolveNT) {
+    const int r = nrhs == 1 ? 0 : t / p, c = nrhs == 1 ? t : t - r * p;
     double *v = wk + (int64_t)r * rows_total + roff;
     const double *xr = x + (int64_t)r * P.n;
     const bool second = apply_d && !posdef && (c > 0) && L[(size_t)c * sf + c - 1] != 0.0;
@@ -2318,8 +2352,8 @@ __global__ void __launch_bounds__(kSolveNT) k_bwd_front(DevPlan P, DevFactor X, 
   }
   __syncthreads();
   if (!apply_lt) {
-    for (int64_t t = threadIdx.x; t < (int64_t)p * nrhs; t += kSolveNT) {
-      const int r = (int)(t / p), i = (int)(t % p);
+    for (int t = threadIdx.x; t < p * nrhs; t += kSolveNT) {
+      const int r = nrhs == 1 ? 0 : t / p, i = nrhs == 1 ? t : t - r * p;
       x[(int64_t)r * P.n + rows[i]] = wk[(int64_t)r * rows_total + roff + i];
     }
     return;
@@ -2384,8 +2418,8 @@ __global__ void __launch_bounds__(kSolveNT) k_bwd_front(DevPlan P, DevFactor X, 
     for (int r = warp; r < nrhs; r += kSolveNT / 32) tri_bwd_warp(wk + (int64_t)r * rows_total + roff, jb, nb, posdef, Ls);
     __syncthreads();
   }
-  for (int64_t t = threadIdx.x; t < (int64_t)p * nrhs; t += kSolveNT) {
-    const int r = (int)(t / p), i = (int)(t % p);
+  for (int t = threadIdx.x; t < p * nrhs; t += kSolveNT) {
+    const int r = nrhs == 1 ? 0 : t / p, i = nrhs == 1 ? t : t - r * p;
     x[(int64_t)r * P.n + rows[i]] = wk[(int64_t)r * rows_total + roff + i];
   }
 }
@@ -2473,6 +2507,24 @@ __device__ __forceinline__ void tri_strip_async(const double *L, size_t sf, int 
   asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
+// Columns [c0, c1) of the block ending at j1 (each from its strip's first
+// row: the strips start at multiples of 32) into L2, 128-byte lines, with
+// their strips' inverse blocks when there are any: the strips past the
+// first kRing are copied to shared memory later, from L2 then.
+__device__ __forceinline__ void tri_prefetch_l2(const double *L, size_t sf, int j1, int c0, int c1,
+                                                const double *inv) {
+  constexpr int kLines = 17;  // 128-byte lines a column of at most 256 rows can touch
+  for (int e = threadIdx.x; e < (c1 - c0) * kLines; e += blockDim.x) {
+    const int c = c0 + e / kLines, q = e % kLines, jb = c & ~31;
+    if (jb + 16 * q < j1) asm volatile("prefetch.global.L2 [%0];" ::"l"(L + (size_t)c * sf + jb + 16 * q));
+  }
+  if (inv) {
+    const int b0 = c0 >> 5, b1 = (c1 + 31) >> 5;
+    for (int e = threadIdx.x; e < (b1 - b0) * 64; e += blockDim.x)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(inv + (size_t)(b0 + e / 64) * 1024 + 16 * (e % 64)));
+  }
+}
+
 // wait until at most `pending` (0..2) of this thread's cp.async groups are in flight
 __device__ __forceinline__ void cp_async_wait_pending(int pending) {
   if (pending >= 2) asm volatile("cp.async.wait_group 2;" ::: "memory");
@@ -2552,9 +2604,13 @@ __device__ __forceinline__ double fwd_chain32(const double (*Lb)[kSBP], int j0, 
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     if (j < nb) {
-      if (lane == j) wi = wi * rdiag;
+      // (selects: no divergent branch in the chain; the values as the
+      // branches would leave them)
+      const double sc = wi * rdiag;
+      wi = lane == j ? sc : wi;
       const double wj = __shfl_sync(0xffffffffu, wi, j);
-      if (lrow[j] != 0.0) wi = fma(-lrow[j], wj, wi);
+      const double u = fma(-lrow[j], wj, wi);
+      wi = lrow[j] != 0.0 ? u : wi;
     }
   }
   if (lane < nb) w[jb - j0 + lane] = wi;
@@ -2587,52 +2643,60 @@ __device__ __forceinline__ double bwd_chain32(const double (*Lb)[kSBP], int j0, 
 #pragma unroll
   for (int j = 31; j >= 0; --j) {
     if (j < nb) {
-      if (lane == j) vi = vi * rdiag;
+      const double sc = vi * rdiag;
+      vi = lane == j ? sc : vi;
       const double xj = __shfl_sync(0xffffffffu, vi, j);
-      if (lcol[j] != 0.0) vi = fma(-lcol[j], xj, vi);
+      const double u = fma(-lcol[j], xj, vi);
+      vi = lcol[j] != 0.0 ? u : vi;
     }
   }
   if (lane < nb) w[jb - j0 + lane] = vi;
   return vi;
 }
 
+// A strip's product with one row (forward) or column (backward) is summed
+// in four interleaved fused multiply-add chains (term u into chain u mod 4),
+// then (c0 + c1) + (c2 + c3): the same sum wherever it is formed (the
+// look-ahead, the rows or columns update, either block-solve form).
+__device__ __forceinline__ double sum4(const double (&a)[4]) { return (a[0] + a[1]) + (a[2] + a[3]); }
+
 // Look-ahead products of a solved strip (values x in the lanes of the
-// warp) with the next strip, summed in strip order by one fused
-// multiply-add chain. Forward: rows jn + lane of the next strip over the
-// columns of this one (Lb: this strip's buffer). Backward: columns jn +
+// warp) with the next strip. Forward: rows jn + lane of the next strip over
+// the columns of this one (Lb: this strip's buffer). Backward: columns jn +
 // lane of the next strip over the rows jb.. of this one (Ln: the next
 // strip's buffer).
 __device__ __forceinline__ double fwd_ahead32(const double (*Lb)[kSBP], int j0, int j1, int jb, double x) {
   const int i = jb + 32 + (int)(threadIdx.x & 31);
-  double la = 0.0;
+  double a[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
   for (int u = 0; u < 32; ++u) {
     const double xu = __shfl_sync(0xffffffffu, x, u);
-    if (i < j1) la = fma(Lb[u][i - j0], xu, la);
+    if (i < j1) a[u & 3] = fma(Lb[u][i - j0], xu, a[u & 3]);
   }
-  return la;
+  return sum4(a);
 }
 __device__ __forceinline__ double bwd_ahead32(const double (*Ln)[kSBP], int j0, int jb, int nb, double x) {
   const int lane = threadIdx.x & 31;
-  double la = 0.0;
+  double a[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
   for (int t = 0; t < 32; ++t) {
     const double xt = __shfl_sync(0xffffffffu, x, t);
-    if (t < nb) la = fma(Ln[lane][jb + t - j0], xt, la);
+    if (t < nb) a[t & 3] = fma(Ln[lane][jb + t - j0], xt, a[t & 3]);
   }
-  return la;
+  return sum4(a);
 }
 
-// The block's rows [r0, j1) minus a strip's products (each row its own fused
-// multiply-add chain over the strip's columns, then one subtraction), for
-// rhs 0..nrhs-1; threads [t0, t0 + nt) take rows in turn.
+// The block's rows [r0, j1) minus a strip's products, for rhs
+// 0..nrhs-1; threads [t0, t0 + nt) take rows in turn.
 __device__ __forceinline__ void fwd_rows_update(const double (*Lb)[kSBP], int j0, int j1, int jb, int nb, int r0,
                                                 int nrhs, TriSmem &sm, int t, int nt) {
   for (int i = r0 + t; i < j1; i += nt) {
     for (int r = 0; r < nrhs; ++r) {
-      double acc = 0.0;
-      for (int u = 0; u < nb; ++u) acc = fma(Lb[u][i - j0], sm.w[r][jb - j0 + u], acc);
-      sm.w[r][i - j0] -= acc;
+      double a[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int u = 0; u < 32; ++u)
+        if (u < nb) a[u & 3] = fma(Lb[u][i - j0], sm.w[r][jb - j0 + u], a[u & 3]);
+      sm.w[r][i - j0] -= sum4(a);
     }
   }
 }
@@ -2643,12 +2707,27 @@ __device__ __forceinline__ void fwd_rows_update(const double (*Lb)[kSBP], int j0
 __device__ __forceinline__ void bwd_cols_update(const double (*L2)[kSBP], int j0, int j1, int j2, int n2, int r0,
                                                 int nrhs, TriSmem &sm, int w0, int nw) {
   const int lane = threadIdx.x & 31;
-  for (int u = w0; u < n2; u += nw) {
+  // four of the warp's columns at a time: their chains and shuffle trees
+  // interleaved (each column's sum as one column alone would form it)
+  for (int u0 = w0; u0 < n2; u0 += 4 * nw) {
     for (int r = 0; r < nrhs; ++r) {
-      double acc = 0.0;
-      for (int i = r0 + lane; i < j1; i += 32) acc = fma(L2[u][i - j0], sm.w[r][i - j0], acc);
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-      if (lane == 0) sm.w[r][j2 - j0 + u] -= acc;
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int i = r0 + lane; i < j1; i += 32) {
+        const double wv = sm.w[r][i - j0];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int u = u0 + q * nw;
+          if (u < n2) acc[q] = fma(L2[u][i - j0], wv, acc[q]);
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+      if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (u0 + q * nw < n2) sm.w[r][j2 - j0 + u0 + q * nw] -= acc[q];
     }
   }
 }
@@ -2749,6 +2828,7 @@ __global__ void __launch_bounds__(kTriNT) k_fwd_tri(DevPlan P, DevFactor X, cons
   // SPD: the diagonal blocks' inverses, when the factorization formed them
   const double *inv = (posdef && X.tri_inv && X.sn_ioff[s] >= 0) ? X.tri_inv + X.sn_ioff[s] : nullptr;
   fwd_block_issue(L, sf, j0, j1, sm, inv);
+  tri_prefetch_l2(L, sf, j1, min(j1, j0 + 32 * kRing), j1, inv);
   pdl_wait();  // the strips of L in flight meanwhile
   pdl_trigger();
   for (int r = 0; r < nrhs; ++r)
@@ -3004,6 +3084,11 @@ __global__ void __launch_bounds__(kTriNT) k_bwd_tri(DevPlan P, DevFactor X, cons
   const size_t sf = (size_t)f;
   const double *inv = (posdef && X.tri_inv && X.sn_ioff[s] >= 0) ? X.tri_inv + X.sn_ioff[s] : nullptr;
   bwd_block_issue(L, sf, j0, j1, sm, inv);
+  {
+    int jl, nl;  // the backward strips past the first kRing: columns [j0, jl)
+    bwd_strip(j0, j1, min(kRing, (j1 - j0 + 31) / 32) - 1, jl, nl);
+    tri_prefetch_l2(L, sf, j1, j0, jl, inv);
+  }
   pdl_wait();  // the strips of L in flight meanwhile
   pdl_trigger();
   for (int r = 0; r < nrhs; ++r)
