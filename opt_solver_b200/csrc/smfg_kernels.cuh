@@ -214,6 +214,23 @@ __global__ void k_level_rows(DevPlan P, DevFactor X, int lo, int hi) {
 // then extend-adds the children's Schur blocks in child order (the
 // reference's order of additions, so every entry is the reference's sum).
 // A child's block is read in place from its own front.
+// First index in [lo, hi) of the increasing a[] whose value is >= key (hi
+// if none), by the 32 lanes of a warp: 32 probes a round (one load
+// latency), about three rounds for a few thousand entries.
+__device__ __forceinline__ int warp_lower_bound(const int *__restrict__ a, int lo, int hi, int key) {
+  const int lane = threadIdx.x & 31;
+  while (hi - lo > 32) {
+    const int step = (hi - lo + 31) / 32;
+    const int pos = min(lo + step * (lane + 1) - 1, hi - 1);
+    const int nl = __popc(__ballot_sync(0xffffffffu, a[pos] < key));  // a prefix of the lanes
+    const int nlo = min(lo + step * nl, hi);
+    hi = nl == 32 ? hi : min(lo + step * (nl + 1), hi);
+    lo = nlo;
+  }
+  const int pos = lo + lane;
+  return lo + __popc(__ballot_sync(0xffffffffu, pos < hi && a[pos] < key));
+}
+
 __global__ void k_level_assemble(DevPlan P, DevFactor X, int lo, int hi, int lvl) {
   unsigned long long *cnt = X.counters;
   if (cnt[kCFlags] & kFAbort) return;
@@ -261,21 +278,11 @@ __global__ void k_level_assemble(DevPlan P, DevFactor X, int lo, int hi, int lvl
       const int q = fc - pc;
       if (q <= 0) continue;
       const int *cmap = X.cbmap + X.sn_roff[c] + pc;
-      if (threadIdx.x == 0) {
-        int lo2 = 0, hi2 = q;  // first jj with cmap[jj] >= j0
-        while (lo2 < hi2) {
-          const int mid = (lo2 + hi2) >> 1;
-          if (cmap[mid] < j0) lo2 = mid + 1;
-          else hi2 = mid;
-        }
-        int lo3 = lo2, hi3 = q;  // first jj with cmap[jj] >= j1
-        while (lo3 < hi3) {
-          const int mid = (lo3 + hi3) >> 1;
-          if (cmap[mid] < j1) lo3 = mid + 1;
-          else hi3 = mid;
-        }
-        rng[0] = lo2;
-        rng[1] = lo3;
+      // the child's CB rows mapped into [j0, j1): warp 0 finds the first
+      // with cmap >= j0, warp 1 the first with cmap >= j1
+      if (warp < 2) {
+        const int r = warp_lower_bound(cmap, 0, q, warp == 0 ? j0 : j1);
+        if (lane == 0) rng[warp] = r;
       }
       __syncthreads();
       const int ja = rng[0], jb = rng[1];
