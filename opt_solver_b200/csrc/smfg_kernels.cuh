@@ -1123,24 +1123,43 @@ __global__ void __launch_bounds__(256, kDBlocksPerSM) k_large_defer(DevPlan P, D
           const int i = i0 + tx + 16 * r, j = j0 + ty + 16 * q;
           c[r][q] = (i < f && j < e && i >= j) ? F[(size_t)j * sf + i] : 0.0;
         }
+      int zw = 0;  // a zero among the tile's w (a skipped update)
 #pragma unroll
       for (int u = 0; u < kDK * kDT / 256; ++u) {
         const int t = tid + 256 * u, p = t >> 6, r = t & 63;
         Ls[p][r] = (p < kk && i0 + r < f) ? F[(size_t)(p0 + p) * sf + i0 + r] : 0.0;
-        Ws[p][r] = (p < kk && j0 + r < e) ? Wp[(size_t)p * sf + j0 + r] : 0.0;
+        const bool real = p < kk && j0 + r < e;
+        const double wv = real ? Wp[(size_t)p * sf + j0 + r] : 0.0;
+        Ws[p][r] = wv;
+        zw |= (real && wv == 0.0) ? 1 : 0;
       }
-      __syncthreads();
-      for (int p = 0; p < kk; ++p) {
-        double av[4], bv[4];
+      if (!__syncthreads_or(zw)) {
+        // no zero w: every update applies (the padding's zeros only reach
+        // entries that are not stored)
+        for (int p = 0; p < kk; ++p) {
+          double av[4], bv[4];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) av[r] = Ls[p][tx + 16 * r];
+          for (int r = 0; r < 4; ++r) av[r] = Ls[p][tx + 16 * r];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) bv[q] = Ws[p][ty + 16 * q];
+          for (int q = 0; q < 4; ++q) bv[q] = Ws[p][ty + 16 * q];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          if (bv[q] != 0.0) {
+          for (int q = 0; q < 4; ++q)
 #pragma unroll
             for (int r = 0; r < 4; ++r) c[r][q] = fma(-av[r], bv[q], c[r][q]);
+        }
+      } else {
+        for (int p = 0; p < kk; ++p) {
+          double av[4], bv[4];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) av[r] = Ls[p][tx + 16 * r];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) bv[q] = Ws[p][ty + 16 * q];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            if (bv[q] != 0.0) {
+#pragma unroll
+              for (int r = 0; r < 4; ++r) c[r][q] = fma(-av[r], bv[q], c[r][q]);
+            }
           }
         }
       }
