@@ -855,7 +855,9 @@ __device__ __forceinline__ void tile_update(double *F, size_t sf, const double *
       c[r][q] = (i < rmax && j < cmax && i >= j) ? F[(size_t)j * sf + i] : 0.0;
     }
   double pa[8], pb[4];
+  int zb = 0;  // a zero among the fetched chunk's B values (a skipped update)
   auto fetch = [&](int k0) {
+    zb = 0;
     const int kc = min(kTK, kk - k0);
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
@@ -871,6 +873,7 @@ __device__ __forceinline__ void tile_update(double *F, size_t sf, const double *
       if (p < kc && j0 + r < cmax) {
         if (SCHUR) bv = ld_entry_g(F, sf, tags, a0 + k0 + p, j0 + r);
         else bv = W[(size_t)(k0 + p) * wld + j0 + r];
+        zb |= bv == 0.0 ? 1 : 0;
       }
       pb[u] = bv;
     }
@@ -891,27 +894,44 @@ __device__ __forceinline__ void tile_update(double *F, size_t sf, const double *
   fetch(0);
   __syncthreads();
   stash(0);
-  __syncthreads();
+  // whether the chunk in sm has a zero B value: without one every update
+  // applies and the loop takes no tests (the padding's zeros only reach
+  // entries that are not stored)
+  int anyz = __syncthreads_or(zb);
   for (int k0 = 0; k0 < kk; k0 += kTK) {
     const int kc = min(kTK, kk - k0);
     if (k0 + kTK < kk) fetch(k0 + kTK);
-    for (int p = 0; p < kc; ++p) {
-      double av[8], bv[4];
+    if (!anyz) {
+      for (int p = 0; p < kc; ++p) {
+        double av[8], bv[4];
 #pragma unroll
-      for (int r = 0; r < 8; ++r) av[r] = sm.A[buf][p][tx + 16 * r];
+        for (int r = 0; r < 8; ++r) av[r] = sm.A[buf][p][tx + 16 * r];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) bv[q] = sm.B[buf][p][ty + 16 * q];
+        for (int q = 0; q < 4; ++q) bv[q] = sm.B[buf][p][ty + 16 * q];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (bv[q] != 0.0) {
+        for (int q = 0; q < 4; ++q)
 #pragma unroll
           for (int r = 0; r < 8; ++r) c[r][q] = fma(-av[r], bv[q], c[r][q]);
+      }
+    } else {
+      for (int p = 0; p < kc; ++p) {
+        double av[8], bv[4];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) av[r] = sm.A[buf][p][tx + 16 * r];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) bv[q] = sm.B[buf][p][ty + 16 * q];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (bv[q] != 0.0) {
+#pragma unroll
+            for (int r = 0; r < 8; ++r) c[r][q] = fma(-av[r], bv[q], c[r][q]);
+          }
         }
       }
     }
     if (k0 + kTK < kk) {
       stash(buf ^ 1);
-      __syncthreads();
+      anyz = __syncthreads_or(zb);
       buf ^= 1;
     }
   }
