@@ -454,16 +454,22 @@ def run_ours(args, rank, world, local):
     # e2e: host buffers through the C ABI (copies inside the timed region)
     prec = smfg.PREC_MIXED if head == "mixed" else smfg.PREC_FP64
     e2e = []
+    # the caller's host buffers in pinned memory (values, right-hand side,
+    # solution): the copies inside the timed region are DMA transfers
+    def pinned(a):
+        return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).pin_memory().numpy()
+    h_vals, h_b = pinned(wl.values), pinned(wl.b)
+    h_x = pinned(np.zeros_like(wl.b))
     # one untimed call first: it captures the factor graph for the staged
     # host values (the timed calls replay it, as a refactor loop would)
-    sv.factor(wl.values, posdef=posdef, precision=prec, scale=wl.scale, graph=use_graph)
+    sv.factor(h_vals, posdef=posdef, precision=prec, scale=wl.scale, graph=use_graph)
     for _ in range(max(2, min(args.steps, 5))):
         torch.cuda.synchronize()
         t = time.perf_counter()
-        sv.factor(wl.values, posdef=posdef, precision=prec, scale=wl.scale, graph=use_graph)
-        x = sv.solve(wl.b)
-        x, _, _, _ = sv.refine(wl.b, x, max_steps=args.refine_max, omega_target=OMEGA_GATE,
-                               method=smfg.REFINE_AUTO)
+        sv.factor(h_vals, posdef=posdef, precision=prec, scale=wl.scale, graph=use_graph)
+        x = sv.solve(h_b, out=h_x)
+        x, _, _, _ = sv.refine(h_b, x, max_steps=args.refine_max, omega_target=OMEGA_GATE,
+                               method=smfg.REFINE_AUTO, inplace=True)
         e2e.append((time.perf_counter() - t) * 1e3)
     e2e_ms = allmax(sum(e2e) / len(e2e), world)
     _, eta, om = sv.residual(wl.b, x)

@@ -527,9 +527,11 @@ class Solver:
                 "factor_ms": info.factor_ms}
 
     # -- solve -------------------------------------------------------------
-    def solve(self, b, job: int = SOLVE_FULL):
+    def solve(self, b, job: int = SOLVE_FULL, out=None):
         """x = A^-1 b. b: (n,) or (nrhs, n) numpy array (returned as a new
-        array), or a CUDA tensor solved in place (returned)."""
+        array, or in `out`, a C-contiguous float64 array of b's shape, e.g. a
+        view of pinned host memory), or a CUDA tensor solved in place
+        (returned)."""
         info = Info()
         if hasattr(b, "data_ptr"):
             nrhs = 1 if b.dim() == 1 else int(b.shape[0])
@@ -539,7 +541,14 @@ class Solver:
                 raise SmfgError(rc, "smfg_solve_device")
             self.info.solve_ms = info.solve_ms
             return b
-        x = np.array(b, dtype=np.float64, copy=True, order="C")
+        if out is not None:
+            if out.dtype != np.float64 or not out.flags.c_contiguous or out.shape != np.shape(b):
+                raise ValueError("out: a C-contiguous float64 array of b's shape")
+            if out is not b:
+                np.copyto(out, b)
+            x = out
+        else:
+            x = np.array(b, dtype=np.float64, copy=True, order="C")
         nrhs = 1 if x.ndim == 1 else x.shape[0]
         rc = lib().smfg_solve(self._h, x.ctypes.data, nrhs, self.n, job, C.byref(info))
         if rc != SMFG_OK:
@@ -641,11 +650,16 @@ class Solver:
         return eta.value, om.value
 
     def refine(self, b, x, max_steps: int = 10, omega_target: float = 1e-8,
-               method: int = REFINE_CLASSICAL, restart: int = 20):
+               method: int = REFINE_CLASSICAL, restart: int = 20, inplace: bool = False):
         """Iterative refinement of x for b (smfg_refine_method): classical,
-        FGMRES or auto; returns (x, eta_inf, omega, solves used)."""
+        FGMRES or auto; returns (x, eta_inf, omega, solves used). inplace:
+        x (a C-contiguous float64 array) is refined in place, not copied."""
         b = np.ascontiguousarray(b, dtype=np.float64)
-        x = np.array(x, dtype=np.float64, copy=True, order="C")
+        if inplace:
+            if x.dtype != np.float64 or not x.flags.c_contiguous:
+                raise ValueError("inplace: x must be a C-contiguous float64 array")
+        else:
+            x = np.array(x, dtype=np.float64, copy=True, order="C")
         nrhs = 1 if b.ndim == 1 else b.shape[0]
         eta, om, st = C.c_double(), C.c_double(), C.c_int()
         rc = lib().smfg_refine_method(self._h, b.reshape(-1), x.reshape(-1), nrhs, method, max_steps,
