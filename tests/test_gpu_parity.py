@@ -201,3 +201,26 @@ def test_streamed_deferred_update_bitwise(f, ne, k):
     r = smfg.kernel_bench_defer(f, ne, k, reps=1)
     assert r["mismatches"] == 0
     assert r["ms"] > 0 and r["bytes"] > 0
+
+
+@pytest.mark.gpu
+def test_solve_into_given_array_and_refine_in_place():
+    """solve(b, out=...) and refine(..., inplace=True) give the same values
+    as the copying calls (the caller's buffers, e.g. pinned host memory)."""
+    from opt_solver_b200 import smfg
+    from opt_solver_b200 import workloads as W
+    n, cp, ri, v = W.laplacian_2d(40)
+    sv = smfg.Solver(smfg.analyse(n, cp, ri))
+    sv.factor(v, posdef=True)
+    b = W.rhs(n, 1, seed=9)
+    x0 = sv.solve(b)
+    out = np.empty_like(b)
+    x1 = sv.solve(b, out=out)
+    assert x1 is out and np.array_equal(x1, x0)
+    with pytest.raises(ValueError):
+        sv.solve(b, out=np.empty(n + 1))
+    xr, e0, o0, s0 = sv.refine(b, x0, max_steps=3, omega_target=1e-15)
+    x2 = x0.copy()
+    xi, e1, o1, s1 = sv.refine(b, x2, max_steps=3, omega_target=1e-15, inplace=True)
+    assert xi is x2 and np.array_equal(xi, xr) and (e0, o0, s0) == (e1, o1, s1)
+    sv.close()
