@@ -384,7 +384,8 @@ CPU_REPS = {"spd3d": 3, "lap2d": 30, "kkt": 5, "traj": 30, "batch": 1}
 
 def run_ours(args, rank, world, local):
     """Both arms on the same workload: plain FP64 and mixed precision, each
-    step = factor + solve + refinement (auto: classical, then FGMRES) until
+    step = factor + solve + refinement (auto: FGMRES on a mixed factor, classical
+    then FGMRES on an FP64 one) until
     eta_inf <= 1e-10 and omega <= 1e-12, all on the device; per arm the
     mean device time of K steps after W warm-up steps, max over ranks."""
     import torch
@@ -790,7 +791,8 @@ def main():
                    "supernodes": r["nsn"], "systems_this_rank": r["systems"],
                    "analysis": r["ordering"],
                    "precision": head, "omega_gate": OMEGA_GATE,
-                   "step": "factor + solve + refinement (auto) to eta_inf <= 1e-10, omega <= 1e-12",
+                   "step": "factor + solve + refinement (auto: FGMRES on a mixed factor) to eta_inf <= 1e-10, "
+                           "omega <= 1e-12",
                    "parallelism": ("systems sharded over ranks" if batch else "replicas") if world > 1 else "1 GPU",
                    "factor_graph_replay": r["graph"],
                    "l2": "inputs larger than L2 (front arena %.1f GB)" % (prof.get("arena_bytes", 0) / 1e9)},
